@@ -1,0 +1,335 @@
+#!/usr/bin/env python3
+"""Benchmark: plain SV bootstrap particle filter, particle-steps/s.
+
+Workload (the reference's headline scaling configuration, at its target size):
+SV model mu=-1.0, phi=0.97, sigma_eta=0.15; observations from the matched DGP
+with seed 7 (T=5000); N=2^24 particles; resample when ESS < 0.5 N. One step =
+one filter pass over the T=5000 series (re-seed + 5000 ticks).
+
+  value  device-resident run: y already in HBM, ticks replayed as a CUDA graph
+  e2e    the same run through gpu_bpf_step_many with host buffers (pinned
+         staging, H2D of y and D2H of the per-tick records inside the timing)
+  roofline  pass-1 / pass-2 kernel durations from CUDA events on the filter
+         stream during a profiled pass of the same workload
+  cpu_baseline  FP32 restatement of the reference tick loop (oracle/), OpenMP
+         over all host cores, on a bounded number of ticks of the same run
+
+`--impl reference` times that CPU restatement alone (rank 0) and prints the
+same metric. Multi-GPU (torchrun): independent replicas, one per GPU, seeds
+differ per rank; no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(REPO, "bootstrap-particle-filter-in-ptx_b200")
+for _p in (REPO, PKG_DIR):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+RHO, SIG, MU = 0.97, 0.15, -1.0
+DEVSTATE_BYTES = 136          # sizeof(bpf::DevState), read back once after a host-buffer run
+RECORD_BYTES = 40             # sizeof(BpfTickRecord)
+L2_NOTE = "working set h 4B + w 4B per particle = 128 MiB per tick at N=2^24 (> 126 MB L2); 256 MiB L2 flush between steps"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1 << 24)
+    ap.add_argument("--ticks", type=int, default=5000)
+    ap.add_argument("--ess", type=float, default=0.5)
+    ap.add_argument("--dgp-seed", type=int, default=7)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes per particle from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "ncu_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 3 and parts[1] == "dram_bytes_per_particle":
+                out[parts[0]] = float(parts[2])
+    return out
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", gpu_id], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1])); mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(n, y, ess, seconds, native=True):
+    """FP32 restatement of the reference tick loop on all host cores, bounded sample."""
+    from oracle import oracle
+    cores = os.cpu_count() or 1
+    oracle.lib(native)
+    t0 = time.perf_counter()
+    oracle.ref_run(n, RHO, SIG, MU, y[:2], seed=42, ess_threshold=ess, nthreads=cores, native=native)
+    per_tick = max((time.perf_counter() - t0) / 2.0, 1e-6)
+    ticks = int(max(2, min(len(y), seconds / per_tick)))
+    t0 = time.perf_counter()
+    oracle.ref_run(n, RHO, SIG, MU, y[:ticks], seed=42, ess_threshold=ess, nthreads=cores, native=native)
+    dt = time.perf_counter() - t0
+    return {"value": n * ticks / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"N={n}, first {ticks} ticks of the DGP-seed-7 series, ESS<{ess}N; oracle/bpf_oracle.c "
+                      f"orc_ref_run (FP32 reference tick loop, OpenMP {cores} threads, -O3 -march=native)",
+            "us_per_tick": dt / ticks * 1e6}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+    from gpubpf import dgp
+    _, ys = dgp.matched_series(args.ticks, RHO, SIG, MU, args.dgp_seed)
+    y = np.asarray(ys, dtype=np.float32)
+    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_baseline(args.n, y, args.ess, per_step)
+    vals, uspt = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = cpu_baseline(args.n, y, args.ess, per_step)
+        vals.append(r["value"]); uspt.append(r["us_per_tick"])
+    wall = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / max(1, args.steps) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain SV BPF (N={args.n}, T={args.ticks}, ESS<{args.ess}N, DGP seed {args.dgp_seed})",
+                   "n_particles": args.n, "ticks": args.ticks, "ess_threshold": args.ess,
+                   "parallelism": "host cores"},
+        "us_per_tick": statistics.mean(uspt),
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": "port",
+                         "sample": r["sample"]},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gpubpf
+    from gpubpf import dgp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=dev)
+
+    lib = gpubpf.load()
+    N, T = args.n, args.ticks
+    _, ys = dgp.matched_series(T, RHO, SIG, MU, args.dgp_seed)
+    y_host = np.asarray(ys, dtype=np.float32)
+    y_dev = torch.from_numpy(y_host).to(dev)
+    rec_dev = torch.zeros(T * RECORD_BYTES, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    f = gpubpf.GpuBpf(N, RHO, SIG, MU, 0.0, 0.0, 1000 + rank, ess_threshold=args.ess)
+    ext = torch.cuda.ExternalStream(f.state.stream, device=dev)
+
+    def one_run(seed):
+        f.reset(seed)
+        f.step_many_device(y_dev.data_ptr(), T, rec_dev.data_ptr())
+        with torch.cuda.stream(ext):
+            flush.zero_()
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    # ---------------- device-resident timed region -------------------------
+    for w in range(max(3, args.warmup)):
+        one_run(2000 + w)
+    barrier()
+    props = torch.cuda.get_device_properties(dev)
+    clk = ClockSampler(str(getattr(props, "uuid", local)) if getattr(props, "uuid", None) else str(local))
+    launches0 = lib.gpu_bpf_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for k in range(args.steps):
+        one_run(3000 + k)
+    e1.record(ext)
+    barrier()
+    clocks = clk.stop()
+    launches = lib.gpu_bpf_launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    value = world * N * T * args.steps / (ms_max / 1e3)
+
+    recs = rec_dev.cpu().numpy().view(np.uint8)
+    resampled = np.frombuffer(recs.tobytes(), dtype=np.int32).reshape(T, RECORD_BYTES // 4)[:, 8]
+    resample_rate = float(resampled.mean())
+
+    # ---------------- per-kernel durations (profiled pass) -----------------
+    f.profile(True)
+    f.reset(3000)
+    f.step_many_device(y_dev.data_ptr(), T, rec_dev.data_ptr())
+    p1_ms, p2_ms, n1, n2 = f.profile_read()
+    f.profile(False)
+    rec = np.frombuffer(rec_dev.cpu().numpy().tobytes(), dtype=np.int32).reshape(T, RECORD_BYTES // 4)[:, 8]
+    carry = np.zeros(T, dtype=np.int64)
+    carry[1:] = 1 - rec[:-1]
+    bytes_p1 = float(N) * float(np.sum(12 + 4 * carry))
+    bytes_p2 = float(N) * 12.0 * float(rec.sum())
+    peak, peak_kind = load_peaks()
+    traffic = load_traffic()
+    ach1 = bytes_p1 / (p1_ms / 1e3) / 1e9
+    ach2 = bytes_p2 / (p2_ms / 1e3) / 1e9 if p2_ms > 0 else 0.0
+    dominant = "pass1" if p1_ms >= p2_ms else "pass2"
+    ach, nl, tms = (ach1, n1, p1_ms) if dominant == "pass1" else (ach2, n2, p2_ms)
+    tr = traffic.get(dominant + "_kernel")
+    roofline = {
+        "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+        "traffic": (tr * N if tr is not None else None),
+        "kernel": dominant + "_kernel", "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+        "algorithmic_bytes_per_launch": (bytes_p1 if dominant == "pass1" else bytes_p2) / max(1, nl),
+        "avg_launch_us": tms / max(1, nl) * 1e3,
+        "pass1": {"ms": p1_ms, "launches": n1, "GBps": ach1, "frac": ach1 / peak},
+        "pass2": {"ms": p2_ms, "launches": n2, "GBps": ach2, "frac": ach2 / peak},
+        "tick": {"GBps": (bytes_p1 + bytes_p2) / ((p1_ms + p2_ms) / 1e3) / 1e9,
+                 "frac": (bytes_p1 + bytes_p2) / ((p1_ms + p2_ms) / 1e3) / 1e9 / peak},
+        "bytes_model": "pass1 12 B/particle (+4 carried weight on ticks after a skipped resample); "
+                       "pass2 12 B/particle on resampling ticks",
+    }
+
+    # ---------------- end-to-end through the host-buffer C ABI -------------
+    e2e = None
+    if not args.no_e2e:
+        out_res = None
+        for w in range(2):
+            f.reset(4000 + w)
+            f.step_many(y_host.tolist())
+        barrier()
+        import ctypes as C
+        ya = (C.c_float * T)(*y_host.tolist())
+        outa = (gpubpf.BpfResult * T)()
+        reca = (gpubpf.BpfTickRecord * T)()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e2.record(ext)
+        for k in range(args.steps):
+            f.reset(5000 + k)
+            gpubpf._lib.check(lib.gpu_bpf_step_many(f._s, ya, T, outa, reca), "gpu_bpf_step_many")
+        e3.record(ext)
+        barrier()
+        wall = time.perf_counter() - t0
+        ms_e2e = max(e2.elapsed_time(e3), wall * 1e3)
+        t2 = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * N * T * args.steps / (float(t2.item()) / 1e3), "unit": "particle-steps/s",
+               "h2d_bytes_per_step": 4 * T,
+               "d2h_bytes_per_step": RECORD_BYTES * T + DEVSTATE_BYTES,
+               "api": "gpu_bpf_reset + gpu_bpf_step_many(host y[T], host BpfResult[T], host BpfTickRecord[T])"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(N, y_host, args.ess, args.cpu_seconds)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (reference matched DGP, seed 7)",
+            "config": {"workload": f"plain SV BPF, N={N}, T={T}, ESS<{args.ess}N, theta=(mu={MU}, phi={RHO}, "
+                                   f"sigma_eta={SIG}), DGP seed {args.dgp_seed}",
+                       "n_particles": N, "ticks": T, "ess_threshold": args.ess, "l2": L2_NOTE,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single filter"},
+            "us_per_tick": ms_max / (args.steps * T) * 1e3,
+            "resample_rate": resample_rate,
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    f.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

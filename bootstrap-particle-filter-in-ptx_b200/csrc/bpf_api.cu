@@ -1,0 +1,679 @@
+// bpf_api.cu — extern "C" entry points of libgpubpf.so (include/gpu_bpf.h).
+//
+// Host tick driver: replaces gpu_bpf/gpu_bpf_ptx_full.cu:340-864. Every tick
+// is two stream-ordered launches (pass 1, pass 2); the resampling decision,
+// the resampling uniform and the buffer swap live on the device, so a tick
+// never waits for the host and runs of ticks are captured in CUDA graphs.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "bpf_plain.cuh"
+
+using namespace bpf;
+
+// ---------------------------------------------------------------------------
+// Status plumbing
+// ---------------------------------------------------------------------------
+static thread_local int g_last_error = BPF_OK;
+static std::atomic<long long> g_launches{0};
+
+static inline int set_err(int code) { g_last_error = code; return code; }
+
+#define CK(call)                                                        \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) {                                            \
+      if (e_ == cudaErrorMemoryAllocation) return set_err(BPF_ERR_ALLOC); \
+      if (e_ == cudaErrorNoDevice || e_ == cudaErrorNoKernelImageForDevice || \
+          e_ == cudaErrorInsufficientDriver) return set_err(BPF_ERR_NODEVICE); \
+      return set_err(BPF_ERR_CUDA);                                     \
+    }                                                                   \
+  } while (0)
+
+namespace {
+
+constexpr int kGraphChunk = 64;   // ticks per captured graph
+
+struct Impl {
+  int device = 0;
+  int seed = 0;
+  Plan plan{};
+  int pass2_grid = 0;
+  cudaStream_t stream = nullptr;
+
+  BpfTickRecord* rec_dev = nullptr;     // [1 + kGraphChunk]: slot 0 single step, 1.. graph ticks
+  BpfTickRecord* rec_pin = nullptr;     // pinned mirror
+  DevState* st_pin = nullptr;           // pinned DevState snapshot
+  float* y_dev = nullptr;               // [kGraphChunk]
+  float* y_pin = nullptr;               // [kGraphChunk]
+  int32_t* anc_dev = nullptr;           // [N] when recording
+  bool record_anc = false;
+  int ll_mode = 0;
+  int ticks_enqueued = 0;
+  int sticky_error = BPF_OK;
+
+  // graph of kGraphChunk ticks, keyed by the launch arguments baked into it
+  cudaGraphExec_t graph = nullptr;
+  float g_mu = NAN, g_rho = NAN, g_sigma = NAN, g_thr = NAN;
+  bool g_anc = false;
+
+  // graph of a whole device-resident run (step_many_device), keyed likewise
+  cudaGraphExec_t dgraph = nullptr;
+  const float* dg_y = nullptr;
+  BpfTickRecord* dg_rec = nullptr;
+  int dg_n = 0;
+  float dg_mu = NAN, dg_rho = NAN, dg_sigma = NAN, dg_thr = NAN;
+  bool dg_anc = false;
+
+  // profiling
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<cudaEvent_t> ev_pending;   // triples (before p1, between, after p2)
+  double prof_p1_ms = 0.0, prof_p2_ms = 0.0;
+  int prof_n1 = 0, prof_n2 = 0;
+
+  ObsModel obs{};
+};
+
+inline Impl* impl_of(GpuBpfState* s) { return s ? reinterpret_cast<Impl*>(s->impl) : nullptr; }
+
+int ensure_device(Impl* m) {
+  int cur = -1;
+  CK(cudaGetDevice(&cur));
+  if (cur != m->device) CK(cudaSetDevice(m->device));
+  return BPF_OK;
+}
+
+TickArgs make_args(GpuBpfState* s, Impl* m, float y, const float* y_ptr, BpfTickRecord* rec) {
+  TickArgs a;
+  a.mu = s->mu; a.rho = s->rho; a.sigma = s->sigma_z;
+  a.ess_threshold = s->ess_threshold;
+  a.obs = m->obs;
+  a.obs.y = y;
+  a.y_ptr = y_ptr;
+  a.rec = rec;
+  a.anc = m->record_anc ? m->anc_dev : nullptr;
+  return a;
+}
+
+int check_options(GpuBpfState* s) {
+  if (!std::isfinite(s->mu) || !std::isfinite(s->rho) || !std::isfinite(s->sigma_z)) return set_err(BPF_ERR_ARG);
+  if (!(std::fabs(s->rho) < 1.0f) || !(s->sigma_z > 0.0f)) return set_err(BPF_ERR_ARG);
+  if (s->silverman_shrink != 0.0f) return set_err(BPF_ERR_UNSUPPORTED);
+  if (std::isnan(s->ess_threshold)) return set_err(BPF_ERR_ARG);
+  return BPF_OK;
+}
+
+cudaEvent_t take_event(Impl* m) {
+  if (!m->ev_pool.empty()) { cudaEvent_t e = m->ev_pool.back(); m->ev_pool.pop_back(); return e; }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+int drain_profile(Impl* m) {
+  for (size_t i = 0; i + 2 < m->ev_pending.size(); i += 3) {
+    float a = 0.f, b = 0.f;
+    CK(cudaEventSynchronize(m->ev_pending[i + 2]));
+    CK(cudaEventElapsedTime(&a, m->ev_pending[i], m->ev_pending[i + 1]));
+    CK(cudaEventElapsedTime(&b, m->ev_pending[i + 1], m->ev_pending[i + 2]));
+    m->prof_p1_ms += a; m->prof_p2_ms += b;
+    m->prof_n1 += 1; m->prof_n2 += 1;
+  }
+  for (cudaEvent_t e : m->ev_pending) m->ev_pool.push_back(e);
+  m->ev_pending.clear();
+  return BPF_OK;
+}
+
+// Enqueue one tick (pass 1 + pass 2) on the filter's stream.
+int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+  if (m->profiling) {
+    e0 = take_event(m); e1 = take_event(m); e2 = take_event(m);
+    CK(cudaEventRecord(e0, m->stream));
+  }
+  CK(launch_pass1(m->plan, a, m->stream));
+  if (m->profiling) CK(cudaEventRecord(e1, m->stream));
+  CK(launch_pass2(m->plan, a, m->pass2_grid, m->stream));
+  if (m->profiling) {
+    CK(cudaEventRecord(e2, m->stream));
+    m->ev_pending.push_back(e0); m->ev_pending.push_back(e1); m->ev_pending.push_back(e2);
+    if (m->ev_pending.size() >= 3 * 4096) { int rc = drain_profile(m); if (rc) return rc; }
+  }
+  g_launches += 2;
+  m->ticks_enqueued += 1;
+  return BPF_OK;
+}
+
+int read_back(GpuBpfState* s, Impl* m, int slot, BpfTickRecord* out) {
+  CK(cudaMemcpyAsync(m->rec_pin + slot, m->rec_dev + slot, sizeof(BpfTickRecord), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  *out = m->rec_pin[slot];
+  s->did_resample = out->resampled;
+  s->resample_count = m->st_pin->resample_count;
+  s->timestep = m->st_pin->tick;
+  s->last_h_est = out->h_mean;
+  if (m->st_pin->error != BPF_OK) m->sticky_error = m->st_pin->error;
+  return BPF_OK;
+}
+
+BpfResult to_result(const Impl* m, const BpfTickRecord& r) {
+  BpfResult o;
+  o.h_mean = r.h_mean;
+  o.log_lik = (float)(m->ll_mode ? r.loglik_ref : r.dloglik);
+  return o;
+}
+
+int free_impl(Impl* m) {
+  if (!m) return BPF_OK;
+  if (m->graph) cudaGraphExecDestroy(m->graph);
+  if (m->dgraph) cudaGraphExecDestroy(m->dgraph);
+  for (cudaEvent_t e : m->ev_pending) cudaEventDestroy(e);
+  for (cudaEvent_t e : m->ev_pool) cudaEventDestroy(e);
+  Plan& p = m->plan;
+  cudaFree(p.h0); cudaFree(p.h1); cudaFree(p.w);
+  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.S); cudaFree(p.Q); cudaFree(p.H);
+  cudaFree(p.P); cudaFree(p.ofirst); cudaFree(p.items); cudaFree(p.st);
+  cudaFree(m->rec_dev); cudaFree(m->y_dev); cudaFree(m->anc_dev);
+  cudaFreeHost(m->rec_pin); cudaFreeHost(m->st_pin); cudaFreeHost(m->y_pin);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return BPF_OK;
+}
+
+int build_graph(GpuBpfState* s, Impl* m) {
+  if (m->graph) { cudaGraphExecDestroy(m->graph); m->graph = nullptr; }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaMemcpyAsync(m->y_dev, m->y_pin, kGraphChunk * sizeof(float), cudaMemcpyHostToDevice, m->stream);
+  for (int k = 0; k < kGraphChunk && err == cudaSuccess; ++k) {
+    TickArgs a = make_args(s, m, 0.0f, m->y_dev + k, m->rec_dev + 1 + k);
+    err = launch_pass1(m->plan, a, m->stream);
+    if (err == cudaSuccess) err = launch_pass2(m->plan, a, m->pass2_grid, m->stream);
+  }
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(m->rec_pin + 1, m->rec_dev + 1, kGraphChunk * sizeof(BpfTickRecord), cudaMemcpyDeviceToHost, m->stream);
+  cudaError_t e2 = cudaStreamEndCapture(m->stream, &g);
+  if (err != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return set_err(BPF_ERR_CUDA); }
+  cudaError_t e3 = cudaGraphInstantiate(&m->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) { m->graph = nullptr; return set_err(BPF_ERR_CUDA); }
+  m->g_mu = s->mu; m->g_rho = s->rho; m->g_sigma = s->sigma_z; m->g_thr = s->ess_threshold;
+  m->g_anc = m->record_anc;
+  return BPF_OK;
+}
+
+constexpr int kMaxGraphTicks = 16384;   // larger device runs launch directly
+
+int build_device_graph(GpuBpfState* s, Impl* m, const float* y_dev, int n, BpfTickRecord* rec_dev) {
+  if (m->dgraph) { cudaGraphExecDestroy(m->dgraph); m->dgraph = nullptr; }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  for (int k = 0; k < n && err == cudaSuccess; ++k) {
+    TickArgs a = make_args(s, m, 0.0f, y_dev + k, rec_dev + k);
+    err = launch_pass1(m->plan, a, m->stream);
+    if (err == cudaSuccess) err = launch_pass2(m->plan, a, m->pass2_grid, m->stream);
+  }
+  cudaError_t e2 = cudaStreamEndCapture(m->stream, &g);
+  if (err != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return set_err(BPF_ERR_CUDA); }
+  cudaError_t e3 = cudaGraphInstantiate(&m->dgraph, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) { m->dgraph = nullptr; return set_err(BPF_ERR_CUDA); }
+  m->dg_y = y_dev; m->dg_rec = rec_dev; m->dg_n = n;
+  m->dg_mu = s->mu; m->dg_rho = s->rho; m->dg_sigma = s->sigma_z; m->dg_thr = s->ess_threshold;
+  m->dg_anc = m->record_anc;
+  return BPF_OK;
+}
+
+bool graph_stale(GpuBpfState* s, Impl* m) {
+  return !m->graph || m->g_mu != s->mu || m->g_rho != s->rho || m->g_sigma != s->sigma_z ||
+         m->g_thr != s->ess_threshold || m->g_anc != m->record_anc;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Reference API
+// ===========================================================================
+extern "C" {
+
+int gpu_bpf_last_error(void) { return g_last_error; }
+
+const char* gpu_bpf_error_string(int code) {
+  switch (code) {
+    case BPF_OK: return "ok";
+    case BPF_ERR_ARG: return "invalid argument";
+    case BPF_ERR_CUDA: return "CUDA runtime error";
+    case BPF_ERR_ALLOC: return "allocation failed";
+    case BPF_ERR_UNSUPPORTED: return "option not supported by this build";
+    case BPF_ERR_STATE: return "invalid filter state";
+    case BPF_ERR_DEGENERATE: return "all particle weights underflowed";
+    case BPF_ERR_NODEVICE: return "no usable CUDA device";
+    default: return "unknown error";
+  }
+}
+
+long long gpu_bpf_launch_count(void) { return g_launches.load(); }
+
+static int create_impl(GpuBpfState* s, Impl* m, int n, float rho, float sigma_z, float mu, float nu_obs, int seed) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return set_err(BPF_ERR_NODEVICE); }
+  CK(cudaGetDevice(&m->device));
+  m->seed = seed;
+  Plan& p = m->plan;
+  p.N = n;
+  p.G = (n + kTile - 1) / kTile;
+  p.max_items = p.G + (n + kOutChunk - 1) / kOutChunk + 1;
+  const size_t npad = (size_t)p.G * kTile;
+  CK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  CK(cudaMalloc(&p.h0, npad * sizeof(float)));
+  CK(cudaMalloc(&p.h1, npad * sizeof(float)));
+  CK(cudaMalloc(&p.w, npad * sizeof(float)));
+  CK(cudaMalloc(&p.nexp, p.G * sizeof(int)));
+  CK(cudaMalloc(&p.E, p.G * sizeof(unsigned long long)));
+  CK(cudaMalloc(&p.S, p.G * sizeof(double)));
+  CK(cudaMalloc(&p.Q, p.G * sizeof(double)));
+  CK(cudaMalloc(&p.H, p.G * sizeof(double)));
+  CK(cudaMalloc(&p.P, p.G * sizeof(unsigned long long)));
+  CK(cudaMalloc(&p.ofirst, (p.G + 1) * sizeof(int)));
+  CK(cudaMalloc(&p.items, p.max_items * sizeof(int4)));
+  CK(cudaMalloc(&p.st, sizeof(DevState)));
+  CK(cudaMalloc(&m->rec_dev, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
+  CK(cudaMalloc(&m->y_dev, kGraphChunk * sizeof(float)));
+  CK(cudaMallocHost(&m->rec_pin, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
+  CK(cudaMallocHost(&m->st_pin, sizeof(DevState)));
+  CK(cudaMallocHost(&m->y_pin, kGraphChunk * sizeof(float)));
+  CK(cudaMemsetAsync(p.nexp, 0, p.G * sizeof(int), m->stream));
+  CK(cudaMemsetAsync(m->rec_dev, 0, (1 + kGraphChunk) * sizeof(BpfTickRecord), m->stream));
+  m->pass2_grid = pass2_grid_size(m->device);
+
+  // observation model (gpu_bpf_ptx_full.cu:406-412)
+  m->obs.nu = nu_obs;
+  if (nu_obs > 0.0f) {
+    m->obs.c_obs = (float)(std::lgamma((nu_obs + 1.0) / 2.0) - std::lgamma(nu_obs / 2.0) -
+                           0.5 * std::log(nu_obs * 3.14159265358979323846));
+    m->obs.inv_nu = 1.0f / nu_obs;
+    m->obs.nu_p1h = (nu_obs + 1.0f) * 0.5f;
+  }
+
+  const float std_stat = sqrtf((sigma_z * sigma_z) / fmaxf(1.0f - rho * rho, 1e-6f));   // :430
+  CK(launch_init(p, mu, std_stat, seed, m->stream));
+  g_launches += 1;
+  CK(cudaStreamSynchronize(m->stream));
+  s->stream = (void*)m->stream;
+  return BPF_OK;
+}
+
+GpuBpfState* gpu_bpf_create(int n_particles, float rho, float sigma_z, float mu,
+                            float nu_state, float nu_obs, int seed) {
+  g_last_error = BPF_OK;
+  if (n_particles <= 0 || n_particles > (1 << 30) || !std::isfinite(rho) || !std::isfinite(sigma_z) ||
+      !std::isfinite(mu) || !(std::fabs(rho) < 1.0f) || !(sigma_z > 0.0f) || !(nu_obs >= 0.0f) ||
+      !std::isfinite(nu_obs) || !(nu_state >= 0.0f)) {
+    set_err(BPF_ERR_ARG);
+    return nullptr;
+  }
+  if (nu_state > 0.0f) { set_err(BPF_ERR_UNSUPPORTED); return nullptr; }
+  GpuBpfState* s = (GpuBpfState*)calloc(1, sizeof(GpuBpfState));
+  if (!s) { set_err(BPF_ERR_ALLOC); return nullptr; }
+  s->n_particles = n_particles;
+  s->rho = rho; s->sigma_z = sigma_z; s->mu = mu;
+  s->nu_state = nu_state; s->nu_obs = nu_obs;
+  s->silverman_shrink = 0.0f;
+  s->ess_threshold = 0.5f;           // gpu_bpf_ptx_full.cu:356
+  s->did_resample = 1;
+  s->last_h_est = mu;
+  Impl* m = new Impl();
+  s->impl = m;
+  int rc = create_impl(s, m, n_particles, rho, sigma_z, mu, nu_obs, seed);
+  if (rc != BPF_OK) {
+    free_impl(m);
+    free(s);
+    set_err(rc);
+    return nullptr;
+  }
+  return s;
+}
+
+void gpu_bpf_destroy(GpuBpfState* s) {
+  if (!s) return;
+  Impl* m = impl_of(s);
+  if (m) { ensure_device(m); cudaStreamSynchronize(m->stream); free_impl(m); }
+  s->impl = nullptr;
+  free(s);
+}
+
+static int step_async_rc(GpuBpfState* s, float y_t) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  if (!std::isfinite(y_t)) return set_err(BPF_ERR_ARG);
+  int rc = check_options(s);
+  if (rc) return rc;
+  rc = ensure_device(m);
+  if (rc) return rc;
+  return enqueue_tick(s, m, make_args(s, m, y_t, nullptr, m->rec_dev));
+}
+
+void gpu_bpf_step_async(GpuBpfState* s, float y_t) { step_async_rc(s, y_t); }
+
+BpfResult gpu_bpf_get_result(GpuBpfState* s) {
+  BpfResult bad; bad.h_mean = NAN; bad.log_lik = NAN;
+  Impl* m = impl_of(s);
+  if (!m) { set_err(BPF_ERR_STATE); return bad; }
+  if (m->ticks_enqueued == 0) { set_err(BPF_ERR_STATE); return bad; }
+  if (ensure_device(m)) return bad;
+  BpfTickRecord r;
+  if (read_back(s, m, 0, &r) != BPF_OK) return bad;
+  return to_result(m, r);
+}
+
+BpfResult gpu_bpf_step(GpuBpfState* s, float y_t) {
+  BpfResult bad; bad.h_mean = NAN; bad.log_lik = NAN;
+  if (step_async_rc(s, y_t) != BPF_OK) return bad;
+  return gpu_bpf_get_result(s);
+}
+
+double gpu_bpf_run_rmse(const double* returns, const double* true_h, int n_ticks,
+                        int n_particles, float rho, float sigma_z, float mu,
+                        float nu_state, float nu_obs, int seed) {
+  if (!returns || !true_h || n_ticks <= 100) { set_err(BPF_ERR_ARG); return NAN; }
+  GpuBpfState* f = gpu_bpf_create(n_particles, rho, sigma_z, mu, nu_state, nu_obs, seed);
+  if (!f) return NAN;
+  std::vector<float> y(n_ticks);
+  for (int t = 0; t < n_ticks; ++t) y[t] = (float)returns[t];
+  std::vector<BpfResult> out(n_ticks);
+  int rc = gpu_bpf_step_many(f, y.data(), n_ticks, out.data(), nullptr);
+  gpu_bpf_destroy(f);
+  if (rc != BPF_OK) { set_err(rc); return NAN; }
+  double sse = 0.0;
+  int count = 0;
+  for (int t = 100; t < n_ticks; ++t) {            // gpu_bpf_ptx_full.cu:841-848
+    const double e = (double)out[t].h_mean - true_h[t];
+    sse += e * e;
+    ++count;
+  }
+  return std::sqrt(sse / (double)count);
+}
+
+void gpu_bpf_set_bands(int n_particles, int n_bands, const float* fracs, const float* scales) {
+  (void)n_particles; (void)fracs;
+  if (n_bands == 1 && scales && scales[0] == 1.0f) { g_last_error = BPF_OK; return; }
+  set_err(BPF_ERR_UNSUPPORTED);
+}
+
+void gpu_bpf_set_adaptive_bands(int, const float*, const float*, int, const float*, const float*, int,
+                                const float*, const float*, int, float, float) {
+  set_err(BPF_ERR_UNSUPPORTED);
+}
+
+void gpu_bpf_set_ess_threshold(GpuBpfState* s, float threshold) {
+  if (!s) { set_err(BPF_ERR_STATE); return; }
+  s->ess_threshold = threshold;
+}
+
+int gpu_bpf_get_resample_count(GpuBpfState* s) {
+  Impl* m = impl_of(s);
+  if (!m) { set_err(BPF_ERR_STATE); return -1; }
+  if (ensure_device(m)) return -1;
+  if (cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
+      cudaStreamSynchronize(m->stream) != cudaSuccess) { set_err(BPF_ERR_CUDA); return -1; }
+  s->resample_count = m->st_pin->resample_count;
+  return s->resample_count;
+}
+
+float gpu_bpf_get_mu(GpuBpfState* s) { return s ? s->mu : NAN; }
+float gpu_bpf_get_rho(GpuBpfState* s) { return s ? s->rho : NAN; }
+void gpu_bpf_set_mu(GpuBpfState* s, float mu) {
+  if (!s || !std::isfinite(mu)) { set_err(BPF_ERR_ARG); return; }
+  s->mu = mu;
+}
+void gpu_bpf_set_rho(GpuBpfState* s, float rho) {
+  if (!s || !std::isfinite(rho)) { set_err(BPF_ERR_ARG); return; }
+  s->rho = fmaxf(fminf(rho, 0.999f), 0.001f);       // gpu_bpf_ptx_full.cu:822
+}
+void gpu_bpf_enable_mu_learning(GpuBpfState*, int, int, float, float, float) { set_err(BPF_ERR_UNSUPPORTED); }
+void gpu_bpf_disable_mu_learning(GpuBpfState*) {}
+void gpu_bpf_enable_rho_learning(GpuBpfState*, int enable) { if (enable) set_err(BPF_ERR_UNSUPPORTED); }
+
+// ===========================================================================
+// Additions
+// ===========================================================================
+int gpu_bpf_step_many(GpuBpfState* s, const float* y, int n_ticks, BpfResult* out, BpfTickRecord* rec) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  if (n_ticks < 0 || (n_ticks > 0 && !y)) return set_err(BPF_ERR_ARG);
+  for (int t = 0; t < n_ticks; ++t) if (!std::isfinite(y[t])) return set_err(BPF_ERR_ARG);
+  int rc = check_options(s);
+  if (rc) return rc;
+  rc = ensure_device(m);
+  if (rc) return rc;
+  int t = 0;
+  if (!m->profiling) {
+    while (n_ticks - t >= kGraphChunk) {
+      if (graph_stale(s, m)) { rc = build_graph(s, m); if (rc) return rc; }
+      std::memcpy(m->y_pin, y + t, kGraphChunk * sizeof(float));
+      CK(cudaGraphLaunch(m->graph, m->stream));
+      CK(cudaStreamSynchronize(m->stream));
+      g_launches += 2 * kGraphChunk;
+      m->ticks_enqueued += kGraphChunk;
+      for (int k = 0; k < kGraphChunk; ++k) {
+        if (out) out[t + k] = to_result(m, m->rec_pin[1 + k]);
+        if (rec) rec[t + k] = m->rec_pin[1 + k];
+      }
+      t += kGraphChunk;
+    }
+  }
+  // remainder (and the profiled path): direct launches into the same record slots
+  while (t < n_ticks) {
+    const int n = std::min(kGraphChunk, n_ticks - t);
+    for (int k = 0; k < n; ++k) {
+      rc = enqueue_tick(s, m, make_args(s, m, y[t + k], nullptr, m->rec_dev + 1 + k));
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(m->rec_pin + 1, m->rec_dev + 1, n * sizeof(BpfTickRecord), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    for (int k = 0; k < n; ++k) {
+      if (out) out[t + k] = to_result(m, m->rec_pin[1 + k]);
+      if (rec) rec[t + k] = m->rec_pin[1 + k];
+    }
+    t += n;
+  }
+  // keep slot 0 = last tick so get_result/get_record see it
+  if (n_ticks > 0) {
+    const int last = (n_ticks - 1) % kGraphChunk;
+    const BpfTickRecord& lr = m->rec_pin[1 + last];
+    CK(cudaMemcpyAsync(m->rec_dev, m->rec_dev + 1 + last, sizeof(BpfTickRecord), cudaMemcpyDeviceToDevice, m->stream));
+    CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    s->did_resample = lr.resampled;
+    s->last_h_est = lr.h_mean;
+    s->resample_count = m->st_pin->resample_count;
+    s->timestep = m->st_pin->tick;
+    if (m->st_pin->error != BPF_OK) { m->sticky_error = m->st_pin->error; return set_err(m->st_pin->error); }
+  }
+  return BPF_OK;
+}
+
+int gpu_bpf_step_many_device(GpuBpfState* s, const float* y_dev, int n_ticks, BpfTickRecord* rec_dev) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  if (n_ticks < 0 || (n_ticks > 0 && (!y_dev || !rec_dev))) return set_err(BPF_ERR_ARG);
+  int rc = check_options(s);
+  if (rc) return rc;
+  rc = ensure_device(m);
+  if (rc) return rc;
+  if (!m->profiling && n_ticks > 0 && n_ticks <= kMaxGraphTicks) {
+    const bool stale = !m->dgraph || m->dg_y != y_dev || m->dg_rec != rec_dev || m->dg_n != n_ticks ||
+                       m->dg_mu != s->mu || m->dg_rho != s->rho || m->dg_sigma != s->sigma_z ||
+                       m->dg_thr != s->ess_threshold || m->dg_anc != m->record_anc;
+    if (stale) { rc = build_device_graph(s, m, y_dev, n_ticks, rec_dev); if (rc) return rc; }
+    CK(cudaGraphLaunch(m->dgraph, m->stream));
+    g_launches += 2LL * n_ticks;
+    m->ticks_enqueued += n_ticks;
+  } else {
+    for (int t = 0; t < n_ticks; ++t) {
+      rc = enqueue_tick(s, m, make_args(s, m, 0.0f, y_dev + t, rec_dev + t));
+      if (rc) return rc;
+    }
+  }
+  if (n_ticks > 0)
+    CK(cudaMemcpyAsync(m->rec_dev, rec_dev + n_ticks - 1, sizeof(BpfTickRecord), cudaMemcpyDeviceToDevice, m->stream));
+  return BPF_OK;
+}
+
+int gpu_bpf_reset(GpuBpfState* s, int seed) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  int rc = check_options(s);
+  if (rc) return rc;
+  rc = ensure_device(m);
+  if (rc) return rc;
+  m->seed = seed;
+  const float std_stat = sqrtf((s->sigma_z * s->sigma_z) / fmaxf(1.0f - s->rho * s->rho, 1e-6f));
+  CK(launch_init(m->plan, s->mu, std_stat, seed, m->stream));   // also resets the DevState
+  g_launches += 1;
+  m->ticks_enqueued = 0;
+  s->timestep = 0; s->did_resample = 1; s->resample_count = 0; s->last_h_est = s->mu;
+  return BPF_OK;
+}
+
+int gpu_bpf_get_record(GpuBpfState* s, BpfTickRecord* out) {
+  Impl* m = impl_of(s);
+  if (!m || !out) return set_err(!m ? BPF_ERR_STATE : BPF_ERR_ARG);
+  if (m->ticks_enqueued == 0) return set_err(BPF_ERR_STATE);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  return read_back(s, m, 0, out);
+}
+
+float gpu_bpf_get_ess(GpuBpfState* s) {
+  BpfTickRecord r;
+  if (gpu_bpf_get_record(s, &r) != BPF_OK) return NAN;
+  return r.ess;
+}
+
+double gpu_bpf_get_loglik_total(GpuBpfState* s) {
+  Impl* m = impl_of(s);
+  if (!m) { set_err(BPF_ERR_STATE); return NAN; }
+  if (ensure_device(m)) return NAN;
+  if (cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
+      cudaStreamSynchronize(m->stream) != cudaSuccess) { set_err(BPF_ERR_CUDA); return NAN; }
+  return m->st_pin->ll_total;
+}
+
+int gpu_bpf_set_loglik_semantics(GpuBpfState* s, int mode) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  if (mode != 0 && mode != 1) return set_err(BPF_ERR_ARG);
+  m->ll_mode = mode;
+  return BPF_OK;
+}
+
+int gpu_bpf_get_particles(GpuBpfState* s, float* h_out) {
+  Impl* m = impl_of(s);
+  if (!m || !h_out) return set_err(!m ? BPF_ERR_STATE : BPF_ERR_ARG);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  const float* src = m->st_pin->cur ? m->plan.h1 : m->plan.h0;
+  CK(cudaMemcpy(h_out, src, (size_t)m->plan.N * sizeof(float), cudaMemcpyDeviceToHost));
+  return BPF_OK;
+}
+
+int gpu_bpf_record_ancestors(GpuBpfState* s, int enable) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  if (enable && !m->anc_dev) {
+    CK(cudaMalloc(&m->anc_dev, (size_t)m->plan.N * sizeof(int32_t)));
+    CK(cudaMemsetAsync(m->anc_dev, 0xff, (size_t)m->plan.N * sizeof(int32_t), m->stream));
+  }
+  m->record_anc = enable != 0;
+  return BPF_OK;
+}
+
+int gpu_bpf_get_ancestors(GpuBpfState* s, int32_t* anc_out) {
+  Impl* m = impl_of(s);
+  if (!m || !anc_out) return -set_err(!m ? BPF_ERR_STATE : BPF_ERR_ARG);
+  if (!m->anc_dev || m->ticks_enqueued == 0) return -set_err(BPF_ERR_STATE);
+  if (ensure_device(m)) return -BPF_ERR_CUDA;
+  BpfTickRecord r;
+  int rc = read_back(s, m, 0, &r);
+  if (rc) return -rc;
+  if (cudaMemcpy(anc_out, m->anc_dev, (size_t)m->plan.N * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -set_err(BPF_ERR_CUDA);
+  return r.resampled ? 1 : 0;
+}
+
+int gpu_bpf_get_resample_inputs(GpuBpfState* s, float* w_out, int32_t* tile_exp_out, uint32_t* u23_out) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  if (w_out) CK(cudaMemcpy(w_out, m->plan.w, (size_t)m->plan.N * sizeof(float), cudaMemcpyDeviceToHost));
+  if (tile_exp_out) CK(cudaMemcpy(tile_exp_out, m->plan.nexp, (size_t)m->plan.G * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (u23_out) *u23_out = m->st_pin->u23;
+  return BPF_OK;
+}
+
+int gpu_bpf_profile(GpuBpfState* s, int enable) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  rc = drain_profile(m);
+  if (rc) return rc;
+  m->profiling = enable != 0;
+  m->prof_p1_ms = m->prof_p2_ms = 0.0;
+  m->prof_n1 = m->prof_n2 = 0;
+  return BPF_OK;
+}
+
+int gpu_bpf_profile_read(GpuBpfState* s, double* p1, double* p2, int* n1, int* n2) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  rc = drain_profile(m);
+  if (rc) return rc;
+  if (p1) *p1 = m->prof_p1_ms;
+  if (p2) *p2 = m->prof_p2_ms;
+  if (n1) *n1 = m->prof_n1;
+  if (n2) *n2 = m->prof_n2;
+  return BPF_OK;
+}
+
+static int debug_probe(int seed, int n, int t, uint32_t* out, float* norm) {
+  if (n <= 0 || t < 0 || (!out && !norm)) return set_err(BPF_ERR_ARG);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return set_err(BPF_ERR_NODEVICE); }
+  uint32_t* d_out = nullptr;
+  float* d_norm = nullptr;
+  CK(cudaMalloc(&d_out, n * sizeof(uint32_t)));
+  CK(cudaMalloc(&d_norm, n * sizeof(float)));
+  cudaError_t e = launch_debug_pcg(seed, n, t, d_out, d_norm, 0);
+  g_launches += 1;
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess && out) e = cudaMemcpy(out, d_out, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && norm) e = cudaMemcpy(norm, d_norm, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d_out);
+  cudaFree(d_norm);
+  CK(e);
+  return BPF_OK;
+}
+
+int gpu_bpf_debug_pcg32(int seed, int n, int t, uint32_t* out) { return debug_probe(seed, n, t, out, nullptr); }
+int gpu_bpf_debug_normals(int seed, int n, int t, float* out) { return debug_probe(seed, n, t, nullptr, out); }
+
+}  // extern "C"

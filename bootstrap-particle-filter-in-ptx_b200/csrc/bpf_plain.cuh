@@ -1,0 +1,73 @@
+// bpf_plain.cuh — device-memory layout and launchers of the plain filter.
+//
+// HBM layout of one filter of N particles, G = ceil(N/4096) tiles
+// (every particle array is padded to G*4096 floats so tile loads never
+// leave the allocation):
+//   h[2][G*4096]  f32  particle ping-pong (current buffer index in DevState)
+//   w[G*4096]     f32  tile-relative weights 2^(x_i - n_k), in [0,1]
+//   tile records  nexp[G] i32, E[G] u64, S/Q/H[G] f64
+//   P[G] u64 exclusive tile prefix of the fixed-point CDF, ofirst[G+1] i32
+//   items[G + N/4096 + 1] int4 pass-2 work items (tile, first out, end out)
+//   DevState      scalars carried from tick to tick
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "bpf_common.cuh"
+#include "../../include/gpu_bpf.h"
+
+namespace bpf {
+
+// Scalars that live on the device from tick to tick (no host round trip).
+struct DevState {
+  uint64_t At, Bt;          // PCG jump constants A^t, sum_{k<t} A^k of the next tick
+  uint64_t u_state;         // resampling-uniform PCG32 (gpu_bpf_ptx_full.cu:353)
+  uint64_t base, delta;     // systematic targets t_i = base + i*delta (fixed point)
+  uint64_t delta_magic;     // floor((2^64-1)/delta)
+  uint64_t total;           // fixed-point CDF total
+  double   logS_prev;       // ln(sum of carried weights) in the carry frame; ln N after a resample
+  double   ll_total;        // FP64 running log-likelihood
+  double   ll_ref;          // log-evidence since the last resample
+  int      tick;            // index of the next tick
+  int      cur;             // h buffer holding the current particles
+  int      src;             // pass-2 gather source buffer
+  int      resampled_prev;  // previous tick resampled (1 before tick 0)
+  int      nM_prev;         // global tile exponent of the previous tick
+  int      do_resample;     // current tick resamples
+  int      nM;              // global tile exponent of the current tick
+  int      Fg;              // global-frame fraction bits
+  int      n_items;         // pass-2 work items of the current tick
+  uint32_t u23;             // resampling uniform of the current tick
+  int      resample_count;
+  unsigned ticket;          // pass-1 CTA completion counter
+  int      error;           // sticky BPF_* error code
+  int      seed;            // filter seed (PCG32 streams, resampling uniform)
+};
+static_assert(sizeof(DevState) == 136, "DevState layout");
+
+struct Plan {
+  int N, G, max_items;
+  float* h0; float* h1; float* w;
+  int* nexp; unsigned long long* E; double* S; double* Q; double* H;
+  unsigned long long* P; int* ofirst; int4* items;
+  DevState* st;
+};
+
+struct TickArgs {
+  float mu, rho, sigma;
+  float ess_threshold;
+  ObsModel obs;              // obs.y is used when y_ptr == nullptr
+  const float* y_ptr;        // device pointer to this tick's observation, or null
+  BpfTickRecord* rec;        // device record slot written by the last pass-1 CTA
+  int32_t* anc;              // ancestors of this tick (N ints) or null
+};
+
+// Host-side launchers (stream-ordered, no synchronisation).
+// Draws h_0 for `seed` and (re)initialises the DevState on the device.
+cudaError_t launch_init(const Plan& p, float mu, float std_stat, int seed, cudaStream_t s);
+cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s);
+cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s);
+int pass2_grid_size(int device);
+size_t pass2_smem_bytes();
+cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s);
+
+}  // namespace bpf

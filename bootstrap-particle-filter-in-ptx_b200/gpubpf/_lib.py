@@ -1,0 +1,136 @@
+"""ctypes binding of libgpubpf.so (declarations in include/gpu_bpf.h).
+
+The library is loaded from this directory only. There is no fallback: if the
+shared object is missing or fails to load, importing a compute entry point
+raises, so a GPU run can never silently execute anything but the CUDA path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgpubpf.so")
+
+BPF_OK = 0
+BPF_ERR_ARG = 1
+BPF_ERR_CUDA = 2
+BPF_ERR_ALLOC = 3
+BPF_ERR_UNSUPPORTED = 4
+BPF_ERR_STATE = 5
+BPF_ERR_DEGENERATE = 6
+BPF_ERR_NODEVICE = 7
+
+
+class BpfResult(C.Structure):
+    """gpu_bpf/gpu_bpf.cuh:21-24 layout."""
+    _fields_ = [("h_mean", C.c_float), ("log_lik", C.c_float)]
+
+
+class BpfTickRecord(C.Structure):
+    _fields_ = [
+        ("dloglik", C.c_double),
+        ("loglik_ref", C.c_double),
+        ("loglik_total", C.c_double),
+        ("h_mean", C.c_float),
+        ("ess", C.c_float),
+        ("resampled", C.c_int32),
+        ("tick", C.c_int32),
+    ]
+
+
+class GpuBpfState(C.Structure):
+    _fields_ = [
+        ("n_particles", C.c_int),
+        ("rho", C.c_float), ("sigma_z", C.c_float), ("mu", C.c_float),
+        ("nu_state", C.c_float), ("nu_obs", C.c_float),
+        ("silverman_shrink", C.c_float),
+        ("ess_threshold", C.c_float),
+        ("did_resample", C.c_int),
+        ("resample_count", C.c_int),
+        ("timestep", C.c_int),
+        ("last_h_est", C.c_float),
+        ("stream", C.c_void_p),
+        ("impl", C.c_void_p),
+    ]
+
+
+P_STATE = C.POINTER(GpuBpfState)
+_f = C.c_float
+_i = C.c_int
+_d = C.c_double
+_vp = C.c_void_p
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    # reference API (gpu_bpf/gpu_bpf.cuh:56-85, gpu_bpf_full.cuh:197-230)
+    "gpu_bpf_create": (P_STATE, [_i, _f, _f, _f, _f, _f, _i]),
+    "gpu_bpf_destroy": (None, [P_STATE]),
+    "gpu_bpf_step": (BpfResult, [P_STATE, _f]),
+    "gpu_bpf_step_async": (None, [P_STATE, _f]),
+    "gpu_bpf_get_result": (BpfResult, [P_STATE]),
+    "gpu_bpf_run_rmse": (_d, [C.POINTER(_d), C.POINTER(_d), _i, _i, _f, _f, _f, _f, _f, _i]),
+    "gpu_bpf_set_bands": (None, [_i, _i, C.POINTER(_f), C.POINTER(_f)]),
+    "gpu_bpf_set_adaptive_bands": (None, [_i, C.POINTER(_f), C.POINTER(_f), _i, C.POINTER(_f), C.POINTER(_f), _i,
+                                          C.POINTER(_f), C.POINTER(_f), _i, _f, _f]),
+    "gpu_bpf_set_ess_threshold": (None, [P_STATE, _f]),
+    "gpu_bpf_get_resample_count": (_i, [P_STATE]),
+    "gpu_bpf_get_mu": (_f, [P_STATE]),
+    "gpu_bpf_get_rho": (_f, [P_STATE]),
+    "gpu_bpf_set_mu": (None, [P_STATE, _f]),
+    "gpu_bpf_set_rho": (None, [P_STATE, _f]),
+    "gpu_bpf_enable_mu_learning": (None, [P_STATE, _i, _i, _f, _f, _f]),
+    "gpu_bpf_disable_mu_learning": (None, [P_STATE]),
+    "gpu_bpf_enable_rho_learning": (None, [P_STATE, _i]),
+    # additions
+    "gpu_bpf_last_error": (_i, []),
+    "gpu_bpf_error_string": (C.c_char_p, [_i]),
+    "gpu_bpf_step_many": (_i, [P_STATE, C.POINTER(_f), _i, C.POINTER(BpfResult), C.POINTER(BpfTickRecord)]),
+    "gpu_bpf_step_many_device": (_i, [P_STATE, _vp, _i, _vp]),
+    "gpu_bpf_reset": (_i, [P_STATE, _i]),
+    "gpu_bpf_get_record": (_i, [P_STATE, C.POINTER(BpfTickRecord)]),
+    "gpu_bpf_get_ess": (_f, [P_STATE]),
+    "gpu_bpf_get_loglik_total": (_d, [P_STATE]),
+    "gpu_bpf_set_loglik_semantics": (_i, [P_STATE, _i]),
+    "gpu_bpf_get_particles": (_i, [P_STATE, C.POINTER(_f)]),
+    "gpu_bpf_record_ancestors": (_i, [P_STATE, _i]),
+    "gpu_bpf_get_ancestors": (_i, [P_STATE, C.POINTER(C.c_int32)]),
+    "gpu_bpf_get_resample_inputs": (_i, [P_STATE, C.POINTER(_f), C.POINTER(C.c_int32), C.POINTER(C.c_uint32)]),
+    "gpu_bpf_profile": (_i, [P_STATE, _i]),
+    "gpu_bpf_profile_read": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_d), C.POINTER(_i), C.POINTER(_i)]),
+    "gpu_bpf_launch_count": (C.c_longlong, []),
+    "gpu_bpf_debug_pcg32": (_i, [_i, _i, _i, C.POINTER(C.c_uint32)]),
+    "gpu_bpf_debug_normals": (_i, [_i, _i, _i, C.POINTER(_f)]),
+}
+
+_LIB = None
+
+
+def load() -> C.CDLL:
+    """Load libgpubpf.so and declare every exported signature (raises if absent)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libgpubpf.so not found at {LIB_PATH}; build it with "
+            "`python bootstrap-particle-filter-in-ptx_b200/build.py`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class BpfError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        lib = load()
+        msg = lib.gpu_bpf_error_string(code).decode()
+        super().__init__(f"{where}: BPF error {code} ({msg})" if where else f"BPF error {code} ({msg})")
+        self.code = code
+
+
+def check(rc: int, where: str = "") -> None:
+    if rc != BPF_OK:
+        raise BpfError(rc, where)

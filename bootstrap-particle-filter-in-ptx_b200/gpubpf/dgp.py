@@ -1,0 +1,76 @@
+"""Synthetic stochastic-volatility series (the reference's matched DGP).
+
+Restates ``generate_matched_series`` and its PCG32 helpers from the reference
+test ``tests/test_bpf_matched_dgp.cu`` (seeding :69-76, doubles :78-80,
+Box-Muller :82-87, series :141-175) for the Gaussian case (nu_state =
+nu_obs = 0), plus the series used by the benchmark configurations.
+"""
+from __future__ import annotations
+
+import math
+
+MASK64 = (1 << 64) - 1
+PCG_MULT = 6364136223846793005
+
+
+class Pcg32:
+    """PCG32 with explicit increment (test_bpf_matched_dgp.cu:59-76)."""
+
+    def __init__(self, seed: int):
+        self.state = 0
+        self.inc = ((seed * 12345) | 1) & MASK64
+        self.next_u32()
+        self.state = (self.state + seed * 67890) & MASK64
+        self.next_u32()
+        self.next_u32()
+
+    def next_u32(self) -> int:
+        old = self.state
+        self.state = (old * PCG_MULT + self.inc) & MASK64
+        xsh = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xsh >> rot) | (xsh << ((-rot) & 31))) & 0xFFFFFFFF
+
+    def next_double(self) -> float:          # :78-80, 21-bit uniform in [0,1)
+        return (self.next_u32() >> 11) * (1.0 / 2097152.0)
+
+    def gaussian(self) -> float:             # :82-87
+        while True:
+            u1 = self.next_double()
+            if u1 >= 1e-10:
+                break
+        u2 = self.next_double()
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * 3.14159265358979323846 * u2)
+
+
+def matched_series(T: int, rho: float, sigma_z: float, mu: float, seed: int):
+    """(true_h[T], y[T]) from generate_matched_series with Gaussian noises."""
+    rng = Pcg32(seed)
+    var_stat = (sigma_z * sigma_z) / max(1.0 - rho * rho, 1e-6)
+    h = mu + math.sqrt(var_stat) * rng.gaussian()
+    hs, ys = [], []
+    for t in range(T):
+        if t > 0:
+            h = mu + rho * (h - mu) + sigma_z * rng.gaussian()
+        h = min(max(h, -12.0), 4.0)
+        hs.append(h)
+        ys.append(math.exp(h / 2.0) * rng.gaussian())
+    return hs, ys
+
+
+def regime_series(T: int, mus=(-1.5, 0.0), period: int = 500, rho: float = 0.97,
+                  sigma_z: float = 0.2, seed: int = 42):
+    """Regime-switching SV series: mu alternates every `period` ticks, same DGP otherwise."""
+    rng = Pcg32(seed)
+    mu0 = mus[0]
+    var_stat = (sigma_z * sigma_z) / max(1.0 - rho * rho, 1e-6)
+    h = mu0 + math.sqrt(var_stat) * rng.gaussian()
+    hs, ys = [], []
+    for t in range(T):
+        mu = mus[(t // period) % len(mus)]
+        if t > 0:
+            h = mu + rho * (h - mu) + sigma_z * rng.gaussian()
+        h = min(max(h, -12.0), 4.0)
+        hs.append(h)
+        ys.append(math.exp(h / 2.0) * rng.gaussian())
+    return hs, ys

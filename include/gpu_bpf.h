@@ -1,0 +1,216 @@
+/*
+ * gpu_bpf.h — C ABI of the B200 (sm_100a) bootstrap particle filter for the
+ * stochastic-volatility model.
+ *
+ * Drop-in for the reference header gpu_bpf/gpu_bpf.cuh (Tugbars/Bootstrap-
+ * Particle-Filter-in-PTX), whose PTX edition gpu_bpf/gpu_bpf_full.cuh declares
+ * the same functions. Every reference entry point keeps its name, argument
+ * list and meaning; each declaration below cites the line it replaces.
+ * Entries marked "addition" have no reference counterpart.
+ *
+ * Model: h_t = mu + rho*(h_{t-1}-mu) + sigma_z*eps_t,  y_t = exp(h_t/2)*eta_t.
+ * Library: libgpubpf.so (plain C ABI, no CUDA or torch types in signatures;
+ * `void* stream` is a cudaStream_t).
+ */
+#ifndef GPU_BPF_H
+#define GPU_BPF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes (addition: the reference reports no errors)                   */
+/* ------------------------------------------------------------------------ */
+#define BPF_OK               0
+#define BPF_ERR_ARG          1  /* invalid argument (N<=0, |rho|>=1, sigma<=0, non-finite y, NULL) */
+#define BPF_ERR_CUDA         2  /* a CUDA runtime call failed                                       */
+#define BPF_ERR_ALLOC        3  /* device or pinned allocation failed                               */
+#define BPF_ERR_UNSUPPORTED  4  /* option outside this build (nu_state>0, bands, Silverman)         */
+#define BPF_ERR_STATE        5  /* call not valid in the filter's current state                     */
+#define BPF_ERR_DEGENERATE   6  /* every particle weight underflowed on a tick                      */
+#define BPF_ERR_NODEVICE     7  /* no CUDA device / kernel image for this GPU                       */
+
+/* Per-tick result, reference layout (gpu_bpf/gpu_bpf.cuh:21-24). */
+typedef struct {
+    float h_mean;   /* filtered mean E[h_t | y_{1:t}]                                */
+    float log_lik;  /* log p(y_t | y_{1:t-1}) (see gpu_bpf_set_loglik_semantics)     */
+} BpfResult;
+
+/* Full per-tick record (addition). 40 bytes. */
+typedef struct {
+    double  dloglik;        /* increment log p(y_t | y_{1:t-1}), FP64                         */
+    double  loglik_ref;     /* reference value: log-evidence since the last resample           */
+    double  loglik_total;   /* FP64 running sum of dloglik since create                        */
+    float   h_mean;         /* filtered mean                                                   */
+    float   ess;            /* effective sample size 1/sum(W^2) before resampling             */
+    int32_t resampled;      /* 1 if this tick resampled                                        */
+    int32_t tick;           /* tick index (0-based)                                            */
+} BpfTickRecord;
+
+/*
+ * Filter state. The reference struct is public (gpu_bpf/gpu_bpf.cuh:30-54;
+ * gpu_bpf_full.cuh:80-126) and its tests read or write some fields
+ * directly, so those fields keep their names and meaning here. Device
+ * buffers live behind `impl`.
+ *   rho, sigma_z, mu   may be changed between ticks (read at every step)
+ *   ess_threshold      0 = always resample, else resample iff ESS/N < it
+ *   silverman_shrink   must stay 0 (jitter is not part of this build)
+ *   did_resample, resample_count, timestep, last_h_est: refreshed whenever a
+ *                      result is read back (gpu_bpf_step / get_result)
+ */
+typedef struct {
+    int    n_particles;
+    float  rho, sigma_z, mu, nu_state, nu_obs;
+    float  silverman_shrink;
+    float  ess_threshold;
+    int    did_resample;
+    int    resample_count;
+    int    timestep;
+    float  last_h_est;
+    void*  stream;          /* cudaStream_t owned by the filter */
+    void*  impl;            /* opaque */
+} GpuBpfState;
+
+/* ---- Reference API ------------------------------------------------------- */
+
+/* gpu_bpf/gpu_bpf.cuh:56-57. Seeds the per-slot PCG32 streams and draws h_0
+ * from N(mu, sigma_z^2/max(1-rho^2,1e-6)) (gpu_bpf_ptx_full.cu:340-438).
+ * Default ess_threshold 0.5 (PTX edition, gpu_bpf_ptx_full.cu:356).
+ * Returns NULL on failure (reason in gpu_bpf_last_error()); nu_state > 0 is
+ * rejected with BPF_ERR_UNSUPPORTED. */
+GpuBpfState* gpu_bpf_create(int n_particles, float rho, float sigma_z, float mu,
+                            float nu_state, float nu_obs, int seed);
+
+/* gpu_bpf/gpu_bpf.cuh:58 (gpu_bpf_ptx_full.cu:444-463). NULL is a no-op. */
+void gpu_bpf_destroy(GpuBpfState* state);
+
+/* gpu_bpf/gpu_bpf.cuh:59 (gpu_bpf_ptx_full.cu:764-771): one tick, synchronous.
+ * On error returns {NaN, NaN} and sets gpu_bpf_last_error(). */
+BpfResult gpu_bpf_step(GpuBpfState* state, float y_t);
+
+/* gpu_bpf/gpu_bpf.cuh:60 (gpu_bpf_ptx_full.cu:550-748): enqueue one tick on
+ * state->stream. Never synchronises (the resampling decision is taken on the
+ * device). */
+void gpu_bpf_step_async(GpuBpfState* state, float y_t);
+
+/* gpu_bpf/gpu_bpf.cuh:61 (gpu_bpf_ptx_full.cu:754-762): result of the last
+ * enqueued tick; waits for it. */
+BpfResult gpu_bpf_get_result(GpuBpfState* state);
+
+/* gpu_bpf/gpu_bpf.cuh:63-67 (gpu_bpf_ptx_full.cu:834-852): run a filter over a
+ * series, RMSE of h_mean vs true_h after the first 100 ticks. Returns NaN on
+ * error. */
+double gpu_bpf_run_rmse(const double* returns, const double* true_h, int n_ticks,
+                        int n_particles, float rho, float sigma_z, float mu,
+                        float nu_state, float nu_obs, int seed);
+
+/* gpu_bpf/gpu_bpf.cuh:71-72. Only the single-band identity configuration
+ * (n_bands == 1, scale 1) is accepted; anything else records
+ * BPF_ERR_UNSUPPORTED. */
+void gpu_bpf_set_bands(int n_particles, int n_bands, const float* fracs, const float* scales);
+
+/* gpu_bpf/gpu_bpf.cuh:75-79. Records BPF_ERR_UNSUPPORTED. */
+void gpu_bpf_set_adaptive_bands(int n_particles,
+                                const float* calm_fracs,  const float* calm_scales,  int calm_nb,
+                                const float* alert_fracs, const float* alert_scales, int alert_nb,
+                                const float* panic_fracs, const float* panic_scales, int panic_nb,
+                                float thresh_alert, float thresh_panic);
+
+/* gpu_bpf/gpu_bpf.cuh:84 (gpu_bpf_ptx_full.cu:858-860; no clamping, as the PTX edition). */
+void gpu_bpf_set_ess_threshold(GpuBpfState* state, float threshold);
+
+/* gpu_bpf/gpu_bpf.cuh:85 (gpu_bpf_ptx_full.cu:862-864). Waits for enqueued ticks. */
+int gpu_bpf_get_resample_count(GpuBpfState* state);
+
+/* gpu_bpf/gpu_bpf_full.cuh:206-230 (gpu_bpf_ptx_full.cu:802-828): parameter
+ * access between ticks. set_rho clamps to (0.001, 0.999) like the reference. */
+float gpu_bpf_get_mu(GpuBpfState* state);
+float gpu_bpf_get_rho(GpuBpfState* state);
+void  gpu_bpf_set_mu(GpuBpfState* state, float mu);
+void  gpu_bpf_set_rho(GpuBpfState* state, float rho);
+
+/* gpu_bpf/gpu_bpf_full.cuh:197-204: online mu/rho learning is not part of
+ * this build (the adjoint form replaces it). enable_* record
+ * BPF_ERR_UNSUPPORTED; disable is a no-op. */
+void gpu_bpf_enable_mu_learning(GpuBpfState* state, int mode, int K, float c, float t0, float gamma);
+void gpu_bpf_disable_mu_learning(GpuBpfState* state);
+void gpu_bpf_enable_rho_learning(GpuBpfState* state, int enable);
+
+/* ---- Additions ------------------------------------------------------------ */
+
+/* Last status recorded by any call on this host thread, and its text. */
+int         gpu_bpf_last_error(void);
+const char* gpu_bpf_error_string(int code);
+
+/* Runs n_ticks ticks on host observations y[0..n_ticks). Inputs are staged
+ * through pinned memory; ticks run as CUDA-graph chunks with no host sync
+ * inside a chunk. out (may be NULL) receives one BpfResult per tick, rec
+ * (may be NULL) one BpfTickRecord per tick. Returns a BPF_* status. */
+int gpu_bpf_step_many(GpuBpfState* state, const float* y, int n_ticks,
+                      BpfResult* out, BpfTickRecord* rec);
+
+/* Same on device memory: y_dev[n_ticks] and rec_dev[n_ticks] are device
+ * pointers; enqueued on state->stream without synchronising. The launch
+ * sequence is captured once into a CUDA graph per (y_dev, rec_dev, n_ticks,
+ * parameters) and replayed on later calls with the same buffers. */
+int gpu_bpf_step_many_device(GpuBpfState* state, const float* y_dev, int n_ticks,
+                             BpfTickRecord* rec_dev);
+
+/* Re-seed the filter in place (addition): h_0 redrawn from the stationary
+ * law of the current (mu, rho, sigma_z) with the given seed, tick counter,
+ * resampling-uniform stream and log-likelihood sums reset. Stream-ordered,
+ * no allocation, no host synchronisation. */
+int gpu_bpf_reset(GpuBpfState* state, int seed);
+
+/* Full record of the last tick (waits). */
+int gpu_bpf_get_record(GpuBpfState* state, BpfTickRecord* out);
+
+/* ESS of the last tick and the FP64 running log-likelihood (wait). */
+float  gpu_bpf_get_ess(GpuBpfState* state);
+double gpu_bpf_get_loglik_total(GpuBpfState* state);
+
+/* BpfResult.log_lik semantics: 0 (default) = increment log p(y_t|y_{1:t-1});
+ * 1 = the reference's value max+ln(sum w/N) over the carried weights, i.e.
+ * the log-evidence since the last resample (bpf_kernels_full.ptx:755-775). */
+int gpu_bpf_set_loglik_semantics(GpuBpfState* state, int mode);
+
+/* Particles h[0..N) of the current state (waits). */
+int gpu_bpf_get_particles(GpuBpfState* state, float* h_out);
+
+/* Ancestor recording: when enabled, every resampling tick stores its
+ * ancestor indices; gpu_bpf_get_ancestors copies the last tick's (waits) and
+ * returns 1 if that tick resampled, 0 if not, <0 on error. */
+int gpu_bpf_record_ancestors(GpuBpfState* state, int enable);
+int gpu_bpf_get_ancestors(GpuBpfState* state, int32_t* anc_out);
+
+/* Resampling inputs of the last tick (waits): the tile-relative FP32
+ * weights w[0..N), the power-of-two exponent of each 4096-particle tile
+ * (n_tiles = ceil(N/4096) entries) and the 23-bit resampling uniform U.
+ * Ancestors are a deterministic function of these. */
+int gpu_bpf_get_resample_inputs(GpuBpfState* state, float* w_out, int32_t* tile_exp_out,
+                                uint32_t* u23_out);
+
+/* Kernel profiling: when enabled, the duration of every pass-1 and pass-2
+ * launch is timed with CUDA events on state->stream. read returns the sums
+ * (ms) and launch counts since enabling. */
+int gpu_bpf_profile(GpuBpfState* state, int enable);
+int gpu_bpf_profile_read(GpuBpfState* state, double* pass1_ms, double* pass2_ms,
+                         int* pass1_launches, int* pass2_launches);
+
+/* Number of kernel launches this library has issued (all filters). */
+long long gpu_bpf_launch_count(void);
+
+/* Device-side PCG32 probes: raw output of draw t for slots 0..n-1 and the
+ * normal the filter derives from it (writes host arrays). */
+int gpu_bpf_debug_pcg32(int seed, int n, int t, uint32_t* out);
+int gpu_bpf_debug_normals(int seed, int n, int t, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPU_BPF_H */

@@ -1,0 +1,482 @@
+/*
+ * bpf_oracle.c — CPU oracle of the SV bootstrap particle filter.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker for libgpubpf.so and the
+ * timed CPU baseline; nothing in the product links or calls it. It restates
+ * the reference algorithm (Tugbars/Bootstrap-Particle-Filter-in-PTX) on the
+ * CPU, each function citing the reference lines it follows:
+ *
+ *   orc_pcg32_*          PCG32 stream of particle slot i
+ *                        (ptx_assembly/bpf_kernels_full.ptx:74-91, :140-157;
+ *                        known-answer formula tests/test_rng_diag.cu:78-96)
+ *   orc_host_pcg32       resampling-uniform stream (gpu_bpf/gpu_bpf_ptx_full.cu:241-251)
+ *   orc_acklam_f64       Acklam inverse normal CDF in FP64 (PTX :166-205 in FP32)
+ *   orc_icdf_f64         the same plus Acklam's published Halley refinement step
+ *                        (erfc-based): the FP64 oracle's inverse normal CDF
+ *   orc_filter_f64       FP64 filter in this build's semantics, optionally
+ *                        replaying resampling decisions and ancestors
+ *   orc_resample_fixed   exact mirror of the GPU fixed-point systematic resampling
+ *   orc_ref_run          FP32 restatement of the reference tick loop
+ *                        (gpu_bpf_ptx_full.cu:340-771 with PTX kernels :51-842),
+ *                        OpenMP over particles: the CPU baseline
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define PCG_A 6364136223846793005ULL
+#define HOST_INC 1442695040888963407ULL
+#define TILE 4096
+#define FIXF 50
+#define NK_EMPTY (-(1 << 30))
+
+/* ------------------------------------------------------------------------- */
+/* PCG32                                                                      */
+/* ------------------------------------------------------------------------- */
+uint32_t orc_pcg32_output(uint64_t old) {
+    uint32_t xsh = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xsh >> rot) | (xsh << ((-rot) & 31u));
+}
+
+/* bpf_init_rng: inc = (2i+1)|1 in 32 bits, state = (seed*A + inc)*A + inc */
+void orc_pcg32_init(int seed, uint32_t i, uint64_t* state, uint64_t* inc) {
+    uint32_t i2 = 2u * i + 1u;
+    uint64_t c = (uint64_t)(i2 | 1u);
+    uint64_t s = (uint64_t)(int64_t)seed * PCG_A + c;
+    s = s * PCG_A + c;
+    *state = s;
+    *inc = c;
+}
+
+/* Output of draw t (t = 0 is the init draw) by stepping the LCG t times. */
+uint32_t orc_pcg32_draw_stepped(int seed, uint32_t i, int t) {
+    uint64_t s, inc;
+    orc_pcg32_init(seed, i, &s, &inc);
+    for (int k = 0; k < t; ++k) s = s * PCG_A + inc;
+    return orc_pcg32_output(s);
+}
+
+/* Jump-ahead constants A^t and sum_{k<t} A^k (mod 2^64), O(log t). */
+void orc_pcg32_jump(uint64_t t, uint64_t* At, uint64_t* Bt) {
+    uint64_t acc_mult = 1, acc_plus = 0, cur_mult = PCG_A, cur_plus = 1;
+    while (t > 0) {
+        if (t & 1) { acc_mult *= cur_mult; acc_plus = acc_plus * cur_mult + cur_plus; }
+        cur_plus = (cur_mult + 1) * cur_plus;
+        cur_mult *= cur_mult;
+        t >>= 1;
+    }
+    *At = acc_mult; *Bt = acc_plus;
+}
+
+uint32_t orc_pcg32_draw_jump(int seed, uint32_t i, int t) {
+    uint64_t s0, inc, At, Bt;
+    orc_pcg32_init(seed, i, &s0, &inc);
+    orc_pcg32_jump((uint64_t)t, &At, &Bt);
+    return orc_pcg32_output(At * s0 + Bt * inc);
+}
+
+/* u = (out >> 9) * 2^-23 clamped to [0x358637BD, 0x3F7FFBCE] (PTX :159-164) */
+float orc_uniform(uint32_t out) {
+    float u = (float)(out >> 9) * 1.1920928955078125e-07f;
+    const float lo = 9.99999997475242708e-07f, hi = 0.999935984611511230f;
+    if (u < lo) u = lo;
+    if (u > hi) u = hi;
+    return u;
+}
+
+/* gpu_bpf_ptx_full.cu:241-251 */
+uint32_t orc_host_pcg32(uint64_t* state) {
+    uint64_t old = *state;
+    *state = old * PCG_A + HOST_INC;
+    return orc_pcg32_output(old);
+}
+uint64_t orc_host_seed(int seed) { return (uint64_t)(int64_t)seed * 67890ULL + 12345ULL; }
+
+/* ------------------------------------------------------------------------- */
+/* Acklam inverse normal CDF (P. J. Acklam 2003, published coefficients)      */
+/* ------------------------------------------------------------------------- */
+static const double AK_A[6] = {-3.969683028665376e+01, 2.209460984245205e+02, -2.759285104469687e+02,
+                               1.383577518672690e+02, -3.066479806614716e+01, 2.506628277459239e+00};
+static const double AK_B[5] = {-5.447609879822406e+01, 1.615858368580409e+02, -1.556989798598866e+02,
+                               6.680131188771972e+01, -1.328068155288572e+01};
+static const double AK_C[6] = {-7.784894002430293e-03, -3.223964580411365e-01, -2.400758277161838e+00,
+                               -2.549732539343734e+00, 4.374664141464968e+00, 2.938163982698783e+00};
+static const double AK_D[4] = {7.784695709041462e-03, 3.224671290700398e-01, 2.445134137142996e+00,
+                               3.754408661907416e+00};
+
+double orc_acklam_f64(double p) {
+    double q = p - 0.5;
+    if (fabs(q) < 0.47575) {
+        double r = q * q;
+        double num = (((((AK_A[0] * r + AK_A[1]) * r + AK_A[2]) * r + AK_A[3]) * r + AK_A[4]) * r + AK_A[5]) * q;
+        double den = ((((AK_B[0] * r + AK_B[1]) * r + AK_B[2]) * r + AK_B[3]) * r + AK_B[4]) * r + 1.0;
+        return num / den;
+    }
+    int low = p < 0.5;
+    double pp = low ? p : 1.0 - p;
+    double s = sqrt(-2.0 * log(pp));
+    double num = ((((AK_C[0] * s + AK_C[1]) * s + AK_C[2]) * s + AK_C[3]) * s + AK_C[4]) * s + AK_C[5];
+    double den = (((AK_D[0] * s + AK_D[1]) * s + AK_D[2]) * s + AK_D[3]) * s + 1.0;
+    double z = num / den;
+    return low ? z : -z;
+}
+
+/* Acklam's refinement: one Halley step on Phi(z) - p, Phi via erfc. The upper
+ * half uses the symmetry z(p) = -z(1-p) so that Phi(z) - p never cancels. */
+double orc_icdf_f64(double p) {
+    if (p > 0.5) return -orc_icdf_f64(1.0 - p);
+    double z = orc_acklam_f64(p);
+    const double e = 0.5 * erfc(-z / 1.41421356237309504880) - p;
+    const double u = e * 2.50662827463100050242 * exp(0.5 * z * z);
+    return z - u / (1.0 + 0.5 * z * u);
+}
+
+/* FP32 Acklam with IEEE operations (reference restatement; PTX :166-205) */
+static float acklam_f32(float u) {
+    float q = u - 0.5f;
+    if (fabsf(q) < 0.475749999284744263f) {
+        float r = q * q;
+        float num = fmaf(-3.969683028665376e+01f, r, 2.209460984245205e+02f);
+        num = fmaf(num, r, -2.759285104469687e+02f);
+        num = fmaf(num, r, 1.383577518672690e+02f);
+        num = fmaf(num, r, -3.066479806614716e+01f);
+        num = fmaf(num, r, 2.506628277459239e+00f);
+        num = q * num;
+        float den = fmaf(-5.447609879822406e+01f, r, 1.615858368580409e+02f);
+        den = fmaf(den, r, -1.556989798598866e+02f);
+        den = fmaf(den, r, 6.680131188771972e+01f);
+        den = fmaf(den, r, -1.328068155288572e+01f);
+        den = fmaf(den, r, 1.0f);
+        return num / den;
+    }
+    int low = u < 0.5f;
+    float p = low ? u : 1.0f - u;
+    float s = sqrtf(-2.0f * logf(p));
+    float num = fmaf(-7.784894002430293e-03f, s, -3.223964580411365e-01f);
+    num = fmaf(num, s, -2.400758277161838e+00f);
+    num = fmaf(num, s, -2.549732539343734e+00f);
+    num = fmaf(num, s, 4.374664141464968e+00f);
+    num = fmaf(num, s, 2.938163982698783e+00f);
+    float den = fmaf(7.784695709041462e-03f, s, 3.224671290700398e-01f);
+    den = fmaf(den, s, 2.445134137142996e+00f);
+    den = fmaf(den, s, 3.754408661907416e+00f);
+    den = fmaf(den, s, 1.0f);
+    float z = num / den;
+    return low ? z : -z;
+}
+float orc_acklam_f32(float u) { return acklam_f32(u); }
+
+/* ------------------------------------------------------------------------- */
+/* Observation log-density (PTX :414-451)                                     */
+/* ------------------------------------------------------------------------- */
+static double obs_logpdf_f64(double y, double h, double nu, double c_obs) {
+    double eta2 = y * y * exp(-h);
+    if (nu > 0.0) return c_obs - 0.5 * (nu + 1.0) * log1p(eta2 / nu) - 0.5 * h;
+    return -0.91893853320467274178 - 0.5 * eta2 - 0.5 * h;
+}
+static double c_obs_of(double nu) {
+    if (!(nu > 0.0)) return 0.0;
+    return lgamma((nu + 1.0) / 2.0) - lgamma(nu / 2.0) - 0.5 * log(nu * 3.14159265358979323846);
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP64 filter (this build's semantics: increment log-likelihood, carried      */
+/* weights on skipped ticks, resampling drawn from the host-formula U stream)  */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int n_particles;
+    float rho, sigma_z, mu, nu_obs;
+    int seed;
+    float ess_threshold;
+} OrcConfig;
+
+static int ceil_log2_u(unsigned n) { int c = 0; while ((1ull << c) < (unsigned long long)n) ++c; return c; }
+
+/*
+ * y[T]; anc_replay: [T][N] ancestors used on resampling ticks (NULL = own FP64
+ * systematic resampling); flags_replay: [T] decisions to replay (NULL = own).
+ * Outputs (each may be NULL): dll[T], ll_ref[T], hmean[T], ess[T], flags_out[T].
+ */
+int orc_filter_f64(const OrcConfig* c, const float* y, int T,
+                   const int32_t* anc_replay, const int32_t* flags_replay,
+                   double* dll, double* ll_ref, double* hmean, double* ess, int32_t* flags_out) {
+    const int N = c->n_particles;
+    if (N <= 0 || T < 0) return 1;
+    double* h = (double*)malloc(sizeof(double) * N);
+    double* hn = (double*)malloc(sizeof(double) * N);
+    double* lw = (double*)malloc(sizeof(double) * N);
+    double* lwc = (double*)malloc(sizeof(double) * N);
+    double* cdf = (double*)malloc(sizeof(double) * N);
+    if (!h || !hn || !lw || !lwc || !cdf) { free(h); free(hn); free(lw); free(lwc); free(cdf); return 2; }
+    const double mu = c->mu, rho = c->rho, sig = c->sigma_z, nu = c->nu_obs, cobs = c_obs_of(nu);
+    const double sstat = sqrt(sig * sig / fmax(1.0 - rho * rho, 1e-6));
+    for (int i = 0; i < N; ++i) {
+        float u = orc_uniform(orc_pcg32_draw_jump(c->seed, (uint32_t)i, 0));
+        h[i] = mu + sstat * orc_icdf_f64((double)u);
+        lwc[i] = 0.0;
+    }
+    uint64_t ustate = orc_host_seed(c->seed);
+    int prev_res = 1;
+    double lse_prev = log((double)N), llr = 0.0;
+    for (int t = 0; t < T; ++t) {
+        if (t > 0) {
+            uint64_t At, Bt;
+            orc_pcg32_jump((uint64_t)t, &At, &Bt);
+            for (int i = 0; i < N; ++i) {
+                uint64_t s0, inc;
+                orc_pcg32_init(c->seed, (uint32_t)i, &s0, &inc);
+                float u = orc_uniform(orc_pcg32_output(At * s0 + Bt * inc));
+                h[i] = mu + rho * (h[i] - mu) + sig * orc_icdf_f64((double)u);
+            }
+        }
+        double M = -INFINITY;
+        for (int i = 0; i < N; ++i) {
+            lw[i] = (prev_res ? 0.0 : lwc[i]) + obs_logpdf_f64((double)y[t], h[i], nu, cobs);
+            if (lw[i] > M) M = lw[i];
+        }
+        double S = 0.0, Q = 0.0, H = 0.0;
+        for (int i = 0; i < N; ++i) {
+            double e = exp(lw[i] - M);
+            S += e; Q += e * e; H += e * h[i];
+            cdf[i] = S;
+        }
+        const double lse = M + log(S);
+        const double d = lse - (prev_res ? log((double)N) : lse_prev);
+        llr = (prev_res ? 0.0 : llr) + d;
+        const double es = S * S / Q;
+        if (dll) dll[t] = d;
+        if (ll_ref) ll_ref[t] = llr;
+        if (hmean) hmean[t] = H / S;
+        if (ess) ess[t] = es;
+        int res = flags_replay ? (flags_replay[t] != 0)
+                               : ((c->ess_threshold <= 0.0f) || (es / (double)N < (double)c->ess_threshold));
+        if (flags_out) flags_out[t] = res;
+        if (res) {
+            uint32_t u23 = orc_host_pcg32(&ustate) >> 9;
+            if (anc_replay) {
+                const int32_t* a = anc_replay + (size_t)t * N;
+                for (int i = 0; i < N; ++i) hn[i] = h[a[i]];
+            } else {
+                const double step = S / (double)N, u0 = (double)u23 * 1.1920928955078125e-07;
+                int j = 0;
+                for (int i = 0; i < N; ++i) {
+                    double target = (u0 + (double)i) * step;
+                    while (j < N - 1 && !(cdf[j] > target)) ++j;
+                    hn[i] = h[j];
+                }
+            }
+            double* tmp = h; h = hn; hn = tmp;
+            prev_res = 1;
+        } else {
+            memcpy(lwc, lw, sizeof(double) * N);
+            lse_prev = lse;
+            prev_res = 0;
+        }
+    }
+    free(h); free(hn); free(lw); free(lwc); free(cdf);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Exact mirror of the GPU fixed-point systematic resampling                 */
+/* ------------------------------------------------------------------------- */
+/*
+ * w[N]: tile-relative FP32 weights in [0,1]; nexp[G]: power-of-two exponent of
+ * each 4096-particle tile; u23: 23-bit uniform. Element mass (tile frame)
+ * I_j = floor(w_j 2^50); tile mass in the global frame Ehat_k = E_k >> r_k with
+ * r_k = nM - n_k + 50 - Fg, Fg = min(50, 62 - ceil(log2 N)); global CDF
+ * C_j = P_k + (L_j >> r_k) with L_j the tile-local inclusive prefix; targets
+ * t_i = base + i*delta, delta = floor(T/N), base = floor(u23*delta/2^23);
+ * ancestor a_i = min{ j : C_j > t_i }.
+ */
+int orc_resample_fixed(int N, const float* w, const int32_t* nexp, uint32_t u23, int32_t* anc) {
+    if (N <= 0) return 1;
+    const int G = (N + TILE - 1) / TILE;
+    int nM = NK_EMPTY;
+    for (int k = 0; k < G; ++k) if (nexp[k] > nM) nM = nexp[k];
+    if (nM == NK_EMPTY) return 2;
+    int Fg = 62 - ceil_log2_u((unsigned)N);
+    if (Fg > FIXF) Fg = FIXF;
+    uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * N);
+    if (!C) return 3;
+    uint64_t P = 0;
+    for (int k = 0; k < G; ++k) {
+        const int j0 = k * TILE, j1 = (j0 + TILE < N) ? j0 + TILE : N;
+        const int r = (nexp[k] == NK_EMPTY) ? 64 : nM - nexp[k] + FIXF - Fg;
+        uint64_t L = 0;
+        for (int j = j0; j < j1; ++j) {
+            L += (uint64_t)(w[j] * 1125899906842624.0f);
+            C[j] = P + (r >= 64 ? 0ull : (L >> r));
+        }
+        P += (r >= 64 ? 0ull : (L >> r));
+    }
+    const uint64_t T = P;
+    uint64_t delta = T / (uint64_t)N;
+    if (delta == 0) delta = 1;
+    const unsigned __int128 prod = (unsigned __int128)u23 * delta;
+    const uint64_t base = (uint64_t)(prod >> 23);
+    int j = 0;
+    for (int i = 0; i < N; ++i) {
+        const uint64_t t = base + (uint64_t)i * delta;
+        while (j < N - 1 && !(C[j] > t)) ++j;
+        anc[i] = j;
+    }
+    free(C);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP32 restatement of the reference tick loop (CPU baseline)                 */
+/* ------------------------------------------------------------------------- */
+/*
+ * Follows gpu_bpf_step_async (gpu_bpf_ptx_full.cu:550-748) with 1 band,
+ * nu_state = 0, Silverman off, no learning: propagate_weight (PTX :231-458),
+ * accumulate on skipped ticks (:601-604), max / exp_sub / sum / scale_wh /
+ * sum(wh) / compute_loglik (PTX :488-775), sum(w^2) and the ESS decision
+ * (:656-685), inclusive scan + systematic resample (:691-706, PTX :782-842).
+ * Transcendentals use libm in FP32 where the PTX uses approximate MUFU ops.
+ * hmean/loglik receive the reference BpfResult of every tick.
+ */
+int orc_ref_run(int N, float rho, float sigma_z, float mu, float nu_obs, int seed, float ess_threshold,
+                const float* y, int T, float* hmean, float* loglik, int nthreads, int* resample_count) {
+    if (N <= 0 || T < 0) return 1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    uint64_t* rng = (uint64_t*)malloc(sizeof(uint64_t) * 2 * (size_t)N);
+    float* h = (float*)malloc(sizeof(float) * N);
+    float* h2 = (float*)malloc(sizeof(float) * N);
+    float* lw = (float*)malloc(sizeof(float) * N);
+    float* lwp = (float*)malloc(sizeof(float) * N);
+    float* w = (float*)malloc(sizeof(float) * N);
+    float* cdf = (float*)malloc(sizeof(float) * N);
+    int nchunk = 1;
+#ifdef _OPENMP
+    nchunk = omp_get_max_threads();
+#endif
+    float* part = (float*)malloc(sizeof(float) * (nchunk + 1));
+    if (!rng || !h || !h2 || !lw || !lwp || !w || !cdf || !part) {
+        free(rng); free(h); free(h2); free(lw); free(lwp); free(w); free(cdf); free(part);
+        return 2;
+    }
+    const float c_obs = (nu_obs > 0.0f) ? (float)c_obs_of(nu_obs) : 0.0f;
+    const float std_stat = sqrtf((sigma_z * sigma_z) / fmaxf(1.0f - rho * rho, 1e-6f));
+    /* bpf_init_rng + bpf_init_particles */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N; ++i) {
+        uint64_t s, inc;
+        orc_pcg32_init(seed, (uint32_t)i, &s, &inc);
+        uint32_t o = orc_pcg32_output(s);
+        s = s * PCG_A + inc;
+        h[i] = fmaf(std_stat, acklam_f32(orc_uniform(o)), mu);
+        rng[2 * (size_t)i] = s;
+        rng[2 * (size_t)i + 1] = inc;
+    }
+    uint64_t host_rng = orc_host_seed(seed);
+    int did_resample = 1, count = 0;
+    const float log2e = 1.44269504088896340736f, ln2 = 0.693147180559945309417f;
+    for (int t = 0; t < T; ++t) {
+        const float yt = y[t];
+        const int do_prop = t > 0;
+        const int acc = (t > 0) && !did_resample;
+        float mx = -1e30f;
+#pragma omp parallel for schedule(static) reduction(max : mx)
+        for (int i = 0; i < N; ++i) {
+            float hi = h[i];
+            if (do_prop) {
+                uint64_t s = rng[2 * (size_t)i], inc = rng[2 * (size_t)i + 1];
+                uint32_t o = orc_pcg32_output(s);
+                rng[2 * (size_t)i] = s * PCG_A + inc;
+                float eps = acklam_f32(orc_uniform(o));
+                float dev = rho * (hi - mu);
+                hi = fmaf(sigma_z, eps, mu + dev);
+                h[i] = hi;
+            }
+            float eta = yt * exp2f(hi * -0.5f * log2e);
+            float l;
+            if (nu_obs > 0.0f) {
+                float ta = eta * eta / nu_obs + 1.0f;
+                l = fmaf(-0.5f, hi, c_obs + (-(nu_obs + 1.0f) * 0.5f) * (log2f(ta) * ln2));
+            } else {
+                l = fmaf(-0.5f, hi, fmaf(-0.5f, eta * eta, -0.918938517570496f));
+            }
+            if (acc) l += lwp[i];
+            lw[i] = l;
+            if (l > mx) mx = l;
+        }
+        float sw = 0.0f;
+#pragma omp parallel for schedule(static) reduction(+ : sw)
+        for (int i = 0; i < N; ++i) { w[i] = exp2f((lw[i] - mx) * log2e); sw += w[i]; }
+        const float inv = 1.0f / sw;
+        float hest = 0.0f, sw2 = 0.0f;
+#pragma omp parallel for schedule(static) reduction(+ : hest, sw2)
+        for (int i = 0; i < N; ++i) { w[i] *= inv; hest += w[i] * h[i]; sw2 += w[i] * w[i]; }
+        float r = sw / (float)N;
+        if (r < 7.27150555e-31f) r = 7.27150555e-31f;
+        hmean[t] = hest;
+        loglik[t] = log2f(r) * ln2 + mx;
+        int do_res = 1;
+        if (ess_threshold > 0.0f) {
+            float essv = 1.0f / fmaxf(sw2, 1e-30f);
+            do_res = (essv / (float)N) < ess_threshold;
+        }
+        if (do_res) {
+            did_resample = 1;
+            ++count;
+            /* inclusive scan (chunked, parallel) */
+#pragma omp parallel
+            {
+                int tid = 0, nt = 1;
+#ifdef _OPENMP
+                tid = omp_get_thread_num(); nt = omp_get_num_threads();
+#endif
+                int a = (int)((long long)N * tid / nt), b = (int)((long long)N * (tid + 1) / nt);
+                float acc2 = 0.0f;
+                for (int i = a; i < b; ++i) { acc2 += w[i]; cdf[i] = acc2; }
+                part[tid + 1] = acc2;
+#pragma omp barrier
+#pragma omp single
+                {
+                    part[0] = 0.0f;
+                    for (int k = 1; k <= nt; ++k) part[k] += part[k - 1];
+                }
+                float off = part[tid];
+                for (int i = a; i < b; ++i) cdf[i] += off;
+            }
+            const float u = (float)(orc_host_pcg32(&host_rng) >> 9) * (1.0f / 8388608.0f) / (float)N;
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < N; ++i) {
+                float target = (float)i / (float)N + u;
+                if (target >= 1.0f) target -= 1.0f;
+                int lo = 0, hi = N - 1;
+                while (lo < hi) {
+                    int mid = (lo + hi) >> 1;
+                    if (cdf[mid] < target) lo = mid + 1; else hi = mid;
+                }
+                h2[i] = h[lo];
+            }
+            float* tmp = h; h = h2; h2 = tmp;
+        } else {
+            did_resample = 0;
+            memcpy(lwp, lw, sizeof(float) * N);
+        }
+    }
+    if (resample_count) *resample_count = count;
+    free(rng); free(h); free(h2); free(lw); free(lwp); free(w); free(cdf); free(part);
+    return 0;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,150 @@
+"""ctypes face of the CPU oracle (oracle/bpf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+as the checker, and by bench.py's CPU-baseline leg. The product never
+imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "bpf_oracle.c")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(BUILD, "liboracle.so")
+
+CFLAGS = ["-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-std=gnu11"]
+
+
+def build(native: bool = False, force: bool = False) -> str:
+    """Compile the oracle; native=True adds -march=native (timed baseline)."""
+    out = os.path.join(BUILD, "liboracle_native.so" if native else "liboracle.so")
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(SRC):
+        return out
+    os.makedirs(BUILD, exist_ok=True)
+    flags = list(CFLAGS)
+    if native:
+        flags[0] = "-O3"
+        flags.append("-march=native")
+    subprocess.run(["gcc", *flags, SRC, "-o", out + ".tmp", "-lm"], check=True)
+    os.replace(out + ".tmp", out)
+    return out
+
+
+class OrcConfig(C.Structure):
+    _fields_ = [
+        ("n_particles", C.c_int),
+        ("rho", C.c_float), ("sigma_z", C.c_float), ("mu", C.c_float), ("nu_obs", C.c_float),
+        ("seed", C.c_int),
+        ("ess_threshold", C.c_float),
+    ]
+
+
+_LIBS: dict = {}
+
+
+def lib(native: bool = False) -> C.CDLL:
+    key = bool(native)
+    if key in _LIBS:
+        return _LIBS[key]
+    path = build(native=native)
+    L = C.CDLL(path)
+    u32, u64, i32, f32, f64 = C.c_uint32, C.c_uint64, C.c_int32, C.c_float, C.c_double
+    P = C.POINTER
+    L.orc_pcg32_output.restype = u32; L.orc_pcg32_output.argtypes = [u64]
+    L.orc_pcg32_init.restype = None; L.orc_pcg32_init.argtypes = [C.c_int, u32, P(u64), P(u64)]
+    L.orc_pcg32_draw_stepped.restype = u32; L.orc_pcg32_draw_stepped.argtypes = [C.c_int, u32, C.c_int]
+    L.orc_pcg32_draw_jump.restype = u32; L.orc_pcg32_draw_jump.argtypes = [C.c_int, u32, C.c_int]
+    L.orc_pcg32_jump.restype = None; L.orc_pcg32_jump.argtypes = [u64, P(u64), P(u64)]
+    L.orc_uniform.restype = f32; L.orc_uniform.argtypes = [u32]
+    L.orc_host_pcg32.restype = u32; L.orc_host_pcg32.argtypes = [P(u64)]
+    L.orc_host_seed.restype = u64; L.orc_host_seed.argtypes = [C.c_int]
+    L.orc_acklam_f64.restype = f64; L.orc_acklam_f64.argtypes = [f64]
+    L.orc_icdf_f64.restype = f64; L.orc_icdf_f64.argtypes = [f64]
+    L.orc_acklam_f32.restype = f32; L.orc_acklam_f32.argtypes = [f32]
+    L.orc_filter_f64.restype = C.c_int
+    L.orc_filter_f64.argtypes = [P(OrcConfig), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_resample_fixed.restype = C.c_int
+    L.orc_resample_fixed.argtypes = [C.c_int, C.c_void_p, C.c_void_p, u32, C.c_void_p]
+    L.orc_ref_run.restype = C.c_int
+    L.orc_ref_run.argtypes = [C.c_int, f32, f32, f32, f32, C.c_int, f32, C.c_void_p, C.c_int,
+                              C.c_void_p, C.c_void_p, C.c_int, P(C.c_int)]
+    L.orc_num_threads.restype = C.c_int; L.orc_num_threads.argtypes = []
+    _LIBS[key] = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def pcg32_draw(seed: int, i: int, t: int, stepped: bool = False) -> int:
+    L = lib()
+    return (L.orc_pcg32_draw_stepped if stepped else L.orc_pcg32_draw_jump)(seed, i, t)
+
+
+def pcg32_init(seed: int, i: int):
+    L = lib()
+    s, inc = C.c_uint64(), C.c_uint64()
+    L.orc_pcg32_init(seed, i, C.byref(s), C.byref(inc))
+    return s.value, inc.value
+
+
+def host_u23_stream(seed: int, n: int):
+    L = lib()
+    st = C.c_uint64(L.orc_host_seed(seed))
+    return [L.orc_host_pcg32(C.byref(st)) >> 9 for _ in range(n)]
+
+
+def filter_f64(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.0, nu_obs=0.0,
+               anc_replay=None, flags_replay=None):
+    """FP64 oracle run. Returns dict of per-tick arrays."""
+    L = lib()
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    T = y.shape[0]
+    cfg = OrcConfig(int(n_particles), rho, sigma_z, mu, nu_obs, int(seed), ess_threshold)
+    out = {k: np.zeros(T, dtype=np.float64) for k in ("dll", "ll_ref", "hmean", "ess")}
+    flags = np.zeros(T, dtype=np.int32)
+    anc = None if anc_replay is None else np.ascontiguousarray(anc_replay, dtype=np.int32)
+    fr = None if flags_replay is None else np.ascontiguousarray(flags_replay, dtype=np.int32)
+    rc = L.orc_filter_f64(C.byref(cfg), _ptr(y), T, _ptr(anc), _ptr(fr), _ptr(out["dll"]), _ptr(out["ll_ref"]),
+                          _ptr(out["hmean"]), _ptr(out["ess"]), _ptr(flags))
+    if rc != 0:
+        raise RuntimeError(f"orc_filter_f64 failed ({rc})")
+    out["resampled"] = flags
+    return out
+
+
+def resample_fixed(w, tile_exp, u23):
+    L = lib()
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    te = np.ascontiguousarray(tile_exp, dtype=np.int32)
+    anc = np.zeros(w.shape[0], dtype=np.int32)
+    rc = L.orc_resample_fixed(int(w.shape[0]), _ptr(w), _ptr(te), int(u23), _ptr(anc))
+    if rc != 0:
+        raise RuntimeError(f"orc_resample_fixed failed ({rc})")
+    return anc
+
+
+def ref_run(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.5, nu_obs=0.0, nthreads=0, native=False):
+    """FP32 restatement of the reference tick loop: (hmean[T], loglik[T], resample_count)."""
+    L = lib(native)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    T = y.shape[0]
+    hm = np.zeros(T, dtype=np.float32)
+    ll = np.zeros(T, dtype=np.float32)
+    cnt = C.c_int(0)
+    rc = L.orc_ref_run(int(n_particles), rho, sigma_z, mu, nu_obs, int(seed), ess_threshold, _ptr(y), T,
+                       _ptr(hm), _ptr(ll), int(nthreads), C.byref(cnt))
+    if rc != 0:
+        raise RuntimeError(f"orc_ref_run failed ({rc})")
+    return hm, ll, cnt.value
+
+
+def num_threads(native: bool = False) -> int:
+    return lib(native).orc_num_threads()

@@ -1,0 +1,111 @@
+"""CPU tests of the C ABI: the library builds for sm_100a, loads, exports every
+symbol include/gpu_bpf.h declares, and validates arguments on the host before
+any CUDA call (no GPU needed)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import PKG_DIR, REPO
+
+HEADER = os.path.join(REPO, "include", "gpu_bpf.h")
+
+
+def header_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gpu_bpf_\w+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bpf_build", os.path.join(PKG_DIR, "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    mod.build_library()
+    import gpubpf
+    return gpubpf.load()
+
+
+def test_header_declares_reference_api():
+    names = header_functions()
+    # gpu_bpf/gpu_bpf.cuh:56-85 and gpu_bpf_full.cuh:197-285
+    for ref in ["gpu_bpf_create", "gpu_bpf_destroy", "gpu_bpf_step", "gpu_bpf_step_async",
+                "gpu_bpf_get_result", "gpu_bpf_run_rmse", "gpu_bpf_set_bands", "gpu_bpf_set_adaptive_bands",
+                "gpu_bpf_set_ess_threshold", "gpu_bpf_get_resample_count", "gpu_bpf_enable_mu_learning",
+                "gpu_bpf_disable_mu_learning", "gpu_bpf_enable_rho_learning", "gpu_bpf_get_mu",
+                "gpu_bpf_get_rho", "gpu_bpf_set_mu", "gpu_bpf_set_rho"]:
+        assert ref in names
+
+
+def test_every_declared_symbol_is_exported(lib):
+    for name in header_functions():
+        assert hasattr(lib, name), name
+
+
+def test_binding_covers_header():
+    from gpubpf import _lib
+    assert set(header_functions()) <= set(_lib.SIGNATURES)
+
+
+def test_result_layouts():
+    from gpubpf import _lib
+    assert C.sizeof(_lib.BpfResult) == 8
+    assert C.sizeof(_lib.BpfTickRecord) == 40
+
+
+def test_host_argument_validation(lib):
+    from gpubpf import _lib
+    bad = [
+        (0, 0.97, 0.15, -1.0, 0.0, 0.0, 42),
+        (-5, 0.97, 0.15, -1.0, 0.0, 0.0, 42),
+        (4096, 1.0, 0.15, -1.0, 0.0, 0.0, 42),
+        (4096, 0.97, 0.0, -1.0, 0.0, 0.0, 42),
+        (4096, 0.97, -0.1, -1.0, 0.0, 0.0, 42),
+        (4096, float("nan"), 0.15, -1.0, 0.0, 0.0, 42),
+        (4096, 0.97, 0.15, float("inf"), 0.0, 0.0, 42),
+        (4096, 0.97, 0.15, -1.0, 0.0, -1.0, 42),
+    ]
+    for args in bad:
+        assert not lib.gpu_bpf_create(*args)
+        assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_ARG
+    assert not lib.gpu_bpf_create(4096, 0.97, 0.15, -1.0, 5.0, 0.0, 42)
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_UNSUPPORTED
+
+
+def test_valid_create_without_gpu_fails_loudly(lib):
+    from gpubpf import _lib
+    s = lib.gpu_bpf_create(4096, 0.97, 0.15, -1.0, 0.0, 0.0, 42)
+    if s:            # a GPU is present: the create must have worked
+        lib.gpu_bpf_destroy(s)
+        pytest.skip("GPU present")
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_NODEVICE
+
+
+def test_null_state_calls_are_safe(lib):
+    from gpubpf import _lib
+    lib.gpu_bpf_destroy(None)
+    r = lib.gpu_bpf_step(None, 0.1)
+    assert r.h_mean != r.h_mean           # NaN
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_STATE
+    assert lib.gpu_bpf_get_resample_count(None) == -1
+
+
+def test_bands_only_identity(lib):
+    from gpubpf import _lib
+    one = (C.c_float * 1)(1.0)
+    lib.gpu_bpf_set_bands(4096, 1, one, one)
+    assert lib.gpu_bpf_last_error() == _lib.BPF_OK
+    two = (C.c_float * 2)(0.5, 0.5)
+    sc = (C.c_float * 2)(1.0, 3.0)
+    lib.gpu_bpf_set_bands(4096, 2, two, sc)
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_UNSUPPORTED
+
+
+def test_error_strings(lib):
+    for code in range(8):
+        assert lib.gpu_bpf_error_string(code)
