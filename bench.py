@@ -216,7 +216,10 @@ def main():
         one_run(2000 + w)
     barrier()
     props = torch.cuda.get_device_properties(dev)
-    clk = ClockSampler(str(getattr(props, "uuid", local)) if getattr(props, "uuid", None) else str(local))
+    gpu_id = str(getattr(props, "uuid", "") or "")
+    if gpu_id and not gpu_id.startswith("GPU-"):
+        gpu_id = "GPU-" + gpu_id
+    clk = ClockSampler(gpu_id or str(local))
     launches0 = lib.gpu_bpf_launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -242,7 +245,8 @@ def main():
     f.profile(True)
     f.reset(3000)
     f.step_many_device(y_dev.data_ptr(), T, rec_dev.data_ptr())
-    p1_ms, p2_ms, n1, n2 = f.profile_read()
+    p1_ms, plan_ms, p2_ms, n1 = f.profile_read()
+    n2 = n1
     f.profile(False)
     rec = np.frombuffer(rec_dev.cpu().numpy().tobytes(), dtype=np.int32).reshape(T, RECORD_BYTES // 4)[:, 8]
     carry = np.zeros(T, dtype=np.int64)
@@ -264,8 +268,9 @@ def main():
         "avg_launch_us": tms / max(1, nl) * 1e3,
         "pass1": {"ms": p1_ms, "launches": n1, "GBps": ach1, "frac": ach1 / peak},
         "pass2": {"ms": p2_ms, "launches": n2, "GBps": ach2, "frac": ach2 / peak},
-        "tick": {"GBps": (bytes_p1 + bytes_p2) / ((p1_ms + p2_ms) / 1e3) / 1e9,
-                 "frac": (bytes_p1 + bytes_p2) / ((p1_ms + p2_ms) / 1e3) / 1e9 / peak},
+        "plan": {"ms": plan_ms, "launches": n1, "us_per_launch": plan_ms / max(1, n1) * 1e3},
+        "tick": {"GBps": (bytes_p1 + bytes_p2) / ((p1_ms + plan_ms + p2_ms) / 1e3) / 1e9,
+                 "frac": (bytes_p1 + bytes_p2) / ((p1_ms + plan_ms + p2_ms) / 1e3) / 1e9 / peak},
         "bytes_model": "pass1 12 B/particle (+4 carried weight on ticks after a skipped resample); "
                        "pass2 12 B/particle on resampling ticks",
     }

@@ -70,11 +70,14 @@ struct Impl {
   float dg_mu = NAN, dg_rho = NAN, dg_sigma = NAN, dg_thr = NAN;
   bool dg_anc = false;
 
+  // programmatic dependent launch between consecutive kernels (off while profiling)
+  bool pdl = true;
+
   // profiling
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
-  std::vector<cudaEvent_t> ev_pending;   // triples (before p1, between, after p2)
-  double prof_p1_ms = 0.0, prof_p2_ms = 0.0;
+  std::vector<cudaEvent_t> ev_pending;   // quadruples: before pass 1, after pass 1, after plan, after pass 2
+  double prof_p1_ms = 0.0, prof_plan_ms = 0.0, prof_p2_ms = 0.0;
   int prof_n1 = 0, prof_n2 = 0;
 
   ObsModel obs{};
@@ -89,10 +92,18 @@ int ensure_device(Impl* m) {
   return BPF_OK;
 }
 
+cudaError_t launch_tick3(Impl* m, const TickArgs& a) {
+  cudaError_t e = launch_pass1(m->plan, a, m->stream, m->pdl);
+  if (e == cudaSuccess) e = launch_plan(m->plan, a, m->stream, m->pdl);
+  if (e == cudaSuccess) e = launch_pass2(m->plan, a, m->pass2_grid, m->stream, m->pdl);
+  return e;
+}
+
 TickArgs make_args(GpuBpfState* s, Impl* m, float y, const float* y_ptr, BpfTickRecord* rec) {
   TickArgs a;
   a.mu = s->mu; a.rho = s->rho; a.sigma = s->sigma_z;
   a.ess_threshold = s->ess_threshold;
+  a.log_n = std::log((double)m->plan.N);
   a.obs = m->obs;
   a.obs.y = y;
   a.y_ptr = y_ptr;
@@ -117,12 +128,13 @@ cudaEvent_t take_event(Impl* m) {
 }
 
 int drain_profile(Impl* m) {
-  for (size_t i = 0; i + 2 < m->ev_pending.size(); i += 3) {
-    float a = 0.f, b = 0.f;
-    CK(cudaEventSynchronize(m->ev_pending[i + 2]));
+  for (size_t i = 0; i + 3 < m->ev_pending.size(); i += 4) {
+    float a = 0.f, b = 0.f, c = 0.f;
+    CK(cudaEventSynchronize(m->ev_pending[i + 3]));
     CK(cudaEventElapsedTime(&a, m->ev_pending[i], m->ev_pending[i + 1]));
     CK(cudaEventElapsedTime(&b, m->ev_pending[i + 1], m->ev_pending[i + 2]));
-    m->prof_p1_ms += a; m->prof_p2_ms += b;
+    CK(cudaEventElapsedTime(&c, m->ev_pending[i + 2], m->ev_pending[i + 3]));
+    m->prof_p1_ms += a; m->prof_plan_ms += b; m->prof_p2_ms += c;
     m->prof_n1 += 1; m->prof_n2 += 1;
   }
   for (cudaEvent_t e : m->ev_pending) m->ev_pool.push_back(e);
@@ -130,22 +142,23 @@ int drain_profile(Impl* m) {
   return BPF_OK;
 }
 
-// Enqueue one tick (pass 1 + pass 2) on the filter's stream.
+// Enqueue one tick (pass 1, plan, pass 2) on the filter's stream.
 int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
-  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
   if (m->profiling) {
-    e0 = take_event(m); e1 = take_event(m); e2 = take_event(m);
-    CK(cudaEventRecord(e0, m->stream));
+    cudaEvent_t ev[4] = {take_event(m), take_event(m), take_event(m), take_event(m)};
+    CK(cudaEventRecord(ev[0], m->stream));
+    CK(launch_pass1(m->plan, a, m->stream, false));
+    CK(cudaEventRecord(ev[1], m->stream));
+    CK(launch_plan(m->plan, a, m->stream, false));
+    CK(cudaEventRecord(ev[2], m->stream));
+    CK(launch_pass2(m->plan, a, m->pass2_grid, m->stream, false));
+    CK(cudaEventRecord(ev[3], m->stream));
+    for (cudaEvent_t e : ev) m->ev_pending.push_back(e);
+    if (m->ev_pending.size() >= 4 * 4096) { int rc = drain_profile(m); if (rc) return rc; }
+  } else {
+    CK(launch_tick3(m, a));
   }
-  CK(launch_pass1(m->plan, a, m->stream));
-  if (m->profiling) CK(cudaEventRecord(e1, m->stream));
-  CK(launch_pass2(m->plan, a, m->pass2_grid, m->stream));
-  if (m->profiling) {
-    CK(cudaEventRecord(e2, m->stream));
-    m->ev_pending.push_back(e0); m->ev_pending.push_back(e1); m->ev_pending.push_back(e2);
-    if (m->ev_pending.size() >= 3 * 4096) { int rc = drain_profile(m); if (rc) return rc; }
-  }
-  g_launches += 2;
+  g_launches += 3;
   m->ticks_enqueued += 1;
   return BPF_OK;
 }
@@ -178,7 +191,7 @@ int free_impl(Impl* m) {
   for (cudaEvent_t e : m->ev_pool) cudaEventDestroy(e);
   Plan& p = m->plan;
   cudaFree(p.h0); cudaFree(p.h1); cudaFree(p.w);
-  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.S); cudaFree(p.Q); cudaFree(p.H);
+  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.rec);
   cudaFree(p.P); cudaFree(p.ofirst); cudaFree(p.items); cudaFree(p.st);
   cudaFree(m->rec_dev); cudaFree(m->y_dev); cudaFree(m->anc_dev);
   cudaFreeHost(m->rec_pin); cudaFreeHost(m->st_pin); cudaFreeHost(m->y_pin);
@@ -194,8 +207,7 @@ int build_graph(GpuBpfState* s, Impl* m) {
   cudaError_t err = cudaMemcpyAsync(m->y_dev, m->y_pin, kGraphChunk * sizeof(float), cudaMemcpyHostToDevice, m->stream);
   for (int k = 0; k < kGraphChunk && err == cudaSuccess; ++k) {
     TickArgs a = make_args(s, m, 0.0f, m->y_dev + k, m->rec_dev + 1 + k);
-    err = launch_pass1(m->plan, a, m->stream);
-    if (err == cudaSuccess) err = launch_pass2(m->plan, a, m->pass2_grid, m->stream);
+    err = launch_tick3(m, a);
   }
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(m->rec_pin + 1, m->rec_dev + 1, kGraphChunk * sizeof(BpfTickRecord), cudaMemcpyDeviceToHost, m->stream);
@@ -218,8 +230,7 @@ int build_device_graph(GpuBpfState* s, Impl* m, const float* y_dev, int n, BpfTi
   cudaError_t err = cudaSuccess;
   for (int k = 0; k < n && err == cudaSuccess; ++k) {
     TickArgs a = make_args(s, m, 0.0f, y_dev + k, rec_dev + k);
-    err = launch_pass1(m->plan, a, m->stream);
-    if (err == cudaSuccess) err = launch_pass2(m->plan, a, m->pass2_grid, m->stream);
+    err = launch_tick3(m, a);
   }
   cudaError_t e2 = cudaStreamEndCapture(m->stream, &g);
   if (err != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return set_err(BPF_ERR_CUDA); }
@@ -278,9 +289,7 @@ static int create_impl(GpuBpfState* s, Impl* m, int n, float rho, float sigma_z,
   CK(cudaMalloc(&p.w, npad * sizeof(float)));
   CK(cudaMalloc(&p.nexp, p.G * sizeof(int)));
   CK(cudaMalloc(&p.E, p.G * sizeof(unsigned long long)));
-  CK(cudaMalloc(&p.S, p.G * sizeof(double)));
-  CK(cudaMalloc(&p.Q, p.G * sizeof(double)));
-  CK(cudaMalloc(&p.H, p.G * sizeof(double)));
+  CK(cudaMalloc(&p.rec, p.G * sizeof(float4)));
   CK(cudaMalloc(&p.P, p.G * sizeof(unsigned long long)));
   CK(cudaMalloc(&p.ofirst, (p.G + 1) * sizeof(int)));
   CK(cudaMalloc(&p.items, p.max_items * sizeof(int4)));
@@ -293,6 +302,7 @@ static int create_impl(GpuBpfState* s, Impl* m, int n, float rho, float sigma_z,
   CK(cudaMemsetAsync(p.nexp, 0, p.G * sizeof(int), m->stream));
   CK(cudaMemsetAsync(m->rec_dev, 0, (1 + kGraphChunk) * sizeof(BpfTickRecord), m->stream));
   m->pass2_grid = pass2_grid_size(m->device);
+  if (const char* v = std::getenv("BPF_DISABLE_PDL")) m->pdl = (v[0] == '0');
 
   // observation model (gpu_bpf_ptx_full.cu:406-412)
   m->obs.nu = nu_obs;
@@ -461,7 +471,7 @@ int gpu_bpf_step_many(GpuBpfState* s, const float* y, int n_ticks, BpfResult* ou
       std::memcpy(m->y_pin, y + t, kGraphChunk * sizeof(float));
       CK(cudaGraphLaunch(m->graph, m->stream));
       CK(cudaStreamSynchronize(m->stream));
-      g_launches += 2 * kGraphChunk;
+      g_launches += 3 * kGraphChunk;
       m->ticks_enqueued += kGraphChunk;
       for (int k = 0; k < kGraphChunk; ++k) {
         if (out) out[t + k] = to_result(m, m->rec_pin[1 + k]);
@@ -515,7 +525,7 @@ int gpu_bpf_step_many_device(GpuBpfState* s, const float* y_dev, int n_ticks, Bp
                        m->dg_thr != s->ess_threshold || m->dg_anc != m->record_anc;
     if (stale) { rc = build_device_graph(s, m, y_dev, n_ticks, rec_dev); if (rc) return rc; }
     CK(cudaGraphLaunch(m->dgraph, m->stream));
-    g_launches += 2LL * n_ticks;
+    g_launches += 3LL * n_ticks;
     m->ticks_enqueued += n_ticks;
   } else {
     for (int t = 0; t < n_ticks; ++t) {
@@ -635,12 +645,12 @@ int gpu_bpf_profile(GpuBpfState* s, int enable) {
   rc = drain_profile(m);
   if (rc) return rc;
   m->profiling = enable != 0;
-  m->prof_p1_ms = m->prof_p2_ms = 0.0;
+  m->prof_p1_ms = m->prof_plan_ms = m->prof_p2_ms = 0.0;
   m->prof_n1 = m->prof_n2 = 0;
   return BPF_OK;
 }
 
-int gpu_bpf_profile_read(GpuBpfState* s, double* p1, double* p2, int* n1, int* n2) {
+int gpu_bpf_profile_read(GpuBpfState* s, double* p1, double* plan, double* p2, int* n1, int* n2) {
   Impl* m = impl_of(s);
   if (!m) return set_err(BPF_ERR_STATE);
   int rc = ensure_device(m);
@@ -648,6 +658,7 @@ int gpu_bpf_profile_read(GpuBpfState* s, double* p1, double* p2, int* n1, int* n
   rc = drain_profile(m);
   if (rc) return rc;
   if (p1) *p1 = m->prof_p1_ms;
+  if (plan) *plan = m->prof_plan_ms;
   if (p2) *p2 = m->prof_p2_ms;
   if (n1) *n1 = m->prof_n1;
   if (n2) *n2 = m->prof_n2;

@@ -25,7 +25,9 @@ namespace bpf {
 constexpr int kThreads   = 256;              // threads per CTA (pass 1 and pass 2)
 constexpr int kPerThread = 16;               // particles per thread
 constexpr int kTile      = kThreads * kPerThread;   // 4096 particles per tile
-constexpr int kOutChunk  = 4096;             // outputs per pass-2 work item
+constexpr int kOutChunk  = 3 * kTile;        // outputs per pass-2 work item (3x the mean per tile)
+constexpr int kPlanThreads = 512;            // threads of the single-CTA plan kernel
+constexpr int kPlanSmemTiles = 12800;        // tiles the plan kernel stages in shared memory (N <= 52.4M)
 constexpr int kFixF      = 50;               // tile-frame fraction bits: 62 - log2(kTile)
 constexpr int kNkEmpty   = -(1 << 30);       // tile exponent of a tile with no mass
 
@@ -63,9 +65,11 @@ __host__ __device__ inline PcgTick pcg_tick_consts(int seed, uint64_t At, uint64
 }
 __host__ __device__ inline uint64_t pcg_inc(uint32_t i) { return (uint64_t)(uint32_t)(2u * i + 1u); }
 
-// u in (0,1): (out >> 9) * 2^-23, clamped like the reference (PTX :159-164)
+// u in (0,1): (out >> 9) * 2^-23, clamped like the reference (PTX :159-164).
+// Formed from the float bit pattern 1.m - 1 (exact) instead of an int->float
+// conversion.
 __device__ __forceinline__ float pcg_uniform(uint32_t out) {
-  float u = __uint2float_rn(out >> 9) * 1.1920928955078125e-07f;
+  float u = __uint_as_float(0x3F800000u | (out >> 9)) - 1.0f;
   u = fmaxf(u, uclamp_lo());
   u = fminf(u, uclamp_hi());
   return u;
@@ -91,37 +95,46 @@ constexpr float kLog2e = 1.44269504088896340736f;
 constexpr float kLn2   = 0.693147180559945309417f;
 
 // ---------------------------------------------------------------------------
-// Inverse normal CDF. The reference evaluates P. J. Acklam's rational
-// approximation in FP32 (PTX :166-205); in FP32 its central rational loses
-// about three digits to cancellation near |u-1/2| = 0.47 (absolute error up to
-// 2.7e-4 in z). This build evaluates M. J. Wichura's algorithm AS 241 (PPND7,
-// Applied Statistics 37, 1988), designed for single precision: positive
-// coefficients in the central branch, absolute error below ~1.1e-6 over the
-// clamped uniform range. Coefficients are Wichura's published ones. The
-// uniform clamp keeps u in [1e-6, 0.99994], so the far-tail branch of AS 241
-// (sqrt(-ln p) > 5) is never reached.
+// Inverse normal CDF, z = sqrt(2) * erfinv(2u - 1), by M. Giles' single-
+// precision erfinv approximation ("Approximating the erfinv function", GPU
+// Computing Gems Jade Edition, 2011; published coefficients). The argument
+// w = -ln(1 - x^2) is formed as -ln(4u(1-u)) straight from u, so there is no
+// cancellation near the clamped ends. Absolute error in z is below 1e-6 over
+// the whole clamped range [1e-6, 0.99994]; the common branch (w < 5, i.e.
+// 0.0017 < u < 0.9983) costs one MUFU lg2 and nine FMAs with no division.
+// The reference evaluates P. J. Acklam's rational approximation in FP32 (PTX
+// :166-205), whose central rational cancels to ~3e-4 absolute error near
+// |u-1/2| = 0.47; the uniform clamp and PCG32 draw are kept bit-for-bit.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float icdf_normal(float u) {
-  const float q = u - 0.5f;
-  if (fabsf(q) <= 0.425f) {
-    const float r = 0.180625f - q * q;
-    float num = fmaf(5.9109374720e+01f, r, 1.5929113202e+02f);
-    num = fmaf(num, r, 5.0434271938e+01f);
-    num = fmaf(num, r, 3.3871327179e+00f);
-    float den = fmaf(6.7187563600e+01f, r, 7.8757757664e+01f);
-    den = fmaf(den, r, 1.7895169469e+01f);
-    den = fmaf(den, r, 1.0f);
-    return div_approx(q * num, den);
+  const float t = u * (1.0f - u);
+  const float l2 = lg2_approx(t);                                       // log2(u(1-u))
+  const float xs = fmaf(2.82842712474619010f, u, -1.41421356237309505f);  // sqrt2 * (2u - 1)
+  float p;
+  if (l2 > -9.21347810f) {   // w = -ln(4u(1-u)) < 5  <=>  log2(u(1-u)) > -5/ln2 - 2
+    const float w = fmaf(-kLn2, l2, -2.0f * kLn2 - 2.5f);              // w - 2.5
+    p = 2.81022636e-08f;
+    p = fmaf(p, w, 3.43273939e-07f);
+    p = fmaf(p, w, -3.5233877e-06f);
+    p = fmaf(p, w, -4.39150654e-06f);
+    p = fmaf(p, w, 0.00021858087f);
+    p = fmaf(p, w, -0.00125372503f);
+    p = fmaf(p, w, -0.00417768164f);
+    p = fmaf(p, w, 0.246640727f);
+    p = fmaf(p, w, 1.50140941f);
+  } else {
+    const float w = sqrt_approx(fmaf(-kLn2, l2, -2.0f * kLn2)) - 3.0f;
+    p = -0.000200214257f;
+    p = fmaf(p, w, 0.000100950558f);
+    p = fmaf(p, w, 0.00134934322f);
+    p = fmaf(p, w, -0.00367342844f);
+    p = fmaf(p, w, 0.00573950773f);
+    p = fmaf(p, w, -0.0076224613f);
+    p = fmaf(p, w, 0.00943887047f);
+    p = fmaf(p, w, 1.00167406f);
+    p = fmaf(p, w, 2.83297682f);
   }
-  const float p = (q < 0.0f) ? u : 1.0f - u;
-  const float r = sqrt_approx(-kLn2 * lg2_approx(p)) - 1.6f;
-  float num = fmaf(1.7023821103e-01f, r, 1.3067284816e+00f);
-  num = fmaf(num, r, 2.7568153900e+00f);
-  num = fmaf(num, r, 1.4234372777e+00f);
-  float den = fmaf(1.2021132975e-01f, r, 7.3700164250e-01f);
-  den = fmaf(den, r, 1.0f);
-  const float z = div_approx(num, den);
-  return (q < 0.0f) ? -z : z;
+  return p * xs;
 }
 
 // ---------------------------------------------------------------------------
@@ -136,6 +149,14 @@ struct ObsModel {
   float inv_nu;     // 1/nu
   float nu_p1h;     // (nu+1)/2
 };
+
+// log2 p(y | h) for the Gaussian model with y2 = y^2:
+//   -log2(e)/2 * (y^2 e^{-h} + h) - log2(e) ln(2 pi)/2
+__device__ __forceinline__ float obs_log2pdf_gauss(float y2, float h) {
+  const float e = ex2_approx(h * -kLog2e);                       // e^{-h}
+  const float s = (y2 > 0.0f) ? fmaf(y2, e, h) : h;
+  return fmaf(-0.5f * kLog2e, s, -1.32574806473616f);           // -log2(e) ln(2 pi)/2
+}
 
 __device__ __forceinline__ float obs_logpdf(const ObsModel& m, float h) {
   const float e = ex2_approx(h * -0.5f * kLog2e);   // exp(-h/2)
@@ -166,8 +187,21 @@ __device__ __forceinline__ uint64_t fix_weight(float w) {
   return __float2ull_rz(w * 1125899906842624.0f);   // 2^50
 }
 
-// Unsigned 64-bit floor division by a constant d, through the reciprocal
-// m = floor((2^64-1)/d) and an exact remainder correction.
+// floor(a / b) for 1 <= b and a < 2^62: FP64 estimate, exact integer correction.
+__device__ __forceinline__ uint64_t udiv_fp64(uint64_t a, uint64_t b) {
+  uint64_t q = __double2ull_rz((double)a / (double)b);
+  while (q > 0ull && q * b > a) --q;
+  while (a - q * b >= b) ++q;
+  return q;
+}
+// Reciprocal for udiv_magic: m <= floor((2^64-1)/d) with a relative deficit
+// below 2^-48, so the quotient estimate is short by at most 3 for a/d < 2^31.
+__device__ __forceinline__ uint64_t udiv_magic_of(uint64_t d) {
+  return __double2ull_rz(18446744073709551615.0 / (double)d * (1.0 - 0x1p-49));
+}
+
+// Unsigned 64-bit floor division by a constant d, through a reciprocal
+// m <= floor((2^64-1)/d) and an exact remainder correction.
 __device__ __forceinline__ uint64_t udiv_magic(uint64_t a, uint64_t d, uint64_t m) {
   uint64_t q = __umul64hi(a, m);
   uint64_t r = a - q * d;

@@ -1,21 +1,30 @@
-// bpf_plain.cu — the plain SV bootstrap-filter tick as two sm_100a kernels.
+// bpf_plain.cu — the plain SV bootstrap-filter tick as three sm_100a kernels.
 //
-//   pass 1  (one CTA per 4096-particle tile)
-//           counter-PCG32 -> AS241 normal -> OU propagate -> log-weight
-//           (+ carried weight on ESS-skipped ticks), tile max as a power-of-two
-//           exponent n_k, tile-relative weights w = 2^(x - n_k) written once,
-//           tile partial sums S=sum w, Q=sum w^2, H=sum w h (FP64) and the exact
-//           fixed-point tile mass E = sum floor(w 2^50).
-//           The last CTA to finish (atomic ticket) combines the tiles in FP64:
+//   pass 1  (one CTA per 4096-particle tile, streaming)
+//           counter-PCG32 -> inverse-CDF normal -> OU propagate -> log2-weight
+//           (+ carried weight on ESS-skipped ticks). The tile max becomes a
+//           power-of-two exponent n_k; tile-relative weights w = 2^(x - n_k)
+//           are written once, with the tile partials S=sum w, Q=sum w^2,
+//           H=sum w h and the exact fixed-point tile mass E = sum floor(w 2^50).
+//   plan    (one CTA of 512 threads)
+//           FP64 combine of the tile partials in the global frame 2^nM:
 //           log-likelihood increment, ESS, filtered mean, the resampling
-//           decision, and — on resampling ticks — the fixed-point CDF tile
-//           prefixes and the pass-2 work list. No host synchronisation.
-//   pass 2  (persistent CTAs over work items)
+//           decision and the next tick's device state; on resampling ticks
+//           also the fixed-point CDF (tile prefixes, total, target spacing)
+//           and the pass-2 work list. No host synchronisation per tick.
+//   pass 2  (persistent CTAs over work items: one tile, a run of outputs)
 //           systematic resampling: exact integer prefix of the tile weights,
-//           merge-path match of the N evenly spaced targets against the CDF,
-//           gather of h[ancestor] through shared memory, coalesced store.
+//           each element writes its index into the output slots of the
+//           evenly spaced targets it owns (heavy elements filled by their
+//           whole warp), gather of h[ancestor] from a bulk-async
+//           (TMA) copy of the tile, coalesced store. Tiles of the next item
+//           are prefetched into a second buffer. Early exit on ticks that do
+//           not resample.
+// Consecutive kernels use programmatic dependent launch: each waits on its
+// predecessor with griddepcontrol.wait and releases its successor after its
+// last store, so launch latency overlaps the predecessor's tail.
 //
-// Reference tick this replaces: gpu_bpf/gpu_bpf_ptx_full.cu:550-748 (≈15
+// Reference tick this replaces: gpu_bpf/gpu_bpf_ptx_full.cu:550-748 (~15
 // launches, float atomics, a host sync for ESS, thrust scan) with kernels
 // ptx_assembly/bpf_kernels_full.ptx:231-842.
 #include "bpf_plain.cuh"
@@ -24,7 +33,55 @@
 namespace bpf {
 
 // ---------------------------------------------------------------------------
-// Small reduction / scan helpers (256-thread CTAs)
+// PTX helpers: dependent launch, mbarrier, bulk async copy, timer
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// 1-D bulk copy global -> shared, completion counted on the mbarrier.
+// Both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ uint64_t global_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for phase `parity` of the mbarrier; gives up after ~1 s and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  const uint64_t t0 = global_timer_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (global_timer_ns() - t0 > 1000000000ull) return false;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Block-wide reductions and scans for NT threads (NT a multiple of 32)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float warp_max_f(float v) {
 #pragma unroll
@@ -46,61 +103,48 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-__device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long long v, int lane) {
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan_add(T v, int lane) {
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const unsigned long long n = __shfl_up_sync(0xffffffffu, v, o);
+    const T n = __shfl_up_sync(0xffffffffu, v, o);
     if (lane >= o) v += n;
   }
   return v;
 }
-__device__ __forceinline__ int warp_incl_scan_i(int v, int lane) {
+// Exclusive prefix sum over the NT threads of a CTA; *total gets the sum.
+// sh holds NT/32 + 1 entries. All threads must call it (it has barriers).
+template <int NT, typename T>
+__device__ T block_excl_scan_add(T v, T* total, T* sh) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T inc = warp_incl_scan_add(v, lane);
+  if (lane == 31) sh[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const T t = lane < W ? sh[lane] : T(0);
+    const T ti = warp_incl_scan_add(t, lane);
+    __syncwarp();
+    if (lane < W) sh[lane] = ti - t;
+    if (lane == W - 1) sh[W] = ti;
+  }
+  __syncthreads();
+  const T r = sh[warp] + inc - v;
+  *total = sh[W];
+  __syncthreads();
+  return r;
+}
+template <int NT>
+__device__ int block_max_i(int v, int* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_max_i(v);
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  int m = sh[0];
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int n = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += n;
-  }
-  return v;
-}
-
-// Exclusive scan over the 256 threads of a CTA; *total receives the sum.
-// sh must hold 9 entries. Contains barriers: call from all threads.
-__device__ unsigned long long block_excl_scan_u64(unsigned long long v, unsigned long long* total,
-                                                  unsigned long long* sh) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned long long inc = warp_incl_scan_u64(v, lane);
-  if (lane == 31) sh[warp] = inc;
+  for (int w = 1; w < NT / 32; ++w) m = max(m, sh[w]);
   __syncthreads();
-  if (warp == 0) {
-    const unsigned long long t = lane < kThreads / 32 ? sh[lane] : 0ull;
-    const unsigned long long ti = warp_incl_scan_u64(t, lane);
-    __syncwarp();
-    if (lane < kThreads / 32) sh[lane] = ti - t;
-    if (lane == kThreads / 32 - 1) sh[kThreads / 32] = ti;
-  }
-  __syncthreads();
-  const unsigned long long r = sh[warp] + inc - v;
-  *total = sh[kThreads / 32];
-  __syncthreads();
-  return r;
-}
-__device__ int block_excl_scan_i(int v, int* total, int* sh) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int inc = warp_incl_scan_i(v, lane);
-  if (lane == 31) sh[warp] = inc;
-  __syncthreads();
-  if (warp == 0) {
-    const int t = lane < kThreads / 32 ? sh[lane] : 0;
-    const int ti = warp_incl_scan_i(t, lane);
-    __syncwarp();
-    if (lane < kThreads / 32) sh[lane] = ti - t;
-    if (lane == kThreads / 32 - 1) sh[kThreads / 32] = ti;
-  }
-  __syncthreads();
-  const int r = sh[warp] + inc - v;
-  *total = sh[kThreads / 32];
-  __syncthreads();
-  return r;
+  return m;
 }
 
 // 2^e as a double (exact IEEE encoding; 0 below the normal range).
@@ -118,8 +162,17 @@ __host__ __device__ inline int ceil_log2_u(unsigned n) {
   return c;
 }
 
+// #{ i in [0,N) : base + i*delta < c } (targets strictly below c)
+__device__ __forceinline__ int targets_below(unsigned long long c, unsigned long long base,
+                                             unsigned long long delta, unsigned long long magic, int N) {
+  if (c <= base) return 0;
+  const unsigned long long q = udiv_magic(c - base - 1ull, delta, magic) + 1ull;
+  return q >= (unsigned long long)N ? N : (int)q;
+}
+
 // ---------------------------------------------------------------------------
-// Init: h_0 = mu + std_stat * z(draw 0)   (bpf_kernels_full.ptx:103-218)
+// Init: h_0 = mu + std_stat * z(draw 0)  (bpf_kernels_full.ptx:103-218);
+// thread 0 also (re)initialises the device state.
 // ---------------------------------------------------------------------------
 __global__ void init_kernel(Plan p, float mu, float std_stat, int seed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,195 +199,31 @@ __global__ void init_kernel(Plan p, float mu, float std_stat, int seed) {
   p.w[i] = 0.0f;
 }
 
-// ---------------------------------------------------------------------------
-// Pass-1 epilogue: run by all 256 threads of the last CTA to finish.
-// ---------------------------------------------------------------------------
-struct EpiShared {
-  unsigned long long scan_u[kThreads / 32 + 1];
-  int scan_i[kThreads / 32 + 1];
-  double red[3][kThreads / 32];
-  int red_i[kThreads / 32];
-  unsigned long long b_base, b_delta, b_magic, b_total;
-  int b_resample, b_nM, b_Fg;
-};
-
-__device__ __forceinline__ int first_target_at_or_above(unsigned long long c, unsigned long long base,
-                                                        unsigned long long delta, unsigned long long magic,
-                                                        int N) {
-  // #{ i in [0,N) : base + i*delta < c }
-  if (c <= base) return 0;
-  const unsigned long long q = udiv_magic(c - base - 1ull, delta, magic) + 1ull;
-  return q >= (unsigned long long)N ? N : (int)q;
-}
-
-__device__ void pass1_epilogue(const Plan& p, const TickArgs& a, int tick, int cur, EpiShared& sh) {
-  DevState* st = p.st;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int G = p.G, N = p.N;
-
-  // 1. global tile exponent
-  int nM = kNkEmpty;
-  for (int k = tid; k < G; k += kThreads) nM = max(nM, __ldcg(p.nexp + k));
-  nM = warp_max_i(nM);
-  if (lane == 0) sh.red_i[warp] = nM;
-  __syncthreads();
-  nM = sh.red_i[0];
-#pragma unroll
-  for (int w = 1; w < kThreads / 32; ++w) nM = max(nM, sh.red_i[w]);
-
-  // 2. FP64 combine of the tile partials, rescaled to the global frame 2^nM
-  double S = 0.0, Q = 0.0, H = 0.0;
-  if (nM != kNkEmpty) {
-    for (int k = tid; k < G; k += kThreads) {
-      const int nk = __ldcg(p.nexp + k);
-      if (nk == kNkEmpty) continue;
-      const double sc = pow2d(nk - nM);
-      S += __ldcg(p.S + k) * sc;
-      Q += __ldcg(p.Q + k) * (sc * sc);
-      H += __ldcg(p.H + k) * sc;
-    }
-  }
-  S = warp_sum_d(S); Q = warp_sum_d(Q); H = warp_sum_d(H);
-  if (lane == 0) { sh.red[0][warp] = S; sh.red[1][warp] = Q; sh.red[2][warp] = H; }
-  __syncthreads();
-
-  // 3. tick statistics and the resampling decision (thread 0)
-  if (tid == 0) {
-    S = 0.0; Q = 0.0; H = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) { S += sh.red[0][w]; Q += sh.red[1][w]; H += sh.red[2][w]; }
-    const bool degenerate = (nM == kNkEmpty) || !(S > 0.0);
-    const double ln2 = 0.693147180559945309417232121458;
-    double dll, ess, hm;
-    int resample = 0;
-    if (degenerate) {
-      dll = -INFINITY; ess = 0.0; hm = nan("");
-      st->error = BPF_ERR_DEGENERATE;
-    } else {
-      const double lse = (double)nM * ln2 + log(S);
-      dll = lse - st->logS_prev;
-      ess = S * S / Q;
-      hm = H / S;
-      resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
-    }
-    const double ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
-    st->ll_ref = ll_ref;
-    st->ll_total += dll;
-    if (a.rec) {
-      BpfTickRecord r;
-      r.dloglik = dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
-      r.h_mean = (float)hm; r.ess = (float)ess; r.resampled = resample; r.tick = tick;
-      *a.rec = r;
-    }
-    // next tick's PCG constants
-    st->At = st->At * kPcgMult;
-    st->Bt = st->Bt * kPcgMult + 1ull;
-    st->tick = tick + 1;
-    st->do_resample = resample;
-    if (resample) {
-      const uint64_t old = st->u_state;
-      st->u_state = old * kPcgMult + kHostInc;
-      st->u23 = pcg_output(old) >> 9;
-      st->logS_prev = log((double)N);
-      st->resampled_prev = 1;
-      st->resample_count += 1;
-      st->src = cur;
-      st->cur = cur ^ 1;
-    } else if (degenerate) {
-      st->logS_prev = log((double)N);   // restart from uniform weights
-      st->resampled_prev = 1;
-    } else {
-      st->logS_prev = log(S);
-      st->resampled_prev = 0;
-      st->nM_prev = nM;
-    }
-    sh.b_resample = resample;
-    sh.b_nM = nM;
-    sh.b_Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
-  }
-  __syncthreads();
-  if (!sh.b_resample) {
-    if (tid == 0) st->ticket = 0u;
-    return;
-  }
-
-  // 4. fixed-point CDF: tile masses in the global frame, prefix, total
-  const int Fg = sh.b_Fg;
-  const int C = (G + kThreads - 1) / kThreads;
-  const int k0 = min(tid * C, G), k1 = min(k0 + C, G);
-  auto ehat = [&](int k) -> unsigned long long {
-    const int nk = __ldcg(p.nexp + k);
-    if (nk == kNkEmpty) return 0ull;
-    return shr64(__ldcg(p.E + k), nM - nk + kFixF - Fg);
-  };
-  unsigned long long part = 0;
-  for (int k = k0; k < k1; ++k) part += ehat(k);
-  unsigned long long total;
-  const unsigned long long excl = block_excl_scan_u64(part, &total, sh.scan_u);
-  if (tid == 0) {
-    unsigned long long delta = total / (unsigned long long)N;
-    if (delta == 0ull) { delta = 1ull; st->error = BPF_ERR_DEGENERATE; }
-    const unsigned long long u = st->u23;
-    const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
-    sh.b_base = (hi << 41) | (lo >> 23);          // floor(u * delta / 2^23)
-    sh.b_delta = delta;
-    sh.b_magic = ~0ull / delta;
-    sh.b_total = total;
-  }
-  __syncthreads();
-  const unsigned long long base = sh.b_base, delta = sh.b_delta, magic = sh.b_magic;
-
-  // 5. per-tile prefix, first output index, number of work items
-  unsigned long long run = excl;
-  int o_prev = first_target_at_or_above(run, base, delta, magic, N);
-  int n_it = 0;
-  for (int k = k0; k < k1; ++k) {
-    p.P[k] = run;
-    p.ofirst[k] = o_prev;
-    run += ehat(k);
-    const int o_next = first_target_at_or_above(run, base, delta, magic, N);
-    n_it += (o_next - o_prev + kOutChunk - 1) / kOutChunk;
-    o_prev = o_next;
-  }
-  if (tid == 0) p.ofirst[G] = N;
-  int n_items_total;
-  const int it0 = block_excl_scan_i(n_it, &n_items_total, sh.scan_i);   // barrier: ofirst visible
-
-  // 6. emit work items (tile, first output, end output)
-  int ib = it0;
-  for (int k = k0; k < k1; ++k) {
-    const int o0 = p.ofirst[k], o1 = p.ofirst[k + 1];
-    for (int o = o0; o < o1; o += kOutChunk) p.items[ib++] = make_int4(k, o, min(o1, o + kOutChunk), 0);
-  }
-  if (tid == 0) {
-    st->n_items = n_items_total;
-    st->base = base; st->delta = delta; st->delta_magic = magic; st->total = sh.b_total;
-    st->nM = nM; st->Fg = Fg;
-    st->ticket = 0u;
-  }
-}
+constexpr int kStWords = (int)(sizeof(DevState) / 8);
 
 // ---------------------------------------------------------------------------
 // Pass 1
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 3) pass1_kernel(Plan p, TickArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
   __shared__ float s_max[kThreads / 32];
   __shared__ double s_red[3][kThreads / 32];
   __shared__ unsigned long long s_redE[kThreads / 32];
-  __shared__ int s_last;
-  __shared__ EpiShared s_epi;
 
+  griddep_wait();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k = blockIdx.x;
   const DevState* st = p.st;
   const int tick = st->tick;
-  const int cur = st->cur;
   const bool carry = st->resampled_prev == 0;
   const int nM_prev = st->nM_prev;
   const PcgTick c = pcg_tick_consts(st->seed, st->At, st->Bt);
-  float* hb = cur ? p.h1 : p.h0;
+  float* hb = st->cur ? p.h1 : p.h0;
 
+  const float y = a.y_ptr ? __ldg(a.y_ptr) : a.obs.y;
+  const bool gauss = !(a.obs.nu > 0.0f);
   ObsModel obs = a.obs;
-  if (a.y_ptr) obs.y = __ldg(a.y_ptr);
+  obs.y = y;
+  const float y2 = y * y;
 
   float carry_off = 0.0f;
   if (carry) {
@@ -368,7 +257,7 @@ __global__ void __launch_bounds__(kThreads, 3) pass1_kernel(Plan p, TickArgs a) 
         h = propagate(h, a.mu, a.rho, a.sigma, z);
       }
       s += step2;
-      float xx = obs_logpdf(obs, h) * kLog2e;
+      float xx = gauss ? obs_log2pdf_gauss(y2, h) : obs_logpdf(obs, h) * kLog2e;
       if (carry) xx += lg2_approx(wp[e]) + carry_off;
       if (i0 + e >= p.N) xx = -INFINITY;
       hh[e] = h;
@@ -409,7 +298,7 @@ __global__ void __launch_bounds__(kThreads, 3) pass1_kernel(Plan p, TickArgs a) 
     }
     *reinterpret_cast<float4*>(p.w + i0) = make_float4(wv[0], wv[1], wv[2], wv[3]);
   }
-  double dS = warp_sum_d((double)fS), dQ = warp_sum_d((double)fQ), dH = warp_sum_d((double)fH);
+  const double dS = warp_sum_d((double)fS), dQ = warp_sum_d((double)fQ), dH = warp_sum_d((double)fH);
   E = warp_sum_u64(E);
   if (lane == 0) { s_red[0][warp] = dS; s_red[1][warp] = dQ; s_red[2][warp] = dH; s_redE[warp] = E; }
   __syncthreads();
@@ -418,64 +307,307 @@ __global__ void __launch_bounds__(kThreads, 3) pass1_kernel(Plan p, TickArgs a) 
     unsigned long long tE = 0ull;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; ++w) { tS += s_red[0][w]; tQ += s_red[1][w]; tH += s_red[2][w]; tE += s_redE[w]; }
-    p.nexp[k] = nk; p.E[k] = tE; p.S[k] = tS; p.Q[k] = tQ; p.H[k] = tH;
-    __threadfence();
-    const unsigned t = atomicAdd(&p.st->ticket, 1u);
-    s_last = (t == (unsigned)(p.G - 1));
+    p.nexp[k] = nk;
+    p.E[k] = tE;
+    p.rec[k] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
   }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  pass1_epilogue(p, a, tick, cur, s_epi);
+  griddep_release();
 }
 
 // ---------------------------------------------------------------------------
-// Pass 2
+// Plan: one CTA of kPlanThreads threads. Every tick it combines the tile
+// records and takes the resampling decision; on resampling ticks it stages
+// the tile exponents and fixed-point masses in shared memory with coalesced
+// loads and builds the prefix, the target spacing and the work list there.
 // ---------------------------------------------------------------------------
-constexpr size_t kPass2Smem = (size_t)kTile * 8 + (size_t)kTile * 4 + (size_t)kOutChunk * 8;
+struct PlanShared {
+  int red_i[kPlanThreads / 32];
+  double red[3][kPlanThreads / 32];
+  double tot[3];
+  double res[4];
+  unsigned long long scan_u[kPlanThreads / 32 + 1];
+  int scan_i[kPlanThreads / 32 + 1];
+  unsigned long long b_base, b_delta, b_magic;
+  int b_resample, b_Fg;
+};
+
+size_t plan_smem_bytes(int G) {
+  return G <= kPlanSmemTiles ? (size_t)G * 8 + (size_t)(2 * G + 1) * 4 : 0;
+}
+
+__global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs a) {
+  __shared__ PlanShared sh;
+  __shared__ __align__(16) DevState s_st;
+  extern __shared__ __align__(16) unsigned char plan_smem[];
+  griddep_wait();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int G = p.G, N = p.N;
+  // the device state lives in shared memory for the whole kernel (one load, one store)
+  if (tid < kStWords)
+    reinterpret_cast<unsigned long long*>(&s_st)[tid] =
+        __ldcg(reinterpret_cast<const unsigned long long*>(p.st) + tid);
+  DevState* st = &s_st;
+  auto store_state = [&]() {
+    __syncthreads();
+    if (tid < kStWords)
+      reinterpret_cast<unsigned long long*>(p.st)[tid] = reinterpret_cast<const unsigned long long*>(&s_st)[tid];
+  };
+
+  // 1. FP64 combine of the tile partials (one 16-byte record per tile, eight in
+  //    flight per thread), per thread in a running frame 2^nrun
+  int nrun = kNkEmpty;
+  double S = 0.0, Q = 0.0, H = 0.0;
+  for (int k0 = 0; k0 < G; k0 += 8 * kPlanThreads) {
+    float4 r8[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = k0 + u * kPlanThreads + tid;
+      r8[u] = (k < G) ? __ldcg(p.rec + k) : make_float4(0.f, 0.f, 0.f, __int_as_float(kNkEmpty));
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int nk = __float_as_int(r8[u].w);
+      if (nk == kNkEmpty) continue;
+      if (nk > nrun) {
+        const double sc = (nrun == kNkEmpty) ? 0.0 : pow2d(nrun - nk);
+        S *= sc; Q *= sc * sc; H *= sc;
+        nrun = nk;
+      }
+      const double sc = pow2d(nk - nrun);
+      S += (double)r8[u].x * sc; Q += (double)r8[u].y * (sc * sc); H += (double)r8[u].z * sc;
+    }
+  }
+  // 2. global frame 2^nM, FP64 block sums
+  const int nM = block_max_i<kPlanThreads>(nrun, sh.red_i);   // barrier: s_st loaded
+  if (nrun != kNkEmpty) {
+    const double sc = pow2d(nrun - nM);
+    S *= sc; Q *= sc * sc; H *= sc;
+  } else {
+    S = Q = H = 0.0;
+  }
+  S = warp_sum_d(S); Q = warp_sum_d(Q); H = warp_sum_d(H);
+  if (lane == 0) { sh.red[0][warp] = S; sh.red[1][warp] = Q; sh.red[2][warp] = H; }
+  __syncthreads();
+
+  // 3. tick statistics: the three FP64 transcendental/division chains run on
+  //    different warps, then thread 0 takes the decision
+  if (lane == 0 && warp < 3) {
+    double v = 0.0;
+    for (int w = 0; w < kPlanThreads / 32; ++w) v += sh.red[warp][w];
+    sh.tot[warp] = v;
+  }
+  __syncthreads();
+  const double tS = sh.tot[0], tQ = sh.tot[1], tH = sh.tot[2];
+  const bool degenerate = (nM == kNkEmpty) || !(tS > 0.0);
+  if (lane == 0 && !degenerate) {
+    if (warp == 0) sh.res[0] = (double)nM * 0.693147180559945309417232121458 + log(tS);   // log-sum in the carry frame
+    if (warp == 1) sh.res[1] = tS * tS / tQ;                                                // ESS
+    if (warp == 2) sh.res[2] = tH / tS;                                                     // filtered mean
+    if (warp == 3) sh.res[3] = log(tS);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int tick = st->tick, cur = st->cur;
+    double dll, ess, hm;
+    int resample = 0;
+    if (degenerate) {
+      dll = -INFINITY; ess = 0.0; hm = __longlong_as_double(0x7FF8000000000000LL);
+      st->error = BPF_ERR_DEGENERATE;
+    } else {
+      dll = sh.res[0] - st->logS_prev;
+      ess = sh.res[1];
+      hm = sh.res[2];
+      resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
+    }
+    const double ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
+    st->ll_ref = ll_ref;
+    st->ll_total += dll;
+    if (a.rec) {
+      BpfTickRecord r;
+      r.dloglik = dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
+      r.h_mean = (float)hm; r.ess = (float)ess; r.resampled = resample; r.tick = tick;
+      *a.rec = r;
+    }
+    st->At = st->At * kPcgMult;            // next tick's jump constants
+    st->Bt = st->Bt * kPcgMult + 1ull;
+    st->tick = tick + 1;
+    st->do_resample = resample;
+    st->nM = nM;
+    if (resample) {
+      const uint64_t old = st->u_state;
+      st->u_state = old * kPcgMult + kHostInc;
+      st->u23 = pcg_output(old) >> 9;
+      st->logS_prev = a.log_n;
+      st->resampled_prev = 1;
+      st->resample_count += 1;
+      st->src = cur;
+      st->cur = cur ^ 1;
+    } else if (degenerate) {
+      st->logS_prev = a.log_n;             // restart from uniform weights
+      st->resampled_prev = 1;
+    } else {
+      st->logS_prev = sh.res[3];
+      st->resampled_prev = 0;
+      st->nM_prev = nM;
+    }
+    sh.b_resample = resample;
+    sh.b_Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
+  }
+  __syncthreads();
+  if (!sh.b_resample) {
+    store_state();
+    griddep_release();
+    return;
+  }
+
+  // staging arrays: shared memory when the tile count fits, else the global copies
+  const bool in_smem = G <= kPlanSmemTiles;
+  unsigned long long* e_s = in_smem ? reinterpret_cast<unsigned long long*>(plan_smem) : p.E;
+  int* n_s = in_smem ? reinterpret_cast<int*>(plan_smem + (size_t)G * 8) : p.nexp;
+  int* o_s = in_smem ? n_s + G : p.ofirst;
+  if (in_smem) {
+    for (int k0 = 0; k0 < G; k0 += 4 * kPlanThreads) {
+      int nk[4]; unsigned long long e4[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = k0 + u * kPlanThreads + tid;
+        if (k < G) { nk[u] = __ldcg(p.nexp + k); e4[u] = __ldcg(p.E + k); }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = k0 + u * kPlanThreads + tid;
+        if (k < G) { n_s[k] = nk[u]; e_s[k] = e4[u]; }
+      }
+    }
+  }
+  __syncthreads();
+
+  // 4. fixed-point CDF over contiguous runs of tiles: masses in the global
+  //    frame, prefix and total
+  const int Fg = sh.b_Fg;
+  const int C = (G + kPlanThreads - 1) / kPlanThreads;
+  const int k0 = min(tid * C, G), k1 = min(k0 + C, G);
+  auto ehat = [&](int k) -> unsigned long long {
+    const int nk = n_s[k];
+    if (nk == kNkEmpty) return 0ull;
+    return shr64(e_s[k], nM - nk + kFixF - Fg);
+  };
+  unsigned long long part = 0ull;
+  for (int k = k0; k < k1; ++k) part += ehat(k);
+  unsigned long long total;
+  const unsigned long long excl = block_excl_scan_add<kPlanThreads>(part, &total, sh.scan_u);
+  if (tid == 0) {
+    unsigned long long delta = udiv_fp64(total, (unsigned long long)N);
+    if (delta == 0ull) { delta = 1ull; st->error = BPF_ERR_DEGENERATE; }
+    const unsigned long long u = st->u23;
+    const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
+    sh.b_base = (hi << 41) | (lo >> 23);          // floor(u * delta / 2^23)
+    sh.b_delta = delta;
+    sh.b_magic = udiv_magic_of(delta);
+    st->base = sh.b_base; st->delta = delta; st->delta_magic = sh.b_magic; st->total = total;
+    st->Fg = Fg;
+  }
+  __syncthreads();
+  const unsigned long long base = sh.b_base, delta = sh.b_delta, magic = sh.b_magic;
+
+  // 5. per tile: prefix, first output index, number of work items
+  unsigned long long run = excl;
+  int o = targets_below(run, base, delta, magic, N);
+  int n_it = 0;
+  for (int k = k0; k < k1; ++k) {
+    p.P[k] = run;
+    o_s[k] = o;
+    run += ehat(k);
+    const int o_next = targets_below(run, base, delta, magic, N);
+    n_it += (o_next - o + kOutChunk - 1) / kOutChunk;
+    o = o_next;
+  }
+  const int o_end = o;     // first output of the next thread's first tile (N for the last)
+  int n_items_total;
+  const int it0 = block_excl_scan_add<kPlanThreads>(n_it, &n_items_total, sh.scan_i);
+
+  // 6. work items (tile, first output, end output); heavy tiles are split
+  int ib = it0;
+  for (int k = k0; k < k1; ++k) {
+    const int o0 = o_s[k];
+    const int o1 = (k + 1 < k1) ? o_s[k + 1] : o_end;
+    for (int oo = o0; oo < o1; oo += kOutChunk) p.items[ib++] = make_int4(k, oo, min(o1, oo + kOutChunk), 0);
+  }
+  if (tid == 0) st->n_items = n_items_total;
+  store_state();
+  griddep_release();
+}
+
+// ---------------------------------------------------------------------------
+// Pass 2: persistent CTAs; the tiles (h and w) of the next work item are
+// fetched by bulk async copies into the other half of a double buffer while
+// the current item is resampled.
+// ---------------------------------------------------------------------------
+constexpr size_t kTileBytes = (size_t)kTile * 4;
+constexpr size_t kMarkBytes = (size_t)kOutChunk * 2;      // u16 ancestor (tile-local + 1) per output
+constexpr size_t kPass2Smem = 4 * kTileBytes + kMarkBytes;
+
+__device__ __forceinline__ void pass2_fetch(const Plan& p, const float* hsrc, int it, unsigned char* buf,
+                                            uint64_t* bar) {
+  const int k = p.items[it].x;
+  mbar_expect_tx(bar, 2u * (uint32_t)kTileBytes);
+  bulk_load(buf, hsrc + (size_t)k * kTile, (uint32_t)kTileBytes, bar);
+  bulk_load(buf + kTileBytes, p.w + (size_t)k * kTile, (uint32_t)kTileBytes, bar);
+}
 
 __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  unsigned long long* Cs = reinterpret_cast<unsigned long long*>(smem);
-  float* hs = reinterpret_cast<float*>(Cs + kTile);
-  float* outb = hs + kTile;
-  int* ancb = reinterpret_cast<int*>(outb + kOutChunk);
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned short* marks = reinterpret_cast<unsigned short*>(smem + 4 * kTileBytes);
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ unsigned long long s_scan[kThreads / 32 + 1];
   __shared__ int s_err;
 
+  griddep_wait();
   const DevState* st = p.st;
-  if (!st->do_resample) return;
+  if (!st->do_resample) {
+    griddep_release();
+    return;
+  }
   const int n_items = st->n_items;
-  const unsigned long long base = st->base, delta = st->delta;
-  const int nM = st->nM, Fg = st->Fg;
+  const unsigned long long base = st->base, delta = st->delta, magic = st->delta_magic;
+  const int nM = st->nM, Fg = st->Fg, N = p.N;
   const int src = st->src;
   const float* hsrc = src ? p.h1 : p.h0;
   float* hdst = src ? p.h0 : p.h1;
   const int tid = threadIdx.x;
-  if (tid == 0) s_err = 0;
+  if (tid == 0) {
+    s_err = 0;
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    if ((int)blockIdx.x < n_items) pass2_fetch(p, hsrc, blockIdx.x, smem, &mbar[0]);
+  }
+  __syncthreads();
 
-  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+  int n = 0;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x, ++n) {
+    const int sb = n & 1;
+    unsigned char* buf = smem + (size_t)sb * 2 * kTileBytes;
+    const float* hs = reinterpret_cast<const float*>(buf);
+    const float* ws = reinterpret_cast<const float*>(buf + kTileBytes);
+    if (tid == 0 && it + (int)gridDim.x < n_items)
+      pass2_fetch(p, hsrc, it + gridDim.x, smem + (size_t)(sb ^ 1) * 2 * kTileBytes, &mbar[sb ^ 1]);
+
     const int4 item = p.items[it];
     const int k = item.x, oa = item.y, ob = item.z;
     const int j0 = k * kTile;
-    const int nA = min(kTile, p.N - j0);
+    const int nA = min(kTile, N - j0);
     const int nB = ob - oa;
     const int r = nM - p.nexp[k] + kFixF - Fg;
     const unsigned long long Pk = p.P[k];
-
-    // stage the h tile (coalesced float4)
-    const float4* hsrc4 = reinterpret_cast<const float4*>(hsrc + j0);
-#pragma unroll
-    for (int v = 0; v < kTile / 4 / kThreads; ++v)
-      reinterpret_cast<float4*>(hs)[tid + kThreads * v] = hsrc4[tid + kThreads * v];
+    const bool ok = mbar_wait_bounded(&mbar[sb], (uint32_t)(n >> 1) & 1u);
+    if (!ok) s_err = 1;
 
     // exact fixed-point prefix of the tile: 16 contiguous weights per thread
-    const float4* wv = reinterpret_cast<const float4*>(p.w + j0 + tid * kPerThread);
     unsigned long long L[kPerThread];
     unsigned long long run = 0ull;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-      const float4 f = wv[v];
+      const float4 f = reinterpret_cast<const float4*>(ws + tid * kPerThread)[v];
       const float ff[4] = {f.x, f.y, f.z, f.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
@@ -485,41 +617,58 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
       }
     }
     unsigned long long tot;
-    const unsigned long long excl = block_excl_scan_u64(run, &tot, s_scan);
-#pragma unroll
-    for (int e = 0; e < kPerThread; ++e) Cs[tid * kPerThread + e] = Pk + shr64(excl + L[e], r);
-    __syncthreads();
+    const unsigned long long excl = block_excl_scan_add<kThreads>(run, &tot, s_scan);
 
-    // merge path: thread's slice [d0, d1) of the merged (elements, targets) order
-    const int total = nA + nB;
-    const int d0 = (int)(((long long)tid * total) / kThreads);
-    const int d1 = (int)(((long long)(tid + 1) * total) / kThreads);
-    int lo = max(0, d0 - nB), hi = min(d0, nA);
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      const unsigned long long tt = base + (unsigned long long)(oa + d0 - mid - 1) * delta;
-      if (Cs[mid] <= tt) lo = mid + 1; else hi = mid;
-    }
-    int j = lo, i = d0 - lo;
-    unsigned long long ti = base + (unsigned long long)(oa + i) * delta;
-    for (int d = d0; d < d1; ++d) {
-      if (i < nB && (j >= nA || ti < Cs[j])) {
-        int jj = j;
-        if (jj >= nA) { jj = nA - 1; s_err = 1; }   // unreachable by construction; keeps the access in bounds
-        outb[i] = hs[jj];
-        ancb[i] = j0 + jj;
-        ++i;
-        ti += delta;
-      } else {
-        ++j;
+    // Each element owns the targets in [C_{j-1}, C_j): write its index into
+    // every owned output slot of this item. Elements with more than four
+    // targets are filled by their whole warp (ballot + broadcast).
+    const int lane = tid & 31;
+    int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
+    unsigned long long tq = base + (unsigned long long)q * delta;
+#pragma unroll
+    for (int e = 0; e < kPerThread; ++e) {
+      const int j = tid * kPerThread + e;
+      const unsigned long long cj = Pk + shr64(excl + L[e], r);
+      int lo = 0, hi = 0;
+      if (j < nA && q < N && tq < cj) {
+        if (((cj - tq) >> 2) > delta) {
+          const int q1 = targets_below(cj, base, delta, magic, N);
+          lo = max(q, oa) - oa;
+          hi = min(q1, ob) - oa;
+          q = q1;
+          tq = base + (unsigned long long)q * delta;
+        } else {
+          do {
+            if (q >= oa && q < ob) marks[q - oa] = (unsigned short)(j + 1);
+            ++q;
+            tq += delta;
+          } while (q < N && tq < cj);
+        }
+      }
+      unsigned heavy = __ballot_sync(0xffffffffu, hi > lo);
+      while (heavy) {
+        const int srcl = __ffs(heavy) - 1;
+        heavy &= heavy - 1u;
+        const int flo = __shfl_sync(0xffffffffu, lo, srcl), fhi = __shfl_sync(0xffffffffu, hi, srcl);
+        const unsigned short v = (unsigned short)(__shfl_sync(0xffffffffu, j, srcl) + 1);
+        for (int qq = flo + lane; qq < fhi; qq += 32) marks[qq] = v;
       }
     }
     __syncthreads();
-    for (int q = tid; q < nB; q += kThreads) hdst[oa + q] = outb[q];
-    if (a.anc) for (int q = tid; q < nB; q += kThreads) a.anc[oa + q] = ancb[q];
+
+    // gather h[ancestor] from the staged tile, coalesced store
+    if (ok) {
+      for (int qq = tid; qq < nB; qq += kThreads) {
+        unsigned jj = marks[qq];
+        if (jj == 0u || jj > (unsigned)nA) { jj = 1u; s_err = 1; }   // unreachable by construction
+        hdst[oa + qq] = hs[jj - 1u];
+        if (a.anc) a.anc[oa + qq] = j0 + (int)(jj - 1u);
+      }
+    }
     __syncthreads();
   }
   if (tid == 0 && s_err) p.st->error = BPF_ERR_STATE;
+  griddep_release();
 }
 
 // ---------------------------------------------------------------------------
@@ -538,14 +687,25 @@ __global__ void debug_pcg_kernel(int seed, int n, unsigned long long At, unsigne
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             bool pdl, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? attr : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 cudaError_t launch_init(const Plan& p, float mu, float std_stat, int seed, cudaStream_t s) {
   const int n = p.G * kTile;
   init_kernel<<<(n + 255) / 256, 256, 0, s>>>(p, mu, std_stat, seed);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s) {
-  pass1_kernel<<<p.G, kThreads, 0, s>>>(p, a);
   return cudaGetLastError();
 }
 
@@ -555,6 +715,8 @@ int pass2_grid_size(int device) {
   static int configured = -1;
   if (configured != device) {
     cudaFuncSetAttribute(pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPass2Smem);
+    cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)plan_smem_bytes(kPlanSmemTiles));
     configured = device;
   }
   int sms = 0, per_sm = 0;
@@ -564,9 +726,14 @@ int pass2_grid_size(int device) {
   return sms * per_sm;
 }
 
-cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s) {
-  pass2_kernel<<<grid, kThreads, kPass2Smem, s>>>(p, a);
-  return cudaGetLastError();
+cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
+  return launch_ex(pass1_kernel, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a);
+}
+cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
+  return launch_ex(plan_kernel, dim3(1), dim3(kPlanThreads), plan_smem_bytes(p.G), s, pdl, p, a);
+}
+cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s, bool pdl) {
+  return launch_ex(pass2_kernel, dim3(grid), dim3(kThreads), kPass2Smem, s, pdl, p, a);
 }
 
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s) {

@@ -5,9 +5,10 @@
 // leave the allocation):
 //   h[2][G*4096]  f32  particle ping-pong (current buffer index in DevState)
 //   w[G*4096]     f32  tile-relative weights 2^(x_i - n_k), in [0,1]
-//   tile records  nexp[G] i32, E[G] u64, S/Q/H[G] f64
+//   tile records  rec[G] f32x4 {S=sum w, Q=sum w^2, H=sum w h, n_k bits},
+//                 nexp[G] i32 (n_k again), E[G] u64 exact fixed-point mass
 //   P[G] u64 exclusive tile prefix of the fixed-point CDF, ofirst[G+1] i32
-//   items[G + N/4096 + 1] int4 pass-2 work items (tile, first out, end out)
+//   items[G + N/12288 + 1] int4 pass-2 work items (tile, first out, end out)
 //   DevState      scalars carried from tick to tick
 #pragma once
 #include <cstdint>
@@ -38,7 +39,7 @@ struct DevState {
   int      n_items;         // pass-2 work items of the current tick
   uint32_t u23;             // resampling uniform of the current tick
   int      resample_count;
-  unsigned ticket;          // pass-1 CTA completion counter
+  int      reserved;
   int      error;           // sticky BPF_* error code
   int      seed;            // filter seed (PCG32 streams, resampling uniform)
 };
@@ -47,7 +48,7 @@ static_assert(sizeof(DevState) == 136, "DevState layout");
 struct Plan {
   int N, G, max_items;
   float* h0; float* h1; float* w;
-  int* nexp; unsigned long long* E; double* S; double* Q; double* H;
+  int* nexp; unsigned long long* E; float4* rec;
   unsigned long long* P; int* ofirst; int4* items;
   DevState* st;
 };
@@ -55,6 +56,7 @@ struct Plan {
 struct TickArgs {
   float mu, rho, sigma;
   float ess_threshold;
+  double log_n;              // ln N
   ObsModel obs;              // obs.y is used when y_ptr == nullptr
   const float* y_ptr;        // device pointer to this tick's observation, or null
   BpfTickRecord* rec;        // device record slot written by the last pass-1 CTA
@@ -64,8 +66,10 @@ struct TickArgs {
 // Host-side launchers (stream-ordered, no synchronisation).
 // Draws h_0 for `seed` and (re)initialises the DevState on the device.
 cudaError_t launch_init(const Plan& p, float mu, float std_stat, int seed, cudaStream_t s);
-cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s);
-cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s);
+// pdl = programmatic dependent launch on the previous kernel in the stream.
+cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
+cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
+cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s, bool pdl);
 int pass2_grid_size(int device);
 size_t pass2_smem_bytes();
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s);

@@ -96,7 +96,8 @@ SIGNATURES = {
     "gpu_bpf_get_ancestors": (_i, [P_STATE, C.POINTER(C.c_int32)]),
     "gpu_bpf_get_resample_inputs": (_i, [P_STATE, C.POINTER(_f), C.POINTER(C.c_int32), C.POINTER(C.c_uint32)]),
     "gpu_bpf_profile": (_i, [P_STATE, _i]),
-    "gpu_bpf_profile_read": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_d), C.POINTER(_i), C.POINTER(_i)]),
+    "gpu_bpf_profile_read": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), C.POINTER(_i),
+                                  C.POINTER(_i)]),
     "gpu_bpf_launch_count": (C.c_longlong, []),
     "gpu_bpf_debug_pcg32": (_i, [_i, _i, _i, C.POINTER(C.c_uint32)]),
     "gpu_bpf_debug_normals": (_i, [_i, _i, _i, C.POINTER(_f)]),

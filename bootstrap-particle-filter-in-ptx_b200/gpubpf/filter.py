@@ -150,11 +150,12 @@ class GpuBpf:
         check(self._lib.gpu_bpf_profile(self._s, int(enable)), "gpu_bpf_profile")
 
     def profile_read(self):
-        p1, p2 = C.c_double(), C.c_double()
+        """(pass1_ms, plan_ms, pass2_ms, ticks) summed since profile(True)."""
+        p1, pl, p2 = C.c_double(), C.c_double(), C.c_double()
         n1, n2 = C.c_int(), C.c_int()
-        check(self._lib.gpu_bpf_profile_read(self._s, C.byref(p1), C.byref(p2), C.byref(n1), C.byref(n2)),
-              "gpu_bpf_profile_read")
-        return p1.value, p2.value, n1.value, n2.value
+        check(self._lib.gpu_bpf_profile_read(self._s, C.byref(p1), C.byref(pl), C.byref(p2), C.byref(n1),
+                                             C.byref(n2)), "gpu_bpf_profile_read")
+        return p1.value, pl.value, p2.value, n1.value
 
 
 def debug_pcg32(seed: int, n: int, t: int):

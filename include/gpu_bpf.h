@@ -194,11 +194,12 @@ int gpu_bpf_get_ancestors(GpuBpfState* state, int32_t* anc_out);
 int gpu_bpf_get_resample_inputs(GpuBpfState* state, float* w_out, int32_t* tile_exp_out,
                                 uint32_t* u23_out);
 
-/* Kernel profiling: when enabled, the duration of every pass-1 and pass-2
- * launch is timed with CUDA events on state->stream. read returns the sums
- * (ms) and launch counts since enabling. */
+/* Kernel profiling: when enabled, every tick's three kernels (pass 1, plan,
+ * pass 2) are timed with CUDA events on state->stream (launched without
+ * programmatic dependent launch so the events bracket each kernel). read
+ * returns the summed durations (ms) and the tick counts since enabling. */
 int gpu_bpf_profile(GpuBpfState* state, int enable);
-int gpu_bpf_profile_read(GpuBpfState* state, double* pass1_ms, double* pass2_ms,
+int gpu_bpf_profile_read(GpuBpfState* state, double* pass1_ms, double* plan_ms, double* pass2_ms,
                          int* pass1_launches, int* pass2_launches);
 
 /* Number of kernel launches this library has issued (all filters). */
