@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "gpubpf", "libgpubpf.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["bpf_plain.cu", "bpf_api.cu"]
+SOURCES = ["bpf_plain.cu", "bpf_api.cu", "bpf_static.cu"]
 HEADERS = ["bpf_common.cuh", "bpf_plain.cuh"]
 
 NVCC_FLAGS = [

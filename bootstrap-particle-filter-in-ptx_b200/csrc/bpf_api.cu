@@ -24,6 +24,9 @@ static std::atomic<long long> g_launches{0};
 
 static inline int set_err(int code) { g_last_error = code; return code; }
 
+int bpf_record_error(int code) { return set_err(code); }
+void bpf_note_launches(long long n) { g_launches += n; }
+
 #define CK(call)                                                        \
   do {                                                                  \
     cudaError_t e_ = (call);                                            \

@@ -75,3 +75,7 @@ size_t pass2_smem_bytes();
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s);
 
 }  // namespace bpf
+
+// Status and launch bookkeeping shared by the C entry points (bpf_api.cu).
+int bpf_record_error(int code);          // sets gpu_bpf_last_error() for this thread, returns code
+void bpf_note_launches(long long n);     // adds to gpu_bpf_launch_count()

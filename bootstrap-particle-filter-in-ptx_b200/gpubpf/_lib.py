@@ -19,6 +19,7 @@ BPF_ERR_UNSUPPORTED = 4
 BPF_ERR_STATE = 5
 BPF_ERR_DEGENERATE = 6
 BPF_ERR_NODEVICE = 7
+BPF_STATIC_MAX_PARTICLES = 262144
 
 
 class BpfResult(C.Structure):
@@ -99,6 +100,7 @@ SIGNATURES = {
     "gpu_bpf_profile_read": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), C.POINTER(_i),
                                   C.POINTER(_i)]),
     "gpu_bpf_launch_count": (C.c_longlong, []),
+    "gpu_bpf_run_static": (_i, [_i, _f, _f, _f, _f, _i, _f, _vp, _i, _vp, _vp]),
     "gpu_bpf_debug_pcg32": (_i, [_i, _i, _i, C.POINTER(C.c_uint32)]),
     "gpu_bpf_debug_normals": (_i, [_i, _i, _i, C.POINTER(_f)]),
 }

@@ -202,6 +202,30 @@ int gpu_bpf_profile(GpuBpfState* state, int enable);
 int gpu_bpf_profile_read(GpuBpfState* state, double* pass1_ms, double* plan_ms, double* pass2_ms,
                          int* pass1_launches, int* pass2_launches);
 
+/* Allocation-free run (addition; no counterpart in the reference).
+ * For callers that may not allocate GPU memory while they run: hosts that
+ * reserve their whole device memory budget at start-up and forbid later
+ * allocations, and latency-critical loops that cannot take cudaFree's
+ * implicit device synchronisation or the allocator's locks.
+ * Runs one plain filter (same algorithm and results as gpu_bpf_create +
+ * gpu_bpf_step_many_device + gpu_bpf_destroy) of n_particles <=
+ * BPF_STATIC_MAX_PARTICLES over the device observations y_dev[0..n_ticks),
+ * writing one BpfTickRecord per tick to the device array rec_dev. All filter
+ * state lives in one fixed scratch area compiled into the library (about
+ * 3 MiB, held by every GPU that loads the library until the process exits);
+ * no cudaMalloc, cudaFree or allocating library call is made. Larger sizes
+ * return BPF_ERR_ARG.
+ * The first call on a device looks the scratch address up with that device
+ * current; make that first call before any stream capture. Every call
+ * re-initialises the whole state, and all calls share the one scratch area:
+ * calls whose GPU work overlaps (other streams or host threads) race and
+ * corrupt each other, so serialise them. Enqueued on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream); does not synchronise. */
+#define BPF_STATIC_MAX_PARTICLES 262144
+int gpu_bpf_run_static(int n_particles, float rho, float sigma_z, float mu, float nu_obs, int seed,
+                       float ess_threshold, const float* y_dev, int n_ticks, BpfTickRecord* rec_dev,
+                       void* stream);
+
 /* Number of kernel launches this library has issued (all filters). */
 long long gpu_bpf_launch_count(void);
 
