@@ -1,0 +1,329 @@
+// bpf_batch.cu — persistent batched SV filter kernel (one filter per CTA at a
+// time, whole filter resident in shared memory for all T ticks).
+//
+// Per tick and filter (N particles, G = ceil(N/4096) tiles, NT threads):
+//   1. propagate + log2-weight (+ carried weight), per-tile max
+//   2. tile-relative weights 2^(x - n_k), tile partial sums and exact
+//      fixed-point tile masses
+//   3. thread 0: FP64 combine, log-likelihood increment, ESS, mean, decision;
+//      on resampling ticks the fixed-point CDF tile prefix, total and spacing
+//   4. resampling: per-thread contiguous chunk scan, per-element count of the
+//      evenly spaced targets, ancestor slots, gather into the other buffer.
+// Particle arrays use a swizzled layout (column c of each 32-float row stored
+// at c ^ row) so both the lane-strided and the per-thread-contiguous access
+// patterns are free of shared-memory bank conflicts.
+#include "bpf_batch.cuh"
+#include "bpf_block.cuh"
+
+namespace bpf {
+
+__device__ __forceinline__ int swz(int i) { return (i & ~31) | ((i ^ (i >> 5)) & 31); }
+
+template <int NT>
+struct BatchShared {
+  float tmax[kBatchMaxTiles][NT / 32];
+  double sred[3][kBatchMaxTiles][NT / 32];
+  unsigned long long ered[kBatchMaxTiles][NT / 32];
+  unsigned long long scan[NT / 32 + 1];
+  unsigned long long excl[NT];
+  unsigned long long Pk[kBatchMaxTiles];
+  float carry_off[kBatchMaxTiles];
+  int rk[kBatchMaxTiles];
+  unsigned long long base, delta, magic;
+  int resample, carry, next;
+};
+
+size_t batch_smem_bytes(int maxn) { return (size_t)maxn * 8 + (((size_t)maxn * 2 + 15) / 16) * 16; }
+
+template <int NT>
+__device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, int b, float* bufA, float* bufB,
+                                 unsigned short* marks, BatchShared<NT>& sh) {
+  constexpr int W = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N = f.n;
+  const int G = (N + kTile - 1) / kTile;
+  const bool gauss = !(f.nu > 0.0f);
+  ObsModel obs;
+  obs.y = 0.0f; obs.nu = f.nu; obs.c_obs = f.c_obs; obs.inv_nu = f.inv_nu; obs.nu_p1h = f.nu_p1h;
+  int chunk = 1;
+  while (chunk * NT < N) chunk <<= 1;           // power of two: chunks never straddle a tile
+
+  // h_0 from draw 0 (stationary law)
+  {
+    const PcgTick c = pcg_tick_consts(f.seed, 1ull, 0ull);
+    for (int i = tid; i < N; i += NT) {
+      const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
+      bufA[swz(i)] = fmaf(f.std_stat, icdf_normal(pcg_uniform(pcg_output(s))), f.mu);
+    }
+  }
+  float* H = bufA;
+  float* Wt = bufB;
+  unsigned long long At = 1ull, Bt = 0ull;
+  // thread-0 filter state
+  double logS_prev = log((double)N), ll_total = 0.0;
+  uint64_t ustate = (unsigned long long)f.seed * 67890ULL + 12345ULL;
+  int n_res = 0;
+  float hm_last = 0.0f;
+  if (tid == 0) sh.carry = 0;
+  __syncthreads();
+
+  for (int t = 0; t < a.T; ++t) {
+    const float y = __ldg(a.y + t);
+    const float y2 = y * y;
+    obs.y = y;
+    const bool carry = sh.carry != 0;
+    const PcgTick c = pcg_tick_consts(f.seed, At, Bt);
+
+    // 1. propagate + log2-weight, per-tile max
+    float tmax[kBatchMaxTiles];
+#pragma unroll
+    for (int k = 0; k < kBatchMaxTiles; ++k) {
+      float m = -INFINITY;
+      if (k < G) {
+        const float coff = carry ? sh.carry_off[k] : 0.0f;
+        const int i1 = min(N, (k + 1) * kTile);
+        for (int i = k * kTile + tid; i < i1; i += NT) {
+          const int si = swz(i);
+          float h = H[si];
+          if (t > 0) {
+            const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
+            h = propagate(h, f.mu, f.rho, f.sigma, icdf_normal(pcg_uniform(pcg_output(s))));
+            H[si] = h;
+          }
+          float x = gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e);
+          if (carry) x += lg2_approx(Wt[si]) + coff;
+          Wt[si] = x;
+          m = fmaxf(m, x);
+        }
+      }
+      tmax[k] = m;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatchMaxTiles; ++k) {
+      const float v = warp_max_f(tmax[k]);
+      if (lane == 0) sh.tmax[k][warp] = v;
+    }
+    __syncthreads();
+    int nk[kBatchMaxTiles];
+#pragma unroll
+    for (int k = 0; k < kBatchMaxTiles; ++k) {
+      float m = -INFINITY;
+      for (int w = 0; w < W; ++w) m = fmaxf(m, sh.tmax[k][w]);
+      nk[k] = (m == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(m, -1.0e9f));
+    }
+
+    // 2. tile-relative weights, partial sums, exact fixed-point tile masses
+#pragma unroll
+    for (int k = 0; k < kBatchMaxTiles; ++k) {
+      float fS = 0.f, fQ = 0.f, fH = 0.f;
+      unsigned long long E = 0ull;
+      if (k < G) {
+        const float fnk = (float)nk[k];
+        const int i1 = min(N, (k + 1) * kTile);
+        for (int i = k * kTile + tid; i < i1; i += NT) {
+          const int si = swz(i);
+          const float w = (nk[k] == kNkEmpty) ? 0.0f : fminf(ex2_approx(Wt[si] - fnk), 1.0f);
+          Wt[si] = w;
+          fS += w;
+          fQ = fmaf(w, w, fQ);
+          fH = fmaf(w, H[si], fH);
+          E += fix_weight(w);
+        }
+      }
+      const double dS = warp_sum_d((double)fS), dQ = warp_sum_d((double)fQ), dH = warp_sum_d((double)fH);
+      E = warp_sum_u64(E);
+      if (lane == 0) { sh.sred[0][k][warp] = dS; sh.sred[1][k][warp] = dQ; sh.sred[2][k][warp] = dH; sh.ered[k][warp] = E; }
+    }
+    __syncthreads();
+
+    // 3. decision (thread 0)
+    if (tid == 0) {
+      int nM = kNkEmpty;
+      for (int k = 0; k < G; ++k) nM = max(nM, nk[k]);
+      double S = 0.0, Q = 0.0, Hm = 0.0;
+      unsigned long long Ek[kBatchMaxTiles];
+      for (int k = 0; k < kBatchMaxTiles; ++k) {
+        Ek[k] = 0ull;
+        if (k >= G || nk[k] == kNkEmpty) continue;
+        double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (int w = 0; w < W; ++w) { s1 += sh.sred[0][k][w]; s2 += sh.sred[1][k][w]; s3 += sh.sred[2][k][w]; Ek[k] += sh.ered[k][w]; }
+        const double sc = pow2d(nk[k] - nM);
+        S += s1 * sc; Q += s2 * sc * sc; Hm += s3 * sc;
+      }
+      const bool degenerate = (nM == kNkEmpty) || !(S > 0.0);
+      double dll;
+      int resample = 0;
+      float hm = __int_as_float(0x7fc00000);
+      if (degenerate) {
+        dll = -INFINITY;
+      } else {
+        dll = (double)nM * 0.693147180559945309417232121458 + log(S) - logS_prev;
+        const double ess = S * S / Q;
+        hm = (float)(Hm / S);
+        resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
+      }
+      ll_total += dll;
+      hm_last = hm;
+      if (a.dll) a.dll[(size_t)b * a.T + t] = dll;
+      if (a.hmean) a.hmean[(size_t)b * a.T + t] = hm;
+      if (resample) {
+        const uint64_t old = ustate;
+        ustate = old * kPcgMult + kHostInc;
+        const unsigned long long u = pcg_output(old) >> 9;
+        logS_prev = log((double)N);
+        ++n_res;
+        const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
+        unsigned long long P = 0ull;
+        for (int k = 0; k < kBatchMaxTiles; ++k) {
+          const int r = (k < G && nk[k] != kNkEmpty) ? nM - nk[k] + kFixF - Fg : 64;
+          sh.rk[k] = r;
+          sh.Pk[k] = P;
+          P += shr64(Ek[k], r);
+        }
+        unsigned long long delta = udiv_fp64(P, (unsigned long long)N);
+        if (delta == 0ull) delta = 1ull;
+        const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
+        sh.base = (hi << 41) | (lo >> 23);
+        sh.delta = delta;
+        sh.magic = udiv_magic_of(delta);
+        sh.carry = 0;
+      } else if (degenerate) {
+        logS_prev = log((double)N);
+        sh.carry = 0;
+      } else {
+        logS_prev = log(S);
+        for (int k = 0; k < kBatchMaxTiles; ++k)
+          sh.carry_off[k] = (k < G && nk[k] != kNkEmpty) ? (float)(nk[k] - nM) : -INFINITY;
+        sh.carry = 1;
+      }
+      sh.resample = resample;
+    }
+    At = At * kPcgMult;
+    Bt = Bt * kPcgMult + 1ull;
+    __syncthreads();
+
+    // 4. systematic resampling (fixed-point CDF, same rule as the plain filter)
+    if (sh.resample) {
+      const unsigned long long base = sh.base, delta = sh.delta, magic = sh.magic;
+      const int j0 = tid * chunk, j1 = min(N, j0 + chunk);
+      unsigned long long run = 0ull;
+      for (int j = j0; j < j1; ++j) run += fix_weight(Wt[swz(j)]);
+      unsigned long long tot;
+      const unsigned long long excl = block_excl_scan_add<NT>(run, &tot, sh.scan);
+      sh.excl[tid] = excl;
+      __syncthreads();
+      int q = 0, k = 0, r = 64;
+      unsigned long long Pk = 0ull, loc = 0ull, tq = 0ull;
+      if (j0 < N) {
+        k = j0 >> 12;
+        r = sh.rk[k];
+        Pk = sh.Pk[k];
+        loc = excl - sh.excl[(k * kTile) / chunk];          // tile-local exclusive prefix
+        q = targets_below(Pk + shr64(loc, r), base, delta, magic, N);
+        tq = base + (unsigned long long)q * delta;
+      }
+      for (int e = 0; e < chunk; ++e) {
+        const int j = j0 + e;
+        int lo = 0, hi = 0;
+        if (j < j1) {
+          loc += fix_weight(Wt[swz(j)]);
+          const unsigned long long cj = Pk + shr64(loc, r);
+          if (q < N && tq < cj) {
+            if (((cj - tq) >> 2) > delta) {
+              const int q1 = targets_below(cj, base, delta, magic, N);
+              lo = q; hi = q1;
+              q = q1;
+              tq = base + (unsigned long long)q * delta;
+            } else {
+              do { marks[q] = (unsigned short)(j + 1); ++q; tq += delta; } while (q < N && tq < cj);
+            }
+          }
+        }
+        unsigned heavy = __ballot_sync(0xffffffffu, hi > lo);
+        while (heavy) {
+          const int sl = __ffs(heavy) - 1;
+          heavy &= heavy - 1u;
+          const int flo = __shfl_sync(0xffffffffu, lo, sl), fhi = __shfl_sync(0xffffffffu, hi, sl);
+          const unsigned short v = (unsigned short)(__shfl_sync(0xffffffffu, j, sl) + 1);
+          for (int qq = flo + lane; qq < fhi; qq += 32) marks[qq] = v;
+        }
+      }
+      __syncthreads();
+      for (int i = tid; i < N; i += NT) {
+        const int anc = (int)marks[i] - 1;
+        Wt[swz(i)] = H[swz(anc)];
+        if (a.anc) a.anc[((size_t)b * a.T + t) * kBatchMaxN + i] = anc;
+      }
+      __syncthreads();
+      float* tmp = H; H = Wt; Wt = tmp;
+    }
+  }
+  if (a.particles)
+    for (int i = tid; i < N; i += NT) a.particles[(size_t)b * kBatchMaxN + i] = H[swz(i)];
+  if (tid == 0) {
+    a.loglik[b] = ll_total;
+    a.h_final[b] = hm_last;
+    a.resamples[b] = n_res;
+  }
+  __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_kernel(BatchArgs a, int maxn) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ BatchShared<NT> sh;
+  float* bufA = reinterpret_cast<float*>(smem);
+  float* bufB = bufA + maxn;
+  unsigned short* marks = reinterpret_cast<unsigned short*>(bufB + maxn);
+  for (;;) {
+    if (threadIdx.x == 0) sh.next = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int idx = sh.next;
+    __syncthreads();
+    if (idx >= a.n_order) break;
+    const int b = a.order[idx];
+    const BatchFilterDev f = a.filters[b];
+    batch_run_filter<NT>(a, f, b, bufA, bufB, marks, sh);
+  }
+}
+
+// The dynamic shared-memory attribute is set by batch_occupancy (called when
+// a class is configured, outside any stream capture).
+template <int NT>
+static cudaError_t launch_nt(const BatchArgs& a, int maxn, int grid, cudaStream_t s) {
+  batch_kernel<NT><<<grid, NT, batch_smem_bytes(maxn), s>>>(a, maxn);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s) {
+  switch (threads) {
+    case 64: return launch_nt<64>(a, maxn, grid, s);
+    case 128: return launch_nt<128>(a, maxn, grid, s);
+    case 256: return launch_nt<256>(a, maxn, grid, s);
+    case 512: return launch_nt<512>(a, maxn, grid, s);
+    case 1024: return launch_nt<1024>(a, maxn, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int NT>
+static int occ_nt(int maxn) {
+  const size_t smem = batch_smem_bytes(maxn);
+  cudaFuncSetAttribute(batch_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<NT>, NT, smem);
+  return per;
+}
+
+int batch_occupancy(int threads, int maxn) {
+  switch (threads) {
+    case 64: return occ_nt<64>(maxn);
+    case 128: return occ_nt<128>(maxn);
+    case 256: return occ_nt<256>(maxn);
+    case 512: return occ_nt<512>(maxn);
+    case 1024: return occ_nt<1024>(maxn);
+    default: return 0;
+  }
+}
+
+}  // namespace bpf

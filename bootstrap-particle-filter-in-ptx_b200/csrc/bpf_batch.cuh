@@ -1,0 +1,55 @@
+// bpf_batch.cuh — many independent SV filters (different theta, N and seed)
+// sharing one observation series, in one persistent launch per size class.
+//
+// A CTA owns one filter at a time and keeps its particles, weights and
+// ancestor slots in shared memory for all T ticks, so the per-tick HBM
+// traffic is zero; the kernel is bound by instruction issue and shared
+// memory. Filters are taken from a per-class work counter in LPT order
+// (largest N first). The arithmetic per particle is the plain filter's
+// (same PCG32 draw, inverse CDF, propagation, log2-weight, tile-relative
+// weights over 4096-particle tiles and the same fixed-point systematic
+// resampling), so a batched filter reproduces the plain filter with the same
+// theta, N and seed: identical ancestors and particles, log-likelihood equal
+// up to the order of floating-point sums.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "bpf_common.cuh"
+#include "../../include/gpu_bpf.h"
+
+namespace bpf {
+
+constexpr int kBatchMaxN = 16384;          // largest filter the shared-memory layout holds
+constexpr int kBatchMaxTiles = kBatchMaxN / kTile;
+
+struct BatchFilterDev {                    // 48 bytes, one per filter
+  float mu, rho, sigma, std_stat;
+  float nu, c_obs, inv_nu, nu_p1h;
+  int n, seed, pad0, pad1;
+};
+
+struct BatchArgs {
+  const BatchFilterDev* filters;
+  const int* order;           // filter indices of this class, largest N first
+  int n_order;
+  int* counter;               // work counter of this class (zeroed before the launch)
+  const float* y;             // observations [T]
+  int T;
+  float ess_threshold;
+  double* loglik;             // [B] total log-likelihood (FP64)
+  double* dll;                // [B*T] per-tick increments, or null
+  float* hmean;               // [B*T] filtered means, or null
+  float* h_final;             // [B] filtered mean at the last tick
+  int* resamples;             // [B] resampling count
+  int32_t* anc;               // [B*T*kBatchMaxN] ancestors, or null (testing)
+  float* particles;           // [B*kBatchMaxN] final particles, or null (testing)
+};
+
+// Dynamic shared memory of the class kernel for filters of at most maxn particles.
+size_t batch_smem_bytes(int maxn);
+// Launches the kernel instance with `threads` threads per CTA (64..1024, power of 2).
+cudaError_t launch_batch_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s);
+// CTAs per SM the class kernel can keep resident.
+int batch_occupancy(int threads, int maxn);
+
+}  // namespace bpf

@@ -1,0 +1,413 @@
+// bpf_batch_api.cu — extern "C" entry points of the batched filter
+// (include/gpu_bpf.h, "Batched filters").
+//
+// Filters are grouped into five size classes by particle count (at most
+// 1024, 2048, 4096, 8192, 16384). Each class runs as one persistent launch
+// whose CTAs pull filters from a work counter in LPT order (largest N
+// first); the classes run concurrently on their own streams, forked from and
+// joined to the batch stream, and a whole run is replayed as one CUDA graph.
+// The threads per CTA of every class are the tile shape the autotuner picks.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "bpf_batch.cuh"
+#include "bpf_plain.cuh"
+
+using namespace bpf;
+
+namespace {
+
+constexpr int kClasses = 5;
+constexpr int kClassMaxN[kClasses] = {1024, 2048, 4096, 8192, 16384};
+constexpr int kDefaultThreads[kClasses] = {128, 256, 256, 512, 1024};
+constexpr int kThreadChoices[] = {64, 128, 256, 512, 1024};
+
+#define BCK(call)                                                             \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) {                                                  \
+      cudaGetLastError();                                                     \
+      return bpf_record_error(e_ == cudaErrorMemoryAllocation ? BPF_ERR_ALLOC : BPF_ERR_CUDA); \
+    }                                                                         \
+  } while (0)
+
+struct GraphKey {
+  const float* y = nullptr;
+  int T = 0;
+  double* loglik = nullptr;
+  double* dll = nullptr;
+  float* hmean = nullptr;
+  int32_t* anc = nullptr;
+  float* particles = nullptr;
+  int threads[kClasses] = {0, 0, 0, 0, 0};
+  bool operator==(const GraphKey& o) const {
+    return y == o.y && T == o.T && loglik == o.loglik && dll == o.dll && hmean == o.hmean && anc == o.anc &&
+           particles == o.particles && std::equal(threads, threads + kClasses, o.threads);
+  }
+};
+
+}  // namespace
+
+struct GpuBpfBatch {
+  int device = 0;
+  int B = 0;
+  float ess_threshold = 0.0f;
+  int sms = 0;
+  BatchFilterDev* d_filters = nullptr;
+  int* d_order = nullptr;
+  int* d_counters = nullptr;
+  float* d_hfinal = nullptr;
+  int* d_resamples = nullptr;
+  double* d_loglik = nullptr;
+  float* d_y = nullptr;
+  int y_cap = 0;
+  int class_off[kClasses] = {0, 0, 0, 0, 0};
+  int class_cnt[kClasses] = {0, 0, 0, 0, 0};
+  int threads[kClasses];
+  int grid[kClasses] = {1, 1, 1, 1, 1};
+  cudaStream_t stream = nullptr;
+  cudaStream_t cls_stream[kClasses] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kClasses] = {};
+  cudaGraphExec_t graph = nullptr;
+  GraphKey key;
+  std::vector<int> n_of;      // particle count per filter
+};
+
+namespace {
+
+void free_batch(GpuBpfBatch* b) {
+  if (!b) return;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  cudaFree(b->d_filters); cudaFree(b->d_order); cudaFree(b->d_counters);
+  cudaFree(b->d_hfinal); cudaFree(b->d_resamples); cudaFree(b->d_loglik); cudaFree(b->d_y);
+  for (int c = 0; c < kClasses; ++c) {
+    if (b->cls_stream[c]) cudaStreamDestroy(b->cls_stream[c]);
+    if (b->join[c]) cudaEventDestroy(b->join[c]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int class_of(int n) {
+  for (int c = 0; c < kClasses; ++c)
+    if (n <= kClassMaxN[c]) return c;
+  return -1;
+}
+
+BatchArgs class_args(GpuBpfBatch* b, int c, const float* y, int T, double* loglik, double* dll, float* hmean,
+                     int32_t* anc, float* particles) {
+  BatchArgs a{};
+  a.filters = b->d_filters;
+  a.order = b->d_order + b->class_off[c];
+  a.n_order = b->class_cnt[c];
+  a.counter = b->d_counters + c;
+  a.y = y;
+  a.T = T;
+  a.ess_threshold = b->ess_threshold;
+  a.loglik = loglik;
+  a.dll = dll;
+  a.hmean = hmean;
+  a.h_final = b->d_hfinal;
+  a.resamples = b->d_resamples;
+  a.anc = anc;
+  a.particles = particles;
+  return a;
+}
+
+// Grid of every class for its current CTA shape (sets the kernel attributes).
+void configure_classes(GpuBpfBatch* b) {
+  for (int c = 0; c < kClasses; ++c) {
+    const int occ = std::max(1, batch_occupancy(b->threads[c], kClassMaxN[c]));
+    b->grid[c] = std::max(1, std::min(b->class_cnt[c], b->sms * occ));
+  }
+}
+
+// Enqueue one run: zero the work counters, fork the classes (largest first),
+// join them back onto the batch stream.
+cudaError_t enqueue_run(GpuBpfBatch* b, const float* y, int T, double* loglik, double* dll, float* hmean,
+                        int32_t* anc, float* particles, int only_class = -1) {
+  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, kClasses * sizeof(int), b->stream);
+  if (e != cudaSuccess) return e;
+  e = cudaEventRecord(b->fork, b->stream);
+  if (e != cudaSuccess) return e;
+  for (int c = kClasses - 1; c >= 0; --c) {
+    if (!b->class_cnt[c] || (only_class >= 0 && c != only_class)) continue;
+    e = cudaStreamWaitEvent(b->cls_stream[c], b->fork, 0);
+    if (e == cudaSuccess)
+      e = launch_batch_class(class_args(b, c, y, T, loglik, dll, hmean, anc, particles), b->threads[c],
+                             kClassMaxN[c], b->grid[c], b->cls_stream[c]);
+    if (e == cudaSuccess) e = cudaEventRecord(b->join[c], b->cls_stream[c]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[c], 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int ensure_device_b(GpuBpfBatch* b) {
+  int cur = -1;
+  BCK(cudaGetDevice(&cur));
+  if (cur != b->device) BCK(cudaSetDevice(b->device));
+  return BPF_OK;
+}
+
+std::string gpu_key(int device) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return "unknown";
+  std::string s = p.name;
+  for (char& ch : s) if (ch == ' ' || ch == '"') ch = '_';
+  return s + "_sm" + std::to_string(p.multiProcessorCount);
+}
+
+// Autotune cache: one line per entry, "<gpu_key> <class> <threads>".
+bool cache_lookup(const char* path, const std::string& key, int cls, int* threads) {
+  if (!path) return false;
+  std::ifstream in(path);
+  std::string k;
+  int c, t;
+  bool found = false;
+  while (in >> k >> c >> t)
+    if (k == key && c == cls) { *threads = t; found = true; }
+  return found;
+}
+void cache_store(const char* path, const std::string& key, int cls, int threads) {
+  if (!path) return;
+  std::ofstream out(path, std::ios::app);
+  out << key << " " << cls << " " << threads << "\n";
+}
+
+}  // namespace
+
+extern "C" {
+
+GpuBpfBatch* gpu_bpf_batch_create(const BpfBatchFilter* filters, int n_filters, float ess_threshold) {
+  if (!filters || n_filters <= 0 || std::isnan(ess_threshold)) { bpf_record_error(BPF_ERR_ARG); return nullptr; }
+  std::vector<BatchFilterDev> tab(n_filters);
+  for (int i = 0; i < n_filters; ++i) {
+    const BpfBatchFilter& f = filters[i];
+    if (f.n_particles <= 0 || f.n_particles > kBatchMaxN || !std::isfinite(f.mu) || !std::isfinite(f.rho) ||
+        !std::isfinite(f.sigma_z) || !(std::fabs(f.rho) < 1.0f) || !(f.sigma_z > 0.0f) || !std::isfinite(f.nu_obs) ||
+        !(f.nu_obs >= 0.0f)) {
+      bpf_record_error(BPF_ERR_ARG);
+      return nullptr;
+    }
+    BatchFilterDev& d = tab[i];
+    d = BatchFilterDev{};
+    d.mu = f.mu; d.rho = f.rho; d.sigma = f.sigma_z;
+    d.std_stat = sqrtf((f.sigma_z * f.sigma_z) / fmaxf(1.0f - f.rho * f.rho, 1e-6f));   // gpu_bpf_ptx_full.cu:430
+    d.nu = f.nu_obs;
+    if (f.nu_obs > 0.0f) {
+      d.c_obs = (float)(std::lgamma((f.nu_obs + 1.0) / 2.0) - std::lgamma(f.nu_obs / 2.0) -
+                        0.5 * std::log(f.nu_obs * 3.14159265358979323846));
+      d.inv_nu = 1.0f / f.nu_obs;
+      d.nu_p1h = (f.nu_obs + 1.0f) * 0.5f;
+    }
+    d.n = f.n_particles;
+    d.seed = f.seed;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); bpf_record_error(BPF_ERR_NODEVICE); return nullptr; }
+
+  GpuBpfBatch* b = new GpuBpfBatch();
+  b->B = n_filters;
+  b->ess_threshold = ess_threshold;
+  std::copy(kDefaultThreads, kDefaultThreads + kClasses, b->threads);
+  b->n_of.resize(n_filters);
+  for (int i = 0; i < n_filters; ++i) b->n_of[i] = tab[i].n;
+  // LPT order inside each class: largest N first
+  std::vector<int> order(n_filters);
+  for (int i = 0; i < n_filters; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const int cx = class_of(tab[x].n), cy = class_of(tab[y].n);
+    if (cx != cy) return cx < cy;
+    return tab[x].n > tab[y].n;
+  });
+  for (int i = 0; i < n_filters; ++i) b->class_cnt[class_of(tab[order[i]].n)]++;
+  for (int c = 1; c < kClasses; ++c) b->class_off[c] = b->class_off[c - 1] + b->class_cnt[c - 1];
+
+  auto fail = [&](int code) { free_batch(b); bpf_record_error(code); return (GpuBpfBatch*)nullptr; };
+  if (cudaGetDevice(&b->device) != cudaSuccess) return fail(BPF_ERR_CUDA);
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(BPF_ERR_CUDA);
+  for (int c = 0; c < kClasses; ++c) {
+    if (cudaStreamCreateWithFlags(&b->cls_stream[c], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join[c], cudaEventDisableTiming) != cudaSuccess)
+      return fail(BPF_ERR_CUDA);
+  }
+  if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return fail(BPF_ERR_CUDA);
+  if (cudaMalloc(&b->d_filters, n_filters * sizeof(BatchFilterDev)) != cudaSuccess ||
+      cudaMalloc(&b->d_order, n_filters * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_counters, kClasses * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_hfinal, n_filters * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&b->d_resamples, n_filters * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_loglik, n_filters * sizeof(double)) != cudaSuccess)
+    return fail(BPF_ERR_ALLOC);
+  if (cudaMemcpy(b->d_filters, tab.data(), n_filters * sizeof(BatchFilterDev), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_order, order.data(), n_filters * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(BPF_ERR_CUDA);
+  configure_classes(b);
+  return b;
+}
+
+void gpu_bpf_batch_destroy(GpuBpfBatch* b) {
+  if (!b) return;
+  ensure_device_b(b);
+  cudaStreamSynchronize(b->stream);
+  free_batch(b);
+}
+
+void* gpu_bpf_batch_stream(GpuBpfBatch* b) { return b ? (void*)b->stream : nullptr; }
+
+int gpu_bpf_batch_size_class(int n_particles) { return class_of(n_particles); }
+
+int gpu_bpf_batch_set_threads(GpuBpfBatch* b, int size_class, int threads) {
+  if (!b || size_class < 0 || size_class >= kClasses) return bpf_record_error(BPF_ERR_ARG);
+  bool ok = false;
+  for (int t : kThreadChoices) ok |= (t == threads);
+  if (!ok) return bpf_record_error(BPF_ERR_ARG);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  if (batch_occupancy(threads, kClassMaxN[size_class]) < 1) return bpf_record_error(BPF_ERR_UNSUPPORTED);
+  b->threads[size_class] = threads;
+  configure_classes(b);
+  return BPF_OK;
+}
+
+int gpu_bpf_batch_get_threads(GpuBpfBatch* b, int size_class) {
+  if (!b || size_class < 0 || size_class >= kClasses) return -bpf_record_error(BPF_ERR_ARG);
+  return b->threads[size_class];
+}
+
+int gpu_bpf_batch_run_device(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* loglik_dev, double* dll_dev,
+                             float* hmean_dev) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  if (n_ticks <= 0 || !y_dev || !loglik_dev) return bpf_record_error(BPF_ERR_ARG);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  GraphKey k;
+  k.y = y_dev; k.T = n_ticks; k.loglik = loglik_dev; k.dll = dll_dev; k.hmean = hmean_dev;
+  std::copy(b->threads, b->threads + kClasses, k.threads);
+  if (!b->graph || !(k == b->key)) {
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_run(b, y_dev, n_ticks, loglik_dev, dll_dev, hmean_dev, nullptr, nullptr);
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->graph = nullptr; cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
+    b->key = k;
+  }
+  BCK(cudaGraphLaunch(b->graph, b->stream));
+  bpf_note_launches(kClasses);
+  return BPF_OK;
+}
+
+int gpu_bpf_batch_run(GpuBpfBatch* b, const float* y, int n_ticks, double* loglik_out, float* hmean_last_out) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  if (n_ticks <= 0 || !y || !loglik_out) return bpf_record_error(BPF_ERR_ARG);
+  for (int t = 0; t < n_ticks; ++t) if (!std::isfinite(y[t])) return bpf_record_error(BPF_ERR_ARG);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  if (b->y_cap < n_ticks) {
+    cudaFree(b->d_y);
+    b->d_y = nullptr;
+    b->y_cap = 0;
+    BCK(cudaMalloc(&b->d_y, n_ticks * sizeof(float)));
+    b->y_cap = n_ticks;
+  }
+  BCK(cudaMemcpyAsync(b->d_y, y, n_ticks * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+  rc = gpu_bpf_batch_run_device(b, b->d_y, n_ticks, b->d_loglik, nullptr, nullptr);
+  if (rc) return rc;
+  BCK(cudaMemcpyAsync(loglik_out, b->d_loglik, b->B * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  if (hmean_last_out)
+    BCK(cudaMemcpyAsync(hmean_last_out, b->d_hfinal, b->B * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return BPF_OK;
+}
+
+int gpu_bpf_batch_run_debug(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* loglik_dev, double* dll_dev,
+                            int32_t* anc_dev, float* particles_dev) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  if (n_ticks <= 0 || !y_dev || !loglik_dev) return bpf_record_error(BPF_ERR_ARG);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  BCK(enqueue_run(b, y_dev, n_ticks, loglik_dev, dll_dev, nullptr, anc_dev, particles_dev));
+  bpf_note_launches(kClasses);
+  return BPF_OK;
+}
+
+int gpu_bpf_batch_resample_counts(GpuBpfBatch* b, int* counts_out, float* hmean_last_out) {
+  if (!b || !counts_out) return bpf_record_error(BPF_ERR_ARG);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  BCK(cudaMemcpyAsync(counts_out, b->d_resamples, b->B * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  if (hmean_last_out)
+    BCK(cudaMemcpyAsync(hmean_last_out, b->d_hfinal, b->B * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return BPF_OK;
+}
+
+int gpu_bpf_batch_autotune(GpuBpfBatch* b, const float* y, int n_ticks, const char* cache_path) {
+  if (!b || !y || n_ticks <= 0) return bpf_record_error(BPF_ERR_ARG);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  const std::string key = gpu_key(b->device);
+  float* d_y = nullptr;
+  double* d_ll = nullptr;
+  BCK(cudaMalloc(&d_y, n_ticks * sizeof(float)));
+  if (cudaMalloc(&d_ll, b->B * sizeof(double)) != cudaSuccess) { cudaFree(d_y); return bpf_record_error(BPF_ERR_ALLOC); }
+  cudaMemcpy(d_y, y, n_ticks * sizeof(float), cudaMemcpyHostToDevice);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int result = BPF_OK;
+  for (int c = 0; c < kClasses && result == BPF_OK; ++c) {
+    if (!b->class_cnt[c]) continue;
+    int cached = 0;
+    if (cache_lookup(cache_path, key, c, &cached)) { b->threads[c] = cached; continue; }
+    float best_ms = 1e30f;
+    int best = b->threads[c];
+    for (int t : kThreadChoices) {
+      if (t > 4 * kClassMaxN[c] || batch_occupancy(t, kClassMaxN[c]) < 1) continue;
+      b->threads[c] = t;
+      configure_classes(b);
+      float ms_min = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {   // first repetition warms up
+        cudaEventRecord(e0, b->stream);
+        if (enqueue_run(b, d_y, n_ticks, d_ll, nullptr, nullptr, nullptr, nullptr, c) != cudaSuccess) {
+          result = bpf_record_error(BPF_ERR_CUDA);
+          break;
+        }
+        cudaEventRecord(e1, b->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep) ms_min = std::min(ms_min, ms);
+      }
+      if (result != BPF_OK) break;
+      if (ms_min < best_ms) { best_ms = ms_min; best = t; }
+    }
+    b->threads[c] = best;
+    configure_classes(b);
+    if (result == BPF_OK) cache_store(cache_path, key, c, best);
+  }
+  configure_classes(b);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_y);
+  cudaFree(d_ll);
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  return result;
+}
+
+}  // extern "C"

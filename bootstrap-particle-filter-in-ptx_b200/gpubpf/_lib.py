@@ -55,6 +55,11 @@ class GpuBpfState(C.Structure):
     ]
 
 
+class BpfBatchFilter(C.Structure):
+    _fields_ = [("mu", C.c_float), ("rho", C.c_float), ("sigma_z", C.c_float), ("nu_obs", C.c_float),
+                ("n_particles", C.c_int), ("seed", C.c_int)]
+
+
 P_STATE = C.POINTER(GpuBpfState)
 _f = C.c_float
 _i = C.c_int
@@ -101,6 +106,18 @@ SIGNATURES = {
                                   C.POINTER(_i)]),
     "gpu_bpf_launch_count": (C.c_longlong, []),
     "gpu_bpf_run_static": (_i, [_i, _f, _f, _f, _f, _i, _f, _vp, _i, _vp, _vp]),
+    # batched filters
+    "gpu_bpf_batch_create": (_vp, [C.POINTER(BpfBatchFilter), _i, _f]),
+    "gpu_bpf_batch_destroy": (None, [_vp]),
+    "gpu_bpf_batch_stream": (_vp, [_vp]),
+    "gpu_bpf_batch_size_class": (_i, [_i]),
+    "gpu_bpf_batch_set_threads": (_i, [_vp, _i, _i]),
+    "gpu_bpf_batch_get_threads": (_i, [_vp, _i]),
+    "gpu_bpf_batch_autotune": (_i, [_vp, C.POINTER(_f), _i, C.c_char_p]),
+    "gpu_bpf_batch_run": (_i, [_vp, C.POINTER(_f), _i, C.POINTER(_d), C.POINTER(_f)]),
+    "gpu_bpf_batch_run_device": (_i, [_vp, _vp, _i, _vp, _vp, _vp]),
+    "gpu_bpf_batch_run_debug": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp]),
+    "gpu_bpf_batch_resample_counts": (_i, [_vp, C.POINTER(_i), C.POINTER(_f)]),
     "gpu_bpf_debug_pcg32": (_i, [_i, _i, _i, C.POINTER(C.c_uint32)]),
     "gpu_bpf_debug_normals": (_i, [_i, _i, _i, C.POINTER(_f)]),
 }

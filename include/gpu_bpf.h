@@ -226,6 +226,50 @@ int gpu_bpf_run_static(int n_particles, float rho, float sigma_z, float mu, floa
                        float ess_threshold, const float* y_dev, int n_ticks, BpfTickRecord* rec_dev,
                        void* stream);
 
+/* ---- Batched filters (addition) -------------------------------------------
+ * Many independent SV filters with their own (mu, rho, sigma_z, nu_obs), particle count
+ * (1..16384) and seed, all on one observation series: the SMC^2 / PMMH inner loop. The
+ * reference runs such filters one per CUDA stream (the IMM pattern, gpu_bpf/gpu_bpf.cu:1033-1047)
+ * or as its own per-theta RBPF CTA (smc2/smc2_rbpf_batch.cu:248-398). Here every filter keeps its
+ * particles in one CTA's shared memory for the whole run; filters are grouped into five size
+ * classes (N <= 1024, 2048, 4096, 8192, 16384), each class is one persistent launch pulling
+ * filters largest-first, and a run is replayed as one CUDA graph. A batched filter computes the
+ * same per-particle arithmetic and the same fixed-point resampling as gpu_bpf_create with the
+ * same parameters and seed. */
+typedef struct {
+    float mu, rho, sigma_z, nu_obs;
+    int   n_particles;
+    int   seed;
+} BpfBatchFilter;
+typedef struct GpuBpfBatch GpuBpfBatch;
+
+/* ess_threshold as gpu_bpf_set_ess_threshold (0 = resample every tick). NULL on error. */
+GpuBpfBatch* gpu_bpf_batch_create(const BpfBatchFilter* filters, int n_filters, float ess_threshold);
+void         gpu_bpf_batch_destroy(GpuBpfBatch* batch);
+void*        gpu_bpf_batch_stream(GpuBpfBatch* batch);          /* cudaStream_t of the batch */
+int          gpu_bpf_batch_size_class(int n_particles);         /* 0..4, or -1 if above 16384 */
+/* Threads per CTA (64, 128, 256, 512, 1024) of one size class: the tile shape. */
+int          gpu_bpf_batch_set_threads(GpuBpfBatch* batch, int size_class, int threads);
+int          gpu_bpf_batch_get_threads(GpuBpfBatch* batch, int size_class);
+/* Project autotuner: times every CTA shape of every non-empty class on n_ticks of y and keeps
+ * the fastest; results are appended to / read from the text cache file cache_path
+ * ("<gpu> <class> <threads>" lines; NULL = no cache). */
+int          gpu_bpf_batch_autotune(GpuBpfBatch* batch, const float* y, int n_ticks, const char* cache_path);
+/* Host buffers: y[n_ticks] in, loglik[n_filters] (FP64 total log-likelihood) and optionally the
+ * last tick's filtered mean out. Synchronous. */
+int          gpu_bpf_batch_run(GpuBpfBatch* batch, const float* y, int n_ticks, double* loglik,
+                               float* hmean_last);
+/* Device buffers, enqueued on the batch stream: loglik_dev[n_filters]; dll_dev[n_filters*n_ticks]
+ * per-tick increments and hmean_dev[n_filters*n_ticks] filtered means (either may be NULL). */
+int          gpu_bpf_batch_run_device(GpuBpfBatch* batch, const float* y_dev, int n_ticks, double* loglik_dev,
+                                      double* dll_dev, float* hmean_dev);
+/* Testing aid: as run_device without a graph, also writing every tick's ancestors
+ * (anc_dev[(f*n_ticks + t)*16384 + i]) and the final particles (particles_dev[f*16384 + i]). */
+int          gpu_bpf_batch_run_debug(GpuBpfBatch* batch, const float* y_dev, int n_ticks, double* loglik_dev,
+                                     double* dll_dev, int32_t* anc_dev, float* particles_dev);
+/* Resampling count and last filtered mean of every filter after a run (waits). */
+int          gpu_bpf_batch_resample_counts(GpuBpfBatch* batch, int* counts, float* hmean_last);
+
 /* Number of kernel launches this library has issued (all filters). */
 long long gpu_bpf_launch_count(void);
 
