@@ -53,6 +53,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-filters", type=int, default=1024)
+    ap.add_argument("--batch-ticks", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -133,6 +136,74 @@ def cpu_baseline(n, y, ess, seconds, native=True):
             "sample": f"N={n}, first {ticks} ticks of the DGP-seed-7 series, ESS<{ess}N; oracle/bpf_oracle.c "
                       f"orc_ref_run (FP32 reference tick loop, OpenMP {cores} threads, -O3 -march=native)",
             "us_per_tick": dt / ticks * 1e6}
+
+
+def bench_batched(dev, args, lib, rank, world, barrier):
+    """Configuration 4: B=1024 filters, theta and N drawn as in gpubpf.configs, T=2000 ticks of one
+    series (mu=-1, phi=0.97, sigma_eta=0.2, DGP seed 42), resampling every tick. Filters are sharded
+    across ranks by LPT on N. Comparator: the plain filter run per filter, each replaying its own
+    CUDA graph on its own stream (all concurrent), on every 16th filter of this rank's shard."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gpubpf
+    from gpubpf import configs, dgp, parallel
+    B, T = args.batch_filters, args.batch_ticks
+    allf = configs.config4(B)
+    idx, fl = parallel.shard(allf, rank, world)
+    _, ys = dgp.matched_series(T, 0.97, 0.2, -1.0, 42)
+    y = np.asarray(ys, dtype=np.float32)
+    y_d = torch.tensor(y, device=dev)
+    steps_local = float(sum(f["n_particles"] for f in fl)) * T
+    steps_total = float(sum(f["n_particles"] for f in allf)) * T
+    b = gpubpf.GpuBpfBatch(fl, ess_threshold=0.0)
+    b.autotune(y[:64].tolist())
+    shapes = [b.get_threads(c) for c in range(5)]
+    ll = torch.zeros(len(fl), dtype=torch.float64, device=dev)
+    bs = torch.cuda.ExternalStream(b.stream, device=dev)
+    for _ in range(3):
+        b.run_device(y_d.data_ptr(), T, ll.data_ptr())
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = max(1, args.steps)
+    e0.record(bs)
+    for _ in range(reps):
+        b.run_device(y_d.data_ptr(), T, ll.data_ptr())
+    e1.record(bs)
+    barrier()
+    ms = torch.tensor([e0.elapsed_time(e1) / reps], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    value = steps_total / (ms / 1e3)
+    finite = bool(torch.isfinite(ll).all().item())
+    b.close()
+
+    # comparator: per-filter plain launches (graph per filter, one stream each)
+    sub = fl[::16]
+    filt = [gpubpf.GpuBpf(f["n_particles"], f["rho"], f["sigma_z"], f["mu"], 0.0, 0.0, f["seed"], ess_threshold=0.0)
+            for f in sub]
+    recs = [torch.zeros(T * RECORD_BYTES, dtype=torch.uint8, device=dev) for _ in sub]
+    for g, r in zip(filt, recs):
+        g.step_many_device(y_d.data_ptr(), T, r.data_ptr())      # builds each filter's graph
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for g, f, r in zip(filt, sub, recs):
+        g.reset(f["seed"])
+        g.step_many_device(y_d.data_ptr(), T, r.data_ptr())
+    torch.cuda.synchronize(dev)
+    dt = time.perf_counter() - t0
+    per_filter = float(sum(f["n_particles"] for f in sub)) * T / dt
+    for g in filt:
+        g.close()
+    return {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "ms_per_run": ms, "filters": B, "ticks": T, "particle_steps_per_run": steps_total,
+            "shard": f"LPT on N over {world} rank(s)", "cta_threads_per_class": shapes,
+            "per_filter_plain": {"value": per_filter, "unit": "particle-steps/s", "filters_timed": len(sub),
+                                 "method": "gpu_bpf_step_many_device per filter, own stream, CUDA graph"},
+            "speedup_vs_per_filter": value / per_filter if world == 1 else None,
+            "loglik_finite": finite}
 
 
 def run_reference(args):
@@ -306,6 +377,9 @@ def main():
                "d2h_bytes_per_step": RECORD_BYTES * T + DEVSTATE_BYTES,
                "api": "gpu_bpf_reset + gpu_bpf_step_many(host y[T], host BpfResult[T], host BpfTickRecord[T])"}
 
+    f.close()
+    batched = None if args.no_batched else bench_batched(dev, args, lib, rank, world, barrier)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(N, y_host, args.ess, args.cpu_seconds)
@@ -328,9 +402,9 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
-    f.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

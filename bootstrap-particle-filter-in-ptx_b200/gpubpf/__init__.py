@@ -2,8 +2,8 @@
 
 Python face of libgpubpf.so (C ABI in include/gpu_bpf.h). The package
 directory is not importable by its hyphenated parent name; put
-``<repo>/bootstrap-particle-filter-in-ptx_b200`` on ``sys.path`` (see
-``gpubpf.paths``) and ``import gpubpf``.
+``<repo>/bootstrap-particle-filter-in-ptx_b200`` on ``sys.path`` and
+``import gpubpf``.
 """
 from ._lib import BpfError, BpfResult, BpfTickRecord, LIB_PATH, load  # noqa: F401
 from .filter import GpuBpf, debug_normals, debug_pcg32, run_rmse  # noqa: F401
