@@ -103,7 +103,7 @@ cudaError_t launch_tick3(Impl* m, const TickArgs& a) {
 }
 
 TickArgs make_args(GpuBpfState* s, Impl* m, float y, const float* y_ptr, BpfTickRecord* rec) {
-  TickArgs a;
+  TickArgs a{};
   a.mu = s->mu; a.rho = s->rho; a.sigma = s->sigma_z;
   a.ess_threshold = s->ess_threshold;
   a.log_n = std::log((double)m->plan.N);
@@ -192,10 +192,7 @@ int free_impl(Impl* m) {
   if (m->dgraph) cudaGraphExecDestroy(m->dgraph);
   for (cudaEvent_t e : m->ev_pending) cudaEventDestroy(e);
   for (cudaEvent_t e : m->ev_pool) cudaEventDestroy(e);
-  Plan& p = m->plan;
-  cudaFree(p.h0); cudaFree(p.h1); cudaFree(p.w);
-  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.rec);
-  cudaFree(p.P); cudaFree(p.ofirst); cudaFree(p.items); cudaFree(p.st);
+  plan_free(m->plan);
   cudaFree(m->rec_dev); cudaFree(m->y_dev); cudaFree(m->anc_dev);
   cudaFreeHost(m->rec_pin); cudaFreeHost(m->st_pin); cudaFreeHost(m->y_pin);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -282,27 +279,13 @@ static int create_impl(GpuBpfState* s, Impl* m, int n, float rho, float sigma_z,
   CK(cudaGetDevice(&m->device));
   m->seed = seed;
   Plan& p = m->plan;
-  p.N = n;
-  p.G = (n + kTile - 1) / kTile;
-  p.max_items = p.G + (n + kOutChunk - 1) / kOutChunk + 1;
-  const size_t npad = (size_t)p.G * kTile;
   CK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
-  CK(cudaMalloc(&p.h0, npad * sizeof(float)));
-  CK(cudaMalloc(&p.h1, npad * sizeof(float)));
-  CK(cudaMalloc(&p.w, npad * sizeof(float)));
-  CK(cudaMalloc(&p.nexp, p.G * sizeof(int)));
-  CK(cudaMalloc(&p.E, p.G * sizeof(unsigned long long)));
-  CK(cudaMalloc(&p.rec, p.G * sizeof(float4)));
-  CK(cudaMalloc(&p.P, p.G * sizeof(unsigned long long)));
-  CK(cudaMalloc(&p.ofirst, (p.G + 1) * sizeof(int)));
-  CK(cudaMalloc(&p.items, p.max_items * sizeof(int4)));
-  CK(cudaMalloc(&p.st, sizeof(DevState)));
+  CK(plan_alloc(p, n));
   CK(cudaMalloc(&m->rec_dev, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
   CK(cudaMalloc(&m->y_dev, kGraphChunk * sizeof(float)));
   CK(cudaMallocHost(&m->rec_pin, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
   CK(cudaMallocHost(&m->st_pin, sizeof(DevState)));
   CK(cudaMallocHost(&m->y_pin, kGraphChunk * sizeof(float)));
-  CK(cudaMemsetAsync(p.nexp, 0, p.G * sizeof(int), m->stream));
   CK(cudaMemsetAsync(m->rec_dev, 0, (1 + kGraphChunk) * sizeof(BpfTickRecord), m->stream));
   m->pass2_grid = pass2_grid_size(m->device);
   if (const char* v = std::getenv("BPF_DISABLE_PDL")) m->pdl = (v[0] == '0');

@@ -103,6 +103,10 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     if (carry) w4[r] = *reinterpret_cast<const float4*>(p.w + i0);
     else w4[r] = make_float4(1.f, 1.f, 1.f, 1.f);
   }
+  if (a.ckpt) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) *reinterpret_cast<float4*>(a.ckpt + tile0 + 4 * (tid + kThreads * r)) = h4[r];
+  }
 
   float x[kPerThread], hv[kPerThread];
   const unsigned long long step2 = 2ull * c.k2;
@@ -285,6 +289,8 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     const double ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
     st->ll_ref = ll_ref;
     st->ll_total += dll;
+    if (a.aux) *a.aux = degenerate ? make_float2(0.0f, __int_as_float(0))
+                                   : make_float2((float)(1.0 / tS), __int_as_float(nM));
     if (a.rec) {
       BpfTickRecord r;
       r.dloglik = dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
@@ -373,7 +379,9 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   __syncthreads();
   const unsigned long long base = sh.b_base, delta = sh.b_delta, magic = sh.b_magic;
 
-  // 5. per tile: prefix, first output index, number of work items
+  // 5. per tile: prefix, first output index, number of work items (a taped
+  //    run gives every tile an item, so pass 2 writes every parent's first child)
+  const int min_items = a.csr ? 1 : 0;
   unsigned long long run = excl;
   int o = targets_below(run, base, delta, magic, N);
   int n_it = 0;
@@ -382,19 +390,24 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     o_s[k] = o;
     run += ehat(k);
     const int o_next = targets_below(run, base, delta, magic, N);
-    n_it += (o_next - o + kOutChunk - 1) / kOutChunk;
+    n_it += max((o_next - o + kOutChunk - 1) / kOutChunk, min_items);
     o = o_next;
   }
   const int o_end = o;     // first output of the next thread's first tile (N for the last)
   int n_items_total;
   const int it0 = block_excl_scan_add<kPlanThreads>(n_it, &n_items_total, sh.scan_i);
 
-  // 6. work items (tile, first output, end output); heavy tiles are split
+  // 6. work items (tile, first output, end output, first item of the tile);
+  //    heavy tiles are split
   int ib = it0;
   for (int k = k0; k < k1; ++k) {
     const int o0 = o_s[k];
     const int o1 = (k + 1 < k1) ? o_s[k + 1] : o_end;
-    for (int oo = o0; oo < o1; oo += kOutChunk) p.items[ib++] = make_int4(k, oo, min(o1, oo + kOutChunk), 0);
+    const int ni = max((o1 - o0 + kOutChunk - 1) / kOutChunk, min_items);
+    for (int u = 0; u < ni; ++u) {
+      const int oo = o0 + u * kOutChunk;
+      p.items[ib++] = make_int4(k, oo, min(o1, oo + kOutChunk), u == 0);
+    }
   }
   if (tid == 0) st->n_items = n_items_total;
   store_state();
@@ -488,9 +501,11 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
     const int lane = tid & 31;
     int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
     unsigned long long tq = base + (unsigned long long)q * delta;
+    int32_t* csr = (a.csr && item.w) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
 #pragma unroll
     for (int e = 0; e < kPerThread; ++e) {
       const int j = tid * kPerThread + e;
+      if (csr && j < nA) csr[j] = q;
       const unsigned long long cj = Pk + shr64(excl + L[e], r);
       int lo = 0, hi = 0;
       if (j < nA && q < N && tq < cj) {
@@ -564,6 +579,35 @@ static cudaError_t launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size
   cfg.attrs = pdl ? attr : nullptr;
   cfg.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+cudaError_t plan_alloc(Plan& p, int N) {
+  p.N = N;
+  p.G = (N + kTile - 1) / kTile;
+  p.max_items = p.G + (N + kOutChunk - 1) / kOutChunk + 1;
+  const size_t npad = (size_t)p.G * kTile;
+  cudaError_t e = cudaSuccess;
+  auto al = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(ptr, bytes); };
+  al(&p.h0, npad * sizeof(float));
+  al(&p.h1, npad * sizeof(float));
+  al(&p.w, npad * sizeof(float));
+  al(&p.nexp, p.G * sizeof(int));
+  al(&p.E, p.G * sizeof(unsigned long long));
+  al(&p.rec, p.G * sizeof(float4));
+  al(&p.P, p.G * sizeof(unsigned long long));
+  al(&p.ofirst, (p.G + 1) * sizeof(int));
+  al(&p.items, p.max_items * sizeof(int4));
+  al(&p.st, sizeof(DevState));
+  if (e == cudaSuccess) e = cudaMemset(p.nexp, 0, p.G * sizeof(int));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();   // visible to every stream before first use
+  return e;
+}
+
+void plan_free(Plan& p) {
+  cudaFree(p.h0); cudaFree(p.h1); cudaFree(p.w);
+  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.rec);
+  cudaFree(p.P); cudaFree(p.ofirst); cudaFree(p.items); cudaFree(p.st);
+  p = Plan{};
 }
 
 cudaError_t launch_init(const Plan& p, float mu, float std_stat, int seed, cudaStream_t s) {

@@ -61,7 +61,15 @@ struct TickArgs {
   const float* y_ptr;        // device pointer to this tick's observation, or null
   BpfTickRecord* rec;        // device record slot written by the last pass-1 CTA
   int32_t* anc;              // ancestors of this tick (N ints) or null
+  // gradient tape (all null outside a taped run)
+  float* ckpt;               // copy of the particles pass 1 reads this tick (G*4096 floats) or null
+  int32_t* csr;              // on resampling ticks: first child slot of every parent (N ints) or null
+  float2* aux;               // {1/S, nM}: normalised weight W_i = 2^(x_i - nM) / S of this tick, or null
 };
+
+// Device buffers of a plan for N particles (G, max_items set; DevState included).
+cudaError_t plan_alloc(Plan& p, int N);
+void plan_free(Plan& p);
 
 // Host-side launchers (stream-ordered, no synchronisation).
 // Draws h_0 for `seed` and (re)initialises the DevState on the device.

@@ -118,6 +118,17 @@ SIGNATURES = {
     "gpu_bpf_batch_run_device": (_i, [_vp, _vp, _i, _vp, _vp, _vp]),
     "gpu_bpf_batch_run_debug": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp]),
     "gpu_bpf_batch_resample_counts": (_i, [_vp, C.POINTER(_i), C.POINTER(_f)]),
+    # gradient
+    "gpu_bpf_grad_create": (_vp, [_i, _i, _i]),
+    "gpu_bpf_grad_destroy": (None, [_vp]),
+    "gpu_bpf_grad_tape_bytes": (C.c_size_t, [_i, _i, _i]),
+    "gpu_bpf_grad_stream": (_vp, [_vp]),
+    "gpu_bpf_grad_checkpoint_every": (_i, [_vp]),
+    "gpu_bpf_grad_forward": (_i, [_vp, _f, _f, _f, _f, _i, _f, _vp, _i, _vp]),
+    "gpu_bpf_grad_backward": (_i, [_vp, _vp]),
+    "gpu_bpf_grad_replay": (_i, [_vp, _d, _d, _d, _vp, _vp]),
+    "gpu_bpf_grad_get_records": (_i, [_vp, C.POINTER(BpfTickRecord), _i]),
+    "gpu_bpf_grad_get_children": (_i, [_vp, _i, C.POINTER(C.c_int32)]),
     "gpu_bpf_debug_pcg32": (_i, [_i, _i, _i, C.POINTER(C.c_uint32)]),
     "gpu_bpf_debug_normals": (_i, [_i, _i, _i, C.POINTER(_f)]),
 }

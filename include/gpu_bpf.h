@@ -270,6 +270,43 @@ int          gpu_bpf_batch_run_debug(GpuBpfBatch* batch, const float* y_dev, int
 /* Resampling count and last filtered mean of every filter after a run (waits). */
 int          gpu_bpf_batch_resample_counts(GpuBpfBatch* batch, int* counts, float* hmean_last);
 
+/* ---- Gradient (addition) ---------------------------------------------------
+ * d loglik / d(mu, rho, sigma_z) of the plain filter with the resampling ancestors held fixed.
+ * The reference differentiates the same loss by autograd with detached resampling indices
+ * (tests/diff_bpf.py:186-237, :35-56, :230-231); here a taped forward run stores, per tick, the
+ * first child slot of every parent (systematic ancestors are non-decreasing, so a parent's
+ * children are a contiguous run of slots) and a checkpoint of the particles every
+ * checkpoint_every ticks; the backward pass recomputes each segment's particles from its
+ * checkpoint, the child lists and the counter-based PCG32 noise, and runs the adjoint
+ *   lambda_t,j = W_t,j dlogp(y_t|h)/dh (h_t,j) + rho * sum_{children i of j} lambda_t+1,i
+ * backward through it, accumulating the parameter adjoints (including the stationary initial
+ * draw) in FP64. Tapes resample every tick (ess_threshold 0, the reference's diff_bpf choice). */
+typedef struct GpuBpfGrad GpuBpfGrad;
+
+/* Tape for up to max_ticks ticks of n_particles (checkpoint_every 0 = 16). NULL on error.
+ * Device memory: gpu_bpf_grad_tape_bytes() (about 4 * n_particles * max_ticks bytes). */
+GpuBpfGrad* gpu_bpf_grad_create(int n_particles, int max_ticks, int checkpoint_every);
+void        gpu_bpf_grad_destroy(GpuBpfGrad* grad);
+size_t      gpu_bpf_grad_tape_bytes(int n_particles, int max_ticks, int checkpoint_every);
+void*       gpu_bpf_grad_stream(GpuBpfGrad* grad);                 /* cudaStream_t of the tape */
+int         gpu_bpf_grad_checkpoint_every(GpuBpfGrad* grad);
+/* Taped forward run from a fresh start (as gpu_bpf_create + reset(seed) + n_ticks steps):
+ * y_dev[n_ticks] in, loglik_dev[0] = FP64 total log-likelihood out. Enqueued on the tape's
+ * stream. ess_threshold must be 0 (BPF_ERR_UNSUPPORTED otherwise). */
+int gpu_bpf_grad_forward(GpuBpfGrad* grad, float mu, float rho, float sigma_z, float nu_obs, int seed,
+                         float ess_threshold, const float* y_dev, int n_ticks, double* loglik_dev);
+/* Adjoint of the last taped run: grad_dev[3] = d loglik / d(mu, rho, sigma_z), FP64. */
+int gpu_bpf_grad_backward(GpuBpfGrad* grad, double* grad_dev);
+/* FP64 re-run of the taped run's noise and ancestors at (mu, rho, sigma_z) with forward-mode
+ * tangents: out_dev[4] = {loglik, d/dmu, d/drho, d/dsigma_z}; per_tick_dev[4*n_ticks] (or NULL)
+ * the same per tick. For finite-difference checks under common random numbers. */
+int gpu_bpf_grad_replay(GpuBpfGrad* grad, double mu, double rho, double sigma_z, double* out_dev,
+                        double* per_tick_dev);
+/* Testing aids (wait for the tape's stream): the taped run's first n records, and the first
+ * child slot of every parent after tick `tick`'s resampling (host arrays). */
+int gpu_bpf_grad_get_records(GpuBpfGrad* grad, BpfTickRecord* out, int n);
+int gpu_bpf_grad_get_children(GpuBpfGrad* grad, int tick, int32_t* first_child);
+
 /* Number of kernel launches this library has issued (all filters). */
 long long gpu_bpf_launch_count(void);
 

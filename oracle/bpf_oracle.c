@@ -15,6 +15,10 @@
  *                        (erfc-based): the FP64 oracle's inverse normal CDF
  *   orc_filter_f64       FP64 filter in this build's semantics, optionally
  *                        replaying resampling decisions and ancestors
+ *   orc_grad_f64         d loglik / d(mu, rho, sigma) of the FP64 filter with the
+ *                        resampling ancestors held fixed (tests/diff_bpf.py:186-237
+ *                        with detached indices :35-56), forward-mode tangents or
+ *                        reverse-mode adjoint
  *   orc_resample_fixed   exact mirror of the GPU fixed-point systematic resampling
  *   orc_ref_run          FP32 restatement of the reference tick loop
  *                        (gpu_bpf_ptx_full.cu:340-771 with PTX kernels :51-842),
@@ -280,6 +284,127 @@ int orc_filter_f64(const OrcConfig* c, const float* y, int T,
     }
     free(h); free(hn); free(lw); free(lwc); free(cdf);
     return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Gradient with the ancestors held fixed                                     */
+/* ------------------------------------------------------------------------- */
+static double obs_dlogpdf_f64(double y, double h, double nu) {
+    double q = y * y * exp(-h);
+    if (nu > 0.0) return -0.5 + 0.5 * (nu + 1.0) * (q / nu) / (1.0 + q / nu);
+    return -0.5 + 0.5 * q;
+}
+
+static double slot_normal(int seed, int i, int t) {
+    return orc_icdf_f64((double)orc_uniform(orc_pcg32_draw_jump(seed, (uint32_t)i, t)));
+}
+
+/*
+ * Every tick resamples; anc[t][i] is the parent (a slot of tick t) of slot i of
+ * tick t+1. The loss is L = sum_t (LSE_t(lw) - ln N). Initial particles
+ * h_0 = mu + sigma z_0 / sqrt(max(1-rho^2, 1e-6)) are differentiated too.
+ * mode 0: forward-mode tangents dh/dtheta carried with the particles;
+ * mode 1: reverse mode, lambda_t,j = W_t,j g_t(h_t,j) + rho sum_{i: anc[t][i]=j} lambda_t+1,i.
+ * Outputs: *ll, grad[3], dll[T] (NULL allowed).
+ */
+int orc_grad_f64(int N, double mu, double rho, double sig, double nu, int seed, const float* y, int T,
+                 const int32_t* anc, int mode, double* ll, double* grad, double* dll) {
+    if (N <= 0 || T <= 0 || !anc) return 1;
+    const double cobs = c_obs_of(nu), logn = log((double)N);
+    const double one_m = 1.0 - rho * rho, s2 = fmax(one_m, 1e-6), sd = sqrt(s2);
+    const double sstat = sig / sd, dsr = one_m > 1e-6 ? sig * rho / (s2 * sd) : 0.0, dss = 1.0 / sd;
+    double* z0 = (double*)malloc(sizeof(double) * N);
+    double* lw = (double*)malloc(sizeof(double) * N);
+    if (!z0 || !lw) { free(z0); free(lw); return 2; }
+    for (int i = 0; i < N; ++i) z0[i] = slot_normal(seed, i, 0);
+    double L = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    int rc = 0;
+    if (mode == 0) {
+        double* st = (double*)malloc(sizeof(double) * 8 * (size_t)N);   /* h, d0, d1, d2 ping-pong */
+        if (!st) { rc = 2; goto out; }
+        double *h = st, *d0 = st + N, *d1 = st + 2 * N, *d2 = st + 3 * N;
+        double *hn = st + 4 * N, *e0 = st + 5 * N, *e1 = st + 6 * N, *e2 = st + 7 * N;
+        for (int i = 0; i < N; ++i) { h[i] = mu + sstat * z0[i]; d0[i] = 1.0; d1[i] = z0[i] * dsr; d2[i] = z0[i] * dss; }
+        for (int t = 0; t < T; ++t) {
+            if (t > 0) {
+                const int32_t* a = anc + (size_t)(t - 1) * N;
+                for (int i = 0; i < N; ++i) {
+                    const int p = a[i];
+                    const double eps = slot_normal(seed, i, t);
+                    hn[i] = mu + rho * (h[p] - mu) + sig * eps;
+                    e0[i] = (1.0 - rho) + rho * d0[p];
+                    e1[i] = (h[p] - mu) + rho * d1[p];
+                    e2[i] = eps + rho * d2[p];
+                }
+                double* tmp;
+                tmp = h; h = hn; hn = tmp; tmp = d0; d0 = e0; e0 = tmp;
+                tmp = d1; d1 = e1; e1 = tmp; tmp = d2; d2 = e2; e2 = tmp;
+            }
+            double M = -INFINITY;
+            for (int i = 0; i < N; ++i) { lw[i] = obs_logpdf_f64((double)y[t], h[i], nu, cobs); if (lw[i] > M) M = lw[i]; }
+            double S = 0.0, G0 = 0.0, G1 = 0.0, G2 = 0.0;
+            for (int i = 0; i < N; ++i) {
+                const double e = exp(lw[i] - M), g = obs_dlogpdf_f64((double)y[t], h[i], nu);
+                S += e; G0 += e * g * d0[i]; G1 += e * g * d1[i]; G2 += e * g * d2[i];
+            }
+            const double d = M + log(S) - logn;
+            if (dll) dll[t] = d;
+            L += d; g0 += G0 / S; g1 += G1 / S; g2 += G2 / S;
+        }
+        free(st);
+    } else {
+        double* H = (double*)malloc(sizeof(double) * (size_t)T * N);
+        double* lse = (double*)malloc(sizeof(double) * T);
+        double* lam = (double*)calloc((size_t)N, sizeof(double));
+        double* lamn = (double*)calloc((size_t)N, sizeof(double));
+        double* cs = (double*)malloc(sizeof(double) * N);
+        if (!H || !lse || !lam || !lamn || !cs) { free(H); free(lse); free(lam); free(lamn); free(cs); rc = 2; goto out; }
+        for (int i = 0; i < N; ++i) H[i] = mu + sstat * z0[i];
+        for (int t = 0; t < T; ++t) {
+            double* h = H + (size_t)t * N;
+            if (t > 0) {
+                const int32_t* a = anc + (size_t)(t - 1) * N;
+                const double* hp = H + (size_t)(t - 1) * N;
+                for (int i = 0; i < N; ++i) h[i] = mu + rho * (hp[a[i]] - mu) + sig * slot_normal(seed, i, t);
+            }
+            double M = -INFINITY, S = 0.0;
+            for (int i = 0; i < N; ++i) { lw[i] = obs_logpdf_f64((double)y[t], h[i], nu, cobs); if (lw[i] > M) M = lw[i]; }
+            for (int i = 0; i < N; ++i) S += exp(lw[i] - M);
+            lse[t] = M + log(S);
+            if (dll) dll[t] = lse[t] - logn;
+            L += lse[t] - logn;
+        }
+        double acs = 0.0, acsh = 0.0, aeps = 0.0;
+        for (int t = T - 1; t >= 0; --t) {
+            const double* h = H + (size_t)t * N;
+            for (int j = 0; j < N; ++j) cs[j] = 0.0;
+            if (t < T - 1) {
+                const int32_t* a = anc + (size_t)t * N;
+                for (int i = 0; i < N; ++i) {
+                    cs[a[i]] += lamn[i];
+                    aeps += lamn[i] * slot_normal(seed, i, t + 1);
+                }
+            }
+            for (int j = 0; j < N; ++j) {
+                const double W = exp(obs_logpdf_f64((double)y[t], h[j], nu, cobs) - lse[t]);
+                lam[j] = W * obs_dlogpdf_f64((double)y[t], h[j], nu) + rho * cs[j];
+                acs += cs[j];
+                acsh += cs[j] * (h[j] - mu);
+            }
+            double* tmp = lam; lam = lamn; lamn = tmp;
+        }
+        double al0 = 0.0, al0z = 0.0;
+        for (int j = 0; j < N; ++j) { al0 += lamn[j]; al0z += lamn[j] * z0[j]; }
+        g0 = (1.0 - rho) * acs + al0;
+        g1 = acsh + al0z * dsr;
+        g2 = aeps + al0z * dss;
+        free(H); free(lse); free(lam); free(lamn); free(cs);
+    }
+    if (ll) *ll = L;
+    if (grad) { grad[0] = g0; grad[1] = g1; grad[2] = g2; }
+out:
+    free(z0); free(lw);
+    return rc;
 }
 
 /* ------------------------------------------------------------------------- */

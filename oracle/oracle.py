@@ -75,6 +75,9 @@ def lib(native: bool = False) -> C.CDLL:
     L.orc_ref_run.argtypes = [C.c_int, f32, f32, f32, f32, C.c_int, f32, C.c_void_p, C.c_int,
                               C.c_void_p, C.c_void_p, C.c_int, P(C.c_int)]
     L.orc_num_threads.restype = C.c_int; L.orc_num_threads.argtypes = []
+    L.orc_grad_f64.restype = C.c_int
+    L.orc_grad_f64.argtypes = [C.c_int, f64, f64, f64, f64, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                               P(f64), C.c_void_p, C.c_void_p]
     _LIBS[key] = L
     return L
 
@@ -144,6 +147,25 @@ def ref_run(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.5, nu_obs
     if rc != 0:
         raise RuntimeError(f"orc_ref_run failed ({rc})")
     return hm, ll, cnt.value
+
+
+def grad_f64(n_particles, mu, rho, sigma_z, y, anc, seed=42, nu_obs=0.0, mode=1):
+    """FP64 loglik and d loglik / d(mu, rho, sigma_z) with ancestors anc[T][N] held fixed.
+
+    mode 0 = forward-mode tangents, 1 = reverse-mode adjoint. Returns (ll, grad[3], dll[T]).
+    """
+    L = lib()
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    T = y.shape[0]
+    anc = np.ascontiguousarray(anc, dtype=np.int32).reshape(T, int(n_particles))
+    ll = C.c_double(0.0)
+    grad = np.zeros(3, dtype=np.float64)
+    dll = np.zeros(T, dtype=np.float64)
+    rc = L.orc_grad_f64(int(n_particles), float(mu), float(rho), float(sigma_z), float(nu_obs), int(seed), _ptr(y), T,
+                        _ptr(anc), int(mode), C.byref(ll), _ptr(grad), _ptr(dll))
+    if rc != 0:
+        raise RuntimeError(f"orc_grad_f64 failed ({rc})")
+    return ll.value, grad, dll
 
 
 def num_threads(native: bool = False) -> int:
