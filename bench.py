@@ -13,6 +13,12 @@ one filter pass over the T=5000 series (re-seed + 5000 ticks).
          stream during a profiled pass of the same workload
   cpu_baseline  FP32 restatement of the reference tick loop (oracle/), OpenMP
          over all host cores, on a bounded number of ticks of the same run
+  batched   1024 filters with their own theta and N (512..16384), T=2000, one
+         persistent launch per size class in one CUDA graph, against the plain
+         filter run per filter
+  gradient  d loglik / d theta at N=2^20, T=2000 (taped forward + adjoint
+         backward) against the plain forward, with the full-size FP64 replay and
+         finite-difference checks
 
 `--impl reference` times that CPU restatement alone (rank 0) and prints the
 same metric. Multi-GPU (torchrun): independent replicas, one per GPU, seeds
@@ -56,6 +62,9 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-filters", type=int, default=1024)
     ap.add_argument("--batch-ticks", type=int, default=2000)
+    ap.add_argument("--no-gradient", action="store_true")
+    ap.add_argument("--grad-n", type=int, default=1 << 20)
+    ap.add_argument("--grad-ticks", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -204,6 +213,85 @@ def bench_batched(dev, args, lib, rank, world, barrier):
                                  "method": "gpu_bpf_step_many_device per filter, own stream, CUDA graph"},
             "speedup_vs_per_filter": value / per_filter if world == 1 else None,
             "loglik_finite": finite}
+
+
+def bench_gradient(dev, args, lib, rank, world, barrier):
+    """Configuration 3: theta=(mu=-0.8, phi=0.95, sigma_eta=0.25), N=2^20, T=2000, DGP seed 42 with the same
+    theta, resampling every tick. Times the plain forward (device graph), the taped forward and the adjoint
+    backward (each one CUDA graph) with events on their streams; checks the adjoint at full size against the
+    FP64 replay's forward-mode tangents and the 5-point central difference (step 1e-3*|theta_k|) of the FP64
+    replay under common random numbers with the taped ancestors. Multi-GPU: replicas (seed per rank)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gpubpf
+    from gpubpf import dgp
+    mu, rho, sig = -0.8, 0.95, 0.25
+    N, T, seed = args.grad_n, args.grad_ticks, 42 + rank
+    _, ys = dgp.matched_series(T, rho, sig, mu, 42)
+    y = torch.tensor(np.asarray(ys, dtype=np.float32), device=dev)
+    reps = max(1, args.steps)
+
+    def timed(stream, fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1) / reps], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # plain forward (the drop-in path), always resample
+    f = gpubpf.GpuBpf(N, rho, sig, mu, 0.0, 0.0, seed, ess_threshold=0.0)
+    rec = torch.zeros(T * RECORD_BYTES, dtype=torch.uint8, device=dev)
+    fs = torch.cuda.ExternalStream(f.state.stream, device=dev)
+
+    def plain():
+        f.reset(seed)
+        f.step_many_device(y.data_ptr(), T, rec.data_ptr())
+    for _ in range(3):
+        plain()
+    barrier()
+    ms_plain = timed(fs, plain)
+    f.close()
+
+    tape = gpubpf.GradTape(N, T)
+    ts = tape.stream
+    for _ in range(3):
+        tape.forward((mu, rho, sig), y, seed=seed)
+        tape.backward()
+    barrier()
+    ms_fwd = timed(ts, lambda: tape.forward((mu, rho, sig), y, seed=seed))
+    ms_bwd = timed(ts, tape.backward)
+    ms_both = timed(ts, lambda: (tape.forward((mu, rho, sig), y, seed=seed), tape.backward()))
+    ll = float(tape.forward((mu, rho, sig), y, seed=seed).item())
+    g = tape.backward().cpu().numpy()
+    rep = tape.replay((mu, rho, sig)).cpu().numpy()
+    fd5 = tape.fd_gradient((mu, rho, sig), rel=1e-3, points=5)
+    fd3 = tape.fd_gradient((mu, rho, sig), rel=1e-3, points=3)
+    scale = float(np.max(np.abs(g)))
+    out = {
+        "workload": f"SV gradient, theta=(mu={mu}, phi={rho}, sigma_eta={sig}), N={N}, T={T}, always resample, "
+                    f"DGP seed 42",
+        "ms_forward_plain": ms_plain, "ms_forward_taped": ms_fwd, "ms_backward": ms_bwd,
+        "ms_forward_plus_backward": ms_both,
+        "grad_over_forward": ms_both / ms_plain,
+        "us_per_tick": {"plain_forward": ms_plain / T * 1e3, "taped_forward": ms_fwd / T * 1e3,
+                        "backward": ms_bwd / T * 1e3},
+        "loglik": ll, "grad": g.tolist(),
+        "replay_fp64": {"loglik": float(rep[0]), "grad": rep[1:].tolist(),
+                        "rel_err": float(np.max(np.abs(g - rep[1:])) / scale)},
+        "fd_5point": {"grad": fd5.tolist(), "rel_err": float(np.max(np.abs(g - fd5)) / scale),
+                      "step": "1e-3*|theta_k|"},
+        "fd_3point": {"grad": fd3.tolist(), "rel_err": float(np.max(np.abs(g - fd3)) / scale)},
+        "tape_bytes": gpubpf.GradTape.tape_bytes(N, T), "checkpoint_every": tape.checkpoint_every,
+        "timing": "CUDA events on the filter / tape stream, mean of --steps runs after 3 warm-ups, max over ranks",
+    }
+    tape.close()
+    return out
 
 
 def run_reference(args):
@@ -379,6 +467,7 @@ def main():
 
     f.close()
     batched = None if args.no_batched else bench_batched(dev, args, lib, rank, world, barrier)
+    gradient = None if args.no_gradient else bench_gradient(dev, args, lib, rank, world, barrier)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -403,6 +492,7 @@ def main():
             "e2e": e2e,
             "clocks": clocks,
             "batched": batched,
+            "gradient": gradient,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
