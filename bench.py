@@ -19,6 +19,8 @@ one filter pass over the T=5000 series (re-seed + 5000 ticks).
   gradient  d loglik / d theta at N=2^20, T=2000 (taped forward + adjoint
          backward) against the plain forward, with the full-size FP64 replay and
          finite-difference checks
+  batch_gradient  forward + backward of 256 filters x 8192 particles over a
+         4000-tick regime-switching series, against the batched forward
 
 `--impl reference` times that CPU restatement alone (rank 0) and prints the
 same metric. Multi-GPU (torchrun): independent replicas, one per GPU, seeds
@@ -65,6 +67,9 @@ def parse_args():
     ap.add_argument("--no-gradient", action="store_true")
     ap.add_argument("--grad-n", type=int, default=1 << 20)
     ap.add_argument("--grad-ticks", type=int, default=2000)
+    ap.add_argument("--no-batch-gradient", action="store_true")
+    ap.add_argument("--bgrad-filters", type=int, default=256)
+    ap.add_argument("--bgrad-ticks", type=int, default=4000)
     return ap.parse_args()
 
 
@@ -294,6 +299,68 @@ def bench_gradient(dev, args, lib, rank, world, barrier):
     return out
 
 
+def bench_batch_gradient(dev, args, lib, rank, world, barrier):
+    """Configuration 5: B=256 filters with N=8192, theta drawn as in configuration 4, T=4000 ticks of the
+    regime-switching series (mu alternating -1.5 / 0.0 every 500 ticks, phi=0.97, sigma_eta=0.2, seed 42);
+    one iteration = forward + backward of every filter (per-filter loglik and d loglik / d theta). Timed
+    against the batched forward alone on the same filters; two filters are checked against plain gradient
+    tapes. Filters are sharded across ranks by LPT on N."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gpubpf
+    from gpubpf import configs, dgp, parallel
+    B, T = args.bgrad_filters, args.bgrad_ticks
+    allf = configs.config5(B)
+    _, fl = parallel.shard(allf, rank, world)
+    _, ys = dgp.regime_series(T, seed=42)
+    y = np.asarray(ys, dtype=np.float32)
+    y_d = torch.tensor(y, device=dev)
+    b = gpubpf.GpuBpfBatch(fl, ess_threshold=0.0)
+    bs = torch.cuda.ExternalStream(b.stream, device=dev)
+    ll = torch.zeros(len(fl), dtype=torch.float64, device=dev)
+    g = torch.zeros(3 * len(fl), dtype=torch.float64, device=dev)
+    reps = max(1, args.steps)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(bs)
+        for _ in range(reps):
+            fn()
+        e1.record(bs)
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1) / reps], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_fwd = timed(lambda: b.run_device(y_d.data_ptr(), T, ll.data_ptr()))
+    ms_both = timed(lambda: b.grad_run(y_d.data_ptr(), T, ll.data_ptr(), g.data_ptr()))
+    llv = ll.cpu().numpy()
+    gv = g.cpu().numpy().reshape(-1, 3)
+    tape_bytes = b.grad_tape_bytes(T)
+    b.close()
+    errs = []
+    for i in (0, len(fl) - 1):
+        f = fl[i]
+        tape = gpubpf.GradTape(f["n_particles"], T, checkpoint_every=8)
+        tape.forward((f["mu"], f["rho"], f["sigma_z"]), y_d, seed=f["seed"])
+        pg = tape.backward().cpu().numpy()
+        tape.close()
+        errs.append(float(np.max(np.abs(gv[i] - pg)) / np.max(np.abs(pg))))
+    steps = float(sum(f["n_particles"] for f in allf)) * T
+    return {"workload": f"batched gradient, B={B} filters x N=8192, T={T} regime-switching series "
+                        f"(mu -1.5/0.0 every 500 ticks, phi=0.97, sigma_eta=0.2, seed 42), always resample",
+            "ms_per_iteration": ms_both, "ms_forward_only": ms_fwd, "grad_over_forward": ms_both / ms_fwd,
+            "particle_steps_per_s": steps / (ms_both / 1e3), "unit": "particle-steps/s (forward+backward)",
+            "loglik_finite": bool(np.all(np.isfinite(llv))), "grad_finite": bool(np.all(np.isfinite(gv))),
+            "check_vs_plain_tape_rel_err": errs, "tape_bytes": tape_bytes,
+            "shard": f"LPT on N over {world} rank(s)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -468,6 +535,7 @@ def main():
     f.close()
     batched = None if args.no_batched else bench_batched(dev, args, lib, rank, world, barrier)
     gradient = None if args.no_gradient else bench_gradient(dev, args, lib, rank, world, barrier)
+    batch_gradient = None if args.no_batch_gradient else bench_batch_gradient(dev, args, lib, rank, world, barrier)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -493,6 +561,7 @@ def main():
             "clocks": clocks,
             "batched": batched,
             "gradient": gradient,
+            "batch_gradient": batch_gradient,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

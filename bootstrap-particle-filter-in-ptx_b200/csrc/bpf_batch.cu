@@ -12,6 +12,16 @@
 // Particle arrays use a swizzled layout (column c of each 32-float row stored
 // at c ^ row) so both the lane-strided and the per-thread-contiguous access
 // patterns are free of shared-memory bank conflicts.
+//
+// Gradient form (batch_grad_kernel): after a filter's taped forward, the same
+// CTA runs its adjoint backward, checkpoint segment by segment from the last:
+// the segment's particles are recomputed from the checkpoint through the
+// taped child lists (parent-centric: every parent writes its children) into
+// a per-CTA global segment buffer, then lambda goes backward through the
+// segment in shared memory. Children sums are taken first (into a scratch
+// array), then lambda is overwritten in place, so one lambda array suffices.
+// The parameter adjoints accumulate per thread in FP64 and are summed once
+// per filter.
 #include "bpf_batch.cuh"
 #include "bpf_block.cuh"
 
@@ -31,13 +41,14 @@ struct BatchShared {
   int rk[kBatchMaxTiles];
   unsigned long long base, delta, magic;
   int resample, carry, next;
+  double gred[5][NT / 32];
 };
 
 size_t batch_smem_bytes(int maxn) { return (size_t)maxn * 8 + (((size_t)maxn * 2 + 15) / 16) * 16; }
 
 template <int NT>
 __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, int b, float* bufA, float* bufB,
-                                 unsigned short* marks, BatchShared<NT>& sh) {
+                                 unsigned short* marks, BatchShared<NT>& sh, int maxn) {
   constexpr int W = NT / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int N = f.n;
@@ -73,6 +84,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
     obs.y = y;
     const bool carry = sh.carry != 0;
     const PcgTick c = pcg_tick_consts(f.seed, At, Bt);
+    float* ck = (a.g_ckpt && t % a.g_K == 0) ? a.g_ckpt + (size_t)(t / a.g_K) * maxn : nullptr;
 
     // 1. propagate + log2-weight, per-tile max
     float tmax[kBatchMaxTiles];
@@ -85,6 +97,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
         for (int i = k * kTile + tid; i < i1; i += NT) {
           const int si = swz(i);
           float h = H[si];
+          if (ck) ck[i] = h;
           if (t > 0) {
             const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
             h = propagate(h, f.mu, f.rho, f.sigma, icdf_normal(pcg_uniform(pcg_output(s))));
@@ -164,6 +177,8 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       }
       ll_total += dll;
       hm_last = hm;
+      if (a.g_norm)
+        a.g_norm[t] = degenerate ? make_float2(0.0f, 0.0f) : make_float2((float)(1.0 / S), __int_as_float(nM));
       if (a.dll) a.dll[(size_t)b * a.T + t] = dll;
       if (a.hmean) a.hmean[(size_t)b * a.T + t] = hm;
       if (resample) {
@@ -222,9 +237,11 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
         q = targets_below(Pk + shr64(loc, r), base, delta, magic, N);
         tq = base + (unsigned long long)q * delta;
       }
+      unsigned short* lst = a.g_list ? a.g_list + (size_t)t * maxn : nullptr;
       for (int e = 0; e < chunk; ++e) {
         const int j = j0 + e;
         int lo = 0, hi = 0;
+        if (lst) lst[e * NT + tid] = (unsigned short)(j < j1 ? q : N);   // children of j start at slot q
         if (j < j1) {
           loc += fix_weight(Wt[swz(j)]);
           const unsigned long long cj = Pk + shr64(loc, r);
@@ -283,7 +300,222 @@ __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_ker
     if (idx >= a.n_order) break;
     const int b = a.order[idx];
     const BatchFilterDev f = a.filters[b];
-    batch_run_filter<NT>(a, f, b, bufA, bufB, marks, sh);
+    batch_run_filter<NT>(a, f, b, bufA, bufB, marks, sh, maxn);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gradient: adjoint backward of one filter after its taped forward
+// ---------------------------------------------------------------------------
+constexpr int kBatchHeavy = 32;   // children above which a parent's walk is shared by its warp
+
+__device__ __forceinline__ float batch_noise(const PcgTick& pc, int i) {
+  return icdf_normal(pcg_uniform(pcg_output(pc.k1 + pc.k2 * pcg_inc((uint32_t)i))));
+}
+
+template <int NT>
+__device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, int b, int maxn, float* lam,
+                                   float* hA, float* hB, BatchShared<NT>& sh) {
+  constexpr int W = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N = f.n, T = a.T, K = a.g_K;
+  int chunk = 1;
+  while (chunk * NT < N) chunk <<= 1;
+  const int j0 = tid * chunk;
+  const bool gauss = !(f.nu > 0.0f);
+  ObsModel obs;
+  obs.y = 0.0f; obs.nu = f.nu; obs.c_obs = f.c_obs; obs.inv_nu = f.inv_nu; obs.nu_p1h = f.nu_p1h;
+  const PcgTick pc0 = pcg_tick_consts(f.seed, 1ull, 0ull);
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  // first child of the thread's e-th parent; e = chunk is the next thread's first parent
+  auto first_child = [&](const unsigned short* lst, int e) -> int {
+    int v;
+    if (e < chunk) v = (j0 + e < N) ? (int)lst[e * NT + tid] : N;
+    else v = (tid + 1 < NT && j0 + chunk < N) ? (int)lst[tid + 1] : N;
+    return min(v, N);
+  };
+
+  const int nseg = (T + K - 1) / K;
+  for (int s = nseg - 1; s >= 0; --s) {
+    const int c = s * K, last = min(c + K, T) - 1;
+    // 1. particles of tick c from the checkpoint
+    {
+      const float* ck = a.g_ckpt + (size_t)s * maxn;
+      const PcgTick pc = pcg_tick_consts(f.seed, a.g_AB[c].x, a.g_AB[c].y);
+      for (int i = tid; i < N; i += NT) {
+        float h = ck[i];
+        if (c > 0) h = propagate(h, f.mu, f.rho, f.sigma, batch_noise(pc, i));
+        hA[swz(i)] = h;
+        if (last > c) a.g_seg[i] = h;
+      }
+    }
+    __syncthreads();
+    float* hp = hA;
+    float* hc = hB;
+    // 2. ticks c+1..last through the child lists of the previous tick
+    for (int t = c + 1; t <= last; ++t) {
+      const PcgTick pc = pcg_tick_consts(f.seed, a.g_AB[t].x, a.g_AB[t].y);
+      const unsigned short* lst = a.g_list + (size_t)(t - 1) * maxn;
+      int lo = first_child(lst, 0);
+      for (int e = 0; e < chunk; ++e) {
+        const int hi = first_child(lst, e + 1);
+        float hpar = 0.0f;
+        int wlo = 0, whi = 0;
+        if (hi > lo) {
+          hpar = hp[swz(j0 + e)];
+          if (hi - lo <= kBatchHeavy) {
+            for (int i = lo; i < hi; ++i) hc[swz(i)] = propagate(hpar, f.mu, f.rho, f.sigma, batch_noise(pc, i));
+          } else {
+            wlo = lo; whi = hi;
+          }
+        }
+        unsigned heavy = __ballot_sync(0xffffffffu, whi > wlo);
+        while (heavy) {
+          const int src = __ffs(heavy) - 1;
+          heavy &= heavy - 1u;
+          const int flo = __shfl_sync(0xffffffffu, wlo, src), fhi = __shfl_sync(0xffffffffu, whi, src);
+          const float fh = __shfl_sync(0xffffffffu, hpar, src);
+          for (int i = flo + lane; i < fhi; i += 32) hc[swz(i)] = propagate(fh, f.mu, f.rho, f.sigma, batch_noise(pc, i));
+        }
+        lo = max(lo, hi);
+      }
+      __syncthreads();
+      if (t < last) {
+        float* sg = a.g_seg + (size_t)(t - c) * maxn;
+        for (int i = tid; i < N; i += NT) sg[i] = hc[swz(i)];
+      }
+      float* tmp = hp; hp = hc; hc = tmp;
+    }
+    // 3. adjoint, ticks last..c (hp holds h_last)
+    for (int t = last; t >= c; --t) {
+      if (t < last) {
+        const float* sg = a.g_seg + (size_t)(t - c) * maxn;
+        for (int i = tid; i < N; i += NT) hp[swz(i)] = sg[i];
+        __syncthreads();
+      }
+      // children sums of lambda_t+1 -> hc, and sum lambda eps over the children
+      float acc_eps = 0.0f;
+      if (t < T - 1) {
+        const PcgTick pcn = pcg_tick_consts(f.seed, a.g_AB[t + 1].x, a.g_AB[t + 1].y);
+        const unsigned short* lst = a.g_list + (size_t)t * maxn;
+        int lo = first_child(lst, 0);
+        for (int e = 0; e < chunk; ++e) {
+          const int hi = first_child(lst, e + 1);
+          float sum = 0.0f;
+          int wlo = 0, whi = 0;
+          if (hi - lo <= kBatchHeavy) {
+            for (int i = lo; i < hi; ++i) {
+              const float l = lam[swz(i)];
+              sum += l;
+              acc_eps = fmaf(l, batch_noise(pcn, i), acc_eps);
+            }
+          } else {
+            wlo = lo; whi = hi;
+          }
+          unsigned heavy = __ballot_sync(0xffffffffu, whi > wlo);
+          while (heavy) {
+            const int src = __ffs(heavy) - 1;
+            heavy &= heavy - 1u;
+            const int flo = __shfl_sync(0xffffffffu, wlo, src), fhi = __shfl_sync(0xffffffffu, whi, src);
+            float p = 0.0f;
+            for (int i = flo + lane; i < fhi; i += 32) {
+              const float l = lam[swz(i)];
+              p += l;
+              acc_eps = fmaf(l, batch_noise(pcn, i), acc_eps);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+            if (lane == src) sum = p;
+          }
+          if (j0 + e < N) hc[swz(j0 + e)] = sum;
+          lo = max(lo, hi);
+        }
+      }
+      __syncthreads();                     // lambda_t+1 fully read
+      const float2 nz = a.g_norm[t];
+      const float invS = nz.x, nM = (float)__float_as_int(nz.y);
+      const float y = __ldg(a.y + t), y2 = y * y;
+      obs.y = y;
+      float acs = 0.f, acsh = 0.f, al0 = 0.f, al0z = 0.f;
+      for (int e = 0; e < chunk; ++e) {
+        const int j = j0 + e;
+        if (j >= N) break;
+        const float h = hp[swz(j)];
+        const float cs = (t < T - 1) ? hc[swz(j)] : 0.0f;
+        float x, g;
+        if (gauss) {
+          x = obs_log2pdf_gauss(y2, h);
+          g = 0.5f * fmaf(y2, ex2_approx(h * -kLog2e), -1.0f);
+        } else {
+          x = __fmul_rn(obs_logpdf(obs, h), kLog2e);
+          const float q = y2 * ex2_approx(h * -kLog2e) * obs.inv_nu;
+          g = fmaf(obs.nu_p1h, div_approx(q, 1.0f + q), -0.5f);
+        }
+        const float l = fmaf(f.rho, cs, (ex2_approx(x - nM) * invS) * g);
+        lam[swz(j)] = l;
+        acs += cs;
+        acsh = fmaf(cs, h - f.mu, acsh);
+        if (t == 0) {
+          const float z0 = batch_noise(pc0, j);
+          al0 += l;
+          al0z = fmaf(l, z0, al0z);
+        }
+      }
+      acc[0] += (double)acs; acc[1] += (double)acsh; acc[2] += (double)acc_eps;
+      acc[3] += (double)al0; acc[4] += (double)al0z;
+      __syncthreads();                     // lambda_t complete
+    }
+  }
+  // 4. per-filter sums -> gradient (initial draw h_0 = mu + sigma z / sqrt(max(1-rho^2, 1e-6)))
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const double v = warp_sum_d(acc[k]);
+    if (lane == 0) sh.gred[k][warp] = v;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double tt[5];
+    for (int k = 0; k < 5; ++k) {
+      tt[k] = 0.0;
+      for (int w = 0; w < W; ++w) tt[k] += sh.gred[k][w];
+    }
+    const double r = (double)f.rho, sg = (double)f.sigma;
+    const double one_m = 1.0 - r * r;
+    const double s2 = fmax(one_m, 1e-6), sd = sqrt(s2);
+    const double ds_drho = one_m > 1e-6 ? sg * r / (s2 * sd) : 0.0;
+    a.grad[3 * (size_t)b + 0] = (1.0 - r) * tt[0] + tt[3];
+    a.grad[3 * (size_t)b + 1] = tt[1] + tt[4] * ds_drho;
+    a.grad[3 * (size_t)b + 2] = tt[2] + tt[4] / sd;
+  }
+  __syncthreads();
+}
+
+size_t batch_grad_smem_bytes(int maxn) { return (size_t)maxn * 12; }
+
+template <int NT>
+__global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_grad_kernel(BatchArgs a, int maxn) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ BatchShared<NT> sh;
+  float* r0 = reinterpret_cast<float*>(smem);
+  float* r1 = r0 + maxn;
+  float* r2 = r1 + maxn;
+  unsigned short* marks = reinterpret_cast<unsigned short*>(r2);
+  const int nck = (a.T + a.g_K - 1) / a.g_K;
+  BatchArgs s = a;                                   // this CTA slot's tape
+  s.g_list = a.g_list + (size_t)blockIdx.x * a.T * maxn;
+  s.g_ckpt = a.g_ckpt + (size_t)blockIdx.x * nck * maxn;
+  s.g_norm = a.g_norm + (size_t)blockIdx.x * a.T;
+  s.g_seg = a.g_seg + (size_t)blockIdx.x * a.g_K * maxn;
+  for (;;) {
+    if (threadIdx.x == 0) sh.next = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int idx = sh.next;
+    __syncthreads();
+    if (idx >= a.n_order) break;
+    const int b = a.order[idx];
+    const BatchFilterDev f = a.filters[b];
+    batch_run_filter<NT>(s, f, b, r0, r1, marks, sh, maxn);
+    batch_run_backward<NT>(s, f, b, maxn, r0, r1, r2, sh);
   }
 }
 
@@ -313,6 +545,43 @@ static int occ_nt(int maxn) {
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<NT>, NT, smem);
   return per;
+}
+
+template <int NT>
+static cudaError_t launch_grad_nt(const BatchArgs& a, int maxn, int grid, cudaStream_t s) {
+  batch_grad_kernel<NT><<<grid, NT, batch_grad_smem_bytes(maxn), s>>>(a, maxn);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_grad_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s) {
+  switch (threads) {
+    case 64: return launch_grad_nt<64>(a, maxn, grid, s);
+    case 128: return launch_grad_nt<128>(a, maxn, grid, s);
+    case 256: return launch_grad_nt<256>(a, maxn, grid, s);
+    case 512: return launch_grad_nt<512>(a, maxn, grid, s);
+    case 1024: return launch_grad_nt<1024>(a, maxn, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int NT>
+static int grad_occ_nt(int maxn) {
+  const size_t smem = batch_grad_smem_bytes(maxn);
+  cudaFuncSetAttribute(batch_grad_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_grad_kernel<NT>, NT, smem);
+  return per;
+}
+
+int batch_grad_occupancy(int threads, int maxn) {
+  switch (threads) {
+    case 64: return grad_occ_nt<64>(maxn);
+    case 128: return grad_occ_nt<128>(maxn);
+    case 256: return grad_occ_nt<256>(maxn);
+    case 512: return grad_occ_nt<512>(maxn);
+    case 1024: return grad_occ_nt<1024>(maxn);
+    default: return 0;
+  }
 }
 
 int batch_occupancy(int threads, int maxn) {

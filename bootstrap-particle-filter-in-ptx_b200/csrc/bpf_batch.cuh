@@ -43,6 +43,15 @@ struct BatchArgs {
   int* resamples;             // [B] resampling count
   int32_t* anc;               // [B*T*kBatchMaxN] ancestors, or null (testing)
   float* particles;           // [B*kBatchMaxN] final particles, or null (testing)
+  // gradient runs: tape of the launch's CTA slots (one filter at a time per slot), all null otherwise.
+  // Strides use the class's largest N (maxn); per-slot bases are taken from blockIdx.x.
+  unsigned short* g_list;     // [slots][T][maxn] first child of every parent, in thread-chunk order
+  float* g_ckpt;              // [slots][ceil(T/K)][maxn] particles entering every K-th tick
+  float2* g_norm;             // [slots][T] {1/S, nM}: W_i = 2^(x_i - nM) / S
+  float* g_seg;               // [slots][K][maxn] recomputed particles of one checkpoint segment
+  const ulonglong2* g_AB;     // [T+1] PCG32 jump constants (A^t, sum_{k<t} A^k)
+  int g_K;                    // checkpoint interval
+  double* grad;               // [3B] d loglik / d(mu, rho, sigma_z)
 };
 
 // Dynamic shared memory of the class kernel for filters of at most maxn particles.
@@ -51,5 +60,12 @@ size_t batch_smem_bytes(int maxn);
 cudaError_t launch_batch_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s);
 // CTAs per SM the class kernel can keep resident.
 int batch_occupancy(int threads, int maxn);
+
+// Gradient form: every CTA runs a filter's taped forward and then its adjoint
+// backward (segment recompute from checkpoints and child lists, lambda in
+// shared memory) before taking the next filter.
+size_t batch_grad_smem_bytes(int maxn);
+cudaError_t launch_batch_grad_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s);
+int batch_grad_occupancy(int threads, int maxn);
 
 }  // namespace bpf

@@ -79,6 +79,16 @@ struct GpuBpfBatch {
   cudaGraphExec_t graph = nullptr;
   GraphKey key;
   std::vector<int> n_of;      // particle count per filter
+
+  // gradient runs: per-class tape for the class's CTA slots, PCG jump table, graph
+  unsigned char* g_tape[kClasses] = {};
+  size_t g_tape_bytes[kClasses] = {0, 0, 0, 0, 0};
+  int g_grid[kClasses] = {1, 1, 1, 1, 1};
+  ulonglong2* d_AB = nullptr;
+  int ab_T = 0;
+  cudaGraphExec_t ggraph = nullptr;
+  GraphKey gkey;
+  double* gkey_grad = nullptr;
 };
 
 namespace {
@@ -86,6 +96,9 @@ namespace {
 void free_batch(GpuBpfBatch* b) {
   if (!b) return;
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->ggraph) cudaGraphExecDestroy(b->ggraph);
+  for (int c = 0; c < kClasses; ++c) cudaFree(b->g_tape[c]);
+  cudaFree(b->d_AB);
   cudaFree(b->d_filters); cudaFree(b->d_order); cudaFree(b->d_counters);
   cudaFree(b->d_hfinal); cudaFree(b->d_resamples); cudaFree(b->d_loglik); cudaFree(b->d_y);
   for (int c = 0; c < kClasses; ++c) {
@@ -145,6 +158,86 @@ cudaError_t enqueue_run(GpuBpfBatch* b, const float* y, int T, double* loglik, d
     if (e == cudaSuccess)
       e = launch_batch_class(class_args(b, c, y, T, loglik, dll, hmean, anc, particles), b->threads[c],
                              kClassMaxN[c], b->grid[c], b->cls_stream[c]);
+    if (e == cudaSuccess) e = cudaEventRecord(b->join[c], b->cls_stream[c]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[c], 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+constexpr int kGradK = 8;   // checkpoint interval of batched gradient runs
+
+// Per-slot tape layout of class c for T ticks (see BatchArgs::g_*).
+struct SlotLayout {
+  size_t list, ckpt, norm, seg, total;   // byte offsets inside one slot, and the slot size
+};
+SlotLayout slot_layout(int maxn, int T) {
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t nck = (size_t)((T + kGradK - 1) / kGradK);
+  SlotLayout L;
+  L.list = 0;
+  L.ckpt = al((size_t)T * maxn * sizeof(unsigned short));
+  L.norm = L.ckpt + al(nck * maxn * sizeof(float));
+  L.seg = L.norm + al((size_t)T * sizeof(float2));
+  L.total = L.seg + al((size_t)kGradK * maxn * sizeof(float));
+  return L;
+}
+
+// Grid of every class's gradient kernel and its tape for T ticks.
+int prepare_grad(GpuBpfBatch* b, int T) {
+  for (int c = 0; c < kClasses; ++c) {
+    if (!b->class_cnt[c]) continue;
+    const int occ = std::max(1, batch_grad_occupancy(b->threads[c], kClassMaxN[c]));
+    b->g_grid[c] = std::max(1, std::min(b->class_cnt[c], b->sms * occ));
+    const size_t need = slot_layout(kClassMaxN[c], T).total * (size_t)b->g_grid[c];
+    if (b->g_tape_bytes[c] < need) {
+      cudaFree(b->g_tape[c]);
+      b->g_tape[c] = nullptr;
+      b->g_tape_bytes[c] = 0;
+      BCK(cudaMalloc(&b->g_tape[c], need));
+      b->g_tape_bytes[c] = need;
+    }
+  }
+  if (b->ab_T < T + 1) {
+    cudaFree(b->d_AB);
+    b->d_AB = nullptr;
+    b->ab_T = 0;
+    BCK(cudaMalloc(&b->d_AB, (size_t)(T + 1) * sizeof(ulonglong2)));
+    std::vector<ulonglong2> ab(T + 1);
+    unsigned long long At = 1ull, Bt = 0ull;
+    for (int t = 0; t <= T; ++t) {
+      ab[t].x = At; ab[t].y = Bt;
+      At *= kPcgMult;
+      Bt = Bt * kPcgMult + 1ull;
+    }
+    BCK(cudaMemcpy(b->d_AB, ab.data(), (size_t)(T + 1) * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+    b->ab_T = T + 1;
+  }
+  return BPF_OK;
+}
+
+cudaError_t enqueue_grad(GpuBpfBatch* b, const float* y, int T, double* loglik, double* grad) {
+  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, kClasses * sizeof(int), b->stream);
+  if (e != cudaSuccess) return e;
+  e = cudaEventRecord(b->fork, b->stream);
+  if (e != cudaSuccess) return e;
+  for (int c = kClasses - 1; c >= 0; --c) {
+    if (!b->class_cnt[c]) continue;
+    BatchArgs a = class_args(b, c, y, T, loglik, nullptr, nullptr, nullptr, nullptr);
+    const SlotLayout L = slot_layout(kClassMaxN[c], T);
+    // slot-major tape: every field is an array over slots with the per-slot stride the kernel uses
+    unsigned char* base = b->g_tape[c];
+    const size_t slots = (size_t)b->g_grid[c];
+    a.g_list = reinterpret_cast<unsigned short*>(base);
+    a.g_ckpt = reinterpret_cast<float*>(base + slots * L.ckpt);
+    a.g_norm = reinterpret_cast<float2*>(base + slots * L.norm);
+    a.g_seg = reinterpret_cast<float*>(base + slots * L.seg);
+    a.g_AB = b->d_AB;
+    a.g_K = kGradK;
+    a.grad = grad;
+    e = cudaStreamWaitEvent(b->cls_stream[c], b->fork, 0);
+    if (e == cudaSuccess)
+      e = launch_batch_grad_class(a, b->threads[c], kClassMaxN[c], b->g_grid[c], b->cls_stream[c]);
     if (e == cudaSuccess) e = cudaEventRecord(b->join[c], b->cls_stream[c]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[c], 0);
     if (e != cudaSuccess) return e;
@@ -310,6 +403,48 @@ int gpu_bpf_batch_run_device(GpuBpfBatch* b, const float* y_dev, int n_ticks, do
   BCK(cudaGraphLaunch(b->graph, b->stream));
   bpf_note_launches(kClasses);
   return BPF_OK;
+}
+
+int gpu_bpf_batch_grad_run(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* loglik_dev, double* grad_dev) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  if (n_ticks <= 0 || !y_dev || !loglik_dev || !grad_dev) return bpf_record_error(BPF_ERR_ARG);
+  if (b->ess_threshold != 0.0f) return bpf_record_error(BPF_ERR_UNSUPPORTED);   // always-resample tapes only
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  GraphKey k;
+  k.y = y_dev; k.T = n_ticks; k.loglik = loglik_dev;
+  std::copy(b->threads, b->threads + kClasses, k.threads);
+  if (!b->ggraph || !(k == b->gkey) || b->gkey_grad != grad_dev) {
+    if (b->ggraph) { cudaGraphExecDestroy(b->ggraph); b->ggraph = nullptr; }
+    BCK(cudaStreamSynchronize(b->stream));           // a resized tape must not be in use
+    rc = prepare_grad(b, n_ticks);
+    if (rc) return rc;
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_grad(b, y_dev, n_ticks, loglik_dev, grad_dev);
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
+    e = cudaGraphInstantiate(&b->ggraph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->ggraph = nullptr; cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
+    b->gkey = k;
+    b->gkey_grad = grad_dev;
+  }
+  BCK(cudaGraphLaunch(b->ggraph, b->stream));
+  bpf_note_launches(kClasses);
+  return BPF_OK;
+}
+
+size_t gpu_bpf_batch_grad_tape_bytes(GpuBpfBatch* b, int n_ticks) {
+  if (!b || n_ticks <= 0) return 0;
+  size_t tot = 0;
+  for (int c = 0; c < kClasses; ++c) {
+    if (!b->class_cnt[c]) continue;
+    const int occ = std::max(1, batch_grad_occupancy(b->threads[c], kClassMaxN[c]));
+    const size_t slots = (size_t)std::max(1, std::min(b->class_cnt[c], b->sms * occ));
+    tot += slots * slot_layout(kClassMaxN[c], n_ticks).total;
+  }
+  return tot + (size_t)(n_ticks + 1) * sizeof(ulonglong2);
 }
 
 int gpu_bpf_batch_run(GpuBpfBatch* b, const float* y, int n_ticks, double* loglik_out, float* hmean_last_out) {

@@ -118,6 +118,8 @@ SIGNATURES = {
     "gpu_bpf_batch_run_device": (_i, [_vp, _vp, _i, _vp, _vp, _vp]),
     "gpu_bpf_batch_run_debug": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp]),
     "gpu_bpf_batch_resample_counts": (_i, [_vp, C.POINTER(_i), C.POINTER(_f)]),
+    "gpu_bpf_batch_grad_run": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "gpu_bpf_batch_grad_tape_bytes": (C.c_size_t, [_vp, _i]),
     # gradient
     "gpu_bpf_grad_create": (_vp, [_i, _i, _i]),
     "gpu_bpf_grad_destroy": (None, [_vp]),

@@ -74,6 +74,15 @@ class GpuBpfBatch:
                                                 C.c_void_p(dll_ptr or None), C.c_void_p(anc_ptr or None),
                                                 C.c_void_p(particles_ptr or None)), "gpu_bpf_batch_run_debug")
 
+    def grad_run(self, y_ptr: int, n_ticks: int, loglik_ptr: int, grad_ptr: int) -> None:
+        """Forward + adjoint backward of every filter: loglik[B] (FP64) and grad[B, 3] = d loglik /
+        d(mu, rho, sigma_z), enqueued on the batch stream (device pointers)."""
+        check(self._lib.gpu_bpf_batch_grad_run(self._h, C.c_void_p(y_ptr), int(n_ticks), C.c_void_p(loglik_ptr),
+                                               C.c_void_p(grad_ptr)), "gpu_bpf_batch_grad_run")
+
+    def grad_tape_bytes(self, n_ticks: int) -> int:
+        return int(self._lib.gpu_bpf_batch_grad_tape_bytes(self._h, int(n_ticks)))
+
     def resample_counts(self):
         cnt = (C.c_int * self.n_filters)()
         hm = (C.c_float * self.n_filters)()

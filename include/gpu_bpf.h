@@ -269,6 +269,17 @@ int          gpu_bpf_batch_run_debug(GpuBpfBatch* batch, const float* y_dev, int
                                      double* dll_dev, int32_t* anc_dev, float* particles_dev);
 /* Resampling count and last filtered mean of every filter after a run (waits). */
 int          gpu_bpf_batch_resample_counts(GpuBpfBatch* batch, int* counts, float* hmean_last);
+/* Batched gradient (the SMC^2 / PMMH inner loop with gradients): one forward and one backward
+ * pass of every filter in one persistent launch per size class (each CTA runs a filter's taped
+ * forward, then its adjoint, as gpu_bpf_grad_forward/backward do for one filter), replayed as
+ * one CUDA graph. Device buffers: loglik_dev[n_filters] (FP64 total log-likelihood) and
+ * grad_dev[3*n_filters] = d loglik / d(mu, rho, sigma_z) per filter, ancestors held fixed.
+ * The batch must resample every tick (ess_threshold 0; BPF_ERR_UNSUPPORTED otherwise). */
+int          gpu_bpf_batch_grad_run(GpuBpfBatch* batch, const float* y_dev, int n_ticks, double* loglik_dev,
+                                    double* grad_dev);
+/* Device memory the gradient tape of gpu_bpf_batch_grad_run takes for n_ticks ticks (it is sized
+ * for the CTAs in flight, not for the number of filters). */
+size_t       gpu_bpf_batch_grad_tape_bytes(GpuBpfBatch* batch, int n_ticks);
 
 /* ---- Gradient (addition) ---------------------------------------------------
  * d loglik / d(mu, rho, sigma_z) of the plain filter with the resampling ancestors held fixed.
