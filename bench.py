@@ -13,6 +13,9 @@ one filter pass over the T=5000 series (re-seed + 5000 ticks).
          stream during a profiled pass of the same workload
   cpu_baseline  FP32 restatement of the reference tick loop (oracle/), OpenMP
          over all host cores, on a bounded number of ticks of the same run
+  sweep     the scaling sweep N = 2^16 .. 51.2M (first 1000 ticks, ESS<0.5N)
+  config1   N=4096, T=1000, always resample: GPU and the CPU restatement on 1
+         core and all cores, loglik against the FP64 oracle
   batched   1024 filters with their own theta and N (512..16384), T=2000, one
          persistent launch per size class in one CUDA graph, against the plain
          filter run per filter
@@ -68,6 +71,9 @@ def parse_args():
     ap.add_argument("--grad-n", type=int, default=1 << 20)
     ap.add_argument("--grad-ticks", type=int, default=2000)
     ap.add_argument("--no-batch-gradient", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--sweep-ticks", type=int, default=1000)
+    ap.add_argument("--no-config1", action="store_true")
     ap.add_argument("--bgrad-filters", type=int, default=256)
     ap.add_argument("--bgrad-ticks", type=int, default=4000)
     return ap.parse_args()
@@ -218,6 +224,114 @@ def bench_batched(dev, args, lib, rank, world, barrier):
                                  "method": "gpu_bpf_step_many_device per filter, own stream, CUDA graph"},
             "speedup_vs_per_filter": value / per_filter if world == 1 else None,
             "loglik_finite": finite}
+
+
+def bench_sweep(dev, args, lib, rank, world, barrier):
+    """Configuration 2 scaling sweep: N in {2^16, 2^18, 2^20, 2^22, 2^24, 51,200,000}, same theta and DGP
+    seed 7, ESS<0.5N, the first --sweep-ticks ticks of the T=5000 series. Device-resident runs (one CUDA
+    graph each), CUDA events on the filter stream, 3 warm-ups, mean of --steps runs, max over ranks.
+    HBM fraction = algorithmic bytes (pass 1 12 B/particle, +4 on carry ticks; pass 2 12 B/particle on
+    resampling ticks) / run time / measured peak."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gpubpf
+    from gpubpf import dgp
+    T = args.sweep_ticks
+    _, ys = dgp.matched_series(5000, RHO, SIG, MU, args.dgp_seed)
+    y = torch.tensor(np.asarray(ys[:T], dtype=np.float32), device=dev)
+    rec = torch.zeros(T * RECORD_BYTES, dtype=torch.uint8, device=dev)
+    peak, _ = load_peaks()
+    out = []
+    for N in (1 << 16, 1 << 18, 1 << 20, 1 << 22, 1 << 24, 51_200_000):
+        f = gpubpf.GpuBpf(N, RHO, SIG, MU, 0.0, 0.0, 1000 + rank, ess_threshold=args.ess)
+        fs = torch.cuda.ExternalStream(f.state.stream, device=dev)
+
+        def run(seed):
+            f.reset(seed)
+            f.step_many_device(y.data_ptr(), T, rec.data_ptr())
+        for w in range(3):
+            run(2000 + w)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, args.steps)
+        e0.record(fs)
+        for k in range(reps):
+            run(3000 + k)
+        e1.record(fs)
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1) / reps], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        res = np.frombuffer(rec.cpu().numpy().tobytes(), dtype=np.int32).reshape(T, RECORD_BYTES // 4)[:, 8]
+        carry = np.zeros(T)
+        carry[1:] = 1 - res[:-1]
+        bytes_run = float(N) * float(np.sum(12 + 4 * carry + 12 * res))
+        out.append({"n_particles": N, "us_per_tick": ms / T * 1e3, "particle_steps_per_s": world * N * T / (ms / 1e3),
+                    "resample_rate": float(res.mean()), "hbm_frac": bytes_run / (ms / 1e3) / 1e9 / peak})
+        f.close()
+    return {"ticks": T, "ess_threshold": args.ess, "points": out,
+            "note": "device-resident CUDA-graph runs, CUDA events; hbm_frac of the measured copy peak"}
+
+
+def bench_config1(dev, args, lib, rank):
+    """Configuration 1 (the reference's CPU-runnable case): N=4096, T=1000, theta=(-1.0, 0.97, 0.15),
+    resampling every tick, DGP seed 42, filter seed 42. GPU: device-resident CUDA-graph runs; CPU: the FP32
+    restatement of the reference tick loop on 1 core and on all cores; total loglik vs the FP64 oracle on
+    the GPU run's ancestors."""
+    import numpy as np
+    import torch
+    import gpubpf
+    from gpubpf import dgp
+    from oracle import oracle
+    N, T = 4096, 1000
+    _, ys = dgp.matched_series(T, RHO, SIG, MU, 42)
+    yh = np.asarray(ys, dtype=np.float32)
+    y = torch.tensor(yh, device=dev)
+    rec = torch.zeros(T * RECORD_BYTES, dtype=torch.uint8, device=dev)
+    f = gpubpf.GpuBpf(N, RHO, SIG, MU, 0.0, 0.0, 42, ess_threshold=0.0)
+    fs = torch.cuda.ExternalStream(f.state.stream, device=dev)
+    for _ in range(3):
+        f.reset(42)
+        f.step_many_device(y.data_ptr(), T, rec.data_ptr())
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(3, args.steps)
+    e0.record(fs)
+    for _ in range(reps):
+        f.reset(42)
+        f.step_many_device(y.data_ptr(), T, rec.data_ptr())
+    e1.record(fs)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / reps
+    f.close()
+    # log-likelihood against the FP64 oracle replaying this run's ancestors
+    g = gpubpf.GpuBpf(N, RHO, SIG, MU, 0.0, 0.0, 42, ess_threshold=0.0)
+    g.record_ancestors(True)
+    anc = np.zeros((T, N), dtype=np.int32)
+    dll = np.zeros(T)
+    for t in range(T):
+        g.step(float(yh[t]))
+        dll[t] = g.get_record().dloglik
+        anc[t] = np.frombuffer(g.get_ancestors()[1], dtype=np.int32)
+    g.close()
+    o = oracle.filter_f64(N, RHO, SIG, MU, yh, seed=42, ess_threshold=0.0, anc_replay=anc,
+                          flags_replay=np.ones(T, dtype=np.int32))
+    err = abs(dll.sum() - o["dll"].sum()) / abs(o["dll"].sum())
+    out = {"workload": "plain SV BPF, N=4096, T=1000, always resample, DGP seed 42, filter seed 42",
+           "gpu": {"us_per_tick": ms / T * 1e3, "particle_steps_per_s": N * T / (ms / 1e3)},
+           "loglik": float(dll.sum()), "loglik_oracle_fp64": float(o["dll"].sum()), "loglik_rel_err": err}
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = {}
+        for label, nt in (("1_core", 1), ("all_cores", os.cpu_count() or 1)):
+            oracle.lib(True)
+            t0 = time.perf_counter()
+            oracle.ref_run(N, RHO, SIG, MU, yh, seed=42, ess_threshold=0.0, nthreads=nt, native=True)
+            dt = time.perf_counter() - t0
+            cpu[label] = {"cores": nt, "us_per_tick": dt / T * 1e6, "particle_steps_per_s": N * T / dt}
+        out["cpu_reference_restatement"] = cpu
+    return out
 
 
 def bench_gradient(dev, args, lib, rank, world, barrier):
@@ -533,6 +647,8 @@ def main():
                "api": "gpu_bpf_reset + gpu_bpf_step_many(host y[T], host BpfResult[T], host BpfTickRecord[T])"}
 
     f.close()
+    sweep = None if args.no_sweep else bench_sweep(dev, args, lib, rank, world, barrier)
+    config1 = None if args.no_config1 else bench_config1(dev, args, lib, rank)
     batched = None if args.no_batched else bench_batched(dev, args, lib, rank, world, barrier)
     gradient = None if args.no_gradient else bench_gradient(dev, args, lib, rank, world, barrier)
     batch_gradient = None if args.no_batch_gradient else bench_batch_gradient(dev, args, lib, rank, world, barrier)
@@ -559,6 +675,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
+            "sweep": sweep,
+            "config1": config1,
             "batched": batched,
             "gradient": gradient,
             "batch_gradient": batch_gradient,
