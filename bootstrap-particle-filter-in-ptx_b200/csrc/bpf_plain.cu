@@ -14,9 +14,9 @@
 //           and the pass-2 work list. No host synchronisation per tick.
 //   pass 2  (persistent CTAs over work items: one tile, a run of outputs)
 //           systematic resampling: exact integer prefix of the tile weights,
-//           each element writes its index into the output slots of the
-//           evenly spaced targets it owns (heavy elements filled by their
-//           whole warp), gather of h[ancestor] from a bulk-async
+//           each element counts the evenly spaced targets it owns and marks
+//           the first of them, a warp max-scan over the marks gives every
+//           output its ancestor, gather of h[ancestor] from a bulk-async
 //           (TMA) copy of the tile, coalesced store. Tiles of the next item
 //           are prefetched into a second buffer. Early exit on ticks that do
 //           not resample.
@@ -436,6 +436,7 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
   unsigned short* marks = reinterpret_cast<unsigned short*>(smem + 4 * kTileBytes);
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ unsigned long long s_scan[kThreads / 32 + 1];
+  __shared__ unsigned s_wmax[kThreads / 32];
   __shared__ int s_err;
 
   griddep_wait();
@@ -478,6 +479,11 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
     const bool ok = mbar_wait_bounded(&mbar[sb], (uint32_t)(n >> 1) & 1u);
     if (!ok) s_err = 1;
 
+    // clear this item's ancestor marks (the previous item's gather has finished:
+    // the loop ends with a barrier; the scan's barriers order this before the marks)
+    const int nB128 = (nB + 127) & ~127;
+    for (int x = tid; x < nB128 / 8; x += kThreads) reinterpret_cast<uint4*>(marks)[x] = make_uint4(0u, 0u, 0u, 0u);
+
     // exact fixed-point prefix of the tile: 16 contiguous weights per thread
     unsigned long long L[kPerThread];
     unsigned long long run = 0ull;
@@ -495,10 +501,11 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
     unsigned long long tot;
     const unsigned long long excl = block_excl_scan_add<kThreads>(run, &tot, s_scan);
 
-    // Each element owns the targets in [C_{j-1}, C_j): write its index into
-    // every owned output slot of this item. Elements with more than four
-    // targets are filled by their whole warp (ballot + broadcast).
-    const int lane = tid & 31;
+    // Element j owns the targets in [C_{j-1}, C_j), i.e. the output slots
+    // [q_j, q_{j+1}). Its child count is found without a loop (four
+    // comparisons; a division only past four children) and the element
+    // writes one start mark, at its first slot inside this item's window.
+    const int lane = tid & 31, warp = tid >> 5;
     int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
     unsigned long long tq = base + (unsigned long long)q * delta;
     int32_t* csr = (a.csr && item.w) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
@@ -507,40 +514,60 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
       const int j = tid * kPerThread + e;
       if (csr && j < nA) csr[j] = q;
       const unsigned long long cj = Pk + shr64(excl + L[e], r);
-      int lo = 0, hi = 0;
       if (j < nA && q < N && tq < cj) {
-        if (((cj - tq) >> 2) > delta) {
-          const int q1 = targets_below(cj, base, delta, magic, N);
-          lo = max(q, oa) - oa;
-          hi = min(q1, ob) - oa;
-          q = q1;
-          tq = base + (unsigned long long)q * delta;
-        } else {
-          do {
-            if (q >= oa && q < ob) marks[q - oa] = (unsigned short)(j + 1);
-            ++q;
-            tq += delta;
-          } while (q < N && tq < cj);
-        }
-      }
-      unsigned heavy = __ballot_sync(0xffffffffu, hi > lo);
-      while (heavy) {
-        const int srcl = __ffs(heavy) - 1;
-        heavy &= heavy - 1u;
-        const int flo = __shfl_sync(0xffffffffu, lo, srcl), fhi = __shfl_sync(0xffffffffu, hi, srcl);
-        const unsigned short v = (unsigned short)(__shfl_sync(0xffffffffu, j, srcl) + 1);
-        for (int qq = flo + lane; qq < fhi; qq += 32) marks[qq] = v;
+        const int c = 1 + (tq + delta < cj) + (tq + 2ull * delta < cj) + (tq + 3ull * delta < cj);
+        const int q1 = (c == 4 && tq + 4ull * delta < cj) ? targets_below(cj, base, delta, magic, N) : min(q + c, N);
+        if (q < ob && q1 > oa) marks[max(q, oa) - oa] = (unsigned short)(j + 1);
+        q = q1;
+        tq = base + (unsigned long long)q * delta;
       }
     }
     __syncthreads();
 
-    // gather h[ancestor] from the staged tile, coalesced store
+    // Gather: the ancestor of window slot o is the last start mark at or
+    // before o (marks increase along the window). Each warp takes a run of
+    // slots in steps of 128 (4 per lane): the running maximum of the marks
+    // is a lane-local scan, a warp max-scan and a carry from the earlier
+    // steps and warps.
+    const int chunk = ((nB + kThreads / 32 - 1) / (kThreads / 32) + 127) & ~127;
+    const int cs = warp * chunk, ce = min(cs + chunk, nB);
+    unsigned wmax = 0u;
+    for (int o0 = cs; o0 < ce; o0 += 128) {
+      const uint2 m = reinterpret_cast<const uint2*>(marks + o0)[lane];
+      wmax = max(wmax, max(max(m.x & 0xffffu, m.x >> 16), max(m.y & 0xffffu, m.y >> 16)));
+    }
+    wmax = __reduce_max_sync(0xffffffffu, wmax);
+    if (lane == 0) s_wmax[warp] = wmax;
+    __syncthreads();
+    unsigned carry = 0u;
+    for (int w = 0; w < warp; ++w) carry = max(carry, s_wmax[w]);
     if (ok) {
-      for (int qq = tid; qq < nB; qq += kThreads) {
-        unsigned jj = marks[qq];
-        if (jj == 0u || jj > (unsigned)nA) { jj = 1u; s_err = 1; }   // unreachable by construction
-        hdst[oa + qq] = hs[jj - 1u];
-        if (a.anc) a.anc[oa + qq] = j0 + (int)(jj - 1u);
+      for (int o0 = cs; o0 < ce; o0 += 128) {
+        const uint2 m = reinterpret_cast<const uint2*>(marks + o0)[lane];
+        unsigned am[4];
+        am[0] = m.x & 0xffffu;
+        am[1] = max(am[0], m.x >> 16);
+        am[2] = max(am[1], m.y & 0xffffu);
+        am[3] = max(am[2], m.y >> 16);
+        unsigned x = am[3];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const unsigned t = __shfl_up_sync(0xffffffffu, x, off);
+          if (lane >= off) x = max(x, t);
+        }
+        unsigned pre = __shfl_up_sync(0xffffffffu, x, 1);
+        pre = max(carry, lane == 0 ? 0u : pre);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int o = o0 + 4 * lane + u;
+          if (o < ce) {
+            unsigned jj = max(pre, am[u]);
+            if (jj == 0u || jj > (unsigned)nA) { jj = 1u; s_err = 1; }   // unreachable by construction
+            hdst[oa + o] = hs[jj - 1u];
+            if (a.anc) a.anc[oa + o] = j0 + (int)(jj - 1u);
+          }
+        }
+        carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
       }
     }
     __syncthreads();
