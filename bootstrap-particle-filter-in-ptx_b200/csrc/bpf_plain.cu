@@ -415,13 +415,16 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
 }
 
 // ---------------------------------------------------------------------------
-// Pass 2: persistent CTAs; the tiles (h and w) of the next work item are
-// fetched by bulk async copies into the other half of a double buffer while
-// the current item is resampled.
+// Pass 2: persistent CTAs, three per SM; the tiles (h and w) of a work item
+// are fetched by bulk async copies into shared memory as soon as the previous
+// item has released the buffer (the other CTAs on the SM hide the latency).
 // ---------------------------------------------------------------------------
 constexpr size_t kTileBytes = (size_t)kTile * 4;
 constexpr size_t kMarkBytes = (size_t)kOutChunk * 2;      // u16 ancestor (tile-local + 1) per output
-constexpr size_t kPass2Smem = 4 * kTileBytes + kMarkBytes;
+constexpr size_t kMarkOffset = 2 * kTileBytes;                 // after the staged h and w tiles
+constexpr size_t kPass2Smem = kMarkOffset + kMarkBytes;         // one staged tile (h, w) + marks
+static_assert(kMarkOffset % 16 == 0 && kMarkBytes % 16 == 0, "marks are cleared with 16-byte stores");
+static_assert((size_t)kOutChunk % 128 == 0, "the gather reads marks in steps of 128 slots");
 
 __device__ __forceinline__ void pass2_fetch(const Plan& p, const float* hsrc, int it, unsigned char* buf,
                                             uint64_t* bar) {
@@ -431,9 +434,9 @@ __device__ __forceinline__ void pass2_fetch(const Plan& p, const float* hsrc, in
   bulk_load(buf + kTileBytes, p.w + (size_t)k * kTile, (uint32_t)kTileBytes, bar);
 }
 
-__global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) pass2_kernel(Plan p, TickArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  unsigned short* marks = reinterpret_cast<unsigned short*>(smem + 4 * kTileBytes);
+  unsigned short* marks = reinterpret_cast<unsigned short*>(smem + kMarkOffset);
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ unsigned long long s_scan[kThreads / 32 + 1];
   __shared__ unsigned s_wmax[kThreads / 32];
@@ -455,19 +458,14 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
   if (tid == 0) {
     s_err = 0;
     mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
     if ((int)blockIdx.x < n_items) pass2_fetch(p, hsrc, blockIdx.x, smem, &mbar[0]);
   }
   __syncthreads();
 
+  const float* hs = reinterpret_cast<const float*>(smem);
+  const float* ws = reinterpret_cast<const float*>(smem + kTileBytes);
   int n = 0;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x, ++n) {
-    const int sb = n & 1;
-    unsigned char* buf = smem + (size_t)sb * 2 * kTileBytes;
-    const float* hs = reinterpret_cast<const float*>(buf);
-    const float* ws = reinterpret_cast<const float*>(buf + kTileBytes);
-    if (tid == 0 && it + (int)gridDim.x < n_items)
-      pass2_fetch(p, hsrc, it + gridDim.x, smem + (size_t)(sb ^ 1) * 2 * kTileBytes, &mbar[sb ^ 1]);
 
     const int4 item = p.items[it];
     const int k = item.x, oa = item.y, ob = item.z;
@@ -476,7 +474,7 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
     const int nB = ob - oa;
     const int r = nM - p.nexp[k] + kFixF - Fg;
     const unsigned long long Pk = p.P[k];
-    const bool ok = mbar_wait_bounded(&mbar[sb], (uint32_t)(n >> 1) & 1u);
+    const bool ok = mbar_wait_bounded(&mbar[0], (uint32_t)n & 1u);
     if (!ok) s_err = 1;
 
     // clear this item's ancestor marks (the previous item's gather has finished:
@@ -485,18 +483,15 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
     for (int x = tid; x < nB128 / 8; x += kThreads) reinterpret_cast<uint4*>(marks)[x] = make_uint4(0u, 0u, 0u, 0u);
 
     // exact fixed-point prefix of the tile: 16 contiguous weights per thread
-    unsigned long long L[kPerThread];
+    // (summed here, rebuilt element by element below from the staged tile)
+    const float4* wt = reinterpret_cast<const float4*>(ws + tid * kPerThread);
     unsigned long long run = 0ull;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-      const float4 f = reinterpret_cast<const float4*>(ws + tid * kPerThread)[v];
+      const float4 f = wt[v];
       const float ff[4] = {f.x, f.y, f.z, f.w};
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int j = tid * kPerThread + 4 * v + e;
-        run += (j < nA) ? fix_weight(ff[e]) : 0ull;
-        L[4 * v + e] = run;
-      }
+      for (int e = 0; e < 4; ++e) run += (tid * kPerThread + 4 * v + e < nA) ? fix_weight(ff[e]) : 0ull;
     }
     unsigned long long tot;
     const unsigned long long excl = block_excl_scan_add<kThreads>(run, &tot, s_scan);
@@ -509,11 +504,16 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
     int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
     unsigned long long tq = base + (unsigned long long)q * delta;
     int32_t* csr = (a.csr && item.w) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
+    unsigned long long accw = excl;
+    float4 f4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int e = 0; e < kPerThread; ++e) {
       const int j = tid * kPerThread + e;
       if (csr && j < nA) csr[j] = q;
-      const unsigned long long cj = Pk + shr64(excl + L[e], r);
+      if ((e & 3) == 0) f4 = wt[e >> 2];
+      const float we = (e & 3) == 0 ? f4.x : (e & 3) == 1 ? f4.y : (e & 3) == 2 ? f4.z : f4.w;
+      accw += (j < nA) ? fix_weight(we) : 0ull;
+      const unsigned long long cj = Pk + shr64(accw, r);
       if (j < nA && q < N && tq < cj) {
         const int c = 1 + (tq + delta < cj) + (tq + 2ull * delta < cj) + (tq + 3ull * delta < cj);
         const int q1 = (c == 4 && tq + 4ull * delta < cj) ? targets_below(cj, base, delta, magic, N) : min(q + c, N);
@@ -570,7 +570,8 @@ __global__ void __launch_bounds__(kThreads, 2) pass2_kernel(Plan p, TickArgs a) 
         carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
       }
     }
-    __syncthreads();
+    __syncthreads();   // the staged tile is free: fetch the next item's
+    if (tid == 0 && it + (int)gridDim.x < n_items) pass2_fetch(p, hsrc, it + gridDim.x, smem, &mbar[0]);
   }
   if (tid == 0 && s_err) p.st->error = BPF_ERR_STATE;
   griddep_release();
