@@ -25,7 +25,7 @@ namespace bpf {
 constexpr int kThreads   = 256;              // threads per CTA (pass 1 and pass 2)
 constexpr int kPerThread = 16;               // particles per thread
 constexpr int kTile      = kThreads * kPerThread;   // 4096 particles per tile
-constexpr int kOutChunk  = 3 * kTile;        // outputs per pass-2 work item (3x the mean per tile)
+constexpr int kOutChunk  = 2 * kTile;        // outputs per pass-2 work item (2x the mean per tile)
 constexpr int kPlanThreads = 512;            // threads of the single-CTA plan kernel
 constexpr int kPlanSmemTiles = 12800;        // tiles the plan kernel stages in shared memory (N <= 52.4M)
 constexpr int kFixF      = 50;               // tile-frame fraction bits: 62 - log2(kTile)

@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
 }
 
 // ---------------------------------------------------------------------------
-// Pass 2: persistent CTAs, three per SM; the tiles (h and w) of a work item
+// Pass 2: persistent CTAs, four per SM; the tiles (h and w) of a work item
 // are fetched by bulk async copies into shared memory as soon as the previous
 // item has released the buffer (the other CTAs on the SM hide the latency).
 // ---------------------------------------------------------------------------
@@ -434,7 +434,7 @@ __device__ __forceinline__ void pass2_fetch(const Plan& p, const float* hsrc, in
   bulk_load(buf + kTileBytes, p.w + (size_t)k * kTile, (uint32_t)kTileBytes, bar);
 }
 
-__global__ void __launch_bounds__(kThreads, 3) pass2_kernel(Plan p, TickArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned short* marks = reinterpret_cast<unsigned short*>(smem + kMarkOffset);
   __shared__ __align__(8) uint64_t mbar[2];
