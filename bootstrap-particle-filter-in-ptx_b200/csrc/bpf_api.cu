@@ -62,7 +62,7 @@ struct Impl {
 
   // graph of kGraphChunk ticks, keyed by the launch arguments baked into it
   cudaGraphExec_t graph = nullptr;
-  float g_mu = NAN, g_rho = NAN, g_sigma = NAN, g_thr = NAN;
+  float g_mu = NAN, g_rho = NAN, g_sigma = NAN, g_thr = NAN, g_nus = NAN;
   bool g_anc = false;
 
   // graph of a whole device-resident run (step_many_device), keyed likewise
@@ -70,7 +70,7 @@ struct Impl {
   const float* dg_y = nullptr;
   BpfTickRecord* dg_rec = nullptr;
   int dg_n = 0;
-  float dg_mu = NAN, dg_rho = NAN, dg_sigma = NAN, dg_thr = NAN;
+  float dg_mu = NAN, dg_rho = NAN, dg_sigma = NAN, dg_thr = NAN, dg_nus = NAN;
   bool dg_anc = false;
 
   // programmatic dependent launch between consecutive kernels (off while profiling)
@@ -112,6 +112,8 @@ TickArgs make_args(GpuBpfState* s, Impl* m, float y, const float* y_ptr, BpfTick
   a.y_ptr = y_ptr;
   a.rec = rec;
   a.anc = m->record_anc ? m->anc_dev : nullptr;
+  a.nu_int = (s->nu_state > 0.0f) ? (int)(s->nu_state + 0.5f) : 0;   // gpu_bpf_ptx_full.cu:392
+  a.nu_state = s->nu_state;
   return a;
 }
 
@@ -119,6 +121,7 @@ int check_options(GpuBpfState* s) {
   if (!std::isfinite(s->mu) || !std::isfinite(s->rho) || !std::isfinite(s->sigma_z)) return set_err(BPF_ERR_ARG);
   if (!(std::fabs(s->rho) < 1.0f) || !(s->sigma_z > 0.0f)) return set_err(BPF_ERR_ARG);
   if (s->silverman_shrink != 0.0f) return set_err(BPF_ERR_UNSUPPORTED);
+  if (!(s->nu_state == 0.0f || (s->nu_state >= 0.5f && std::isfinite(s->nu_state)))) return set_err(BPF_ERR_ARG);
   if (std::isnan(s->ess_threshold)) return set_err(BPF_ERR_ARG);
   return BPF_OK;
 }
@@ -216,7 +219,7 @@ int build_graph(GpuBpfState* s, Impl* m) {
   cudaError_t e3 = cudaGraphInstantiate(&m->graph, g, 0);
   cudaGraphDestroy(g);
   if (e3 != cudaSuccess) { m->graph = nullptr; return set_err(BPF_ERR_CUDA); }
-  m->g_mu = s->mu; m->g_rho = s->rho; m->g_sigma = s->sigma_z; m->g_thr = s->ess_threshold;
+  m->g_mu = s->mu; m->g_rho = s->rho; m->g_sigma = s->sigma_z; m->g_thr = s->ess_threshold; m->g_nus = s->nu_state;
   m->g_anc = m->record_anc;
   return BPF_OK;
 }
@@ -239,13 +242,14 @@ int build_device_graph(GpuBpfState* s, Impl* m, const float* y_dev, int n, BpfTi
   if (e3 != cudaSuccess) { m->dgraph = nullptr; return set_err(BPF_ERR_CUDA); }
   m->dg_y = y_dev; m->dg_rec = rec_dev; m->dg_n = n;
   m->dg_mu = s->mu; m->dg_rho = s->rho; m->dg_sigma = s->sigma_z; m->dg_thr = s->ess_threshold;
+  m->dg_nus = s->nu_state;
   m->dg_anc = m->record_anc;
   return BPF_OK;
 }
 
 bool graph_stale(GpuBpfState* s, Impl* m) {
   return !m->graph || m->g_mu != s->mu || m->g_rho != s->rho || m->g_sigma != s->sigma_z ||
-         m->g_thr != s->ess_threshold || m->g_anc != m->record_anc;
+         m->g_thr != s->ess_threshold || m->g_nus != s->nu_state || m->g_anc != m->record_anc;
 }
 
 }  // namespace
@@ -316,7 +320,7 @@ GpuBpfState* gpu_bpf_create(int n_particles, float rho, float sigma_z, float mu,
     set_err(BPF_ERR_ARG);
     return nullptr;
   }
-  if (nu_state > 0.0f) { set_err(BPF_ERR_UNSUPPORTED); return nullptr; }
+  if (nu_state > 0.0f && nu_state < 0.5f) { set_err(BPF_ERR_ARG); return nullptr; }   // round(nu_state) >= 1
   GpuBpfState* s = (GpuBpfState*)calloc(1, sizeof(GpuBpfState));
   if (!s) { set_err(BPF_ERR_ALLOC); return nullptr; }
   s->n_particles = n_particles;
@@ -508,7 +512,7 @@ int gpu_bpf_step_many_device(GpuBpfState* s, const float* y_dev, int n_ticks, Bp
   if (!m->profiling && n_ticks > 0 && n_ticks <= kMaxGraphTicks) {
     const bool stale = !m->dgraph || m->dg_y != y_dev || m->dg_rec != rec_dev || m->dg_n != n_ticks ||
                        m->dg_mu != s->mu || m->dg_rho != s->rho || m->dg_sigma != s->sigma_z ||
-                       m->dg_thr != s->ess_threshold || m->dg_anc != m->record_anc;
+                       m->dg_thr != s->ess_threshold || m->dg_nus != s->nu_state || m->dg_anc != m->record_anc;
     if (stale) { rc = build_device_graph(s, m, y_dev, n_ticks, rec_dev); if (rc) return rc; }
     CK(cudaGraphLaunch(m->dgraph, m->stream));
     g_launches += 3LL * n_ticks;

@@ -100,7 +100,9 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
           if (ck) ck[i] = h;
           if (t > 0) {
             const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
-            h = propagate(h, f.mu, f.rho, f.sigma, icdf_normal(pcg_uniform(pcg_output(s))));
+            float z = icdf_normal(pcg_uniform(pcg_output(s)));
+            if (f.nu_int > 0) z *= tstate_scale(c, (uint32_t)i, f.nu_int, f.nu_state);
+            h = propagate(h, f.mu, f.rho, f.sigma, z);
             H[si] = h;
           }
           float x = gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e);
@@ -309,9 +311,7 @@ __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_ker
 // ---------------------------------------------------------------------------
 constexpr int kBatchHeavy = 32;   // children above which a parent's walk is shared by its warp
 
-__device__ __forceinline__ float batch_noise(const PcgTick& pc, int i) {
-  return icdf_normal(pcg_uniform(pcg_output(pc.k1 + pc.k2 * pcg_inc((uint32_t)i))));
-}
+
 
 template <int NT>
 __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, int b, int maxn, float* lam,
@@ -344,7 +344,7 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
       const PcgTick pc = pcg_tick_consts(f.seed, a.g_AB[c].x, a.g_AB[c].y);
       for (int i = tid; i < N; i += NT) {
         float h = ck[i];
-        if (c > 0) h = propagate(h, f.mu, f.rho, f.sigma, batch_noise(pc, i));
+        if (c > 0) h = propagate(h, f.mu, f.rho, f.sigma, state_noise(pc, (uint32_t)i, f.nu_int, f.nu_state));
         hA[swz(i)] = h;
         if (last > c) a.g_seg[i] = h;
       }
@@ -364,7 +364,7 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
         if (hi > lo) {
           hpar = hp[swz(j0 + e)];
           if (hi - lo <= kBatchHeavy) {
-            for (int i = lo; i < hi; ++i) hc[swz(i)] = propagate(hpar, f.mu, f.rho, f.sigma, batch_noise(pc, i));
+            for (int i = lo; i < hi; ++i) hc[swz(i)] = propagate(hpar, f.mu, f.rho, f.sigma, state_noise(pc, (uint32_t)i, f.nu_int, f.nu_state));
           } else {
             wlo = lo; whi = hi;
           }
@@ -375,7 +375,7 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
           heavy &= heavy - 1u;
           const int flo = __shfl_sync(0xffffffffu, wlo, src), fhi = __shfl_sync(0xffffffffu, whi, src);
           const float fh = __shfl_sync(0xffffffffu, hpar, src);
-          for (int i = flo + lane; i < fhi; i += 32) hc[swz(i)] = propagate(fh, f.mu, f.rho, f.sigma, batch_noise(pc, i));
+          for (int i = flo + lane; i < fhi; i += 32) hc[swz(i)] = propagate(fh, f.mu, f.rho, f.sigma, state_noise(pc, (uint32_t)i, f.nu_int, f.nu_state));
         }
         lo = max(lo, hi);
       }
@@ -407,7 +407,7 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
             for (int i = lo; i < hi; ++i) {
               const float l = lam[swz(i)];
               sum += l;
-              acc_eps = fmaf(l, batch_noise(pcn, i), acc_eps);
+              acc_eps = fmaf(l, state_noise(pcn, (uint32_t)i, f.nu_int, f.nu_state), acc_eps);
             }
           } else {
             wlo = lo; whi = hi;
@@ -421,7 +421,7 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
             for (int i = flo + lane; i < fhi; i += 32) {
               const float l = lam[swz(i)];
               p += l;
-              acc_eps = fmaf(l, batch_noise(pcn, i), acc_eps);
+              acc_eps = fmaf(l, state_noise(pcn, (uint32_t)i, f.nu_int, f.nu_state), acc_eps);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
@@ -456,7 +456,7 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
         acs += cs;
         acsh = fmaf(cs, h - f.mu, acsh);
         if (t == 0) {
-          const float z0 = batch_noise(pc0, j);
+          const float z0 = state_noise(pc0, (uint32_t)j, 0, 0.0f);
           al0 += l;
           al0z = fmaf(l, z0, al0z);
         }

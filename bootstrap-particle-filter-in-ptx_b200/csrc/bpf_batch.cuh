@@ -25,7 +25,9 @@ constexpr int kBatchMaxTiles = kBatchMaxN / kTile;
 struct BatchFilterDev {                    // 48 bytes, one per filter
   float mu, rho, sigma, std_stat;
   float nu, c_obs, inv_nu, nu_p1h;
-  int n, seed, pad0, pad1;
+  int n, seed;
+  int nu_int;                              // Student-t state noise dof round(nu_state), 0 = Gaussian
+  float nu_state;
 };
 
 struct BatchArgs {

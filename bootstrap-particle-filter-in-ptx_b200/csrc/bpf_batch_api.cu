@@ -288,7 +288,7 @@ GpuBpfBatch* gpu_bpf_batch_create(const BpfBatchFilter* filters, int n_filters, 
     const BpfBatchFilter& f = filters[i];
     if (f.n_particles <= 0 || f.n_particles > kBatchMaxN || !std::isfinite(f.mu) || !std::isfinite(f.rho) ||
         !std::isfinite(f.sigma_z) || !(std::fabs(f.rho) < 1.0f) || !(f.sigma_z > 0.0f) || !std::isfinite(f.nu_obs) ||
-        !(f.nu_obs >= 0.0f)) {
+        !(f.nu_obs >= 0.0f) || !(f.nu_state == 0.0f || (f.nu_state >= 0.5f && std::isfinite(f.nu_state)))) {
       bpf_record_error(BPF_ERR_ARG);
       return nullptr;
     }
@@ -305,6 +305,8 @@ GpuBpfBatch* gpu_bpf_batch_create(const BpfBatchFilter* filters, int n_filters, 
     }
     d.n = f.n_particles;
     d.seed = f.seed;
+    d.nu_int = (f.nu_state > 0.0f) ? (int)(f.nu_state + 0.5f) : 0;   // gpu_bpf_ptx_full.cu:392
+    d.nu_state = f.nu_state;
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); bpf_record_error(BPF_ERR_NODEVICE); return nullptr; }

@@ -171,6 +171,42 @@ __device__ __forceinline__ float obs_logpdf(const ObsModel& m, float h) {
   return fmaf(-0.5f, h, lw);
 }
 
+// ---------------------------------------------------------------------------
+// Student-t state noise (nu_state > 0). The reference scales the normal draw by
+// rsqrt(chi2 / nu_state), chi2 the sum of round(nu_state) squared normals from
+// a separate cuRAND stream (gpu_bpf/gpu_bpf_ptx_full.cu:392-400,574-583;
+// ptx_assembly/bpf_kernels_full.ptx:394-404). Here chi2 with k = round(nu_state)
+// degrees of freedom is drawn exactly and statelessly: -2 ln(U_1 ... U_{k/2})
+// (a sum of k/2 exponentials of mean 2) plus Z^2 when k is odd. Component c of
+// slot i at tick t is draw t of the PCG32 stream with the particle's seed and
+// increment ((c+1) << 33) | (2i+1), which no particle stream uses (their
+// increments are below 2^32), so the counter-based jump of the tick applies
+// unchanged. The log is summed in log2 (no underflow for large k).
+// ---------------------------------------------------------------------------
+__host__ __device__ inline uint64_t tstate_inc(uint32_t i, int c) {
+  return ((uint64_t)(c + 1) << 33) | (uint64_t)(2u * i + 1u);
+}
+
+__device__ __forceinline__ float tstate_scale(const PcgTick& pc, uint32_t i, int nu_int, float nu_state) {
+  const int pairs = nu_int >> 1;
+  float l2sum = 0.0f;
+  for (int c = 0; c < pairs; ++c)
+    l2sum += lg2_approx(pcg_uniform(pcg_output(pc.k1 + pc.k2 * tstate_inc(i, c))));
+  float chi2 = (-2.0f * kLn2) * l2sum;
+  if (nu_int & 1) {
+    const float z = icdf_normal(pcg_uniform(pcg_output(pc.k1 + pc.k2 * tstate_inc(i, pairs))));
+    chi2 = fmaf(z, z, chi2);
+  }
+  return sqrt_approx(div_approx(nu_state, chi2));
+}
+
+// State noise eps of slot i at the tick of pc: N(0,1), or Student-t when nu_int > 0.
+__device__ __forceinline__ float state_noise(const PcgTick& pc, uint32_t i, int nu_int, float nu_state) {
+  float z = icdf_normal(pcg_uniform(pcg_output(pc.k1 + pc.k2 * pcg_inc(i))));
+  if (nu_int > 0) z *= tstate_scale(pc, i, nu_int, nu_state);
+  return z;
+}
+
 // OU transition with the reference's operation order (PTX :406-411):
 //   dev = rho*(h-mu); h = mu + dev; h = fma(sigma, eps, h)
 __device__ __forceinline__ float propagate(float h, float mu, float rho, float sigma, float eps) {

@@ -23,9 +23,6 @@
 
 namespace bpf {
 
-__device__ __forceinline__ float noise_of(const PcgTick& pc, int i) {
-  return icdf_normal(pcg_uniform(pcg_output(pc.k1 + pc.k2 * pcg_inc((uint32_t)i))));
-}
 
 // First child of each of the thread's four parents and the end of the last
 // one's children: children of parent e are [f[e], f[e+1]). Parents at or past
@@ -67,7 +64,7 @@ __device__ __forceinline__ float warp_sum_f(float v) {
 __global__ void __launch_bounds__(kGradThreads) grad_seed_kernel(int N, const float* __restrict__ ckpt,
                                                                   float* __restrict__ h_out, PcgTick pc,
                                                                   int propagate_tick, float mu, float rho,
-                                                                  float sigma) {
+                                                                  float sigma, int nu_int, float nu_state) {
   griddep_wait();
   const int j0 = (blockIdx.x * kGradThreads + threadIdx.x) * kGradGroup;
   float4 h4 = *reinterpret_cast<const float4*>(ckpt + j0);
@@ -75,7 +72,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_seed_kernel(int N, const fl
     float hh[4] = {h4.x, h4.y, h4.z, h4.w};
 #pragma unroll
     for (int e = 0; e < kGradGroup; ++e)
-      if (j0 + e < N) hh[e] = propagate(hh[e], mu, rho, sigma, noise_of(pc, j0 + e));
+      if (j0 + e < N) hh[e] = propagate(hh[e], mu, rho, sigma, state_noise(pc, (uint32_t)(j0 + e), nu_int, nu_state));
     h4 = make_float4(hh[0], hh[1], hh[2], hh[3]);
   }
   *reinterpret_cast<float4*>(h_out + j0) = h4;
@@ -85,7 +82,8 @@ __global__ void __launch_bounds__(kGradThreads) grad_seed_kernel(int N, const fl
 __global__ void __launch_bounds__(kGradThreads) grad_recompute_kernel(int N, const int32_t* __restrict__ csr,
                                                                        const float* __restrict__ hp,
                                                                        float* __restrict__ hc, PcgTick pc,
-                                                                       float mu, float rho, float sigma) {
+                                                                       float mu, float rho, float sigma, int nu_int,
+                                                                       float nu_state) {
   griddep_wait();
   const int lane = threadIdx.x & 31;
   const int j0 = (blockIdx.x * kGradThreads + threadIdx.x) * kGradGroup;
@@ -98,7 +96,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_recompute_kernel(int N, con
     int c = f[0];
 #pragma unroll
     for (int e = 0; e < kGradGroup; ++e)
-      for (; c < f[e + 1]; ++c) hc[c] = propagate(hv[e], mu, rho, sigma, noise_of(pc, c));
+      for (; c < f[e + 1]; ++c) hc[c] = propagate(hv[e], mu, rho, sigma, state_noise(pc, (uint32_t)c, nu_int, nu_state));
   }
   unsigned hm = __ballot_sync(0xffffffffu, heavy);
   while (hm) {
@@ -112,7 +110,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_recompute_kernel(int N, con
     for (int e = 0; e < 4; ++e) hs[e] = __shfl_sync(0xffffffffu, hv[e], src);
     for (int c = g[0] + lane; c < g[4]; c += 32) {
       const float h = pick4(parent_of(c, g), hs[0], hs[1], hs[2], hs[3]);
-      hc[c] = propagate(h, mu, rho, sigma, noise_of(pc, c));
+      hc[c] = propagate(h, mu, rho, sigma, state_noise(pc, (uint32_t)c, nu_int, nu_state));
     }
   }
   griddep_release();
@@ -144,7 +142,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_adjoint_kernel(GradAdjArgs 
         for (; c < f[e + 1]; ++c) {
           const float l = a.lam_next[c];
           cs[e] += l;
-          acc_eps = fmaf(l, noise_of(a.pc_next, c), acc_eps);
+          acc_eps = fmaf(l, state_noise(a.pc_next, (uint32_t)c, a.nu_int, a.nu_state), acc_eps);
         }
     }
     unsigned hm = __ballot_sync(0xffffffffu, heavy);
@@ -162,7 +160,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_adjoint_kernel(GradAdjArgs 
         p[1] += (e == 1) ? l : 0.f;
         p[2] += (e == 2) ? l : 0.f;
         p[3] += (e == 3) ? l : 0.f;
-        acc_eps = fmaf(l, noise_of(a.pc_next, c), acc_eps);
+        acc_eps = fmaf(l, state_noise(a.pc_next, (uint32_t)c, a.nu_int, a.nu_state), acc_eps);
       }
 #pragma unroll
       for (int e = 0; e < 4; ++e) p[e] = warp_sum_f(p[e]);
@@ -202,7 +200,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_adjoint_kernel(GradAdjArgs 
       acc_cs += cs[e];
       acc_csh = fmaf(cs[e], h - a.mu, acc_csh);
       if (a.first) {
-        const float z0 = noise_of(a.pc0, j);
+        const float z0 = state_noise(a.pc0, (uint32_t)j, 0, 0.0f);
         acc_l0 += l;
         acc_l0z = fmaf(l, z0, acc_l0z);
       }
@@ -338,7 +336,7 @@ __global__ void __launch_bounds__(kGradThreads) replay_init_kernel(ReplayArgs a)
   for (int e = 0; e < kGradGroup; ++e) {
     const int j = j0 + e;
     if (j >= a.N) break;
-    const double z = (double)noise_of(a.pc, j);
+    const double z = (double)state_noise(a.pc, (uint32_t)j, 0, 0.0f);
     const double h = fma(sstat, z, mu), d0 = 1.0, d1 = z * ds_drho, d2 = z * ds_dsig;
     a.hc[j] = h; a.hc[a.stride + j] = d0; a.hc[2 * (size_t)a.stride + j] = d1; a.hc[3 * (size_t)a.stride + j] = d2;
     double lw, g;
@@ -364,7 +362,7 @@ __global__ void __launch_bounds__(kGradThreads) replay_tick_kernel(ReplayArgs a)
   OnlineLse acc;
   acc.init();
   auto child = [&](int c, double hpar, double d0p, double d1p, double d2p) {
-    const double eps = (double)noise_of(a.pc, c);
+    const double eps = (double)state_noise(a.pc, (uint32_t)c, a.nu_int, a.nu_state);
     const double h = mu + rho * (hpar - mu) + sg * eps;
     const double d0 = (1.0 - rho) + rho * d0p, d1 = (hpar - mu) + rho * d1p, d2 = eps + rho * d2p;
     a.hc[c] = h; a.hc[S + c] = d0; a.hc[2 * S + c] = d1; a.hc[3 * S + c] = d2;
@@ -467,12 +465,14 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), int grid, cudaStream_t s, 
 }
 
 cudaError_t launch_grad_seed(int N, const float* ckpt, float* h_out, PcgTick pc, int propagate_tick, float mu,
-                             float rho, float sigma, cudaStream_t s, bool pdl) {
-  return launch_pdl(grad_seed_kernel, grad_ctas(N), s, pdl, N, ckpt, h_out, pc, propagate_tick, mu, rho, sigma);
+                             float rho, float sigma, int nu_int, float nu_state, cudaStream_t s, bool pdl) {
+  return launch_pdl(grad_seed_kernel, grad_ctas(N), s, pdl, N, ckpt, h_out, pc, propagate_tick, mu, rho, sigma,
+                    nu_int, nu_state);
 }
 cudaError_t launch_grad_recompute(int N, const int32_t* csr, const float* hp, float* hc, PcgTick pc, float mu,
-                                  float rho, float sigma, cudaStream_t s, bool pdl) {
-  return launch_pdl(grad_recompute_kernel, grad_ctas(N), s, pdl, N, csr, hp, hc, pc, mu, rho, sigma);
+                                  float rho, float sigma, int nu_int, float nu_state, cudaStream_t s, bool pdl) {
+  return launch_pdl(grad_recompute_kernel, grad_ctas(N), s, pdl, N, csr, hp, hc, pc, mu, rho, sigma, nu_int,
+                    nu_state);
 }
 cudaError_t launch_grad_adjoint(const GradAdjArgs& a, cudaStream_t s, bool pdl) {
   return launch_pdl(grad_adjoint_kernel, grad_ctas(a.N), s, pdl, a);

@@ -19,7 +19,7 @@
 // and the parameter adjoints accumulate per CTA in FP64:
 //   dL/dmu    += (1-rho) sum_i lambda_t+1,i          (h_t+1 = mu(1-rho) + rho h~ + sigma eps)
 //   dL/drho   += sum_j cs_t,j (h_t,j - mu)           (cs = children sum)
-//   dL/dsigma += sum_i lambda_t+1,i eps_t+1,i
+//   dL/dsigma += sum_i lambda_t+1,i eps_t+1,i       (eps Gaussian or Student-t state noise)
 // plus the stationary initial draw h_0 = mu + sigma z / sqrt(1-rho^2).
 //
 // Reference: tests/diff_bpf.py:186-237 differentiates the same loss by autograd
@@ -57,6 +57,8 @@ struct GradAdjArgs {
   PcgTick pc_next;         // noise constants of tick t+1
   PcgTick pc0;             // draw-0 constants (initial particles)
   int first;               // t == 0
+  int nu_int;              // Student-t state noise dof (0 = Gaussian)
+  float nu_state;
   double* acc;             // [CTAs][kGradAcc]
 };
 
@@ -70,6 +72,8 @@ struct ReplayArgs {
   double* hc;              // state of tick t (out)
   int stride;              // N4
   PcgTick pc;              // noise constants of tick t
+  int nu_int;              // Student-t state noise dof (0 = Gaussian)
+  float nu_state;
   double* part;            // [CTAs][5]: (max, sum, sum*g*dh/dmu, .. drho, .. dsigma) of this tick
 };
 
@@ -77,9 +81,9 @@ inline int grad_ctas(int N) { return (N + kGradTile - 1) / kGradTile; }
 inline int grad_stride(int N) { return grad_ctas(N) * kGradTile; }
 
 cudaError_t launch_grad_seed(int N, const float* ckpt, float* h_out, PcgTick pc, int propagate, float mu,
-                             float rho, float sigma, cudaStream_t s, bool pdl);
+                             float rho, float sigma, int nu_int, float nu_state, cudaStream_t s, bool pdl);
 cudaError_t launch_grad_recompute(int N, const int32_t* csr, const float* hp, float* hc, PcgTick pc, float mu,
-                                  float rho, float sigma, cudaStream_t s, bool pdl);
+                                  float rho, float sigma, int nu_int, float nu_state, cudaStream_t s, bool pdl);
 cudaError_t launch_grad_adjoint(const GradAdjArgs& a, cudaStream_t s, bool pdl);
 cudaError_t launch_grad_finish(int ctas, const double* acc, float mu, float rho, float sigma, double* grad,
                                cudaStream_t s, bool pdl);

@@ -34,11 +34,12 @@ constexpr int kDefaultCheckpoint = 16;
 
 struct FwdKey {
   int T = -1, seed = 0;
-  float mu = NAN, rho = NAN, sigma = NAN, nu = NAN;
+  float mu = NAN, rho = NAN, sigma = NAN, nu = NAN, nu_state = NAN;
   const float* y = nullptr;
   double* ll = nullptr;
   bool operator==(const FwdKey& o) const {
     return T == o.T && seed == o.seed && mu == o.mu && rho == o.rho && sigma == o.sigma && nu == o.nu &&
+           nu_state == o.nu_state &&
            y == o.y && ll == o.ll;
   }
 };
@@ -47,6 +48,8 @@ struct BwdKey {
   double* grad = nullptr;
   bool operator==(const BwdKey& o) const { return f == o.f && grad == o.grad; }
 };
+
+int nu_int_of(float nu_state) { return nu_state > 0.0f ? (int)(nu_state + 0.5f) : 0; }   // gpu_bpf_ptx_full.cu:392
 
 ObsModel make_obs(float nu_obs) {
   ObsModel o{};
@@ -145,6 +148,8 @@ cudaError_t enqueue_forward(GpuBpfGrad* g, const FwdKey& k) {
     a.ckpt = (t % g->K == 0) ? g->ckpt + (size_t)(t / g->K) * g->ckpt_stride : nullptr;
     a.csr = g->csr + (size_t)t * g->N4;
     a.aux = g->aux + t;
+    a.nu_int = nu_int_of(k.nu_state);
+    a.nu_state = k.nu_state;
     e = launch_pass1(g->plan, a, g->stream, g->pdl);
     if (e == cudaSuccess) e = launch_plan(g->plan, a, g->stream, g->pdl);
     if (e == cudaSuccess) e = launch_pass2(g->plan, a, g->pass2_grid, g->stream, g->pdl);
@@ -158,17 +163,18 @@ cudaError_t enqueue_backward(GpuBpfGrad* g, const BwdKey& bk) {
   const FwdKey& k = bk.f;
   const int T = k.T, N = g->N, K = g->K;
   const ObsModel obs = make_obs(k.nu);
+  const int nui = nu_int_of(k.nu_state);
   cudaError_t e = cudaMemsetAsync(g->acc, 0, (size_t)g->G1 * kGradAcc * sizeof(double), g->stream);
   const int nseg = (T + K - 1) / K;
   for (int s = nseg - 1; s >= 0 && e == cudaSuccess; --s) {
     const int c = s * K, last = std::min(c + K, T) - 1;
     // recompute h_c .. h_last into seg[0 .. last-c]
     e = launch_grad_seed(N, g->ckpt + (size_t)s * g->ckpt_stride, g->seg, g->pcs[c], c > 0 ? 1 : 0, k.mu, k.rho,
-                         k.sigma, g->stream, g->pdl);
+                         k.sigma, nui, k.nu_state, g->stream, g->pdl);
     for (int t = c + 1; t <= last && e == cudaSuccess; ++t)
       e = launch_grad_recompute(N, g->csr + (size_t)(t - 1) * g->N4, g->seg + (size_t)(t - 1 - c) * g->N4,
-                                g->seg + (size_t)(t - c) * g->N4, g->pcs[t], k.mu, k.rho, k.sigma, g->stream,
-                                g->pdl);
+                                g->seg + (size_t)(t - c) * g->N4, g->pcs[t], k.mu, k.rho, k.sigma, nui,
+                                k.nu_state, g->stream, g->pdl);
     // adjoint last .. c
     for (int t = last; t >= c && e == cudaSuccess; --t) {
       GradAdjArgs a{};
@@ -184,6 +190,8 @@ cudaError_t enqueue_backward(GpuBpfGrad* g, const BwdKey& bk) {
       a.pc_next = g->pcs[t + 1];
       a.pc0 = g->pcs[0];
       a.first = (t == 0);
+      a.nu_int = nui;
+      a.nu_state = k.nu_state;
       a.acc = g->acc;
       e = launch_grad_adjoint(a, g->stream, g->pdl);
     }
@@ -280,18 +288,20 @@ void* gpu_bpf_grad_stream(GpuBpfGrad* g) { return g ? (void*)g->stream : nullptr
 
 int gpu_bpf_grad_checkpoint_every(GpuBpfGrad* g) { return g ? g->K : -bpf_record_error(BPF_ERR_STATE); }
 
-int gpu_bpf_grad_forward(GpuBpfGrad* g, float mu, float rho, float sigma_z, float nu_obs, int seed,
+int gpu_bpf_grad_forward(GpuBpfGrad* g, float mu, float rho, float sigma_z, float nu_state, float nu_obs, int seed,
                          float ess_threshold, const float* y_dev, int n_ticks, double* loglik_dev) {
   if (!g) return bpf_record_error(BPF_ERR_STATE);
   if (!y_dev || !loglik_dev || n_ticks <= 0 || n_ticks > g->T_max) return bpf_record_error(BPF_ERR_ARG);
   if (!std::isfinite(mu) || !std::isfinite(rho) || !std::isfinite(sigma_z) || !(std::fabs(rho) < 1.0f) ||
-      !(sigma_z > 0.0f) || !(nu_obs >= 0.0f) || !std::isfinite(nu_obs))
+      !(sigma_z > 0.0f) || !(nu_obs >= 0.0f) || !std::isfinite(nu_obs) ||
+      !(nu_state == 0.0f || (nu_state >= 0.5f && std::isfinite(nu_state))))
     return bpf_record_error(BPF_ERR_ARG);
   if (ess_threshold != 0.0f) return bpf_record_error(BPF_ERR_UNSUPPORTED);   // always-resample tapes only
   int rc = ensure_dev(g);
   if (rc) return rc;
   FwdKey k;
-  k.T = n_ticks; k.seed = seed; k.mu = mu; k.rho = rho; k.sigma = sigma_z; k.nu = nu_obs; k.y = y_dev; k.ll = loglik_dev;
+  k.T = n_ticks; k.seed = seed; k.mu = mu; k.rho = rho; k.sigma = sigma_z; k.nu = nu_obs; k.nu_state = nu_state;
+  k.y = y_dev; k.ll = loglik_dev;
   if (!g->fgraph || !(g->fkey == k)) {
     GCK(capture(g, &g->fgraph, [&]() { return enqueue_forward(g, k); }));
     g->fkey = k;
@@ -353,6 +363,8 @@ int gpu_bpf_grad_replay(GpuBpfGrad* g, double mu, double rho, double sigma_z, do
   a.N = g->N;
   a.mu = mu; a.rho = rho; a.sigma = sigma_z;
   a.obs = make_obs(k.nu);
+  a.nu_int = nu_int_of(k.nu_state);
+  a.nu_state = k.nu_state;
   a.stride = g->N4;
   for (int t = 0; t < k.T; ++t) {
     a.y = k.y + t;

@@ -1,7 +1,8 @@
 // bpf_plain.cu — the plain SV bootstrap-filter tick as three sm_100a kernels.
 //
 //   pass 1  (one CTA per 4096-particle tile, streaming)
-//           counter-PCG32 -> inverse-CDF normal -> OU propagate -> log2-weight
+//           counter-PCG32 -> inverse-CDF normal (x Student-t scale when
+//           nu_state > 0) -> OU propagate -> log2-weight
 //           (+ carried weight on ESS-skipped ticks). The tile max becomes a
 //           power-of-two exponent n_k; tile-relative weights w = 2^(x - n_k)
 //           are written once, with the tile partials S=sum w, Q=sum w^2,
@@ -67,6 +68,7 @@ constexpr int kStWords = (int)(sizeof(DevState) / 8);
 // ---------------------------------------------------------------------------
 // Pass 1
 // ---------------------------------------------------------------------------
+template <bool TSTATE>
 __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
   __shared__ float s_max[kThreads / 32];
   __shared__ double s_red[3][kThreads / 32];
@@ -120,7 +122,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     for (int e = 0; e < 4; ++e) {
       float h = hh[e];
       if (tick > 0) {
-        const float z = icdf_normal(pcg_uniform(pcg_output(s)));
+        float z = icdf_normal(pcg_uniform(pcg_output(s)));
+        if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
         h = propagate(h, a.mu, a.rho, a.sigma, z);
       }
       s += step2;
@@ -662,7 +665,8 @@ int pass2_grid_size(int device) {
 }
 
 cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
-  return launch_ex(pass1_kernel, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a);
+  if (a.nu_int > 0) return launch_ex(pass1_kernel<true>, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a);
+  return launch_ex(pass1_kernel<false>, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a);
 }
 cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
   return launch_ex(plan_kernel, dim3(1), dim3(kPlanThreads), plan_smem_bytes(p.G), s, pdl, p, a);

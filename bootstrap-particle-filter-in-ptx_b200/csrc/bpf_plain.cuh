@@ -61,6 +61,8 @@ struct TickArgs {
   const float* y_ptr;        // device pointer to this tick's observation, or null
   BpfTickRecord* rec;        // device record slot written by the last pass-1 CTA
   int32_t* anc;              // ancestors of this tick (N ints) or null
+  int nu_int;                // Student-t state noise: round(nu_state) degrees of freedom, 0 = Gaussian
+  float nu_state;            // Student-t state noise scale parameter
   // gradient tape (all null outside a taped run)
   float* ckpt;               // copy of the particles pass 1 reads this tick (G*4096 floats) or null
   int32_t* csr;              // on resampling ticks: first child slot of every parent (N ints) or null

@@ -57,7 +57,7 @@ class GpuBpfState(C.Structure):
 
 class BpfBatchFilter(C.Structure):
     _fields_ = [("mu", C.c_float), ("rho", C.c_float), ("sigma_z", C.c_float), ("nu_obs", C.c_float),
-                ("n_particles", C.c_int), ("seed", C.c_int)]
+                ("n_particles", C.c_int), ("seed", C.c_int), ("nu_state", C.c_float)]
 
 
 P_STATE = C.POINTER(GpuBpfState)
@@ -126,7 +126,7 @@ SIGNATURES = {
     "gpu_bpf_grad_tape_bytes": (C.c_size_t, [_i, _i, _i]),
     "gpu_bpf_grad_stream": (_vp, [_vp]),
     "gpu_bpf_grad_checkpoint_every": (_i, [_vp]),
-    "gpu_bpf_grad_forward": (_i, [_vp, _f, _f, _f, _f, _i, _f, _vp, _i, _vp]),
+    "gpu_bpf_grad_forward": (_i, [_vp, _f, _f, _f, _f, _f, _i, _f, _vp, _i, _vp]),
     "gpu_bpf_grad_backward": (_i, [_vp, _vp]),
     "gpu_bpf_grad_replay": (_i, [_vp, _d, _d, _d, _vp, _vp]),
     "gpu_bpf_grad_get_records": (_i, [_vp, C.POINTER(BpfTickRecord), _i]),

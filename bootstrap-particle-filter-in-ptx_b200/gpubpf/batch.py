@@ -19,7 +19,8 @@ class GpuBpfBatch:
         arr = (BpfBatchFilter * len(fl))()
         for i, f in enumerate(fl):
             arr[i] = BpfBatchFilter(float(f["mu"]), float(f["rho"]), float(f["sigma_z"]),
-                                    float(f.get("nu_obs", 0.0)), int(f["n_particles"]), int(f["seed"]))
+                                    float(f.get("nu_obs", 0.0)), int(f["n_particles"]), int(f["seed"]),
+                                    float(f.get("nu_state", 0.0)))
         h = self._lib.gpu_bpf_batch_create(arr, len(fl), float(ess_threshold))
         if not h:
             raise BpfError(self._lib.gpu_bpf_last_error(), "gpu_bpf_batch_create")

@@ -85,7 +85,8 @@ class GradTape:
         ev.record(self._stream)
         torch.cuda.current_stream(self.device).wait_event(ev)
 
-    def forward(self, theta: Sequence[float], y: torch.Tensor, seed: int = 42, nu_obs: float = 0.0) -> torch.Tensor:
+    def forward(self, theta: Sequence[float], y: torch.Tensor, seed: int = 42, nu_obs: float = 0.0,
+                nu_state: float = 0.0) -> torch.Tensor:
         """Taped run at theta = (mu, rho, sigma_z) on y (device float32): FP64 total loglik (0-d tensor)."""
         mu, rho, sig = (float(v) for v in theta)
         T = int(y.shape[0])
@@ -94,7 +95,7 @@ class GradTape:
         with torch.cuda.device(self.device):
             self._y[:T].copy_(y.reshape(-1).to(device=self.device, dtype=torch.float32))
             self._enter()
-            check(self._lib.gpu_bpf_grad_forward(self._h, mu, rho, sig, float(nu_obs), int(seed), 0.0,
+            check(self._lib.gpu_bpf_grad_forward(self._h, mu, rho, sig, float(nu_state), float(nu_obs), int(seed), 0.0,
                                                  C.c_void_p(self._y.data_ptr()), T, C.c_void_p(self._ll.data_ptr())),
                   "gpu_bpf_grad_forward")
             self._leave()

@@ -29,7 +29,7 @@ extern "C" {
 #define BPF_ERR_ARG          1  /* invalid argument (N<=0, |rho|>=1, sigma<=0, non-finite y, NULL) */
 #define BPF_ERR_CUDA         2  /* a CUDA runtime call failed                                       */
 #define BPF_ERR_ALLOC        3  /* device or pinned allocation failed                               */
-#define BPF_ERR_UNSUPPORTED  4  /* option outside this build (nu_state>0, bands, Silverman)         */
+#define BPF_ERR_UNSUPPORTED  4  /* option outside this build (bands, Silverman, learning)            */
 #define BPF_ERR_STATE        5  /* call not valid in the filter's current state                     */
 #define BPF_ERR_DEGENERATE   6  /* every particle weight underflowed on a tick                      */
 #define BPF_ERR_NODEVICE     7  /* no CUDA device / kernel image for this GPU                       */
@@ -80,8 +80,10 @@ typedef struct {
 /* gpu_bpf/gpu_bpf.cuh:56-57. Seeds the per-slot PCG32 streams and draws h_0
  * from N(mu, sigma_z^2/max(1-rho^2,1e-6)) (gpu_bpf_ptx_full.cu:340-438).
  * Default ess_threshold 0.5 (PTX edition, gpu_bpf_ptx_full.cu:356).
- * Returns NULL on failure (reason in gpu_bpf_last_error()); nu_state > 0 is
- * rejected with BPF_ERR_UNSUPPORTED. */
+ * Returns NULL on failure (reason in gpu_bpf_last_error()). nu_state > 0 selects
+ * Student-t state noise eps = z sqrt(nu_state / chi2), chi2 with round(nu_state)
+ * degrees of freedom (the reference's law, drawn from counter-based PCG32 streams
+ * instead of a cuRAND pre-pass); 0 < nu_state < 0.5 is rejected (BPF_ERR_ARG). */
 GpuBpfState* gpu_bpf_create(int n_particles, float rho, float sigma_z, float mu,
                             float nu_state, float nu_obs, int seed);
 
@@ -240,6 +242,7 @@ typedef struct {
     float mu, rho, sigma_z, nu_obs;
     int   n_particles;
     int   seed;
+    float nu_state;   /* Student-t state noise as in gpu_bpf_create (0 = Gaussian) */
 } BpfBatchFilter;
 typedef struct GpuBpfBatch GpuBpfBatch;
 
@@ -301,11 +304,12 @@ void        gpu_bpf_grad_destroy(GpuBpfGrad* grad);
 size_t      gpu_bpf_grad_tape_bytes(int n_particles, int max_ticks, int checkpoint_every);
 void*       gpu_bpf_grad_stream(GpuBpfGrad* grad);                 /* cudaStream_t of the tape */
 int         gpu_bpf_grad_checkpoint_every(GpuBpfGrad* grad);
-/* Taped forward run from a fresh start (as gpu_bpf_create + reset(seed) + n_ticks steps):
+/* Taped forward run from a fresh start (as gpu_bpf_create + reset(seed) + n_ticks steps;
+ * nu_state and nu_obs as in gpu_bpf_create):
  * y_dev[n_ticks] in, loglik_dev[0] = FP64 total log-likelihood out. Enqueued on the tape's
  * stream. ess_threshold must be 0 (BPF_ERR_UNSUPPORTED otherwise). */
-int gpu_bpf_grad_forward(GpuBpfGrad* grad, float mu, float rho, float sigma_z, float nu_obs, int seed,
-                         float ess_threshold, const float* y_dev, int n_ticks, double* loglik_dev);
+int gpu_bpf_grad_forward(GpuBpfGrad* grad, float mu, float rho, float sigma_z, float nu_state, float nu_obs,
+                         int seed, float ess_threshold, const float* y_dev, int n_ticks, double* loglik_dev);
 /* Adjoint of the last taped run: grad_dev[3] = d loglik / d(mu, rho, sigma_z), FP64. */
 int gpu_bpf_grad_backward(GpuBpfGrad* grad, double* grad_dev);
 /* FP64 re-run of the taped run's noise and ancestors at (mu, rho, sigma_z) with forward-mode

@@ -19,6 +19,7 @@
  *                        resampling ancestors held fixed (tests/diff_bpf.py:186-237
  *                        with detached indices :35-56), forward-mode tangents or
  *                        reverse-mode adjoint
+ *   orc_tstate_scale     Student-t state-noise scale (counter-based chi2 draws)
  *   orc_resample_fixed   exact mirror of the GPU fixed-point systematic resampling
  *   orc_ref_run          FP32 restatement of the reference tick loop
  *                        (gpu_bpf_ptx_full.cu:340-771 with PTX kernels :51-842),
@@ -197,7 +198,38 @@ typedef struct {
     float rho, sigma_z, mu, nu_obs;
     int seed;
     float ess_threshold;
+    float nu_state;        /* Student-t state noise, 0 = Gaussian */
 } OrcConfig;
+
+/*
+ * Student-t state-noise scale sqrt(nu_state / chi2) of slot i at tick t, chi2
+ * with k = round(nu_state) degrees of freedom drawn as -2 ln(U_1 ... U_{k/2})
+ * (+ Z^2 when k is odd). Component c is draw t of the PCG32 stream with the
+ * filter seed and increment ((c+1) << 33) | (2i+1). This build's counter-based
+ * restatement of the reference's chi2 pre-pass (gpu_bpf/gpu_bpf_ptx_full.cu:
+ * 392-400,574-583, PTX :394-404), evaluated in FP64.
+ */
+static uint32_t pcg_draw_inc(int seed, uint64_t inc, int t) {
+    uint64_t s0 = ((uint64_t)(int64_t)seed * PCG_A + inc) * PCG_A + inc, At, Bt;
+    orc_pcg32_jump((uint64_t)t, &At, &Bt);
+    return orc_pcg32_output(At * s0 + Bt * inc);
+}
+double orc_tstate_scale(int seed, uint32_t i, int t, int nu_int, double nu_state) {
+    const int pairs = nu_int >> 1;
+    double l = 0.0;
+    for (int c = 0; c < pairs; ++c) {
+        uint64_t inc = ((uint64_t)(c + 1) << 33) | (uint64_t)(2u * i + 1u);
+        l += log((double)orc_uniform(pcg_draw_inc(seed, inc, t)));
+    }
+    double chi2 = -2.0 * l;
+    if (nu_int & 1) {
+        uint64_t inc = ((uint64_t)(pairs + 1) << 33) | (uint64_t)(2u * i + 1u);
+        double z = orc_icdf_f64((double)orc_uniform(pcg_draw_inc(seed, inc, t)));
+        chi2 += z * z;
+    }
+    return sqrt(nu_state / chi2);
+}
+static int nu_int_of(double nu_state) { return nu_state > 0.0 ? (int)(nu_state + 0.5) : 0; }
 
 static int ceil_log2_u(unsigned n) { int c = 0; while ((1ull << c) < (unsigned long long)n) ++c; return c; }
 
@@ -218,6 +250,7 @@ int orc_filter_f64(const OrcConfig* c, const float* y, int T,
     double* cdf = (double*)malloc(sizeof(double) * N);
     if (!h || !hn || !lw || !lwc || !cdf) { free(h); free(hn); free(lw); free(lwc); free(cdf); return 2; }
     const double mu = c->mu, rho = c->rho, sig = c->sigma_z, nu = c->nu_obs, cobs = c_obs_of(nu);
+    const int nu_int = nu_int_of((double)c->nu_state);
     const double sstat = sqrt(sig * sig / fmax(1.0 - rho * rho, 1e-6));
     for (int i = 0; i < N; ++i) {
         float u = orc_uniform(orc_pcg32_draw_jump(c->seed, (uint32_t)i, 0));
@@ -235,7 +268,9 @@ int orc_filter_f64(const OrcConfig* c, const float* y, int T,
                 uint64_t s0, inc;
                 orc_pcg32_init(c->seed, (uint32_t)i, &s0, &inc);
                 float u = orc_uniform(orc_pcg32_output(At * s0 + Bt * inc));
-                h[i] = mu + rho * (h[i] - mu) + sig * orc_icdf_f64((double)u);
+                double eps = orc_icdf_f64((double)u);
+                if (nu_int > 0) eps *= orc_tstate_scale(c->seed, (uint32_t)i, t, nu_int, (double)c->nu_state);
+                h[i] = mu + rho * (h[i] - mu) + sig * eps;
             }
         }
         double M = -INFINITY;
@@ -307,10 +342,13 @@ static double slot_normal(int seed, int i, int t) {
  * mode 1: reverse mode, lambda_t,j = W_t,j g_t(h_t,j) + rho sum_{i: anc[t][i]=j} lambda_t+1,i.
  * Outputs: *ll, grad[3], dll[T] (NULL allowed).
  */
-int orc_grad_f64(int N, double mu, double rho, double sig, double nu, int seed, const float* y, int T,
-                 const int32_t* anc, int mode, double* ll, double* grad, double* dll) {
+int orc_grad_f64(int N, double mu, double rho, double sig, double nu, double nu_state, int seed, const float* y,
+                 int T, const int32_t* anc, int mode, double* ll, double* grad, double* dll) {
     if (N <= 0 || T <= 0 || !anc) return 1;
     const double cobs = c_obs_of(nu), logn = log((double)N);
+    const int nu_int = nu_int_of(nu_state);
+#define STATE_EPS(i_, t_) (slot_normal(seed, (i_), (t_)) * \
+                           (nu_int > 0 ? orc_tstate_scale(seed, (uint32_t)(i_), (t_), nu_int, nu_state) : 1.0))
     const double one_m = 1.0 - rho * rho, s2 = fmax(one_m, 1e-6), sd = sqrt(s2);
     const double sstat = sig / sd, dsr = one_m > 1e-6 ? sig * rho / (s2 * sd) : 0.0, dss = 1.0 / sd;
     double* z0 = (double*)malloc(sizeof(double) * N);
@@ -330,7 +368,7 @@ int orc_grad_f64(int N, double mu, double rho, double sig, double nu, int seed, 
                 const int32_t* a = anc + (size_t)(t - 1) * N;
                 for (int i = 0; i < N; ++i) {
                     const int p = a[i];
-                    const double eps = slot_normal(seed, i, t);
+                    const double eps = STATE_EPS(i, t);
                     hn[i] = mu + rho * (h[p] - mu) + sig * eps;
                     e0[i] = (1.0 - rho) + rho * d0[p];
                     e1[i] = (h[p] - mu) + rho * d1[p];
@@ -365,7 +403,7 @@ int orc_grad_f64(int N, double mu, double rho, double sig, double nu, int seed, 
             if (t > 0) {
                 const int32_t* a = anc + (size_t)(t - 1) * N;
                 const double* hp = H + (size_t)(t - 1) * N;
-                for (int i = 0; i < N; ++i) h[i] = mu + rho * (hp[a[i]] - mu) + sig * slot_normal(seed, i, t);
+                for (int i = 0; i < N; ++i) h[i] = mu + rho * (hp[a[i]] - mu) + sig * STATE_EPS(i, t);
             }
             double M = -INFINITY, S = 0.0;
             for (int i = 0; i < N; ++i) { lw[i] = obs_logpdf_f64((double)y[t], h[i], nu, cobs); if (lw[i] > M) M = lw[i]; }
@@ -382,7 +420,7 @@ int orc_grad_f64(int N, double mu, double rho, double sig, double nu, int seed, 
                 const int32_t* a = anc + (size_t)t * N;
                 for (int i = 0; i < N; ++i) {
                     cs[a[i]] += lamn[i];
-                    aeps += lamn[i] * slot_normal(seed, i, t + 1);
+                    aeps += lamn[i] * STATE_EPS(i, t + 1);
                 }
             }
             for (int j = 0; j < N; ++j) {
@@ -405,6 +443,7 @@ int orc_grad_f64(int N, double mu, double rho, double sig, double nu, int seed, 
 out:
     free(z0); free(lw);
     return rc;
+#undef STATE_EPS
 }
 
 /* ------------------------------------------------------------------------- */

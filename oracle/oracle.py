@@ -41,6 +41,7 @@ class OrcConfig(C.Structure):
         ("rho", C.c_float), ("sigma_z", C.c_float), ("mu", C.c_float), ("nu_obs", C.c_float),
         ("seed", C.c_int),
         ("ess_threshold", C.c_float),
+        ("nu_state", C.c_float),
     ]
 
 
@@ -75,8 +76,10 @@ def lib(native: bool = False) -> C.CDLL:
     L.orc_ref_run.argtypes = [C.c_int, f32, f32, f32, f32, C.c_int, f32, C.c_void_p, C.c_int,
                               C.c_void_p, C.c_void_p, C.c_int, P(C.c_int)]
     L.orc_num_threads.restype = C.c_int; L.orc_num_threads.argtypes = []
+    L.orc_tstate_scale.restype = f64
+    L.orc_tstate_scale.argtypes = [C.c_int, u32, C.c_int, C.c_int, f64]
     L.orc_grad_f64.restype = C.c_int
-    L.orc_grad_f64.argtypes = [C.c_int, f64, f64, f64, f64, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+    L.orc_grad_f64.argtypes = [C.c_int, f64, f64, f64, f64, f64, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                P(f64), C.c_void_p, C.c_void_p]
     _LIBS[key] = L
     return L
@@ -105,12 +108,12 @@ def host_u23_stream(seed: int, n: int):
 
 
 def filter_f64(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.0, nu_obs=0.0,
-               anc_replay=None, flags_replay=None):
+               anc_replay=None, flags_replay=None, nu_state=0.0):
     """FP64 oracle run. Returns dict of per-tick arrays."""
     L = lib()
     y = np.ascontiguousarray(y, dtype=np.float32)
     T = y.shape[0]
-    cfg = OrcConfig(int(n_particles), rho, sigma_z, mu, nu_obs, int(seed), ess_threshold)
+    cfg = OrcConfig(int(n_particles), rho, sigma_z, mu, nu_obs, int(seed), ess_threshold, nu_state)
     out = {k: np.zeros(T, dtype=np.float64) for k in ("dll", "ll_ref", "hmean", "ess")}
     flags = np.zeros(T, dtype=np.int32)
     anc = None if anc_replay is None else np.ascontiguousarray(anc_replay, dtype=np.int32)
@@ -149,7 +152,7 @@ def ref_run(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.5, nu_obs
     return hm, ll, cnt.value
 
 
-def grad_f64(n_particles, mu, rho, sigma_z, y, anc, seed=42, nu_obs=0.0, mode=1):
+def grad_f64(n_particles, mu, rho, sigma_z, y, anc, seed=42, nu_obs=0.0, mode=1, nu_state=0.0):
     """FP64 loglik and d loglik / d(mu, rho, sigma_z) with ancestors anc[T][N] held fixed.
 
     mode 0 = forward-mode tangents, 1 = reverse-mode adjoint. Returns (ll, grad[3], dll[T]).
@@ -161,7 +164,8 @@ def grad_f64(n_particles, mu, rho, sigma_z, y, anc, seed=42, nu_obs=0.0, mode=1)
     ll = C.c_double(0.0)
     grad = np.zeros(3, dtype=np.float64)
     dll = np.zeros(T, dtype=np.float64)
-    rc = L.orc_grad_f64(int(n_particles), float(mu), float(rho), float(sigma_z), float(nu_obs), int(seed), _ptr(y), T,
+    rc = L.orc_grad_f64(int(n_particles), float(mu), float(rho), float(sigma_z), float(nu_obs), float(nu_state),
+                        int(seed), _ptr(y), T,
                         _ptr(anc), int(mode), C.byref(ll), _ptr(grad), _ptr(dll))
     if rc != 0:
         raise RuntimeError(f"orc_grad_f64 failed ({rc})")

@@ -154,10 +154,10 @@ def test_errors(bpf):
         tape.backward()                                   # no forward yet
     y = torch.zeros(10, device="cuda")
     lib = bpf.load()
-    rc = lib.gpu_bpf_grad_forward(tape._h, -1.0, 0.9, 0.2, 0.0, 1, 0.5, y.data_ptr(), 10, tape._ll.data_ptr())
+    rc = lib.gpu_bpf_grad_forward(tape._h, -1.0, 0.9, 0.2, 0.0, 0.0, 1, 0.5, y.data_ptr(), 10, tape._ll.data_ptr())
     assert rc == 4                                        # BPF_ERR_UNSUPPORTED: ESS-mode tapes
-    rc = lib.gpu_bpf_grad_forward(tape._h, -1.0, 0.9, 0.2, 0.0, 1, 0.0, y.data_ptr(), 11, tape._ll.data_ptr())
+    rc = lib.gpu_bpf_grad_forward(tape._h, -1.0, 0.9, 0.2, 0.0, 0.0, 1, 0.0, y.data_ptr(), 11, tape._ll.data_ptr())
     assert rc == 1                                        # more ticks than the tape holds
-    rc = lib.gpu_bpf_grad_forward(tape._h, -1.0, 1.0, 0.2, 0.0, 1, 0.0, y.data_ptr(), 10, tape._ll.data_ptr())
+    rc = lib.gpu_bpf_grad_forward(tape._h, -1.0, 1.0, 0.2, 0.0, 0.0, 1, 0.0, y.data_ptr(), 10, tape._ll.data_ptr())
     assert rc == 1                                        # |rho| >= 1
     tape.close()

@@ -69,12 +69,16 @@ def test_host_argument_validation(lib):
         (4096, float("nan"), 0.15, -1.0, 0.0, 0.0, 42),
         (4096, 0.97, 0.15, float("inf"), 0.0, 0.0, 42),
         (4096, 0.97, 0.15, -1.0, 0.0, -1.0, 42),
+        (4096, 0.97, 0.15, -1.0, 0.3, 0.0, 42),     # Student-t state noise needs round(nu_state) >= 1
     ]
     for args in bad:
         assert not lib.gpu_bpf_create(*args)
         assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_ARG
-    assert not lib.gpu_bpf_create(4096, 0.97, 0.15, -1.0, 5.0, 0.0, 42)
-    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_UNSUPPORTED
+    s = lib.gpu_bpf_create(4096, 0.97, 0.15, -1.0, 5.0, 5.0, 42)   # Student-t state and observations
+    if s:
+        lib.gpu_bpf_destroy(s)
+    else:
+        assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_NODEVICE
 
 
 def test_valid_create_without_gpu_fails_loudly(lib):

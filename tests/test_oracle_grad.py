@@ -24,28 +24,28 @@ def _case(N=256, T=30, seed=0):
 THETA = (-0.8, 0.95, 0.25)
 
 
-@pytest.mark.parametrize("nu", [0.0, 5.0])
-def test_forward_and_reverse_mode_agree(orc, nu):
+@pytest.mark.parametrize("nu,nu_state", [(0.0, 0.0), (5.0, 0.0), (5.0, 5.0)])
+def test_forward_and_reverse_mode_agree(orc, nu, nu_state):
     anc, y = _case()
-    l0, g0, d0 = orc.grad_f64(256, *THETA, y, anc, seed=7, nu_obs=nu, mode=0)
-    l1, g1, d1 = orc.grad_f64(256, *THETA, y, anc, seed=7, nu_obs=nu, mode=1)
+    l0, g0, d0 = orc.grad_f64(256, *THETA, y, anc, seed=7, nu_obs=nu, mode=0, nu_state=nu_state)
+    l1, g1, d1 = orc.grad_f64(256, *THETA, y, anc, seed=7, nu_obs=nu, mode=1, nu_state=nu_state)
     assert abs(l0 - l1) <= 1e-10 * abs(l0)
     np.testing.assert_allclose(g0, g1, rtol=1e-9, atol=1e-10)
     np.testing.assert_allclose(d0, d1, rtol=0, atol=1e-11)
 
 
-@pytest.mark.parametrize("nu", [0.0, 5.0])
-def test_gradient_matches_central_differences(orc, nu):
+@pytest.mark.parametrize("nu,nu_state", [(0.0, 0.0), (5.0, 0.0), (0.0, 4.0)])
+def test_gradient_matches_central_differences(orc, nu, nu_state):
     anc, y = _case(N=300, T=40, seed=3)
-    _, g, _ = orc.grad_f64(300, *THETA, y, anc, seed=11, nu_obs=nu, mode=1)
+    _, g, _ = orc.grad_f64(300, *THETA, y, anc, seed=11, nu_obs=nu, mode=1, nu_state=nu_state)
     th = np.array(THETA)
     for k in range(3):
         d = 1e-5 * abs(th[k])
         tp, tm = th.copy(), th.copy()
         tp[k] += d
         tm[k] -= d
-        lp = orc.grad_f64(300, *tp, y, anc, seed=11, nu_obs=nu, mode=0)[0]
-        lm = orc.grad_f64(300, *tm, y, anc, seed=11, nu_obs=nu, mode=0)[0]
+        lp = orc.grad_f64(300, *tp, y, anc, seed=11, nu_obs=nu, mode=0, nu_state=nu_state)[0]
+        lm = orc.grad_f64(300, *tm, y, anc, seed=11, nu_obs=nu, mode=0, nu_state=nu_state)[0]
         fd = (lp - lm) / (2 * d)
         assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g[k])), (k, fd, g[k])
 
@@ -73,3 +73,18 @@ def test_gradient_matches_torch_autograd(orc):
     ll, g, _ = orc.grad_f64(N, *THETA, y, anc, seed=seed, mode=1)
     assert abs(ll - loss.item()) <= 1e-10 * abs(ll)
     np.testing.assert_allclose(g, th.grad.numpy(), rtol=1e-9, atol=1e-10)
+
+
+def test_tstate_noise_distribution(orc):
+    """Student-t state noise: z * sqrt(nu / chi2_k), k = round(nu). Sample moments of the oracle's
+    counter-based draws against t(5): mean 0, variance nu/(nu-2) = 5/3 (reference test
+    tests/test_icdf_diag.cu:251-253 expects std 1.291), and chi2 draws with k = 4 dof have mean 4."""
+    L = orc.lib()
+    n = 40000
+    z = np.array([L.orc_icdf_f64(L.orc_uniform(L.orc_pcg32_draw_jump(42, i, 3))) for i in range(n)])
+    sc = np.array([L.orc_tstate_scale(42, i, 3, 5, 5.0) for i in range(n)])
+    e = z * sc
+    assert abs(e.mean()) < 0.03
+    assert abs(e.std() - math.sqrt(5.0 / 3.0)) < 0.04
+    chi2 = 4.0 / np.array([L.orc_tstate_scale(7, i, 1, 4, 4.0) for i in range(n)]) ** 2
+    assert abs(chi2.mean() - 4.0) < 0.06 and abs(chi2.var() - 8.0) < 0.5
