@@ -46,7 +46,7 @@ struct BatchShared {
 
 size_t batch_smem_bytes(int maxn) { return (size_t)maxn * 8 + (((size_t)maxn * 2 + 15) / 16) * 16; }
 
-template <int NT>
+template <int NT, bool RESUMABLE>
 __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, int b, float* bufA, float* bufB,
                                  unsigned short* marks, BatchShared<NT>& sh, int maxn) {
   constexpr int W = NT / 32;
@@ -59,27 +59,42 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
   int chunk = 1;
   while (chunk * NT < N) chunk <<= 1;           // power of two: chunks never straddle a tile
 
-  // h_0 from draw 0 (stationary law)
-  {
-    const PcgTick c = pcg_tick_consts(f.seed, 1ull, 0ull);
-    for (int i = tid; i < N; i += NT) {
-      const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
-      bufA[swz(i)] = fmaf(f.std_stat, icdf_normal(pcg_uniform(pcg_output(s))), f.mu);
-    }
-  }
   float* H = bufA;
   float* Wt = bufB;
-  unsigned long long At = 1ull, Bt = 0ull;
+  uint64_t At = 1ull, Bt = 0ull;
   // thread-0 filter state
   double logS_prev = log((double)N), ll_total = 0.0;
   uint64_t ustate = (unsigned long long)f.seed * 67890ULL + 12345ULL;
   int n_res = 0;
   float hm_last = 0.0f;
-  if (tid == 0) sh.carry = 0;
+  const int t0 = (RESUMABLE && a.t0_dev) ? *a.t0_dev : 0;
+  BatchFilterState* fs = (RESUMABLE && a.st) ? a.st + b : nullptr;
+  const long long soff = (RESUMABLE && a.st) ? a.st_off[b] : 0;
+  if (fs && t0 > 0) {
+    // resume from the state saved at the end of the previous launch
+    const BatchFilterState r = *fs;
+    for (int i = tid; i < N; i += NT) H[swz(i)] = a.st_h[soff + i];
+    if (r.carry)
+      for (int i = tid; i < N; i += NT) Wt[swz(i)] = a.st_w[soff + i];
+    pcg_jump((uint64_t)t0, &At, &Bt);
+    logS_prev = r.logS_prev; ll_total = r.ll_total; ustate = r.ustate; n_res = r.n_res; hm_last = r.hm_last;
+    if (tid == 0) {
+      sh.carry = r.carry;
+      for (int k = 0; k < kBatchMaxTiles; ++k) sh.carry_off[k] = r.carry_off[k];
+    }
+  } else {
+    // h_0 from draw 0 (stationary law)
+    const PcgTick c = pcg_tick_consts(f.seed, 1ull, 0ull);
+    for (int i = tid; i < N; i += NT) {
+      const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
+      bufA[swz(i)] = fmaf(f.std_stat, icdf_normal(pcg_uniform(pcg_output(s))), f.mu);
+    }
+    if (tid == 0) sh.carry = 0;
+  }
   __syncthreads();
 
-  for (int t = 0; t < a.T; ++t) {
-    const float y = __ldg(a.y + t);
+  for (int t = t0; t < t0 + a.T; ++t) {
+    const float y = __ldg(a.y + (t - t0));
     const float y2 = y * y;
     obs.y = y;
     const bool carry = sh.carry != 0;
@@ -181,8 +196,8 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       hm_last = hm;
       if (a.g_norm)
         a.g_norm[t] = degenerate ? make_float2(0.0f, 0.0f) : make_float2((float)(1.0 / S), __int_as_float(nM));
-      if (a.dll) a.dll[(size_t)b * a.T + t] = dll;
-      if (a.hmean) a.hmean[(size_t)b * a.T + t] = hm;
+      if (a.dll) a.dll[(size_t)b * a.T + (t - t0)] = dll;
+      if (a.hmean) a.hmean[(size_t)b * a.T + (t - t0)] = hm;
       if (resample) {
         const uint64_t old = ustate;
         ustate = old * kPcgMult + kHostInc;
@@ -271,7 +286,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       for (int i = tid; i < N; i += NT) {
         const int anc = (int)marks[i] - 1;
         Wt[swz(i)] = H[swz(anc)];
-        if (a.anc) a.anc[((size_t)b * a.T + t) * kBatchMaxN + i] = anc;
+        if (a.anc) a.anc[((size_t)b * a.T + (t - t0)) * kBatchMaxN + i] = anc;
       }
       __syncthreads();
       float* tmp = H; H = Wt; Wt = tmp;
@@ -279,10 +294,22 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
   }
   if (a.particles)
     for (int i = tid; i < N; i += NT) a.particles[(size_t)b * kBatchMaxN + i] = H[swz(i)];
+  if (fs) {
+    for (int i = tid; i < N; i += NT) a.st_h[soff + i] = H[swz(i)];
+    if (sh.carry)
+      for (int i = tid; i < N; i += NT) a.st_w[soff + i] = Wt[swz(i)];
+  }
   if (tid == 0) {
     a.loglik[b] = ll_total;
     a.h_final[b] = hm_last;
     a.resamples[b] = n_res;
+    if (fs) {
+      BatchFilterState r;
+      r.logS_prev = logS_prev; r.ll_total = ll_total; r.ustate = ustate;
+      r.carry = sh.carry; r.n_res = n_res; r.hm_last = hm_last; r.pad = 0;
+      for (int k = 0; k < kBatchMaxTiles; ++k) r.carry_off[k] = sh.carry_off[k];
+      *fs = r;
+    }
   }
   __syncthreads();
 }
@@ -302,7 +329,7 @@ __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_ker
     if (idx >= a.n_order) break;
     const int b = a.order[idx];
     const BatchFilterDev f = a.filters[b];
-    batch_run_filter<NT>(a, f, b, bufA, bufB, marks, sh, maxn);
+    batch_run_filter<NT, true>(a, f, b, bufA, bufB, marks, sh, maxn);
   }
 }
 
@@ -492,6 +519,13 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
 
 size_t batch_grad_smem_bytes(int maxn) { return (size_t)maxn * 12; }
 
+__global__ void batch_advance_kernel(int* tick, int n) { *tick += n; }
+
+cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s) {
+  batch_advance_kernel<<<1, 1, 0, s>>>(tick, n);
+  return cudaGetLastError();
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_grad_kernel(BatchArgs a, int maxn) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -514,7 +548,7 @@ __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_gra
     if (idx >= a.n_order) break;
     const int b = a.order[idx];
     const BatchFilterDev f = a.filters[b];
-    batch_run_filter<NT>(s, f, b, r0, r1, marks, sh, maxn);
+    batch_run_filter<NT, false>(s, f, b, r0, r1, marks, sh, maxn);
     batch_run_backward<NT>(s, f, b, maxn, r0, r1, r2, sh);
   }
 }

@@ -30,6 +30,18 @@ struct BatchFilterDev {                    // 48 bytes, one per filter
   float nu_state;
 };
 
+// Resumable state of one filter between launches (runs that continue from a
+// saved tick: the IMM step and any caller that steps the batch a few ticks at
+// a time). The particle and carried-weight arrays live at st_off[b] in st_h/st_w.
+struct BatchFilterState {
+  double logS_prev, ll_total;
+  unsigned long long ustate;   // resampling-uniform PCG32 state
+  int carry, n_res;
+  float carry_off[kBatchMaxTiles];
+  float hm_last;
+  int pad;
+};
+
 struct BatchArgs {
   const BatchFilterDev* filters;
   const int* order;           // filter indices of this class, largest N first
@@ -54,6 +66,12 @@ struct BatchArgs {
   const ulonglong2* g_AB;     // [T+1] PCG32 jump constants (A^t, sum_{k<t} A^k)
   int g_K;                    // checkpoint interval
   double* grad;               // [3B] d loglik / d(mu, rho, sigma_z)
+  // resumable runs (all null for a run from tick 0 that keeps nothing)
+  const int* t0_dev;          // first tick of this launch (device); y, dll, hmean are indexed from it
+  BatchFilterState* st;       // [B] state saved at the end and, when *t0_dev > 0, loaded at the start
+  float* st_h;                // particles of every filter at st_off[b]
+  float* st_w;                // carried weights of every filter at st_off[b]
+  const long long* st_off;    // [B]
 };
 
 // Dynamic shared memory of the class kernel for filters of at most maxn particles.
@@ -69,5 +87,7 @@ int batch_occupancy(int threads, int maxn);
 size_t batch_grad_smem_bytes(int maxn);
 cudaError_t launch_batch_grad_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s);
 int batch_grad_occupancy(int threads, int maxn);
+// Adds n to the device tick counter of resumable runs (one thread).
+cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s);
 
 }  // namespace bpf

@@ -89,6 +89,17 @@ struct GpuBpfBatch {
   cudaGraphExec_t ggraph = nullptr;
   GraphKey gkey;
   double* gkey_grad = nullptr;
+
+  // resumable stepping (allocated on the first step): per-filter state, particle and
+  // carried-weight arrays, the device tick counter and the step graph
+  BatchFilterState* d_st = nullptr;
+  float* d_sth = nullptr;
+  float* d_stw = nullptr;
+  long long* d_stoff = nullptr;
+  int* d_tick = nullptr;
+  int host_tick = 0;
+  cudaGraphExec_t sgraph = nullptr;
+  GraphKey skey;
 };
 
 namespace {
@@ -97,6 +108,8 @@ void free_batch(GpuBpfBatch* b) {
   if (!b) return;
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->ggraph) cudaGraphExecDestroy(b->ggraph);
+  if (b->sgraph) cudaGraphExecDestroy(b->sgraph);
+  cudaFree(b->d_st); cudaFree(b->d_sth); cudaFree(b->d_stw); cudaFree(b->d_stoff); cudaFree(b->d_tick);
   for (int c = 0; c < kClasses; ++c) cudaFree(b->g_tape[c]);
   cudaFree(b->d_AB);
   cudaFree(b->d_filters); cudaFree(b->d_order); cudaFree(b->d_counters);
@@ -243,6 +256,45 @@ cudaError_t enqueue_grad(GpuBpfBatch* b, const float* y, int T, double* loglik, 
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+int prepare_steps(GpuBpfBatch* b) {
+  if (b->d_st) return BPF_OK;
+  std::vector<long long> off(b->B);
+  long long tot = 0;
+  for (int i = 0; i < b->B; ++i) { off[i] = tot; tot += (b->n_of[i] + 3) & ~3; }
+  BCK(cudaMalloc(&b->d_st, (size_t)b->B * sizeof(BatchFilterState)));
+  BCK(cudaMalloc(&b->d_sth, (size_t)tot * sizeof(float)));
+  BCK(cudaMalloc(&b->d_stw, (size_t)tot * sizeof(float)));
+  BCK(cudaMalloc(&b->d_stoff, (size_t)b->B * sizeof(long long)));
+  BCK(cudaMalloc(&b->d_tick, sizeof(int)));
+  BCK(cudaMemcpy(b->d_stoff, off.data(), (size_t)b->B * sizeof(long long), cudaMemcpyHostToDevice));
+  BCK(cudaMemset(b->d_tick, 0, sizeof(int)));
+  b->host_tick = 0;
+  return BPF_OK;
+}
+
+// Advance every filter by T ticks from its saved state (tick 0 = fresh start).
+cudaError_t enqueue_step(GpuBpfBatch* b, const float* y, int T, double* dll, float* hmean) {
+  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, kClasses * sizeof(int), b->stream);
+  if (e != cudaSuccess) return e;
+  e = cudaEventRecord(b->fork, b->stream);
+  if (e != cudaSuccess) return e;
+  for (int c = kClasses - 1; c >= 0; --c) {
+    if (!b->class_cnt[c]) continue;
+    BatchArgs a = class_args(b, c, y, T, b->d_loglik, dll, hmean, nullptr, nullptr);
+    a.t0_dev = b->d_tick;
+    a.st = b->d_st;
+    a.st_h = b->d_sth;
+    a.st_w = b->d_stw;
+    a.st_off = b->d_stoff;
+    e = cudaStreamWaitEvent(b->cls_stream[c], b->fork, 0);
+    if (e == cudaSuccess) e = launch_batch_class(a, b->threads[c], kClassMaxN[c], b->grid[c], b->cls_stream[c]);
+    if (e == cudaSuccess) e = cudaEventRecord(b->join[c], b->cls_stream[c]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[c], 0);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_batch_advance(b->d_tick, T, b->stream);
 }
 
 int ensure_device_b(GpuBpfBatch* b) {
@@ -436,6 +488,47 @@ int gpu_bpf_batch_grad_run(GpuBpfBatch* b, const float* y_dev, int n_ticks, doub
   bpf_note_launches(kClasses);
   return BPF_OK;
 }
+
+int gpu_bpf_batch_step_device(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* dll_dev, float* hmean_dev) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  if (n_ticks <= 0 || !y_dev) return bpf_record_error(BPF_ERR_ARG);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  rc = prepare_steps(b);
+  if (rc) return rc;
+  GraphKey k;
+  k.y = y_dev; k.T = n_ticks; k.dll = dll_dev; k.hmean = hmean_dev;
+  std::copy(b->threads, b->threads + kClasses, k.threads);
+  if (!b->sgraph || !(k == b->skey)) {
+    if (b->sgraph) { cudaGraphExecDestroy(b->sgraph); b->sgraph = nullptr; }
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_step(b, y_dev, n_ticks, dll_dev, hmean_dev);
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
+    e = cudaGraphInstantiate(&b->sgraph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->sgraph = nullptr; cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
+    b->skey = k;
+  }
+  BCK(cudaGraphLaunch(b->sgraph, b->stream));
+  bpf_note_launches(kClasses + 1);
+  b->host_tick += n_ticks;
+  return BPF_OK;
+}
+
+int gpu_bpf_batch_reset(GpuBpfBatch* b) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  int rc = ensure_device_b(b);
+  if (rc) return rc;
+  if (b->d_tick) BCK(cudaMemsetAsync(b->d_tick, 0, sizeof(int), b->stream));
+  b->host_tick = 0;
+  return BPF_OK;
+}
+
+int gpu_bpf_batch_tick(GpuBpfBatch* b) { return b ? b->host_tick : -bpf_record_error(BPF_ERR_STATE); }
+
+double* gpu_bpf_batch_loglik_device(GpuBpfBatch* b) { return b ? b->d_loglik : nullptr; }
 
 size_t gpu_bpf_batch_grad_tape_bytes(GpuBpfBatch* b, int n_ticks) {
   if (!b || n_ticks <= 0) return 0;

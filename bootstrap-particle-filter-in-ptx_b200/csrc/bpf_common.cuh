@@ -65,6 +65,20 @@ __host__ __device__ inline PcgTick pcg_tick_consts(int seed, uint64_t At, uint64
 }
 __host__ __device__ inline uint64_t pcg_inc(uint32_t i) { return (uint64_t)(uint32_t)(2u * i + 1u); }
 
+// Jump constants of draw t: A^t and sum_{k<t} A^k (mod 2^64), by composing the
+// affine maps x -> A x + 1 in O(log t) steps.
+__host__ __device__ inline void pcg_jump(uint64_t t, uint64_t* At, uint64_t* Bt) {
+  uint64_t am = 1ull, ap = 0ull, cm = kPcgMult, cp = 1ull;
+  while (t) {
+    if (t & 1ull) { am *= cm; ap = ap * cm + cp; }
+    cp = (cm + 1ull) * cp;
+    cm *= cm;
+    t >>= 1;
+  }
+  *At = am;
+  *Bt = ap;
+}
+
 // u in (0,1): (out >> 9) * 2^-23, clamped like the reference (PTX :159-164).
 // Formed from the float bit pattern 1.m - 1 (exact) instead of an int->float
 // conversion.

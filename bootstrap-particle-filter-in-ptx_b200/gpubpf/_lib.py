@@ -60,7 +60,24 @@ class BpfBatchFilter(C.Structure):
                 ("n_particles", C.c_int), ("seed", C.c_int), ("nu_state", C.c_float)]
 
 
+class ImmModelParams(C.Structure):
+    _fields_ = [("rho", C.c_float), ("sigma_z", C.c_float), ("mu", C.c_float), ("nu_state", C.c_float),
+                ("nu_obs", C.c_float)]
+
+
+class ImmResult(C.Structure):
+    _fields_ = [("h_mean", C.c_float), ("vol", C.c_float), ("log_lik", C.c_float), ("best_model", C.c_int),
+                ("best_prob", C.c_float)]
+
+
+class GpuImmState(C.Structure):
+    _fields_ = [("filters", C.c_void_p), ("n_models", C.c_int), ("n_particles_per_model", C.c_int),
+                ("log_pi", C.POINTER(C.c_double)), ("log_pi_pred", C.POINTER(C.c_double)),
+                ("log_T", C.POINTER(C.c_double)), ("timestep", C.c_int), ("impl", C.c_void_p)]
+
+
 P_STATE = C.POINTER(GpuBpfState)
+P_IMM = C.POINTER(GpuImmState)
 _f = C.c_float
 _i = C.c_int
 _d = C.c_double
@@ -119,7 +136,19 @@ SIGNATURES = {
     "gpu_bpf_batch_run_debug": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp]),
     "gpu_bpf_batch_resample_counts": (_i, [_vp, C.POINTER(_i), C.POINTER(_f)]),
     "gpu_bpf_batch_grad_run": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "gpu_bpf_batch_step_device": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "gpu_bpf_batch_reset": (_i, [_vp]),
+    "gpu_bpf_batch_tick": (_i, [_vp]),
+    "gpu_bpf_batch_loglik_device": (_vp, [_vp]),
     "gpu_bpf_batch_grad_tape_bytes": (C.c_size_t, [_vp, _i]),
+    # IMM (gpu_bpf/gpu_bpf.cuh:131-164)
+    "gpu_imm_create": (P_IMM, [C.POINTER(ImmModelParams), _i, _i, C.POINTER(_f), _i]),
+    "gpu_imm_step": (ImmResult, [P_IMM, _f]),
+    "gpu_imm_get_prob": (_f, [P_IMM, _i]),
+    "gpu_imm_get_probs": (None, [P_IMM, C.POINTER(_f)]),
+    "gpu_imm_destroy": (None, [P_IMM]),
+    "gpu_imm_build_grid": (C.POINTER(ImmModelParams), [C.POINTER(_f), _i, C.POINTER(_f), _i, C.POINTER(_f), _i,
+                                                        _f, _f, C.POINTER(_i)]),
     # gradient
     "gpu_bpf_grad_create": (_vp, [_i, _i, _i]),
     "gpu_bpf_grad_destroy": (None, [_vp]),

@@ -81,6 +81,22 @@ class GpuBpfBatch:
         check(self._lib.gpu_bpf_batch_grad_run(self._h, C.c_void_p(y_ptr), int(n_ticks), C.c_void_p(loglik_ptr),
                                                C.c_void_p(grad_ptr)), "gpu_bpf_batch_grad_run")
 
+    def step_device(self, y_ptr: int, n_ticks: int, dll_ptr: int = 0, hmean_ptr: int = 0) -> None:
+        """Advance every filter n_ticks from its saved state (device pointers, batch stream)."""
+        check(self._lib.gpu_bpf_batch_step_device(self._h, C.c_void_p(y_ptr), int(n_ticks), C.c_void_p(dll_ptr or None),
+                                                  C.c_void_p(hmean_ptr or None)), "gpu_bpf_batch_step_device")
+
+    def reset(self) -> None:
+        check(self._lib.gpu_bpf_batch_reset(self._h), "gpu_bpf_batch_reset")
+
+    @property
+    def tick(self) -> int:
+        return self._lib.gpu_bpf_batch_tick(self._h)
+
+    @property
+    def loglik_ptr(self) -> int:
+        return self._lib.gpu_bpf_batch_loglik_device(self._h)
+
     def grad_tape_bytes(self, n_ticks: int) -> int:
         return int(self._lib.gpu_bpf_batch_grad_tape_bytes(self._h, int(n_ticks)))
 

@@ -228,6 +228,43 @@ int gpu_bpf_run_static(int n_particles, float rho, float sigma_z, float mu, floa
                        float ess_threshold, const float* y_dev, int n_ticks, BpfTickRecord* rec_dev,
                        void* stream);
 
+/* ---- IMM: interacting multiple model (gpu_bpf/gpu_bpf.cuh:131-164) ----------
+ * K SV models stepped on the same observations; model probabilities follow a Markov switching
+ * prior (transition matrix T[j*K + k] = P(j -> k), row-major; NULL = 0.95 stay, the rest spread
+ * evenly) and each tick's log-likelihood increment. Models run as one resumable batch (one graph
+ * launch per tick) when n_particles_per_model <= 16384, else as K plain filters. Model k uses the
+ * seed seed + 7919 k and the plain filter's default ESS threshold 0.5 (as the reference). */
+#define IMM_MAX_MODELS 64
+
+typedef struct {
+    float rho, sigma_z, mu, nu_state, nu_obs;
+} ImmModelParams;                                            /* gpu_bpf/gpu_bpf.cuh:135-137 */
+
+typedef struct {
+    float h_mean, vol, log_lik;    /* mixed filtered mean, exp(h_mean/2), log p(y_t | y_{1:t-1}) */
+    int   best_model;
+    float best_prob;
+} ImmResult;                                                 /* gpu_bpf/gpu_bpf.cuh:139-143 */
+
+typedef struct {
+    GpuBpfState** filters;         /* the K plain filters when they are used, else NULL */
+    int     n_models, n_particles_per_model;
+    double *log_pi, *log_pi_pred, *log_T;
+    int     timestep;
+    void*   impl;                  /* batched models and staging buffers */
+} GpuImmState;                                               /* gpu_bpf/gpu_bpf.cuh:145-150 */
+
+/* gpu_bpf/gpu_bpf.cuh:151-153. NULL when n_models is outside 1..64 or a model is invalid. */
+GpuImmState* gpu_imm_create(const ImmModelParams* models, int n_models, int n_particles_per_model,
+                            const float* transition_matrix, int seed);
+ImmResult    gpu_imm_step(GpuImmState* state, float y_t);           /* gpu_bpf/gpu_bpf.cuh:154; waits */
+float        gpu_imm_get_prob(const GpuImmState* state, int k);     /* gpu_bpf/gpu_bpf.cuh:155 */
+void         gpu_imm_get_probs(const GpuImmState* state, float* probs_out);   /* gpu_bpf/gpu_bpf.cuh:156 */
+void         gpu_imm_destroy(GpuImmState* state);                   /* gpu_bpf/gpu_bpf.cuh:157 */
+/* gpu_bpf/gpu_bpf.cuh:159-162: the rho x sigma_z x mu grid (rho-major), malloc'd; free() it. */
+ImmModelParams* gpu_imm_build_grid(const float* rhos, int n_rho, const float* sigma_zs, int n_sigma,
+                                   const float* mus, int n_mu, float nu_state, float nu_obs, int* out_n_models);
+
 /* ---- Batched filters (addition) -------------------------------------------
  * Many independent SV filters with their own (mu, rho, sigma_z, nu_obs), particle count
  * (1..16384) and seed, all on one observation series: the SMC^2 / PMMH inner loop. The
@@ -272,6 +309,18 @@ int          gpu_bpf_batch_run_debug(GpuBpfBatch* batch, const float* y_dev, int
                                      double* dll_dev, int32_t* anc_dev, float* particles_dev);
 /* Resampling count and last filtered mean of every filter after a run (waits). */
 int          gpu_bpf_batch_resample_counts(GpuBpfBatch* batch, int* counts, float* hmean_last);
+/* Resumable stepping: advance every filter by n_ticks from where the previous step left it
+ * (the first step after create or gpu_bpf_batch_reset starts at tick 0), enqueued on the batch
+ * stream as one CUDA graph. Device buffers: y_dev[n_ticks]; dll_dev[n_filters*n_ticks] and
+ * hmean_dev[n_filters*n_ticks] (either may be NULL) receive this step's per-tick increments and
+ * filtered means. The filters' state lives on the device between steps (8 B per particle). A
+ * batch stepped in pieces is bit-identical to one run over the whole series. */
+int          gpu_bpf_batch_step_device(GpuBpfBatch* batch, const float* y_dev, int n_ticks, double* dll_dev,
+                                       float* hmean_dev);
+int          gpu_bpf_batch_reset(GpuBpfBatch* batch);   /* next step starts again at tick 0 */
+int          gpu_bpf_batch_tick(GpuBpfBatch* batch);    /* ticks stepped since create / reset */
+/* Device array [n_filters] of FP64 total log-likelihoods, updated by every run or step. */
+double*      gpu_bpf_batch_loglik_device(GpuBpfBatch* batch);
 /* Batched gradient (the SMC^2 / PMMH inner loop with gradients): one forward and one backward
  * pass of every filter in one persistent launch per size class (each CTA runs a filter's taped
  * forward, then its adjoint, as gpu_bpf_grad_forward/backward do for one filter), replayed as

@@ -113,3 +113,19 @@ def test_bands_only_identity(lib):
 def test_error_strings(lib):
     for code in range(8):
         assert lib.gpu_bpf_error_string(code)
+
+
+def test_imm_host_side(lib):
+    """gpu_imm_build_grid (host only) and gpu_imm_create's argument checks."""
+    import ctypes as C
+    from gpubpf import _lib, imm
+    g = imm.build_grid([0.9, 0.97], [0.1, 0.2, 0.3], [-1.0, -0.5], nu_state=0.0, nu_obs=5.0)
+    assert len(g) == 12
+    assert [(round(m["rho"], 3), round(m["sigma_z"], 3), m["mu"]) for m in g[:3]] == \
+        [(0.9, 0.1, -1.0), (0.9, 0.1, -0.5), (0.9, 0.2, -1.0)]             # rho-major, mu fastest
+    assert all(m["nu_obs"] == 5.0 for m in g)
+    models = (_lib.ImmModelParams * 65)()
+    assert not lib.gpu_imm_create(models, 65, 1000, None, 1)               # IMM_MAX_MODELS = 64
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_ARG
+    assert not lib.gpu_imm_create(models, 0, 1000, None, 1)
+    assert lib.gpu_imm_get_prob(None, 0) == 0.0
