@@ -94,7 +94,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
   __syncthreads();
 
   for (int t = t0; t < t0 + a.T; ++t) {
-    const float y = __ldg(a.y + (t - t0));
+    const float y = __ldg(a.y + (a.y_abs ? t : t - t0));
     const float y2 = y * y;
     obs.y = y;
     const bool carry = sh.carry != 0;
@@ -520,6 +520,39 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
 size_t batch_grad_smem_bytes(int maxn) { return (size_t)maxn * 12; }
 
 __global__ void batch_advance_kernel(int* tick, int n) { *tick += n; }
+
+__global__ void batch_gather_kernel(BatchFilterDev* dst_tab, BatchFilterState* dst_st, float* dst_h, float* dst_w,
+                                    const BatchFilterDev* src_tab, const BatchFilterState* src_st,
+                                    const float* __restrict__ src_h, const float* __restrict__ src_w,
+                                    const long long* off, const int* idx, const int* mask, const int* new_seed, int n) {
+  const int b = blockIdx.x;
+  if (mask && !mask[b]) return;
+  const int sidx = idx ? idx[b] : b;
+  const long long od = off[b], os = off[sidx];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    dst_h[od + i] = src_h[os + i];
+    dst_w[od + i] = src_w[os + i];
+  }
+  if (threadIdx.x == 0) {
+    BatchFilterDev f = src_tab[sidx];
+    BatchFilterState r = src_st[sidx];
+    if (new_seed) {
+      f.seed = new_seed[b];
+      r.ustate = (unsigned long long)new_seed[b] * 67890ULL + 12345ULL;   // gpu_bpf_ptx_full.cu:353
+    }
+    dst_tab[b] = f;
+    dst_st[b] = r;
+  }
+}
+
+cudaError_t launch_batch_gather(BatchFilterDev* dst_tab, BatchFilterState* dst_st, float* dst_h, float* dst_w,
+                                const BatchFilterDev* src_tab, const BatchFilterState* src_st, const float* src_h,
+                                const float* src_w, const long long* off, const int* idx, const int* mask,
+                                const int* new_seed, int n, int B, cudaStream_t s) {
+  batch_gather_kernel<<<B, 256, 0, s>>>(dst_tab, dst_st, dst_h, dst_w, src_tab, src_st, src_h, src_w, off, idx, mask,
+                                        new_seed, n);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s) {
   batch_advance_kernel<<<1, 1, 0, s>>>(tick, n);

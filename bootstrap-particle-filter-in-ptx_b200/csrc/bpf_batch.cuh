@@ -72,6 +72,7 @@ struct BatchArgs {
   float* st_h;                // particles of every filter at st_off[b]
   float* st_w;                // carried weights of every filter at st_off[b]
   const long long* st_off;    // [B]
+  int y_abs;                  // 1: y is indexed by the absolute tick (y[t]) instead of from t0
 };
 
 // Dynamic shared memory of the class kernel for filters of at most maxn particles.
@@ -89,5 +90,13 @@ cudaError_t launch_batch_grad_class(const BatchArgs& a, int threads, int maxn, i
 int batch_grad_occupancy(int threads, int maxn);
 // Adds n to the device tick counter of resumable runs (one thread).
 cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s);
+// Filter j of dst takes the resumable state and table entry of filter idx[j] of src (every j, or
+// those with mask[j] != 0); with new_seed, filter j continues with seed new_seed[j] (fresh noise
+// streams and resampling uniforms). Filters have n particles each at offsets off[]; src and dst
+// must not alias.
+cudaError_t launch_batch_gather(BatchFilterDev* dst_tab, BatchFilterState* dst_st, float* dst_h, float* dst_w,
+                                const BatchFilterDev* src_tab, const BatchFilterState* src_st, const float* src_h,
+                                const float* src_w, const long long* off, const int* idx, const int* mask,
+                                const int* new_seed, int n, int B, cudaStream_t s);
 
 }  // namespace bpf

@@ -22,85 +22,8 @@
 
 using namespace bpf;
 
-namespace {
+#include "bpf_batch_internal.cuh"
 
-constexpr int kClasses = 5;
-constexpr int kClassMaxN[kClasses] = {1024, 2048, 4096, 8192, 16384};
-constexpr int kDefaultThreads[kClasses] = {128, 256, 256, 512, 1024};
-constexpr int kThreadChoices[] = {64, 128, 256, 512, 1024};
-
-#define BCK(call)                                                             \
-  do {                                                                        \
-    cudaError_t e_ = (call);                                                  \
-    if (e_ != cudaSuccess) {                                                  \
-      cudaGetLastError();                                                     \
-      return bpf_record_error(e_ == cudaErrorMemoryAllocation ? BPF_ERR_ALLOC : BPF_ERR_CUDA); \
-    }                                                                         \
-  } while (0)
-
-struct GraphKey {
-  const float* y = nullptr;
-  int T = 0;
-  double* loglik = nullptr;
-  double* dll = nullptr;
-  float* hmean = nullptr;
-  int32_t* anc = nullptr;
-  float* particles = nullptr;
-  int threads[kClasses] = {0, 0, 0, 0, 0};
-  bool operator==(const GraphKey& o) const {
-    return y == o.y && T == o.T && loglik == o.loglik && dll == o.dll && hmean == o.hmean && anc == o.anc &&
-           particles == o.particles && std::equal(threads, threads + kClasses, o.threads);
-  }
-};
-
-}  // namespace
-
-struct GpuBpfBatch {
-  int device = 0;
-  int B = 0;
-  float ess_threshold = 0.0f;
-  int sms = 0;
-  BatchFilterDev* d_filters = nullptr;
-  int* d_order = nullptr;
-  int* d_counters = nullptr;
-  float* d_hfinal = nullptr;
-  int* d_resamples = nullptr;
-  double* d_loglik = nullptr;
-  float* d_y = nullptr;
-  int y_cap = 0;
-  int class_off[kClasses] = {0, 0, 0, 0, 0};
-  int class_cnt[kClasses] = {0, 0, 0, 0, 0};
-  int threads[kClasses];
-  int grid[kClasses] = {1, 1, 1, 1, 1};
-  cudaStream_t stream = nullptr;
-  cudaStream_t cls_stream[kClasses] = {};
-  cudaEvent_t fork = nullptr;
-  cudaEvent_t join[kClasses] = {};
-  cudaGraphExec_t graph = nullptr;
-  GraphKey key;
-  std::vector<int> n_of;      // particle count per filter
-
-  // gradient runs: per-class tape for the class's CTA slots, PCG jump table, graph
-  unsigned char* g_tape[kClasses] = {};
-  size_t g_tape_bytes[kClasses] = {0, 0, 0, 0, 0};
-  int g_grid[kClasses] = {1, 1, 1, 1, 1};
-  ulonglong2* d_AB = nullptr;
-  int ab_T = 0;
-  cudaGraphExec_t ggraph = nullptr;
-  GraphKey gkey;
-  double* gkey_grad = nullptr;
-
-  // resumable stepping (allocated on the first step): per-filter state, particle and
-  // carried-weight arrays, the device tick counter and the step graph
-  BatchFilterState* d_st = nullptr;
-  float* d_sth = nullptr;
-  float* d_stw = nullptr;
-  long long* d_stoff = nullptr;
-  int* d_tick = nullptr;
-  int host_tick = 0;
-  cudaGraphExec_t sgraph = nullptr;
-  GraphKey skey;
-};
 
 namespace {
 
@@ -258,7 +181,9 @@ cudaError_t enqueue_grad(GpuBpfBatch* b, const float* y, int T, double* loglik, 
   return cudaSuccess;
 }
 
-int prepare_steps(GpuBpfBatch* b) {
+}  // namespace
+
+int batch_prepare_steps(GpuBpfBatch* b) {
   if (b->d_st) return BPF_OK;
   std::vector<long long> off(b->B);
   long long tot = 0;
@@ -274,8 +199,10 @@ int prepare_steps(GpuBpfBatch* b) {
   return BPF_OK;
 }
 
+namespace {
+
 // Advance every filter by T ticks from its saved state (tick 0 = fresh start).
-cudaError_t enqueue_step(GpuBpfBatch* b, const float* y, int T, double* dll, float* hmean) {
+cudaError_t enqueue_step(GpuBpfBatch* b, const float* y, int T, double* dll, float* hmean, int y_abs) {
   cudaError_t e = cudaMemsetAsync(b->d_counters, 0, kClasses * sizeof(int), b->stream);
   if (e != cudaSuccess) return e;
   e = cudaEventRecord(b->fork, b->stream);
@@ -288,6 +215,7 @@ cudaError_t enqueue_step(GpuBpfBatch* b, const float* y, int T, double* dll, flo
     a.st_h = b->d_sth;
     a.st_w = b->d_stw;
     a.st_off = b->d_stoff;
+    a.y_abs = y_abs;
     e = cudaStreamWaitEvent(b->cls_stream[c], b->fork, 0);
     if (e == cudaSuccess) e = launch_batch_class(a, b->threads[c], kClassMaxN[c], b->grid[c], b->cls_stream[c]);
     if (e == cudaSuccess) e = cudaEventRecord(b->join[c], b->cls_stream[c]);
@@ -331,35 +259,61 @@ void cache_store(const char* path, const std::string& key, int cls, int threads)
 
 }  // namespace
 
+// Device table entry of one filter; false for invalid parameters.
+static bool make_filter_dev(const BpfBatchFilter& f, BatchFilterDev* out) {
+  if (f.n_particles <= 0 || f.n_particles > kBatchMaxN || !std::isfinite(f.mu) || !std::isfinite(f.rho) ||
+      !std::isfinite(f.sigma_z) || !(std::fabs(f.rho) < 1.0f) || !(f.sigma_z > 0.0f) || !std::isfinite(f.nu_obs) ||
+      !(f.nu_obs >= 0.0f) || !(f.nu_state == 0.0f || (f.nu_state >= 0.5f && std::isfinite(f.nu_state))))
+    return false;
+  BatchFilterDev d{};
+  d.mu = f.mu; d.rho = f.rho; d.sigma = f.sigma_z;
+  d.std_stat = sqrtf((f.sigma_z * f.sigma_z) / fmaxf(1.0f - f.rho * f.rho, 1e-6f));   // gpu_bpf_ptx_full.cu:430
+  d.nu = f.nu_obs;
+  if (f.nu_obs > 0.0f) {
+    d.c_obs = (float)(std::lgamma((f.nu_obs + 1.0) / 2.0) - std::lgamma(f.nu_obs / 2.0) -
+                      0.5 * std::log(f.nu_obs * 3.14159265358979323846));
+    d.inv_nu = 1.0f / f.nu_obs;
+    d.nu_p1h = (f.nu_obs + 1.0f) * 0.5f;
+  }
+  d.n = f.n_particles;
+  d.seed = f.seed;
+  d.nu_int = (f.nu_state > 0.0f) ? (int)(f.nu_state + 0.5f) : 0;   // gpu_bpf_ptx_full.cu:392
+  d.nu_state = f.nu_state;
+  *out = d;
+  return true;
+}
+
+int batch_set_filters(GpuBpfBatch* b, const BpfBatchFilter* filters) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  if (!filters) return bpf_record_error(BPF_ERR_ARG);
+  std::vector<BatchFilterDev> tab(b->B);
+  for (int i = 0; i < b->B; ++i)
+    if (filters[i].n_particles != b->n_of[i] || !make_filter_dev(filters[i], &tab[i])) return bpf_record_error(BPF_ERR_ARG);
+  BCK(cudaMemcpyAsync(b->d_filters, tab.data(), (size_t)b->B * sizeof(BatchFilterDev), cudaMemcpyHostToDevice,
+                      b->stream));
+  BCK(cudaStreamSynchronize(b->stream));   // the host table goes out of scope
+  return BPF_OK;
+}
+
 extern "C" {
+
+int gpu_bpf_batch_set_filters(GpuBpfBatch* b, const BpfBatchFilter* filters) {
+  if (b) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || (cur != b->device && cudaSetDevice(b->device) != cudaSuccess))
+      return bpf_record_error(BPF_ERR_CUDA);
+  }
+  return batch_set_filters(b, filters);
+}
 
 GpuBpfBatch* gpu_bpf_batch_create(const BpfBatchFilter* filters, int n_filters, float ess_threshold) {
   if (!filters || n_filters <= 0 || std::isnan(ess_threshold)) { bpf_record_error(BPF_ERR_ARG); return nullptr; }
   std::vector<BatchFilterDev> tab(n_filters);
-  for (int i = 0; i < n_filters; ++i) {
-    const BpfBatchFilter& f = filters[i];
-    if (f.n_particles <= 0 || f.n_particles > kBatchMaxN || !std::isfinite(f.mu) || !std::isfinite(f.rho) ||
-        !std::isfinite(f.sigma_z) || !(std::fabs(f.rho) < 1.0f) || !(f.sigma_z > 0.0f) || !std::isfinite(f.nu_obs) ||
-        !(f.nu_obs >= 0.0f) || !(f.nu_state == 0.0f || (f.nu_state >= 0.5f && std::isfinite(f.nu_state)))) {
+  for (int i = 0; i < n_filters; ++i)
+    if (!make_filter_dev(filters[i], &tab[i])) {
       bpf_record_error(BPF_ERR_ARG);
       return nullptr;
     }
-    BatchFilterDev& d = tab[i];
-    d = BatchFilterDev{};
-    d.mu = f.mu; d.rho = f.rho; d.sigma = f.sigma_z;
-    d.std_stat = sqrtf((f.sigma_z * f.sigma_z) / fmaxf(1.0f - f.rho * f.rho, 1e-6f));   // gpu_bpf_ptx_full.cu:430
-    d.nu = f.nu_obs;
-    if (f.nu_obs > 0.0f) {
-      d.c_obs = (float)(std::lgamma((f.nu_obs + 1.0) / 2.0) - std::lgamma(f.nu_obs / 2.0) -
-                        0.5 * std::log(f.nu_obs * 3.14159265358979323846));
-      d.inv_nu = 1.0f / f.nu_obs;
-      d.nu_p1h = (f.nu_obs + 1.0f) * 0.5f;
-    }
-    d.n = f.n_particles;
-    d.seed = f.seed;
-    d.nu_int = (f.nu_state > 0.0f) ? (int)(f.nu_state + 0.5f) : 0;   // gpu_bpf_ptx_full.cu:392
-    d.nu_state = f.nu_state;
-  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); bpf_record_error(BPF_ERR_NODEVICE); return nullptr; }
 
@@ -489,21 +443,24 @@ int gpu_bpf_batch_grad_run(GpuBpfBatch* b, const float* y_dev, int n_ticks, doub
   return BPF_OK;
 }
 
-int gpu_bpf_batch_step_device(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* dll_dev, float* hmean_dev) {
+}  // extern "C"
+
+static int step_common(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* dll_dev, float* hmean_dev,
+                       int y_abs) {
   if (!b) return bpf_record_error(BPF_ERR_STATE);
   if (n_ticks <= 0 || !y_dev) return bpf_record_error(BPF_ERR_ARG);
   int rc = ensure_device_b(b);
   if (rc) return rc;
-  rc = prepare_steps(b);
+  rc = batch_prepare_steps(b);
   if (rc) return rc;
   GraphKey k;
-  k.y = y_dev; k.T = n_ticks; k.dll = dll_dev; k.hmean = hmean_dev;
+  k.y = y_dev; k.T = n_ticks; k.dll = dll_dev; k.hmean = hmean_dev; k.y_abs = y_abs;
   std::copy(b->threads, b->threads + kClasses, k.threads);
   if (!b->sgraph || !(k == b->skey)) {
     if (b->sgraph) { cudaGraphExecDestroy(b->sgraph); b->sgraph = nullptr; }
     cudaGraph_t g = nullptr;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = enqueue_step(b, y_dev, n_ticks, dll_dev, hmean_dev);
+    cudaError_t e = enqueue_step(b, y_dev, n_ticks, dll_dev, hmean_dev, y_abs);
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
     e = cudaGraphInstantiate(&b->sgraph, g, 0);
@@ -515,6 +472,25 @@ int gpu_bpf_batch_step_device(GpuBpfBatch* b, const float* y_dev, int n_ticks, d
   bpf_note_launches(kClasses + 1);
   b->host_tick += n_ticks;
   return BPF_OK;
+}
+
+int batch_step_abs(GpuBpfBatch* b, const float* y_base, int n, double* dll_dev) {
+  return step_common(b, y_base, n, dll_dev, nullptr, 1);
+}
+
+int batch_set_tick(GpuBpfBatch* b, int tick) {
+  int rc = batch_prepare_steps(b);
+  if (rc) return rc;
+  BCK(cudaMemcpyAsync(b->d_tick, &tick, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  b->host_tick = tick;
+  return BPF_OK;
+}
+
+extern "C" {
+
+int gpu_bpf_batch_step_device(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* dll_dev, float* hmean_dev) {
+  return step_common(b, y_dev, n_ticks, dll_dev, hmean_dev, 0);
 }
 
 int gpu_bpf_batch_reset(GpuBpfBatch* b) {

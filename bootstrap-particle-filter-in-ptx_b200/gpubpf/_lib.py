@@ -76,6 +76,11 @@ class GpuImmState(C.Structure):
                 ("log_T", C.POINTER(C.c_double)), ("timestep", C.c_int), ("impl", C.c_void_p)]
 
 
+class BpfSmc2Prior(C.Structure):
+    _fields_ = [("mu_mean", C.c_float), ("mu_sd", C.c_float), ("rho_lo", C.c_float), ("rho_hi", C.c_float),
+                ("sigma_lo", C.c_float), ("sigma_hi", C.c_float)]
+
+
 P_STATE = C.POINTER(GpuBpfState)
 P_IMM = C.POINTER(GpuImmState)
 _f = C.c_float
@@ -138,6 +143,7 @@ SIGNATURES = {
     "gpu_bpf_batch_grad_run": (_i, [_vp, _vp, _i, _vp, _vp]),
     "gpu_bpf_batch_step_device": (_i, [_vp, _vp, _i, _vp, _vp]),
     "gpu_bpf_batch_reset": (_i, [_vp]),
+    "gpu_bpf_batch_set_filters": (_i, [_vp, C.POINTER(BpfBatchFilter)]),
     "gpu_bpf_batch_tick": (_i, [_vp]),
     "gpu_bpf_batch_loglik_device": (_vp, [_vp]),
     "gpu_bpf_batch_grad_tape_bytes": (C.c_size_t, [_vp, _i]),
@@ -149,6 +155,15 @@ SIGNATURES = {
     "gpu_imm_destroy": (None, [P_IMM]),
     "gpu_imm_build_grid": (C.POINTER(ImmModelParams), [C.POINTER(_f), _i, C.POINTER(_f), _i, C.POINTER(_f), _i,
                                                         _f, _f, C.POINTER(_i)]),
+    # SMC^2
+    "gpu_bpf_smc2_create": (_vp, [_i, _i, _i, C.POINTER(BpfSmc2Prior), C.c_ulonglong]),
+    "gpu_bpf_smc2_destroy": (None, [_vp]),
+    "gpu_bpf_smc2_set_moves": (_i, [_vp, _i, _f, _f]),
+    "gpu_bpf_smc2_update": (_f, [_vp, _f]),
+    "gpu_bpf_smc2_get_outer_ess": (_f, [_vp]),
+    "gpu_bpf_smc2_get_theta": (_i, [_vp, C.POINTER(_f), C.POINTER(_f)]),
+    "gpu_bpf_smc2_get_particles": (_i, [_vp, _vp, _vp, _vp]),
+    "gpu_bpf_smc2_stats": (_i, [_vp, C.POINTER(_i), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     # gradient
     "gpu_bpf_grad_create": (_vp, [_i, _i, _i]),
     "gpu_bpf_grad_destroy": (None, [_vp]),

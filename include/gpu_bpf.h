@@ -318,6 +318,10 @@ int          gpu_bpf_batch_resample_counts(GpuBpfBatch* batch, int* counts, floa
 int          gpu_bpf_batch_step_device(GpuBpfBatch* batch, const float* y_dev, int n_ticks, double* dll_dev,
                                        float* hmean_dev);
 int          gpu_bpf_batch_reset(GpuBpfBatch* batch);   /* next step starts again at tick 0 */
+/* New (mu, rho, sigma_z, nu_obs, nu_state, seed) for every filter; each n_particles must equal the
+ * filter's count at creation. Takes effect at the next run or step; the saved state is kept.
+ * Waits for the batch stream. */
+int          gpu_bpf_batch_set_filters(GpuBpfBatch* batch, const BpfBatchFilter* filters);
 int          gpu_bpf_batch_tick(GpuBpfBatch* batch);    /* ticks stepped since create / reset */
 /* Device array [n_filters] of FP64 total log-likelihoods, updated by every run or step. */
 double*      gpu_bpf_batch_loglik_device(GpuBpfBatch* batch);
@@ -370,6 +374,42 @@ int gpu_bpf_grad_replay(GpuBpfGrad* grad, double mu, double rho, double sigma_z,
  * child slot of every parent after tick `tick`'s resampling (host arrays). */
 int gpu_bpf_grad_get_records(GpuBpfGrad* grad, BpfTickRecord* out, int n);
 int gpu_bpf_grad_get_children(GpuBpfGrad* grad, int tick, int32_t* first_child);
+
+/* ---- SMC^2 over the SV parameters (addition) ---------------------------------
+ * Online Bayesian learning of theta = (mu, rho, sigma_z) by SMC^2: n_theta theta-particles, each
+ * with an inner bootstrap filter of n_particles (<= 16384) run as one resumable batch; outer
+ * weights are the inner log-likelihood increments; when the outer ESS falls below the
+ * threshold the theta-particles are resampled and rejuvenated by particle marginal
+ * Metropolis-Hastings moves whose proposals are scored by fresh inner filters over the whole
+ * history. The outer loop of the reference's smc2_cuda_update
+ * (smc2/smc2_rbpf_batch.cu:1329-1502, host API smc2/smc2_rbpf_batch.cuh:461-489) on this build's
+ * SV model; the reference's regime-switching RBPF inner model and correlated-noise moves are not
+ * part of it. Prior: mu ~ N(mu_mean, mu_sd^2), rho ~ U(rho_lo, rho_hi), sigma_z ~ U(sigma_lo,
+ * sigma_hi) (NULL = N(-1, 0.5^2), U(0.85, 0.995), U(0.05, 0.4)). Deterministic given the seed. */
+typedef struct {
+    float mu_mean, mu_sd, rho_lo, rho_hi, sigma_lo, sigma_hi;
+} BpfSmc2Prior;
+typedef struct GpuBpfSmc2 GpuBpfSmc2;
+
+/* ~ smc2_cuda_alloc + smc2_cuda_set_seed + smc2_cuda_init_from_prior. max_ticks bounds the
+ * observation history kept on the device. NULL on error. */
+GpuBpfSmc2* gpu_bpf_smc2_create(int n_theta, int n_particles, int max_ticks, const BpfSmc2Prior* prior,
+                                unsigned long long seed);
+void        gpu_bpf_smc2_destroy(GpuBpfSmc2* smc2);                              /* ~ smc2_cuda_free */
+/* Rejuvenation: PMMH moves per resampling (default 1), outer ESS threshold as a fraction of
+ * n_theta (default 0.5), random-walk scale relative to 2.38^2/3 times the theta covariance (1). */
+int         gpu_bpf_smc2_set_moves(GpuBpfSmc2* smc2, int n_moves, float outer_ess_threshold,
+                                   float proposal_scale);
+/* ~ smc2_cuda_update: one observation; returns the outer ESS after it (NaN on error). Waits. */
+float       gpu_bpf_smc2_update(GpuBpfSmc2* smc2, float y);
+float       gpu_bpf_smc2_get_outer_ess(GpuBpfSmc2* smc2);                        /* ~ smc2_cuda_get_outer_ess */
+/* ~ smc2_cuda_get_theta_mean / _std: weighted posterior mean and std of (mu, rho, sigma_z). */
+int         gpu_bpf_smc2_get_theta(GpuBpfSmc2* smc2, float* mean3, float* std3);
+/* theta[3*n_theta] (mu, rho, sigma_z per particle), outer log-weights and inner total
+ * log-likelihoods (each may be NULL). */
+int         gpu_bpf_smc2_get_particles(GpuBpfSmc2* smc2, float* theta, double* logw, double* loglik);
+int         gpu_bpf_smc2_stats(GpuBpfSmc2* smc2, int* n_rejuvenations, long long* n_proposed,
+                               long long* n_accepted);
 
 /* Number of kernel launches this library has issued (all filters). */
 long long gpu_bpf_launch_count(void);
