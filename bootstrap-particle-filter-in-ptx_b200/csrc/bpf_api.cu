@@ -78,6 +78,10 @@ struct Impl {
 
   // profiling
   bool profiling = false;
+
+  // online mu / rho learning (gpu_bpf_ptx_full.cu:469-544, settings :363-371,777-800)
+  int learn_mode = 0, learn_rho = 0, update_K = 50, grad_count = 0, rm_step = 0;
+  float rm_c = 0.1f, rm_t0 = 10.0f, rm_gamma = 0.667f, grad_clip = 5.0f;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<cudaEvent_t> ev_pending;   // quadruples: before pass 1, after pass 1, after plan, after pass 2
   double prof_p1_ms = 0.0, prof_plan_ms = 0.0, prof_p2_ms = 0.0;
@@ -114,6 +118,7 @@ TickArgs make_args(GpuBpfState* s, Impl* m, float y, const float* y_ptr, BpfTick
   a.anc = m->record_anc ? m->anc_dev : nullptr;
   a.nu_int = (s->nu_state > 0.0f) ? (int)(s->nu_state + 0.5f) : 0;   // gpu_bpf_ptx_full.cu:392
   a.nu_state = s->nu_state;
+  a.learn = m->learn_mode ? 1 : 0;
   return a;
 }
 
@@ -148,6 +153,38 @@ int drain_profile(Impl* m) {
   return BPF_OK;
 }
 
+int zero_learning_sums(Impl* m) {
+  CK(cudaMemsetAsync(&m->plan.st->learn[0], 0, sizeof(m->plan.st->learn), m->stream));
+  return BPF_OK;
+}
+
+// Robbins-Monro natural-gradient step on alpha = mu (1 - rho) and on rho from the
+// score sums of the last update_K ticks (gpu_bpf_ptx_full.cu:489-543): step size
+// c / (k + t0)^gamma, direction mean score / mean Fisher information (mode 1; the
+// mean score itself in mode 2), clipped to +-5, gated by min(SNR / 2, 1) with
+// SNR = |mean score| / sqrt(mean Fisher / K). Waits for the filter's stream.
+int learning_update(GpuBpfState* s, Impl* m) {
+  CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  const double* sums = m->st_pin->learn;
+  m->rm_step += 1;
+  const double eta = m->rm_c / std::pow((double)m->rm_step + m->rm_t0, (double)m->rm_gamma);
+  const double K = (double)m->grad_count;
+  auto step = [&](double g_sum, double f_sum) {
+    const double mean_g = g_sum / K, mean_f = f_sum / K;
+    double dir = (m->learn_mode == 2) ? mean_g : mean_g / std::fmax(mean_f, 1e-8);
+    if (m->grad_clip > 0.0f && std::fabs(dir) > m->grad_clip) dir *= m->grad_clip / std::fabs(dir);
+    const double snr = std::fabs(mean_g) / std::fmax(std::sqrt(mean_f / K), 1e-10);
+    return eta * std::fmin(snr / 2.0, 1.0) * dir;
+  };
+  const double rho = s->rho;
+  const double alpha = (double)s->mu * (1.0 - rho) + step(sums[0], sums[1]);
+  s->mu = (float)std::fmax(std::fmin(alpha / std::fmax(1.0 - rho, 1e-6), 2.0), -5.0);
+  if (m->learn_rho) s->rho = (float)std::fmax(std::fmin(rho + step(sums[2], sums[3]), 0.999), 0.001);
+  m->grad_count = 0;
+  return zero_learning_sums(m);
+}
+
 // Enqueue one tick (pass 1, plan, pass 2) on the filter's stream.
 int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
   if (m->profiling) {
@@ -165,7 +202,9 @@ int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
     CK(launch_tick3(m, a));
   }
   g_launches += 3;
+  const int tick = m->ticks_enqueued;
   m->ticks_enqueued += 1;
+  if (m->learn_mode && tick > 0 && ++m->grad_count >= m->update_K) return learning_update(s, m);
   return BPF_OK;
 }
 
@@ -430,17 +469,56 @@ int gpu_bpf_get_resample_count(GpuBpfState* s) {
 
 float gpu_bpf_get_mu(GpuBpfState* s) { return s ? s->mu : NAN; }
 float gpu_bpf_get_rho(GpuBpfState* s) { return s ? s->rho : NAN; }
+// An external parameter push restarts the Robbins-Monro schedule (gpu_bpf_ptx_full.cu:812-828).
+static void restart_learning(GpuBpfState* s) {
+  Impl* m = impl_of(s);
+  if (!m) return;
+  m->rm_step = 0;
+  m->grad_count = 0;
+  if (ensure_device(m) == BPF_OK) zero_learning_sums(m);
+}
 void gpu_bpf_set_mu(GpuBpfState* s, float mu) {
   if (!s || !std::isfinite(mu)) { set_err(BPF_ERR_ARG); return; }
   s->mu = mu;
+  restart_learning(s);
 }
 void gpu_bpf_set_rho(GpuBpfState* s, float rho) {
   if (!s || !std::isfinite(rho)) { set_err(BPF_ERR_ARG); return; }
   s->rho = fmaxf(fminf(rho, 0.999f), 0.001f);       // gpu_bpf_ptx_full.cu:822
+  restart_learning(s);
 }
-void gpu_bpf_enable_mu_learning(GpuBpfState*, int, int, float, float, float) { set_err(BPF_ERR_UNSUPPORTED); }
-void gpu_bpf_disable_mu_learning(GpuBpfState*) {}
-void gpu_bpf_enable_rho_learning(GpuBpfState*, int enable) { if (enable) set_err(BPF_ERR_UNSUPPORTED); }
+void gpu_bpf_enable_mu_learning(GpuBpfState* s, int mode, int K, float c, float t0, float gamma) {
+  Impl* m = impl_of(s);
+  if (!m) { set_err(BPF_ERR_STATE); return; }
+  if (mode < 0 || mode > 2 || K < 1 || !(c > 0.0f) || !(t0 >= 0.0f) || !(gamma > 0.0f)) { set_err(BPF_ERR_ARG); return; }
+  m->learn_mode = mode;                              // gpu_bpf_ptx_full.cu:777-790
+  m->update_K = K;
+  m->grad_clip = 5.0f;
+  m->rm_c = c; m->rm_t0 = t0; m->rm_gamma = gamma;
+  restart_learning(s);
+}
+void gpu_bpf_disable_mu_learning(GpuBpfState* s) {
+  Impl* m = impl_of(s);
+  if (!m) { set_err(BPF_ERR_STATE); return; }
+  m->learn_mode = 0;
+  m->learn_rho = 0;
+}
+void gpu_bpf_enable_rho_learning(GpuBpfState* s, int enable) {
+  Impl* m = impl_of(s);
+  if (!m) { set_err(BPF_ERR_STATE); return; }
+  m->learn_rho = enable ? 1 : 0;
+}
+int gpu_bpf_get_learning_sums(GpuBpfState* s, double* sums4, int* ticks) {
+  Impl* m = impl_of(s);
+  if (!m || !sums4) return set_err(!m ? BPF_ERR_STATE : BPF_ERR_ARG);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  for (int i = 0; i < 4; ++i) sums4[i] = m->st_pin->learn[i];
+  if (ticks) *ticks = m->grad_count;
+  return BPF_OK;
+}
 
 // ===========================================================================
 // Additions
@@ -455,7 +533,7 @@ int gpu_bpf_step_many(GpuBpfState* s, const float* y, int n_ticks, BpfResult* ou
   rc = ensure_device(m);
   if (rc) return rc;
   int t = 0;
-  if (!m->profiling) {
+  if (!m->profiling && !m->learn_mode) {            // learning updates need the host every K ticks
     while (n_ticks - t >= kGraphChunk) {
       if (graph_stale(s, m)) { rc = build_graph(s, m); if (rc) return rc; }
       std::memcpy(m->y_pin, y + t, kGraphChunk * sizeof(float));
@@ -509,7 +587,7 @@ int gpu_bpf_step_many_device(GpuBpfState* s, const float* y_dev, int n_ticks, Bp
   if (rc) return rc;
   rc = ensure_device(m);
   if (rc) return rc;
-  if (!m->profiling && n_ticks > 0 && n_ticks <= kMaxGraphTicks) {
+  if (!m->profiling && !m->learn_mode && n_ticks > 0 && n_ticks <= kMaxGraphTicks) {
     const bool stale = !m->dgraph || m->dg_y != y_dev || m->dg_rec != rec_dev || m->dg_n != n_ticks ||
                        m->dg_mu != s->mu || m->dg_rho != s->rho || m->dg_sigma != s->sigma_z ||
                        m->dg_thr != s->ess_threshold || m->dg_nus != s->nu_state || m->dg_anc != m->record_anc;
@@ -540,6 +618,7 @@ int gpu_bpf_reset(GpuBpfState* s, int seed) {
   CK(launch_init(m->plan, s->mu, std_stat, seed, m->stream));   // also resets the DevState
   g_launches += 1;
   m->ticks_enqueued = 0;
+  m->grad_count = 0;                               // the init kernel zeroes the device sums
   s->timestep = 0; s->did_resample = 1; s->resample_count = 0; s->last_h_est = s->mu;
   return BPF_OK;
 }

@@ -68,7 +68,7 @@ constexpr int kStWords = (int)(sizeof(DevState) / 8);
 // ---------------------------------------------------------------------------
 // Pass 1
 // ---------------------------------------------------------------------------
-template <bool TSTATE>
+template <bool TSTATE, bool LEARN>
 __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
   __shared__ float s_max[kThreads / 32];
   __shared__ double s_red[3][kThreads / 32];
@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   }
 
   float x[kPerThread], hv[kPerThread];
+  float hpv[LEARN ? kPerThread : 1];     // particles before this tick's propagation (learning only)
   const unsigned long long step2 = 2ull * c.k2;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -121,6 +122,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       float h = hh[e];
+      if (LEARN) hpv[4 * r + e] = h;
       if (tick > 0) {
         float z = icdf_normal(pcg_uniform(pcg_output(s)));
         if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
@@ -151,6 +153,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   const float fnk = (float)nk;
 
   float fS = 0.f, fQ = 0.f, fH = 0.f;
+  float lG0 = 0.f, lF0 = 0.f, lG1 = 0.f, lF1 = 0.f;   // online-learning score sums (tile frame)
   unsigned long long E = 0ull;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -165,6 +168,18 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
       fQ = fmaf(w, w, fQ);
       fH = fmaf(w, hv[idx], fH);
       E += fix_weight(w);
+      if (LEARN) {
+        // d log p(y|h)/dh at h_t (PTX :1187-1204) and d h_t / d rho = h_{t-1} - mu
+        const float q = y2 * ex2_approx(hv[idx] * -kLog2e);
+        const float dlw = gauss ? 0.5f * (q - 1.0f)
+                                : fmaf(obs.nu_p1h, div_approx(q * obs.inv_nu, 1.0f + q * obs.inv_nu), -0.5f);
+        const float dh = hpv[idx] - a.mu;
+        const float wd = w * dlw, wd2 = wd * dlw;
+        lG0 += wd;
+        lF0 += wd2;
+        lG1 = fmaf(wd, dh, lG1);
+        lF1 = fmaf(wd2, dh * dh, lF1);
+      }
     }
     *reinterpret_cast<float4*>(p.w + i0) = make_float4(wv[0], wv[1], wv[2], wv[3]);
   }
@@ -181,6 +196,21 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     p.E[k] = tE;
     p.rec[k] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
   }
+  if (LEARN) {
+    __syncthreads();                                 // s_red is reused
+    const double g0 = warp_sum_d((double)lG0), f0 = warp_sum_d((double)lF0);
+    const double g1 = warp_sum_d((double)lG1), f1 = warp_sum_d((double)lF1);
+    if (lane == 0) { s_red[0][warp] = g0; s_red[1][warp] = f0; s_red[2][warp] = g1; s_redE[warp] = 0ull; }
+    __shared__ double s_red4[kThreads / 32];
+    if (lane == 0) s_red4[warp] = f1;
+    __syncthreads();
+    if (tid == 0) {
+      double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w) { t0 += s_red[0][w]; t1 += s_red[1][w]; t2 += s_red[2][w]; t3 += s_red4[w]; }
+      p.rec2[k] = make_float4((float)t0, (float)t1, (float)t2, (float)t3);
+    }
+  }
   griddep_release();
 }
 
@@ -193,6 +223,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
 struct PlanShared {
   int red_i[kPlanThreads / 32];
   double red[3][kPlanThreads / 32];
+  double learn3[kPlanThreads / 32];
   double tot[3];
   double res[4];
   unsigned long long scan_u[kPlanThreads / 32 + 1];
@@ -276,6 +307,29 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     if (warp == 3) sh.res[3] = log(tS);
   }
   __syncthreads();
+  // online learning: normalised score sums of this tick, FP64 in the global frame
+  if (a.learn && p.rec2 && st->tick > 0 && !degenerate) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = tid; k < G; k += kPlanThreads) {
+      const int nk = __float_as_int(__ldcg(p.rec + k).w);
+      if (nk == kNkEmpty) continue;
+      const float4 r2 = __ldcg(p.rec2 + k);
+      const double sc = pow2d(nk - nM);
+      v[0] += (double)r2.x * sc; v[1] += (double)r2.y * sc; v[2] += (double)r2.z * sc; v[3] += (double)r2.w * sc;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = warp_sum_d(v[q]);
+    __syncthreads();                                  // sh.red is free again
+    if (lane == 0) { sh.red[0][warp] = v[0]; sh.red[1][warp] = v[1]; sh.red[2][warp] = v[2]; }
+    if (lane == 0) sh.learn3[warp] = v[3];
+    __syncthreads();
+    if (tid < 4) {
+      double t = 0.0;
+      for (int w = 0; w < kPlanThreads / 32; ++w) t += (tid < 3) ? sh.red[tid][w] : sh.learn3[w];
+      st->learn[tid] += t / tS;
+    }
+    __syncthreads();
+  }
   if (tid == 0) {
     const int tick = st->tick, cur = st->cur;
     double dll, ess, hm;
@@ -625,6 +679,7 @@ cudaError_t plan_alloc(Plan& p, int N) {
   al(&p.nexp, p.G * sizeof(int));
   al(&p.E, p.G * sizeof(unsigned long long));
   al(&p.rec, p.G * sizeof(float4));
+  al(&p.rec2, p.G * sizeof(float4));
   al(&p.P, p.G * sizeof(unsigned long long));
   al(&p.ofirst, (p.G + 1) * sizeof(int));
   al(&p.items, p.max_items * sizeof(int4));
@@ -636,7 +691,7 @@ cudaError_t plan_alloc(Plan& p, int N) {
 
 void plan_free(Plan& p) {
   cudaFree(p.h0); cudaFree(p.h1); cudaFree(p.w);
-  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.rec);
+  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.rec); cudaFree(p.rec2);
   cudaFree(p.P); cudaFree(p.ofirst); cudaFree(p.items); cudaFree(p.st);
   p = Plan{};
 }
@@ -665,8 +720,13 @@ int pass2_grid_size(int device) {
 }
 
 cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
-  if (a.nu_int > 0) return launch_ex(pass1_kernel<true>, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a);
-  return launch_ex(pass1_kernel<false>, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a);
+  const dim3 grid(p.G), block(kThreads);
+  if (a.learn && p.rec2) {
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, true>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, true>, grid, block, 0, s, pdl, p, a);
+  }
+  if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false>, grid, block, 0, s, pdl, p, a);
+  return launch_ex(pass1_kernel<false, false>, grid, block, 0, s, pdl, p, a);
 }
 cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
   return launch_ex(plan_kernel, dim3(1), dim3(kPlanThreads), plan_smem_bytes(p.G), s, pdl, p, a);

@@ -42,13 +42,16 @@ struct DevState {
   int      reserved;
   int      error;           // sticky BPF_* error code
   int      seed;            // filter seed (PCG32 streams, resampling uniform)
+  double   learn[4];        // online learning sums since the last update: sum_t of
+                            // sum W dlw, sum W dlw^2, sum W dlw (h_prev-mu), sum W dlw^2 (h_prev-mu)^2
 };
-static_assert(sizeof(DevState) == 136, "DevState layout");
+static_assert(sizeof(DevState) == 168, "DevState layout");
 
 struct Plan {
   int N, G, max_items;
   float* h0; float* h1; float* w;
   int* nexp; unsigned long long* E; float4* rec;
+  float4* rec2;              // per tile, online learning only: tile-frame sums of w dlw, w dlw^2, w dlw dh, w dlw^2 dh^2
   unsigned long long* P; int* ofirst; int4* items;
   DevState* st;
 };
@@ -63,6 +66,7 @@ struct TickArgs {
   int32_t* anc;              // ancestors of this tick (N ints) or null
   int nu_int;                // Student-t state noise: round(nu_state) degrees of freedom, 0 = Gaussian
   float nu_state;            // Student-t state noise scale parameter
+  int learn;                 // accumulate the online-learning score sums of this tick (needs p.rec2)
   // gradient tape (all null outside a taped run)
   float* ckpt;               // copy of the particles pass 1 reads this tick (G*4096 floats) or null
   int32_t* csr;              // on resampling ticks: first child slot of every parent (N ints) or null

@@ -127,6 +127,7 @@ SIGNATURES = {
     "gpu_bpf_profile_read": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), C.POINTER(_i),
                                   C.POINTER(_i)]),
     "gpu_bpf_launch_count": (C.c_longlong, []),
+    "gpu_bpf_get_learning_sums": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_i)]),
     "gpu_bpf_run_static": (_i, [_i, _f, _f, _f, _f, _i, _f, _vp, _i, _vp, _vp]),
     # batched filters
     "gpu_bpf_batch_create": (_vp, [C.POINTER(BpfBatchFilter), _i, _f]),

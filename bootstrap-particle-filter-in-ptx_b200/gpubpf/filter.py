@@ -51,6 +51,23 @@ class GpuBpf:
     def state(self) -> _lib.GpuBpfState:
         return self._s.contents
 
+    # -- online mu / rho learning (gpu_bpf/gpu_bpf_full.cuh:176-204) --------
+    def enable_mu_learning(self, mode: int = 1, K: int = 50, c: float = 0.1, t0: float = 10.0,
+                           gamma: float = 0.667) -> None:
+        self._lib.gpu_bpf_enable_mu_learning(self._s, int(mode), int(K), float(c), float(t0), float(gamma))
+
+    def disable_mu_learning(self) -> None:
+        self._lib.gpu_bpf_disable_mu_learning(self._s)
+
+    def enable_rho_learning(self, enable: bool = True) -> None:
+        self._lib.gpu_bpf_enable_rho_learning(self._s, int(bool(enable)))
+
+    def learning_sums(self):
+        arr = (C.c_double * 4)()
+        n = C.c_int(0)
+        check(self._lib.gpu_bpf_get_learning_sums(self._s, arr, C.byref(n)), "gpu_bpf_get_learning_sums")
+        return list(arr), n.value
+
     # -- reference API ----------------------------------------------------
     def step(self, y_t: float) -> BpfResult:
         r = self._lib.gpu_bpf_step(self._s, float(y_t))

@@ -29,7 +29,7 @@ extern "C" {
 #define BPF_ERR_ARG          1  /* invalid argument (N<=0, |rho|>=1, sigma<=0, non-finite y, NULL) */
 #define BPF_ERR_CUDA         2  /* a CUDA runtime call failed                                       */
 #define BPF_ERR_ALLOC        3  /* device or pinned allocation failed                               */
-#define BPF_ERR_UNSUPPORTED  4  /* option outside this build (bands, Silverman, learning)            */
+#define BPF_ERR_UNSUPPORTED  4  /* option outside this build (bands, Silverman jitter)               */
 #define BPF_ERR_STATE        5  /* call not valid in the filter's current state                     */
 #define BPF_ERR_DEGENERATE   6  /* every particle weight underflowed on a tick                      */
 #define BPF_ERR_NODEVICE     7  /* no CUDA device / kernel image for this GPU                       */
@@ -129,18 +129,28 @@ void gpu_bpf_set_ess_threshold(GpuBpfState* state, float threshold);
 int gpu_bpf_get_resample_count(GpuBpfState* state);
 
 /* gpu_bpf/gpu_bpf_full.cuh:206-230 (gpu_bpf_ptx_full.cu:802-828): parameter
- * access between ticks. set_rho clamps to (0.001, 0.999) like the reference. */
+ * access between ticks. set_rho clamps to (0.001, 0.999) like the reference; both
+ * setters restart the online-learning step-size schedule. */
 float gpu_bpf_get_mu(GpuBpfState* state);
 float gpu_bpf_get_rho(GpuBpfState* state);
 void  gpu_bpf_set_mu(GpuBpfState* state, float mu);
 void  gpu_bpf_set_rho(GpuBpfState* state, float rho);
 
-/* gpu_bpf/gpu_bpf_full.cuh:197-204: online mu/rho learning is not part of
- * this build (the adjoint form replaces it). enable_* record
- * BPF_ERR_UNSUPPORTED; disable is a no-op. */
+/* gpu_bpf/gpu_bpf_full.cuh:176-204 (gpu_bpf_ptx_full.cu:469-544,777-800): online
+ * learning of mu (and of rho after enable_rho_learning). Every tick after the first adds the
+ * one-step score sums sum W dlw, sum W dlw^2, sum W dlw (h_{t-1}-mu), sum W dlw^2 (h_{t-1}-mu)^2
+ * (W the normalised weights, dlw = d log p(y_t|h)/dh at h_t; computed inside pass 1 and the
+ * plan kernel); every K such ticks mu is moved through alpha = mu (1 - rho) by a Robbins-Monro
+ * step c / (k + t0)^gamma times the direction (mode 1: mean score / mean Fisher information,
+ * mode 2: mean score), clipped to +-5 and gated by min(SNR / 2, 1); mu stays in [-5, 2] and rho
+ * in [0.001, 0.999]. mode 0 switches learning off. An update reads the device state back, so
+ * learning filters synchronise every K ticks (as the reference) and step_many runs them
+ * without CUDA graphs. */
 void gpu_bpf_enable_mu_learning(GpuBpfState* state, int mode, int K, float c, float t0, float gamma);
 void gpu_bpf_disable_mu_learning(GpuBpfState* state);
 void gpu_bpf_enable_rho_learning(GpuBpfState* state, int enable);
+/* Addition: the score sums accumulated since the last update, and how many ticks they cover. */
+int  gpu_bpf_get_learning_sums(GpuBpfState* state, double* sums4, int* ticks);
 
 /* ---- Additions ------------------------------------------------------------ */
 
