@@ -26,7 +26,9 @@ one filter pass over the T=5000 series (re-seed + 5000 ticks).
          4000-tick regime-switching series, against the batched forward
 
 `--impl reference` times that CPU restatement alone (rank 0) and prints the
-same metric. Multi-GPU (torchrun): independent replicas, one per GPU, seeds
+same metric; when oracle/_ref holds the reference's own GPU filter (built from
+the reference sources) its line adds `reference_gpu`, that filter timed on this
+GPU on the same workload. Multi-GPU (torchrun): independent replicas, one per GPU, seeds
 differ per rank; no collective on the data path.
 """
 from __future__ import annotations
@@ -505,9 +507,52 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": "port",
                          "sample": r["sample"]},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu(args, y),
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_gpu(args, y):
+    """The reference's own GPU filter (its PTX edition, built into oracle/_ref/ from the reference
+    sources) on this GPU, same workload: a fresh gpu_bpf_create per step (untimed), then the T-tick
+    gpu_bpf_step_async loop with its per-tick host ESS decision, wall-clocked to the final stream
+    synchronise. Also configuration 1 (N=4096, T=1000, always resample). None when the library
+    was not built or no GPU is visible."""
+    try:
+        import torch
+        from oracle import refgpu
+        if not (refgpu.available() and torch.cuda.is_available()):
+            return None
+    except Exception:
+        return None
+    import numpy as np
+
+    def timed(n, yy, ess, steps, warmup):
+        ms, last, count = [], None, 0
+        for k in range(warmup + steps):
+            f = refgpu.RefGpuFilter(n, RHO, SIG, MU, seed=42, ess_threshold=ess)
+            t, hm, ll = f.time_run(yy)
+            count = f.resample_count
+            f.close()
+            if k >= warmup:
+                ms.append(t)
+                last = (hm, ll)
+        m = statistics.mean(ms)
+        return {"value": n * len(yy) / (m / 1e3), "unit": "particle-steps/s", "ms_per_step": m,
+                "us_per_tick": m * 1e3 / len(yy), "resample_count": count,
+                "last_tick": {"h_mean": last[0], "log_lik": last[1]}}
+
+    out = timed(args.n, y, args.ess, max(1, min(args.steps, 3)), 1)
+    out["kind"] = ("reference PTX edition (gpu_bpf/gpu_bpf_ptx_full.cu + ptx_assembly/bpf_kernels_full.ptx, "
+                   "JIT for sm_100a) on this GPU")
+    out["workload"] = f"N={args.n}, T={len(y)}, ESS<{args.ess}N, DGP seed {args.dgp_seed}, filter seed 42"
+    from gpubpf import dgp
+    _, y1 = dgp.matched_series(1000, RHO, SIG, MU, 42)
+    c1 = timed(4096, np.asarray(y1, dtype=np.float32), 0.0, 3, 1)
+    out["config1"] = {"us_per_tick": c1["us_per_tick"], "value": c1["value"], "unit": c1["unit"],
+                      "workload": "N=4096, T=1000, always resample, DGP seed 42"}
+    return out
 
 
 def main():

@@ -15,6 +15,8 @@
  *                        (erfc-based): the FP64 oracle's inverse normal CDF
  *   orc_filter_f64       FP64 filter in this build's semantics, optionally
  *                        replaying resampling decisions and ancestors
+ *   orc_apf_f64          FP64 auxiliary particle filter (gpu_bpf_ptx_full.cu:990-1175)
+ *                        with the PCG32 streams, optionally replaying ancestors
  *   orc_grad_f64         d loglik / d(mu, rho, sigma) of the FP64 filter with the
  *                        resampling ancestors held fixed (tests/diff_bpf.py:186-237
  *                        with detached indices :35-56), forward-mode tangents or
@@ -24,6 +26,9 @@
  *   orc_ref_run          FP32 restatement of the reference tick loop
  *                        (gpu_bpf_ptx_full.cu:340-771 with PTX kernels :51-842),
  *                        OpenMP over particles: the CPU baseline
+ *   orc_ref_init,        the same initial state, tick and resampling stage by
+ *   orc_ref_tick,        stage on given particles (lock-step check against the
+ *   orc_ref_resample     reference run on a GPU)
  */
 #include <math.h>
 #include <stdint.h>
@@ -322,6 +327,116 @@ int orc_filter_f64(const OrcConfig* c, const float* y, int T,
 }
 
 /* ------------------------------------------------------------------------- */
+/* FP64 auxiliary particle filter (gpu_bpf/gpu_bpf_ptx_full.cu:990-1175)      */
+/* ------------------------------------------------------------------------- */
+/*
+ * Tick 0 is a bootstrap tick (weights from h_0, resample). Tick t >= 1:
+ *   first stage   m_i = mu + rho (h_i - mu), v_i = p(y_t | m_i), resample the
+ *                 pairs (h, m) by v (apf_first_stage, apf_resample_pair)
+ *   second stage  h_i = m_i + sigma eps_i,t,  w_i = p(y_t | h_i) / p(y_t | m_i)
+ *                 (apf_propagate_correct), mean and log-likelihood from w,
+ *                 resample by w
+ * The reference reports log mean w as BpfResult.log_lik (ll_ref here); the APF
+ * estimate of log p(y_t | y_{1:t-1}) is log mean v + log mean w (dll here).
+ * eps is draw t of slot i's PCG32 stream (Student-t scaled as the bootstrap
+ * filter's); the reference draws it from cuRAND (apf_init_rng_k). Both stages
+ * draw their uniform from the host stream, in order. anc1 / anc2: [T][N]
+ * ancestors of the two stages to replay (anc1 row 0 unused), NULL = own FP64
+ * systematic resampling. Outputs (each may be NULL): dll, ll_ref, hmean, ess [T].
+ */
+static void sys_resample_f64(int N, const double* cdf, double S, uint32_t u23, int32_t* a) {
+    const double step = S / (double)N, u0 = (double)u23 * 1.1920928955078125e-07;
+    int j = 0;
+    for (int i = 0; i < N; ++i) {
+        double target = (u0 + (double)i) * step;
+        while (j < N - 1 && !(cdf[j] > target)) ++j;
+        a[i] = j;
+    }
+}
+
+int orc_apf_f64(const OrcConfig* c, const float* y, int T, const int32_t* anc1, const int32_t* anc2,
+                double* dll, double* ll_ref, double* hmean, double* ess) {
+    const int N = c->n_particles;
+    if (N <= 0 || T < 0) return 1;
+    double* h = (double*)malloc(sizeof(double) * N);
+    double* m = (double*)malloc(sizeof(double) * N);
+    double* hn = (double*)malloc(sizeof(double) * N);
+    double* mn = (double*)malloc(sizeof(double) * N);
+    double* lw = (double*)malloc(sizeof(double) * N);
+    double* cdf = (double*)malloc(sizeof(double) * N);
+    int32_t* a = (int32_t*)malloc(sizeof(int32_t) * N);
+    if (!h || !m || !hn || !mn || !lw || !cdf || !a) {
+        free(h); free(m); free(hn); free(mn); free(lw); free(cdf); free(a);
+        return 2;
+    }
+    const double mu = c->mu, rho = c->rho, sig = c->sigma_z, nu = c->nu_obs, cobs = c_obs_of(nu);
+    const int nu_int = nu_int_of((double)c->nu_state);
+    const double sstat = sqrt(sig * sig / fmax(1.0 - rho * rho, 1e-6)), lnN = log((double)N);
+    for (int i = 0; i < N; ++i) {
+        float u = orc_uniform(orc_pcg32_draw_jump(c->seed, (uint32_t)i, 0));
+        h[i] = mu + sstat * orc_icdf_f64((double)u);
+    }
+    uint64_t ustate = orc_host_seed(c->seed);
+    for (int t = 0; t < T; ++t) {
+        const double yt = (double)y[t];
+        double lmv = 0.0;
+        if (t > 0) {
+            /* first stage */
+            double M = -INFINITY;
+            for (int i = 0; i < N; ++i) {
+                m[i] = mu + rho * (h[i] - mu);
+                lw[i] = obs_logpdf_f64(yt, m[i], nu, cobs);
+                if (lw[i] > M) M = lw[i];
+            }
+            double S = 0.0;
+            for (int i = 0; i < N; ++i) { S += exp(lw[i] - M); cdf[i] = S; }
+            lmv = M + log(S) - lnN;
+            uint32_t u23 = orc_host_pcg32(&ustate) >> 9;
+            const int32_t* ar = anc1 ? anc1 + (size_t)t * N : a;
+            if (!anc1) sys_resample_f64(N, cdf, S, u23, a);
+            for (int i = 0; i < N; ++i) { hn[i] = h[ar[i]]; mn[i] = m[ar[i]]; }
+            double* tmp = h; h = hn; hn = tmp;
+            tmp = m; m = mn; mn = tmp;
+            /* second stage: propagate from the resampled parents */
+            uint64_t At, Bt;
+            orc_pcg32_jump((uint64_t)t, &At, &Bt);
+            for (int i = 0; i < N; ++i) {
+                uint64_t s0, inc;
+                orc_pcg32_init(c->seed, (uint32_t)i, &s0, &inc);
+                float u = orc_uniform(orc_pcg32_output(At * s0 + Bt * inc));
+                double eps = orc_icdf_f64((double)u);
+                if (nu_int > 0) eps *= orc_tstate_scale(c->seed, (uint32_t)i, t, nu_int, (double)c->nu_state);
+                h[i] = m[i] + sig * eps;
+            }
+        }
+        double M = -INFINITY;
+        for (int i = 0; i < N; ++i) {
+            lw[i] = obs_logpdf_f64(yt, h[i], nu, cobs);
+            if (t > 0) lw[i] -= obs_logpdf_f64(yt, m[i], nu, cobs);
+            if (lw[i] > M) M = lw[i];
+        }
+        double S = 0.0, Q = 0.0, H = 0.0;
+        for (int i = 0; i < N; ++i) {
+            double e = exp(lw[i] - M);
+            S += e; Q += e * e; H += e * h[i];
+            cdf[i] = S;
+        }
+        const double lmw = M + log(S) - lnN;
+        if (dll) dll[t] = lmv + lmw;
+        if (ll_ref) ll_ref[t] = lmw;
+        if (hmean) hmean[t] = H / S;
+        if (ess) ess[t] = S * S / Q;
+        uint32_t u23 = orc_host_pcg32(&ustate) >> 9;
+        const int32_t* ar = anc2 ? anc2 + (size_t)t * N : a;
+        if (!anc2) sys_resample_f64(N, cdf, S, u23, a);
+        for (int i = 0; i < N; ++i) hn[i] = h[ar[i]];
+        double* tmp = h; h = hn; hn = tmp;
+    }
+    free(h); free(m); free(hn); free(mn); free(lw); free(cdf); free(a);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Gradient with the ancestors held fixed                                     */
 /* ------------------------------------------------------------------------- */
 static double obs_dlogpdf_f64(double y, double h, double nu) {
@@ -499,11 +614,123 @@ int orc_resample_fixed(int N, const float* w, const int32_t* nexp, uint32_t u23,
 /* ------------------------------------------------------------------------- */
 /*
  * Follows gpu_bpf_step_async (gpu_bpf_ptx_full.cu:550-748) with 1 band,
- * nu_state = 0, Silverman off, no learning: propagate_weight (PTX :231-458),
- * accumulate on skipped ticks (:601-604), max / exp_sub / sum / scale_wh /
- * sum(wh) / compute_loglik (PTX :488-775), sum(w^2) and the ESS decision
- * (:656-685), inclusive scan + systematic resample (:691-706, PTX :782-842).
+ * nu_state = 0, Silverman off, no learning, one stage per helper:
+ *   ref_propagate_weight  propagate_weight (PTX :231-458) and the accumulation
+ *                         of skipped ticks (:601-604); returns max(lw) (PTX :488-576)
+ *   ref_normalise         exp_sub / sum / scale_wh / sum(wh) / compute_loglik
+ *                         (PTX :586-775) and sum(w^2) for the ESS (:656-685)
+ *   ref_resample          inclusive scan + systematic resample (:691-706, PTX :782-842)
  * Transcendentals use libm in FP32 where the PTX uses approximate MUFU ops.
+ */
+static const float kRefLog2e = 1.44269504088896340736f, kRefLn2 = 0.693147180559945309417f;
+
+static float ref_propagate_weight(int N, uint64_t* rng, float* h, float* lw, const float* lwp, int do_prop, int acc,
+                                  float rho, float sigma_z, float mu, float nu_obs, float c_obs, float yt) {
+    float mx = -1e30f;
+#pragma omp parallel for schedule(static) reduction(max : mx)
+    for (int i = 0; i < N; ++i) {
+        float hi = h[i];
+        if (do_prop) {
+            uint64_t s = rng[2 * (size_t)i], inc = rng[2 * (size_t)i + 1];
+            uint32_t o = orc_pcg32_output(s);
+            rng[2 * (size_t)i] = s * PCG_A + inc;
+            float eps = acklam_f32(orc_uniform(o));
+            float dev = rho * (hi - mu);
+            hi = fmaf(sigma_z, eps, mu + dev);
+            h[i] = hi;
+        }
+        float eta = yt * exp2f(hi * -0.5f * kRefLog2e);
+        float l;
+        if (nu_obs > 0.0f) {
+            float ta = eta * eta / nu_obs + 1.0f;
+            l = fmaf(-0.5f, hi, c_obs + (-(nu_obs + 1.0f) * 0.5f) * (log2f(ta) * kRefLn2));
+        } else {
+            l = fmaf(-0.5f, hi, fmaf(-0.5f, eta * eta, -0.918938517570496f));
+        }
+        if (acc) l += lwp[i];
+        lw[i] = l;
+        if (l > mx) mx = l;
+    }
+    return mx;
+}
+
+/* w = normalised weights; out: h_mean, loglik (the reference BpfResult), sum of w^2 */
+static void ref_normalise(int N, const float* lw, float mx, const float* h, float* w,
+                          float* hmean, float* loglik, float* sumsq) {
+    float sw = 0.0f;
+#pragma omp parallel for schedule(static) reduction(+ : sw)
+    for (int i = 0; i < N; ++i) { w[i] = exp2f((lw[i] - mx) * kRefLog2e); sw += w[i]; }
+    const float inv = 1.0f / sw;
+    float hest = 0.0f, sw2 = 0.0f;
+#pragma omp parallel for schedule(static) reduction(+ : hest, sw2)
+    for (int i = 0; i < N; ++i) { w[i] *= inv; hest += w[i] * h[i]; sw2 += w[i] * w[i]; }
+    float r = sw / (float)N;
+    if (r < 7.27150555e-31f) r = 7.27150555e-31f;
+    *hmean = hest;
+    *loglik = log2f(r) * kRefLn2 + mx;
+    *sumsq = sw2;
+}
+
+/* FP32 inclusive scan of w into cdf (chunked over threads; part holds nchunk+1
+ * floats), then anc[i] = lower bound of u + i/N (wrapped below 1) in cdf. */
+static void ref_resample(int N, const float* w, float* cdf, float* part, float u, int32_t* anc) {
+#pragma omp parallel
+    {
+        int tid = 0, nt = 1;
+#ifdef _OPENMP
+        tid = omp_get_thread_num(); nt = omp_get_num_threads();
+#endif
+        int a = (int)((long long)N * tid / nt), b = (int)((long long)N * (tid + 1) / nt);
+        float acc2 = 0.0f;
+        for (int i = a; i < b; ++i) { acc2 += w[i]; cdf[i] = acc2; }
+        part[tid + 1] = acc2;
+#pragma omp barrier
+#pragma omp single
+        {
+            part[0] = 0.0f;
+            for (int k = 1; k <= nt; ++k) part[k] += part[k - 1];
+        }
+        float off = part[tid];
+        for (int i = a; i < b; ++i) cdf[i] += off;
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N; ++i) {
+        float target = (float)i / (float)N + u;
+        if (target >= 1.0f) target -= 1.0f;
+        int lo = 0, hi = N - 1;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (cdf[mid] < target) lo = mid + 1; else hi = mid;
+        }
+        anc[i] = lo;
+    }
+}
+
+/* bpf_init_rng + bpf_init_particles (PTX :74-91, :103-218; std_stat as
+ * gpu_bpf_ptx_full.cu:430): rng [state, inc] after draw 0, h = mu + std_stat z_0 */
+static void ref_init(int N, int seed, float rho, float sigma_z, float mu, uint64_t* rng, float* h) {
+    const float std_stat = sqrtf((sigma_z * sigma_z) / fmaxf(1.0f - rho * rho, 1e-6f));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N; ++i) {
+        uint64_t s, inc;
+        orc_pcg32_init(seed, (uint32_t)i, &s, &inc);
+        uint32_t o = orc_pcg32_output(s);
+        s = s * PCG_A + inc;
+        h[i] = fmaf(std_stat, acklam_f32(orc_uniform(o)), mu);
+        rng[2 * (size_t)i] = s;
+        rng[2 * (size_t)i + 1] = inc;
+    }
+}
+
+static int ref_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/*
  * hmean/loglik receive the reference BpfResult of every tick.
  */
 int orc_ref_run(int N, float rho, float sigma_z, float mu, float nu_obs, int seed, float ess_threshold,
@@ -521,71 +748,21 @@ int orc_ref_run(int N, float rho, float sigma_z, float mu, float nu_obs, int see
     float* lwp = (float*)malloc(sizeof(float) * N);
     float* w = (float*)malloc(sizeof(float) * N);
     float* cdf = (float*)malloc(sizeof(float) * N);
-    int nchunk = 1;
-#ifdef _OPENMP
-    nchunk = omp_get_max_threads();
-#endif
-    float* part = (float*)malloc(sizeof(float) * (nchunk + 1));
-    if (!rng || !h || !h2 || !lw || !lwp || !w || !cdf || !part) {
-        free(rng); free(h); free(h2); free(lw); free(lwp); free(w); free(cdf); free(part);
+    int32_t* anc = (int32_t*)malloc(sizeof(int32_t) * N);
+    float* part = (float*)malloc(sizeof(float) * (ref_max_threads() + 1));
+    if (!rng || !h || !h2 || !lw || !lwp || !w || !cdf || !anc || !part) {
+        free(rng); free(h); free(h2); free(lw); free(lwp); free(w); free(cdf); free(anc); free(part);
         return 2;
     }
     const float c_obs = (nu_obs > 0.0f) ? (float)c_obs_of(nu_obs) : 0.0f;
-    const float std_stat = sqrtf((sigma_z * sigma_z) / fmaxf(1.0f - rho * rho, 1e-6f));
-    /* bpf_init_rng + bpf_init_particles */
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < N; ++i) {
-        uint64_t s, inc;
-        orc_pcg32_init(seed, (uint32_t)i, &s, &inc);
-        uint32_t o = orc_pcg32_output(s);
-        s = s * PCG_A + inc;
-        h[i] = fmaf(std_stat, acklam_f32(orc_uniform(o)), mu);
-        rng[2 * (size_t)i] = s;
-        rng[2 * (size_t)i + 1] = inc;
-    }
+    ref_init(N, seed, rho, sigma_z, mu, rng, h);
     uint64_t host_rng = orc_host_seed(seed);
     int did_resample = 1, count = 0;
-    const float log2e = 1.44269504088896340736f, ln2 = 0.693147180559945309417f;
     for (int t = 0; t < T; ++t) {
-        const float yt = y[t];
-        const int do_prop = t > 0;
-        const int acc = (t > 0) && !did_resample;
-        float mx = -1e30f;
-#pragma omp parallel for schedule(static) reduction(max : mx)
-        for (int i = 0; i < N; ++i) {
-            float hi = h[i];
-            if (do_prop) {
-                uint64_t s = rng[2 * (size_t)i], inc = rng[2 * (size_t)i + 1];
-                uint32_t o = orc_pcg32_output(s);
-                rng[2 * (size_t)i] = s * PCG_A + inc;
-                float eps = acklam_f32(orc_uniform(o));
-                float dev = rho * (hi - mu);
-                hi = fmaf(sigma_z, eps, mu + dev);
-                h[i] = hi;
-            }
-            float eta = yt * exp2f(hi * -0.5f * log2e);
-            float l;
-            if (nu_obs > 0.0f) {
-                float ta = eta * eta / nu_obs + 1.0f;
-                l = fmaf(-0.5f, hi, c_obs + (-(nu_obs + 1.0f) * 0.5f) * (log2f(ta) * ln2));
-            } else {
-                l = fmaf(-0.5f, hi, fmaf(-0.5f, eta * eta, -0.918938517570496f));
-            }
-            if (acc) l += lwp[i];
-            lw[i] = l;
-            if (l > mx) mx = l;
-        }
-        float sw = 0.0f;
-#pragma omp parallel for schedule(static) reduction(+ : sw)
-        for (int i = 0; i < N; ++i) { w[i] = exp2f((lw[i] - mx) * log2e); sw += w[i]; }
-        const float inv = 1.0f / sw;
-        float hest = 0.0f, sw2 = 0.0f;
-#pragma omp parallel for schedule(static) reduction(+ : hest, sw2)
-        for (int i = 0; i < N; ++i) { w[i] *= inv; hest += w[i] * h[i]; sw2 += w[i] * w[i]; }
-        float r = sw / (float)N;
-        if (r < 7.27150555e-31f) r = 7.27150555e-31f;
-        hmean[t] = hest;
-        loglik[t] = log2f(r) * ln2 + mx;
+        const float mx = ref_propagate_weight(N, rng, h, lw, lwp, t > 0, (t > 0) && !did_resample,
+                                              rho, sigma_z, mu, nu_obs, c_obs, y[t]);
+        float sw2;
+        ref_normalise(N, lw, mx, h, w, &hmean[t], &loglik[t], &sw2);
         int do_res = 1;
         if (ess_threshold > 0.0f) {
             float essv = 1.0f / fmaxf(sw2, 1e-30f);
@@ -594,38 +771,10 @@ int orc_ref_run(int N, float rho, float sigma_z, float mu, float nu_obs, int see
         if (do_res) {
             did_resample = 1;
             ++count;
-            /* inclusive scan (chunked, parallel) */
-#pragma omp parallel
-            {
-                int tid = 0, nt = 1;
-#ifdef _OPENMP
-                tid = omp_get_thread_num(); nt = omp_get_num_threads();
-#endif
-                int a = (int)((long long)N * tid / nt), b = (int)((long long)N * (tid + 1) / nt);
-                float acc2 = 0.0f;
-                for (int i = a; i < b; ++i) { acc2 += w[i]; cdf[i] = acc2; }
-                part[tid + 1] = acc2;
-#pragma omp barrier
-#pragma omp single
-                {
-                    part[0] = 0.0f;
-                    for (int k = 1; k <= nt; ++k) part[k] += part[k - 1];
-                }
-                float off = part[tid];
-                for (int i = a; i < b; ++i) cdf[i] += off;
-            }
             const float u = (float)(orc_host_pcg32(&host_rng) >> 9) * (1.0f / 8388608.0f) / (float)N;
+            ref_resample(N, w, cdf, part, u, anc);
 #pragma omp parallel for schedule(static)
-            for (int i = 0; i < N; ++i) {
-                float target = (float)i / (float)N + u;
-                if (target >= 1.0f) target -= 1.0f;
-                int lo = 0, hi = N - 1;
-                while (lo < hi) {
-                    int mid = (lo + hi) >> 1;
-                    if (cdf[mid] < target) lo = mid + 1; else hi = mid;
-                }
-                h2[i] = h[lo];
-            }
+            for (int i = 0; i < N; ++i) h2[i] = h[anc[i]];
             float* tmp = h; h = h2; h2 = tmp;
         } else {
             did_resample = 0;
@@ -633,7 +782,46 @@ int orc_ref_run(int N, float rho, float sigma_z, float mu, float nu_obs, int see
         }
     }
     if (resample_count) *resample_count = count;
-    free(rng); free(h); free(h2); free(lw); free(lwp); free(w); free(cdf); free(part);
+    free(rng); free(h); free(h2); free(lw); free(lwp); free(w); free(cdf); free(anc); free(part);
+    return 0;
+}
+
+/* The reference's initial state: PCG32 [state, inc] x N after draw 0 and the initial particles. */
+int orc_ref_init(int N, int seed, float rho, float sigma_z, float mu, uint64_t* rng, float* h) {
+    if (N <= 0) return 1;
+    ref_init(N, seed, rho, sigma_z, mu, rng, h);
+    return 0;
+}
+
+/*
+ * One reference tick on given particles, for a lock-step comparison with the
+ * reference run on a GPU: rng [state, inc] x N is advanced in place when
+ * propagate != 0, h holds the previous particles on entry and the propagated
+ * ones on return, w the normalised weights; out3 = h_mean, loglik, 1/sum(w^2).
+ * No carried weights (the always-resample schedule).
+ */
+int orc_ref_tick(int N, uint64_t* rng, float* h, float rho, float sigma_z, float mu, float nu_obs, float y,
+                 int propagate, float* w, float* out3) {
+    if (N <= 0) return 1;
+    float* lw = (float*)malloc(sizeof(float) * N);
+    if (!lw) return 2;
+    const float c_obs = (nu_obs > 0.0f) ? (float)c_obs_of(nu_obs) : 0.0f;
+    const float mx = ref_propagate_weight(N, rng, h, lw, NULL, propagate, 0, rho, sigma_z, mu, nu_obs, c_obs, y);
+    float sw2;
+    ref_normalise(N, lw, mx, h, w, &out3[0], &out3[1], &sw2);
+    out3[2] = 1.0f / fmaxf(sw2, 1e-30f);
+    free(lw);
+    return 0;
+}
+
+/* The reference's systematic resampling of normalised FP32 weights with offset u = U/N. */
+int orc_ref_resample(int N, const float* w, float u, int32_t* anc) {
+    if (N <= 0) return 1;
+    float* cdf = (float*)malloc(sizeof(float) * N);
+    float* part = (float*)malloc(sizeof(float) * (ref_max_threads() + 1));
+    if (!cdf || !part) { free(cdf); free(part); return 2; }
+    ref_resample(N, w, cdf, part, u, anc);
+    free(cdf); free(part);
     return 0;
 }
 

@@ -75,6 +75,16 @@ def lib(native: bool = False) -> C.CDLL:
     L.orc_ref_run.restype = C.c_int
     L.orc_ref_run.argtypes = [C.c_int, f32, f32, f32, f32, C.c_int, f32, C.c_void_p, C.c_int,
                               C.c_void_p, C.c_void_p, C.c_int, P(C.c_int)]
+    L.orc_apf_f64.restype = C.c_int
+    L.orc_apf_f64.argtypes = [P(OrcConfig), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_ref_init.restype = C.c_int
+    L.orc_ref_init.argtypes = [C.c_int, C.c_int, f32, f32, f32, C.c_void_p, C.c_void_p]
+    L.orc_ref_tick.restype = C.c_int
+    L.orc_ref_tick.argtypes = [C.c_int, C.c_void_p, C.c_void_p, f32, f32, f32, f32, f32, C.c_int, C.c_void_p,
+                               C.c_void_p]
+    L.orc_ref_resample.restype = C.c_int
+    L.orc_ref_resample.argtypes = [C.c_int, C.c_void_p, f32, C.c_void_p]
     L.orc_num_threads.restype = C.c_int; L.orc_num_threads.argtypes = []
     L.orc_tstate_scale.restype = f64
     L.orc_tstate_scale.argtypes = [C.c_int, u32, C.c_int, C.c_int, f64]
@@ -126,6 +136,24 @@ def filter_f64(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.0, nu_
     return out
 
 
+def apf_f64(n_particles, rho, sigma_z, mu, y, seed=42, nu_obs=0.0, nu_state=0.0, anc1=None, anc2=None):
+    """FP64 auxiliary particle filter; anc1 / anc2 [T][N] replay the two stages' ancestors.
+    Returns dict of per-tick arrays: dll (APF increment), ll_ref (the reference's log mean
+    second-stage weight), hmean, ess."""
+    L = lib()
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    T = y.shape[0]
+    cfg = OrcConfig(int(n_particles), rho, sigma_z, mu, nu_obs, int(seed), 0.0, nu_state)
+    out = {k: np.zeros(T, dtype=np.float64) for k in ("dll", "ll_ref", "hmean", "ess")}
+    a1 = None if anc1 is None else np.ascontiguousarray(anc1, dtype=np.int32)
+    a2 = None if anc2 is None else np.ascontiguousarray(anc2, dtype=np.int32)
+    rc = L.orc_apf_f64(C.byref(cfg), _ptr(y), T, _ptr(a1), _ptr(a2), _ptr(out["dll"]), _ptr(out["ll_ref"]),
+                       _ptr(out["hmean"]), _ptr(out["ess"]))
+    if rc != 0:
+        raise RuntimeError(f"orc_apf_f64 failed ({rc})")
+    return out
+
+
 def resample_fixed(w, tile_exp, u23):
     L = lib()
     w = np.ascontiguousarray(w, dtype=np.float32)
@@ -150,6 +178,46 @@ def ref_run(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.5, nu_obs
     if rc != 0:
         raise RuntimeError(f"orc_ref_run failed ({rc})")
     return hm, ll, cnt.value
+
+
+def ref_init(n_particles, rho, sigma_z, mu, seed=42):
+    """The reference's initial state: (rng uint64 [N, 2] after draw 0, h0 float32 [N])."""
+    L = lib()
+    rng = np.zeros((int(n_particles), 2), dtype=np.uint64)
+    h = np.zeros(int(n_particles), dtype=np.float32)
+    rc = L.orc_ref_init(int(n_particles), int(seed), rho, sigma_z, mu, _ptr(rng), _ptr(h))
+    if rc != 0:
+        raise RuntimeError(f"orc_ref_init failed ({rc})")
+    return rng, h
+
+
+def ref_tick(rng, h, rho, sigma_z, mu, y, propagate=True, nu_obs=0.0):
+    """One reference tick on given particles (FP32 restatement, stage by stage).
+
+    rng: uint64 [N, 2] (state, inc), advanced in place when propagating; h: float32 [N] previous
+    particles. Returns (propagated h, normalised w, h_mean, loglik, ess)."""
+    L = lib()
+    assert rng.dtype == np.uint64 and rng.flags.c_contiguous
+    h = np.array(h, dtype=np.float32, copy=True)
+    N = h.shape[0]
+    w = np.zeros(N, dtype=np.float32)
+    out = np.zeros(3, dtype=np.float32)
+    rc = L.orc_ref_tick(N, _ptr(rng), _ptr(h), rho, sigma_z, mu, nu_obs, float(y), int(bool(propagate)), _ptr(w),
+                        _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"orc_ref_tick failed ({rc})")
+    return h, w, float(out[0]), float(out[1]), float(out[2])
+
+
+def ref_resample(w, u):
+    """The reference's systematic resampling (FP32 CDF, lower-bound search) with offset u = U/N."""
+    L = lib()
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    anc = np.zeros(w.shape[0], dtype=np.int32)
+    rc = L.orc_ref_resample(int(w.shape[0]), _ptr(w), float(u), _ptr(anc))
+    if rc != 0:
+        raise RuntimeError(f"orc_ref_resample failed ({rc})")
+    return anc
 
 
 def grad_f64(n_particles, mu, rho, sigma_z, y, anc, seed=42, nu_obs=0.0, mode=1, nu_state=0.0):

@@ -1,0 +1,111 @@
+"""ctypes face of the reference's own GPU filter built into oracle/_ref/ by oracle/build_ref.py.
+
+TEST INFRASTRUCTURE ONLY: used by tests/ to pin the oracle and the CUDA path
+against the reference itself run on the same GPU, and by bench.py's reference
+arm to time it. The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import build_ref
+
+_LIB = None
+
+
+def available() -> bool:
+    return build_ref.available()
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not build_ref.available():
+            raise RuntimeError("oracle/_ref is not built (the reference tree was absent at build time)")
+        L = C.CDLL(build_ref.LIB)
+        vp, f32, i32, f64 = C.c_void_p, C.c_float, C.c_int, C.c_double
+        L.refgpu_create.restype = vp
+        L.refgpu_create.argtypes = [i32, f32, f32, f32, f32, f32, i32]
+        L.refgpu_destroy.argtypes = [vp]
+        L.refgpu_set_ess.argtypes = [vp, f32]
+        L.refgpu_resample_count.restype = i32
+        L.refgpu_resample_count.argtypes = [vp]
+        L.refgpu_timestep.restype = i32
+        L.refgpu_timestep.argtypes = [vp]
+        L.refgpu_run.restype = i32
+        L.refgpu_run.argtypes = [vp, vp, i32, vp, vp]
+        L.refgpu_time_run.restype = f64
+        L.refgpu_time_run.argtypes = [vp, vp, i32, vp]
+        for name in ("refgpu_copy_rng", "refgpu_copy_h", "refgpu_copy_h2", "refgpu_copy_w"):
+            getattr(L, name).restype = i32
+            getattr(L, name).argtypes = [vp, vp, i32]
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class RefGpuFilter:
+    """gpu_bpf_create / gpu_bpf_step / gpu_bpf_destroy of the reference's PTX edition."""
+
+    def __init__(self, n, rho, sigma_z, mu, nu_state=0.0, nu_obs=0.0, seed=42, ess_threshold=0.5):
+        self.L = lib()
+        self.n = int(n)
+        self.s = self.L.refgpu_create(self.n, rho, sigma_z, mu, nu_state, nu_obs, int(seed))
+        if not self.s:
+            raise RuntimeError("reference gpu_bpf_create failed")
+        self.L.refgpu_set_ess(self.s, float(ess_threshold))
+
+    def run(self, y):
+        """One gpu_bpf_step per observation: (h_mean[T], log_lik[T]) as float32."""
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        hm = np.zeros(y.shape[0], dtype=np.float32)
+        ll = np.zeros(y.shape[0], dtype=np.float32)
+        rc = self.L.refgpu_run(self.s, _p(y), int(y.shape[0]), _p(hm), _p(ll))
+        if rc != 0:
+            raise RuntimeError(f"reference tick loop failed (CUDA error {rc})")
+        return hm, ll
+
+    def time_run(self, y):
+        """gpu_bpf_step_async over y, one result at the end: (milliseconds, h_mean, log_lik)."""
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        last = np.zeros(2, dtype=np.float32)
+        ms = self.L.refgpu_time_run(self.s, _p(y), int(y.shape[0]), _p(last))
+        return ms, float(last[0]), float(last[1])
+
+    def _copy(self, name, dtype, count):
+        out = np.zeros(count, dtype=dtype)
+        rc = getattr(self.L, name)(self.s, _p(out), self.n)
+        if rc != 0:
+            raise RuntimeError(f"{name} failed (CUDA error {rc})")
+        return out
+
+    def rng(self):
+        """PCG32 [state, inc] per particle, shape (N, 2) uint64."""
+        return self._copy("refgpu_copy_rng", np.uint64, 2 * self.n).reshape(self.n, 2)
+
+    def particles(self):
+        return self._copy("refgpu_copy_h", np.float32, self.n)
+
+    def pre_resample_particles(self):
+        return self._copy("refgpu_copy_h2", np.float32, self.n)
+
+    def weights(self):
+        return self._copy("refgpu_copy_w", np.float32, self.n)
+
+    @property
+    def resample_count(self):
+        return self.L.refgpu_resample_count(self.s)
+
+    @property
+    def timestep(self):
+        return self.L.refgpu_timestep(self.s)
+
+    def close(self):
+        if self.s:
+            self.L.refgpu_destroy(self.s)
+            self.s = None
