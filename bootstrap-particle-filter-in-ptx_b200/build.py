@@ -16,7 +16,7 @@ OUT = os.path.join(HERE, "gpubpf", "libgpubpf.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["bpf_plain.cu", "bpf_api.cu", "bpf_static.cu", "bpf_batch.cu", "bpf_batch_api.cu", "bpf_grad.cu",
-           "bpf_grad_api.cu", "bpf_imm.cu", "bpf_smc2.cu"]
+           "bpf_grad_api.cu", "bpf_imm.cu", "bpf_smc2.cu", "bpf_apf.cu"]
 HEADERS = ["bpf_common.cuh", "bpf_plain.cuh", "bpf_block.cuh", "bpf_batch.cuh", "bpf_grad.cuh",
            "bpf_batch_internal.cuh"]
 

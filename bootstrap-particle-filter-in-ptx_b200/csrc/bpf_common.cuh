@@ -223,9 +223,11 @@ __device__ __forceinline__ float state_noise(const PcgTick& pc, uint32_t i, int 
 
 // OU transition with the reference's operation order (PTX :406-411):
 //   dev = rho*(h-mu); h = mu + dev; h = fma(sigma, eps, h)
+__device__ __forceinline__ float propagate_mean(float h, float mu, float rho) {
+  return __fadd_rn(mu, __fmul_rn(rho, __fsub_rn(h, mu)));
+}
 __device__ __forceinline__ float propagate(float h, float mu, float rho, float sigma, float eps) {
-  const float dev = __fmul_rn(rho, __fsub_rn(h, mu));
-  return fmaf(sigma, eps, __fadd_rn(mu, dev));
+  return fmaf(sigma, eps, propagate_mean(h, mu, rho));
 }
 
 // ---------------------------------------------------------------------------

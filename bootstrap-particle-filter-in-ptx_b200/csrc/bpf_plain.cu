@@ -68,7 +68,13 @@ constexpr int kStWords = (int)(sizeof(DevState) / 8);
 // ---------------------------------------------------------------------------
 // Pass 1
 // ---------------------------------------------------------------------------
-template <bool TSTATE, bool LEARN>
+// APF = 0: bootstrap tick; 1 / 2: the two stages of an auxiliary-particle-filter
+// tick (gpu_bpf_ptx_full.cu:990-1047): stage 1 weights each particle by
+// p(y | m), m = mu + rho (h - mu), and leaves the particles in place; stage 2
+// runs on the particles resampled by those weights, propagates them
+// (h = m + sigma eps, the same operations as a bootstrap tick) and weights them
+// by p(y | h) / p(y | m).
+template <bool TSTATE, bool LEARN, int APF>
 __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
   __shared__ float s_max[kThreads / 32];
   __shared__ double s_red[3][kThreads / 32];
@@ -79,7 +85,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   const int k = blockIdx.x;
   const DevState* st = p.st;
   const int tick = st->tick;
-  const bool carry = st->resampled_prev == 0;
+  const bool carry = APF == 0 && st->resampled_prev == 0;
   const int nM_prev = st->nM_prev;
   const PcgTick c = pcg_tick_consts(st->seed, st->At, st->Bt);
   float* hb = st->cur ? p.h1 : p.h0;
@@ -123,20 +129,34 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     for (int e = 0; e < 4; ++e) {
       float h = hh[e];
       if (LEARN) hpv[4 * r + e] = h;
-      if (tick > 0) {
-        float z = icdf_normal(pcg_uniform(pcg_output(s)));
-        if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
-        h = propagate(h, a.mu, a.rho, a.sigma, z);
+      float xx;
+      if (APF == 0) {
+        if (tick > 0) {
+          float z = icdf_normal(pcg_uniform(pcg_output(s)));
+          if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
+          h = propagate(h, a.mu, a.rho, a.sigma, z);
+        }
+        xx = gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e);
+      } else {
+        const float m = propagate_mean(h, a.mu, a.rho);
+        const float lm = gauss ? obs_log2pdf_gauss(y2, m) : __fmul_rn(obs_logpdf(obs, m), kLog2e);
+        if (APF == 1) {
+          xx = lm;
+        } else {
+          float z = icdf_normal(pcg_uniform(pcg_output(s)));
+          if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
+          h = fmaf(a.sigma, z, m);
+          xx = (gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e)) - lm;
+        }
       }
       s += step2;
-      float xx = gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e);
       if (carry) xx += lg2_approx(wp[e]) + carry_off;
       if (i0 + e >= p.N) xx = -INFINITY;
       hh[e] = h;
       x[4 * r + e] = xx;
       hv[4 * r + e] = h;
     }
-    *reinterpret_cast<float4*>(hb + i0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
+    if (APF != 1) *reinterpret_cast<float4*>(hb + i0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
   }
 
   // tile max -> power-of-two exponent n_k (all tile weights <= 1)
@@ -343,20 +363,34 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
       hm = sh.res[2];
       resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
     }
-    const double ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
+    // Auxiliary particle filter: the first stage leaves log mean v (its weights)
+    // in ll_ref for the second, whose increment is log mean v + log mean w; the
+    // record's loglik_ref is log mean w, the value the reference reports
+    // (gpu_bpf_ptx_full.cu:1155-1164). The tick advances after the second stage.
+    double rec_dll = dll, ll_ref;
+    if (a.apf == 1) {
+      ll_ref = dll;
+    } else if (a.apf == 2) {
+      rec_dll = st->ll_ref + dll;
+      ll_ref = dll;
+    } else {
+      ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
+    }
     st->ll_ref = ll_ref;
-    st->ll_total += dll;
+    if (a.apf != 1) st->ll_total += rec_dll;
     if (a.aux) *a.aux = degenerate ? make_float2(0.0f, __int_as_float(0))
                                    : make_float2((float)(1.0 / tS), __int_as_float(nM));
     if (a.rec) {
       BpfTickRecord r;
-      r.dloglik = dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
+      r.dloglik = rec_dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
       r.h_mean = (float)hm; r.ess = (float)ess; r.resampled = resample; r.tick = tick;
       *a.rec = r;
     }
-    st->At = st->At * kPcgMult;            // next tick's jump constants
-    st->Bt = st->Bt * kPcgMult + 1ull;
-    st->tick = tick + 1;
+    if (a.apf != 1) {
+      st->At = st->At * kPcgMult;          // next tick's jump constants
+      st->Bt = st->Bt * kPcgMult + 1ull;
+      st->tick = tick + 1;
+    }
     st->do_resample = resample;
     st->nM = nM;
     if (resample) {
@@ -721,12 +755,17 @@ int pass2_grid_size(int device) {
 
 cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
   const dim3 grid(p.G), block(kThreads);
-  if (a.learn && p.rec2) {
-    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, true>, grid, block, 0, s, pdl, p, a);
-    return launch_ex(pass1_kernel<false, true>, grid, block, 0, s, pdl, p, a);
+  if (a.apf == 1) return launch_ex(pass1_kernel<false, false, 1>, grid, block, 0, s, pdl, p, a);
+  if (a.apf == 2) {
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 2>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, false, 2>, grid, block, 0, s, pdl, p, a);
   }
-  if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false>, grid, block, 0, s, pdl, p, a);
-  return launch_ex(pass1_kernel<false, false>, grid, block, 0, s, pdl, p, a);
+  if (a.learn && p.rec2) {
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, true, 0>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, true, 0>, grid, block, 0, s, pdl, p, a);
+  }
+  if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 0>, grid, block, 0, s, pdl, p, a);
+  return launch_ex(pass1_kernel<false, false, 0>, grid, block, 0, s, pdl, p, a);
 }
 cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
   return launch_ex(plan_kernel, dim3(1), dim3(kPlanThreads), plan_smem_bytes(p.G), s, pdl, p, a);

@@ -67,6 +67,9 @@ struct TickArgs {
   int nu_int;                // Student-t state noise: round(nu_state) degrees of freedom, 0 = Gaussian
   float nu_state;            // Student-t state noise scale parameter
   int learn;                 // accumulate the online-learning score sums of this tick (needs p.rec2)
+  int apf;                   // auxiliary particle filter stage: 0 = bootstrap tick, 1 = first stage
+                             // (weights p(y | mu + rho (h - mu)), particles unchanged, tick not
+                             // advanced), 2 = second stage (propagate, weights p(y|h) / p(y|m))
   // gradient tape (all null outside a taped run)
   float* ckpt;               // copy of the particles pass 1 reads this tick (G*4096 floats) or null
   int32_t* csr;              // on resampling ticks: first child slot of every parent (N ints) or null

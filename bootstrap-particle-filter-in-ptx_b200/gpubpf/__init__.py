@@ -10,6 +10,7 @@ from .filter import GpuBpf, debug_normals, debug_pcg32, run_rmse  # noqa: F401
 from .batch import GpuBpfBatch  # noqa: F401
 from .grad import BpfLoglik, GradTape, ancestors_from_children, bpf_loglik  # noqa: F401
 from .imm import Imm, build_grid  # noqa: F401
+from .apf import GpuApf, apf_run_rmse  # noqa: F401
 from .smc2 import Smc2  # noqa: F401
 from . import configs, dgp  # noqa: F401
 

@@ -81,7 +81,15 @@ class BpfSmc2Prior(C.Structure):
                 ("sigma_lo", C.c_float), ("sigma_hi", C.c_float)]
 
 
+class GpuApfState(C.Structure):
+    _fields_ = [("n_particles", C.c_int),
+                ("rho", C.c_float), ("sigma_z", C.c_float), ("mu", C.c_float),
+                ("nu_state", C.c_float), ("nu_obs", C.c_float),
+                ("timestep", C.c_int), ("stream", C.c_void_p), ("impl", C.c_void_p)]
+
+
 P_STATE = C.POINTER(GpuBpfState)
+P_APF = C.POINTER(GpuApfState)
 P_IMM = C.POINTER(GpuImmState)
 _f = C.c_float
 _i = C.c_int
@@ -148,6 +156,17 @@ SIGNATURES = {
     "gpu_bpf_batch_tick": (_i, [_vp]),
     "gpu_bpf_batch_loglik_device": (_vp, [_vp]),
     "gpu_bpf_batch_grad_tape_bytes": (C.c_size_t, [_vp, _i]),
+    # APF (gpu_bpf/gpu_bpf.cuh:114-126)
+    "gpu_apf_create": (P_APF, [_i, _f, _f, _f, _f, _f, _i]),
+    "gpu_apf_destroy": (None, [P_APF]),
+    "gpu_apf_step": (BpfResult, [P_APF, _f]),
+    "gpu_apf_run_rmse": (_d, [C.POINTER(_d), C.POINTER(_d), _i, _i, _f, _f, _f, _f, _f, _i]),
+    "gpu_apf_step_many": (_i, [P_APF, C.POINTER(_f), _i, C.POINTER(BpfResult), C.POINTER(BpfTickRecord)]),
+    "gpu_apf_get_record": (_i, [P_APF, C.POINTER(BpfTickRecord)]),
+    "gpu_apf_get_loglik_total": (_d, [P_APF]),
+    "gpu_apf_get_particles": (_i, [P_APF, C.POINTER(_f)]),
+    "gpu_apf_record_ancestors": (_i, [P_APF, _i]),
+    "gpu_apf_get_ancestors": (_i, [P_APF, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     # IMM (gpu_bpf/gpu_bpf.cuh:131-164)
     "gpu_imm_create": (P_IMM, [C.POINTER(ImmModelParams), _i, _i, C.POINTER(_f), _i]),
     "gpu_imm_step": (ImmResult, [P_IMM, _f]),

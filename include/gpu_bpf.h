@@ -238,6 +238,49 @@ int gpu_bpf_run_static(int n_particles, float rho, float sigma_z, float mu, floa
                        float ess_threshold, const float* y_dev, int n_ticks, BpfTickRecord* rec_dev,
                        void* stream);
 
+/* ---- APF: auxiliary particle filter (gpu_bpf/gpu_bpf.cuh:114-126) ---------------
+ * Behaviour of gpu_bpf/gpu_bpf_ptx_full.cu:990-1190. Tick 0 is a bootstrap tick; every later
+ * tick resamples twice: by the first-stage weights v_i = p(y_t | mu + rho (h_i - mu)), then,
+ * after propagating the resampled particles, by w_i = p(y_t | h_i) / p(y_t | m_i). The reference
+ * public struct (gpu_bpf_full.cuh:314-337) holds device pointers and cuRAND states; this one keeps
+ * the parameter fields and puts the buffers behind `impl`. The state noise is drawn from the
+ * per-slot PCG32 streams (draw t of slot i at tick t, as the bootstrap filter's) instead of
+ * cuRAND XORWOW; the resampling uniforms come from the reference's host-formula stream, two per
+ * tick after tick 0. rho / sigma_z / mu may change between ticks. */
+typedef struct {
+    int    n_particles;
+    float  rho, sigma_z, mu, nu_state, nu_obs;
+    int    timestep;        /* refreshed whenever results are read back */
+    void*  stream;          /* cudaStream_t owned by the filter */
+    void*  impl;            /* opaque */
+} GpuApfState;
+
+/* gpu_bpf/gpu_bpf.cuh:119-120 (gpu_bpf_ptx_full.cu:1050-1082). NULL on failure (gpu_bpf_last_error()). */
+GpuApfState* gpu_apf_create(int n_particles, float rho, float sigma_z, float mu,
+                            float nu_state, float nu_obs, int seed);
+/* gpu_bpf/gpu_bpf.cuh:121 (gpu_bpf_ptx_full.cu:1084-1093). NULL is a no-op. */
+void gpu_apf_destroy(GpuApfState* state);
+/* gpu_bpf/gpu_bpf.cuh:122 (gpu_bpf_ptx_full.cu:1102-1175): one tick, synchronous. log_lik is the
+ * reference's value, log mean of the second-stage weights; the APF estimate of
+ * log p(y_t | y_{1:t-1}) (adds log mean of the first-stage weights) is BpfTickRecord.dloglik of
+ * gpu_apf_get_record. {NaN, NaN} on error. */
+BpfResult gpu_apf_step(GpuApfState* state, float y_t);
+/* gpu_bpf/gpu_bpf.cuh:124-126 (gpu_bpf_ptx_full.cu:1177-1190): RMSE of h_mean vs true_h after the
+ * first 100 ticks. NaN on error. */
+double gpu_apf_run_rmse(const double* returns, const double* true_h, int n_ticks,
+                        int n_particles, float rho, float sigma_z, float mu,
+                        float nu_state, float nu_obs, int seed);
+/* Additions: n_ticks ticks in one call (CUDA graphs of 64 ticks after tick 0), results and/or
+ * records per tick (either may be NULL); the last tick's record; the FP64 running sum of the
+ * APF increments; the particles; the ancestors of both resampling stages of the last tick
+ * (after gpu_apf_record_ancestors(state, 1); tick 0 writes only the second). */
+int    gpu_apf_step_many(GpuApfState* state, const float* y, int n_ticks, BpfResult* out, BpfTickRecord* rec);
+int    gpu_apf_get_record(GpuApfState* state, BpfTickRecord* out);
+double gpu_apf_get_loglik_total(GpuApfState* state);
+int    gpu_apf_get_particles(GpuApfState* state, float* h_out);
+int    gpu_apf_record_ancestors(GpuApfState* state, int enable);
+int    gpu_apf_get_ancestors(GpuApfState* state, int32_t* anc_first, int32_t* anc_second);
+
 /* ---- IMM: interacting multiple model (gpu_bpf/gpu_bpf.cuh:131-164) ----------
  * K SV models stepped on the same observations; model probabilities follow a Markov switching
  * prior (transition matrix T[j*K + k] = P(j -> k), row-major; NULL = 0.95 stay, the rest spread

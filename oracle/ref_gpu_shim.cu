@@ -111,4 +111,22 @@ int refgpu_copy_w(void* sv, float* out, int n) {
   return (int)cudaMemcpy(out, s->d_w, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
 }
 
+// The reference's auxiliary particle filter (gpu_bpf_ptx_full.cu:1050-1175;
+// cuRAND state noise, so comparisons with it are statistical).
+void* refgpu_apf_create(int n, float rho, float sigma_z, float mu, float nu_state, float nu_obs, int seed) {
+  return gpu_apf_create(n, rho, sigma_z, mu, nu_state, nu_obs, seed);
+}
+
+void refgpu_apf_destroy(void* s) { gpu_apf_destroy(static_cast<GpuApfState*>(s)); }
+
+int refgpu_apf_run(void* sv, const float* y, int T, float* h_mean, float* log_lik) {
+  GpuApfState* s = static_cast<GpuApfState*>(sv);
+  for (int t = 0; t < T; ++t) {
+    const BpfResult r = gpu_apf_step(s, y[t]);
+    h_mean[t] = r.h_mean;
+    log_lik[t] = r.log_lik;
+  }
+  return (int)cudaGetLastError();
+}
+
 }  // extern "C"

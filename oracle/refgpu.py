@@ -38,6 +38,11 @@ def lib() -> C.CDLL:
         L.refgpu_run.argtypes = [vp, vp, i32, vp, vp]
         L.refgpu_time_run.restype = f64
         L.refgpu_time_run.argtypes = [vp, vp, i32, vp]
+        L.refgpu_apf_create.restype = vp
+        L.refgpu_apf_create.argtypes = [i32, f32, f32, f32, f32, f32, i32]
+        L.refgpu_apf_destroy.argtypes = [vp]
+        L.refgpu_apf_run.restype = i32
+        L.refgpu_apf_run.argtypes = [vp, vp, i32, vp, vp]
         for name in ("refgpu_copy_rng", "refgpu_copy_h", "refgpu_copy_h2", "refgpu_copy_w"):
             getattr(L, name).restype = i32
             getattr(L, name).argtypes = [vp, vp, i32]
@@ -109,3 +114,21 @@ class RefGpuFilter:
         if self.s:
             self.L.refgpu_destroy(self.s)
             self.s = None
+
+
+def apf_run(n, rho, sigma_z, mu, y, nu_state=0.0, nu_obs=0.0, seed=42):
+    """The reference's gpu_apf_create / gpu_apf_step loop: (h_mean[T], log_lik[T]) float32."""
+    L = lib()
+    s = L.refgpu_apf_create(int(n), rho, sigma_z, mu, nu_state, nu_obs, int(seed))
+    if not s:
+        raise RuntimeError("reference gpu_apf_create failed")
+    try:
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        hm = np.zeros(y.shape[0], dtype=np.float32)
+        ll = np.zeros(y.shape[0], dtype=np.float32)
+        rc = L.refgpu_apf_run(s, _p(y), int(y.shape[0]), _p(hm), _p(ll))
+        if rc != 0:
+            raise RuntimeError(f"reference APF loop failed (CUDA error {rc})")
+        return hm, ll
+    finally:
+        L.refgpu_apf_destroy(s)

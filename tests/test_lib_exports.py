@@ -17,7 +17,7 @@ HEADER = os.path.join(REPO, "include", "gpu_bpf.h")
 def header_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(gpu_bpf_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(gpu_(?:bpf|imm|apf)_\w+)\s*\(", src)))
 
 
 @pytest.fixture(scope="module")
@@ -129,3 +129,23 @@ def test_imm_host_side(lib):
     assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_ARG
     assert not lib.gpu_imm_create(models, 0, 1000, None, 1)
     assert lib.gpu_imm_get_prob(None, 0) == 0.0
+
+
+def test_apf_host_side(lib):
+    """gpu_apf_create's argument checks, NULL-state calls and the no-GPU failure."""
+    from gpubpf import _lib
+    for args in [(0, 0.97, 0.15, -1.0, 0.0, 0.0, 1), (4096, 1.0, 0.15, -1.0, 0.0, 0.0, 1),
+                 (4096, 0.97, 0.0, -1.0, 0.0, 0.0, 1), (4096, 0.97, 0.15, -1.0, 0.3, 0.0, 1),
+                 (4096, 0.97, 0.15, -1.0, 0.0, -2.0, 1), (4096, 0.97, 0.15, float("nan"), 0.0, 0.0, 1)]:
+        assert not lib.gpu_apf_create(*args)
+        assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_ARG
+    lib.gpu_apf_destroy(None)
+    r = lib.gpu_apf_step(None, 0.1)
+    assert r.h_mean != r.h_mean
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_STATE
+    assert lib.gpu_apf_get_loglik_total(None) != lib.gpu_apf_get_loglik_total(None)    # NaN
+    s = lib.gpu_apf_create(4096, 0.97, 0.15, -1.0, 5.0, 5.0, 42)
+    if s:
+        lib.gpu_apf_destroy(s)
+        pytest.skip("GPU present")
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_NODEVICE
