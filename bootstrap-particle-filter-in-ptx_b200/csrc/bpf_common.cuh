@@ -221,10 +221,13 @@ __device__ __forceinline__ float state_noise(const PcgTick& pc, uint32_t i, int 
   return z;
 }
 
-// OU transition with the reference's operation order (PTX :406-411):
-//   dev = rho*(h-mu); h = mu + dev; h = fma(sigma, eps, h)
+// OU transition h' = mu + rho (h - mu) + sigma eps (PTX :406-411 evaluates
+// mu + rho*(h-mu) in three roundings); here rho h + mu (1 - rho) as one FMA
+// with the constant rounded once, then fma(sigma, eps, .). Every kernel that
+// propagates (pass 1, the batched kernels, the gradient recompute, the APF)
+// goes through these two helpers, so their particles agree bit for bit.
 __device__ __forceinline__ float propagate_mean(float h, float mu, float rho) {
-  return __fadd_rn(mu, __fmul_rn(rho, __fsub_rn(h, mu)));
+  return fmaf(rho, h, __fmul_rn(mu, __fsub_rn(1.0f, rho)));
 }
 __device__ __forceinline__ float propagate(float h, float mu, float rho, float sigma, float eps) {
   return fmaf(sigma, eps, propagate_mean(h, mu, rho));

@@ -77,7 +77,9 @@ constexpr int kStWords = (int)(sizeof(DevState) / 8);
 template <bool TSTATE, bool LEARN, int APF>
 __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
   __shared__ float s_max[kThreads / 32];
-  __shared__ double s_red[3][kThreads / 32];
+  __shared__ float s_part[3][kThreads];
+  __shared__ unsigned long long s_E[kThreads];
+  __shared__ double s_red[3][kThreads / 32];          // online-learning sums
   __shared__ unsigned long long s_redE[kThreads / 32];
 
   griddep_wait();
@@ -103,6 +105,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   }
 
   const int tile0 = k * kTile;
+  const bool full = tile0 + kTile <= p.N;      // every slot of the tile holds a particle
   float4 h4[4], w4[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -151,12 +154,16 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
       }
       s += step2;
       if (carry) xx += lg2_approx(wp[e]) + carry_off;
-      if (i0 + e >= p.N) xx = -INFINITY;
       hh[e] = h;
       x[4 * r + e] = xx;
       hv[4 * r + e] = h;
     }
     if (APF != 1) *reinterpret_cast<float4*>(hb + i0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
+  }
+  if (!full) {                                   // the last tile's padding slots carry no weight
+#pragma unroll
+    for (int idx = 0; idx < kPerThread; ++idx)
+      if (tile0 + 4 * (tid + kThreads * (idx >> 2)) + (idx & 3) >= p.N) x[idx] = -INFINITY;
   }
 
   // tile max -> power-of-two exponent n_k (all tile weights <= 1)
@@ -170,7 +177,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
 #pragma unroll
   for (int w = 1; w < kThreads / 32; ++w) mx = fmaxf(mx, s_max[w]);
   const int nk = (mx == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(mx, -1.0e9f));
-  const float fnk = (float)nk;
+  // an empty tile (every log-weight -inf) gets the frame +inf: 2^(-inf) = 0 for all of it
+  const float fnk = (nk == kNkEmpty) ? INFINITY : (float)nk;
 
   float fS = 0.f, fQ = 0.f, fH = 0.f;
   float lG0 = 0.f, lF0 = 0.f, lG1 = 0.f, lF1 = 0.f;   // online-learning score sums (tile frame)
@@ -182,7 +190,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int idx = 4 * r + e;
-      const float w = (nk == kNkEmpty) ? 0.0f : fminf(ex2_approx(x[idx] - fnk), 1.0f);
+      const float w = fminf(ex2_approx(x[idx] - fnk), 1.0f);
       wv[e] = w;
       fS += w;
       fQ = fmaf(w, w, fQ);
@@ -203,18 +211,27 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     }
     *reinterpret_cast<float4*>(p.w + i0) = make_float4(wv[0], wv[1], wv[2], wv[3]);
   }
-  const double dS = warp_sum_d((double)fS), dQ = warp_sum_d((double)fQ), dH = warp_sum_d((double)fH);
-  E = warp_sum_u64(E);
-  if (lane == 0) { s_red[0][warp] = dS; s_red[1][warp] = dQ; s_red[2][warp] = dH; s_redE[warp] = E; }
+  // tile partials: the per-thread FP32 sums are staged in shared memory and one
+  // warp adds them in FP64 (and the exact masses in u64), in a fixed order
+  s_part[0][tid] = fS; s_part[1][tid] = fQ; s_part[2][tid] = fH; s_E[tid] = E;
   __syncthreads();
-  if (tid == 0) {
+  if (warp == 0) {
     double tS = 0.0, tQ = 0.0, tH = 0.0;
     unsigned long long tE = 0ull;
 #pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) { tS += s_red[0][w]; tQ += s_red[1][w]; tH += s_red[2][w]; tE += s_redE[w]; }
-    p.nexp[k] = nk;
-    p.E[k] = tE;
-    p.rec[k] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
+    for (int w = 0; w < kThreads / 32; ++w) {
+      tS += (double)s_part[0][lane + 32 * w];
+      tQ += (double)s_part[1][lane + 32 * w];
+      tH += (double)s_part[2][lane + 32 * w];
+      tE += s_E[lane + 32 * w];
+    }
+    tS = warp_sum_d(tS); tQ = warp_sum_d(tQ); tH = warp_sum_d(tH);
+    tE = warp_sum_u64(tE);
+    if (lane == 0) {
+      p.nexp[k] = nk;
+      p.E[k] = tE;
+      p.rec[k] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
+    }
   }
   if (LEARN) {
     __syncthreads();                                 // s_red is reused
