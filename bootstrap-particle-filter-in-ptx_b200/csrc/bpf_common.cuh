@@ -120,33 +120,55 @@ constexpr float kLn2   = 0.693147180559945309417f;
 // :166-205), whose central rational cancels to ~3e-4 absolute error near
 // |u-1/2| = 0.47; the uniform clamp and PCG32 draw are kept bit-for-bit.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float icdf_central_poly(float l2) {      // w < 5
+  const float w = fmaf(-kLn2, l2, -2.0f * kLn2 - 2.5f);                // w - 2.5
+  float p = 2.81022636e-08f;
+  p = fmaf(p, w, 3.43273939e-07f);
+  p = fmaf(p, w, -3.5233877e-06f);
+  p = fmaf(p, w, -4.39150654e-06f);
+  p = fmaf(p, w, 0.00021858087f);
+  p = fmaf(p, w, -0.00125372503f);
+  p = fmaf(p, w, -0.00417768164f);
+  p = fmaf(p, w, 0.246640727f);
+  p = fmaf(p, w, 1.50140941f);
+  return p;
+}
+__device__ __forceinline__ float icdf_tail_poly(float l2) {         // w >= 5
+  const float w = sqrt_approx(fmaf(-kLn2, l2, -2.0f * kLn2)) - 3.0f;
+  float p = -0.000200214257f;
+  p = fmaf(p, w, 0.000100950558f);
+  p = fmaf(p, w, 0.00134934322f);
+  p = fmaf(p, w, -0.00367342844f);
+  p = fmaf(p, w, 0.00573950773f);
+  p = fmaf(p, w, -0.0076224613f);
+  p = fmaf(p, w, 0.00943887047f);
+  p = fmaf(p, w, 1.00167406f);
+  p = fmaf(p, w, 2.83297682f);
+  return p;
+}
+constexpr float kIcdfTailL2 = -9.21347810f;   // w = -ln(4u(1-u)) < 5  <=>  log2(u(1-u)) > -5/ln2 - 2
+
 __device__ __forceinline__ float icdf_normal(float u) {
   const float t = u * (1.0f - u);
   const float l2 = lg2_approx(t);                                       // log2(u(1-u))
   const float xs = fmaf(2.82842712474619010f, u, -1.41421356237309505f);  // sqrt2 * (2u - 1)
-  float p;
-  if (l2 > -9.21347810f) {   // w = -ln(4u(1-u)) < 5  <=>  log2(u(1-u)) > -5/ln2 - 2
-    const float w = fmaf(-kLn2, l2, -2.0f * kLn2 - 2.5f);              // w - 2.5
-    p = 2.81022636e-08f;
-    p = fmaf(p, w, 3.43273939e-07f);
-    p = fmaf(p, w, -3.5233877e-06f);
-    p = fmaf(p, w, -4.39150654e-06f);
-    p = fmaf(p, w, 0.00021858087f);
-    p = fmaf(p, w, -0.00125372503f);
-    p = fmaf(p, w, -0.00417768164f);
-    p = fmaf(p, w, 0.246640727f);
-    p = fmaf(p, w, 1.50140941f);
-  } else {
-    const float w = sqrt_approx(fmaf(-kLn2, l2, -2.0f * kLn2)) - 3.0f;
-    p = -0.000200214257f;
-    p = fmaf(p, w, 0.000100950558f);
-    p = fmaf(p, w, 0.00134934322f);
-    p = fmaf(p, w, -0.00367342844f);
-    p = fmaf(p, w, 0.00573950773f);
-    p = fmaf(p, w, -0.0076224613f);
-    p = fmaf(p, w, 0.00943887047f);
-    p = fmaf(p, w, 1.00167406f);
-    p = fmaf(p, w, 2.83297682f);
+  const float p = (l2 > kIcdfTailL2) ? icdf_central_poly(l2) : icdf_tail_poly(l2);
+  return p * xs;
+}
+
+// The same function for a full warp in convergent code: the tail polynomial
+// (u < 0.0017 or u > 0.9983, about one draw in 290) runs behind a warp vote,
+// so the common case costs the central polynomial alone. Results are identical
+// to icdf_normal bit for bit.
+__device__ __forceinline__ float icdf_normal_warp(float u) {
+  const float t = u * (1.0f - u);
+  const float l2 = lg2_approx(t);
+  const float xs = fmaf(2.82842712474619010f, u, -1.41421356237309505f);
+  float p = icdf_central_poly(l2);
+  const bool tail = !(l2 > kIcdfTailL2);
+  if (__any_sync(0xffffffffu, tail)) {
+    const float pt = icdf_tail_poly(l2);
+    if (tail) p = pt;
   }
   return p * xs;
 }

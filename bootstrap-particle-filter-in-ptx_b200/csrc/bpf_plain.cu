@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
       float xx;
       if (APF == 0) {
         if (tick > 0) {
-          float z = icdf_normal(pcg_uniform(pcg_output(s)));
+          float z = icdf_normal_warp(pcg_uniform(pcg_output(s)));
           if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
           h = propagate(h, a.mu, a.rho, a.sigma, z);
         }
