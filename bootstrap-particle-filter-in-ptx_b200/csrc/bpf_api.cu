@@ -700,7 +700,16 @@ int gpu_bpf_get_resample_inputs(GpuBpfState* s, float* w_out, int32_t* tile_exp_
   if (rc) return rc;
   CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
   CK(cudaStreamSynchronize(m->stream));
-  if (w_out) CK(cudaMemcpy(w_out, m->plan.w, (size_t)m->plan.N * sizeof(float), cudaMemcpyDeviceToHost));
+  if (w_out) {
+    float* w_dev = nullptr;
+    CK(cudaMalloc(&w_dev, (size_t)m->plan.N * sizeof(float)));
+    cudaError_t e = launch_tile_weights(m->plan, w_dev, m->stream);
+    g_launches += 1;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(w_out, w_dev, (size_t)m->plan.N * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(w_dev);
+    CK(e);
+  }
   if (tile_exp_out) CK(cudaMemcpy(tile_exp_out, m->plan.nexp, (size_t)m->plan.G * sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (u23_out) *u23_out = m->st_pin->u23;
   return BPF_OK;

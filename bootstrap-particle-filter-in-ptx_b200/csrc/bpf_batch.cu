@@ -2,9 +2,9 @@
 // time, whole filter resident in shared memory for all T ticks).
 //
 // Per tick and filter (N particles, G = ceil(N/4096) tiles, NT threads):
-//   1. propagate + log2-weight (+ carried weight), per-tile max
-//   2. tile-relative weights 2^(x - n_k), tile partial sums and exact
-//      fixed-point tile masses
+//   1. propagate + log2-weight (+ carried tile-relative log2-weight), per-tile max
+//   2. tile-relative log2-weights d = x - n_k (kept for the next tick's carry),
+//      weights 2^d, tile partial sums and exact fixed-point tile masses
 //   3. thread 0: FP64 combine, log-likelihood increment, ESS, mean, decision;
 //      on resampling ticks the fixed-point CDF tile prefix, total and spacing
 //   4. resampling: per-thread contiguous chunk scan, per-element count of the
@@ -120,8 +120,10 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
             h = propagate(h, f.mu, f.rho, f.sigma, z);
             H[si] = h;
           }
-          float x = gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e);
-          if (carry) x += lg2_approx(Wt[si]) + coff;
+          // same operation sequence as the plain filter's pass 1 (bit-identical x)
+          float x = gauss ? obs_log2pdf_gauss_plus(y2, h, kGaussLog2C + coff)
+                          : __fmul_rn(obs_logpdf(obs, h), kLog2e) + coff;
+          if (carry) x += Wt[si];                  // carried tile-relative log2-weight
           Wt[si] = x;
           m = fmaxf(m, x);
         }
@@ -148,12 +150,13 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       float fS = 0.f, fQ = 0.f, fH = 0.f;
       unsigned long long E = 0ull;
       if (k < G) {
-        const float fnk = (float)nk[k];
+        const float fnk = (nk[k] == kNkEmpty) ? INFINITY : (float)nk[k];   // empty tile: every 2^d = 0
         const int i1 = min(N, (k + 1) * kTile);
         for (int i = k * kTile + tid; i < i1; i += NT) {
           const int si = swz(i);
-          const float w = (nk[k] == kNkEmpty) ? 0.0f : fminf(ex2_approx(Wt[si] - fnk), 1.0f);
-          Wt[si] = w;
+          const float d = Wt[si] - fnk;
+          const float w = tile_weight(d);
+          Wt[si] = d;                              // stored as the tile-relative log2-weight
           fS += w;
           fQ = fmaf(w, w, fQ);
           fH = fmaf(w, H[si], fH);
@@ -239,7 +242,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       const unsigned long long base = sh.base, delta = sh.delta, magic = sh.magic;
       const int j0 = tid * chunk, j1 = min(N, j0 + chunk);
       unsigned long long run = 0ull;
-      for (int j = j0; j < j1; ++j) run += fix_weight(Wt[swz(j)]);
+      for (int j = j0; j < j1; ++j) run += fix_weight(tile_weight(Wt[swz(j)]));
       unsigned long long tot;
       const unsigned long long excl = block_excl_scan_add<NT>(run, &tot, sh.scan);
       sh.excl[tid] = excl;
@@ -260,7 +263,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
         int lo = 0, hi = 0;
         if (lst) lst[e * NT + tid] = (unsigned short)(j < j1 ? q : N);   // children of j start at slot q
         if (j < j1) {
-          loc += fix_weight(Wt[swz(j)]);
+          loc += fix_weight(tile_weight(Wt[swz(j)]));
           const unsigned long long cj = Pk + shr64(loc, r);
           if (q < N && tq < cj) {
             if (((cj - tq) >> 2) > delta) {

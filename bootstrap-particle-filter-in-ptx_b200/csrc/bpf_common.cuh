@@ -188,11 +188,20 @@ struct ObsModel {
 
 // log2 p(y | h) for the Gaussian model with y2 = y^2:
 //   -log2(e)/2 * (y^2 e^{-h} + h) - log2(e) ln(2 pi)/2
-__device__ __forceinline__ float obs_log2pdf_gauss(float y2, float h) {
+constexpr float kGaussLog2C = -1.32574806473616f;               // -log2(e) ln(2 pi)/2
+__device__ __forceinline__ float obs_log2pdf_gauss_plus(float y2, float h, float c) {   // + (c - kGaussLog2C)
   const float e = ex2_approx(h * -kLog2e);                       // e^{-h}
   const float s = (y2 > 0.0f) ? fmaf(y2, e, h) : h;
-  return fmaf(-0.5f * kLog2e, s, -1.32574806473616f);           // -log2(e) ln(2 pi)/2
+  return fmaf(-0.5f * kLog2e, s, c);
 }
+__device__ __forceinline__ float obs_log2pdf_gauss(float y2, float h) {
+  return obs_log2pdf_gauss_plus(y2, h, kGaussLog2C);
+}
+
+// Tile-relative weight 2^d of a tile-relative log2-weight d <= 0 (the stored
+// form). Pass 1 and pass 2 both evaluate it with this one instruction sequence,
+// so the fixed-point masses agree bit for bit.
+__device__ __forceinline__ float tile_weight(float d) { return fminf(ex2_approx(d), 1.0f); }
 
 __device__ __forceinline__ float obs_logpdf(const ObsModel& m, float h) {
   const float e = ex2_approx(h * -0.5f * kLog2e);   // exp(-h/2)

@@ -3,10 +3,12 @@
 //   pass 1  (one CTA per 4096-particle tile, streaming)
 //           counter-PCG32 -> inverse-CDF normal (x Student-t scale when
 //           nu_state > 0) -> OU propagate -> log2-weight
-//           (+ carried weight on ESS-skipped ticks). The tile max becomes a
-//           power-of-two exponent n_k; tile-relative weights w = 2^(x - n_k)
-//           are written once, with the tile partials S=sum w, Q=sum w^2,
-//           H=sum w h and the exact fixed-point tile mass E = sum floor(w 2^50).
+//           (+ carried log2-weight on ESS-skipped ticks). The tile max becomes a
+//           power-of-two exponent n_k; the tile-relative log2-weights
+//           d = x - n_k <= 0 are written once (w = 2^d is re-derived by pass 2
+//           and by the next tick's carry without a log), with the tile partials
+//           S=sum w, Q=sum w^2, H=sum w h and the exact fixed-point tile mass
+//           E = sum floor(w 2^50).
 //   plan    (one CTA of 512 threads)
 //           FP64 combine of the tile partials in the global frame 2^nM:
 //           log-likelihood increment, ESS, filtered mean, the resampling
@@ -103,6 +105,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     const int nkp = p.nexp[k];
     carry_off = (nkp == kNkEmpty) ? -INFINITY : (float)(nkp - nM_prev);
   }
+  const float gauss_c = kGaussLog2C + carry_off;   // the carry offset folded into the Gaussian constant
 
   const int tile0 = k * kTile;
   const bool full = tile0 + kTile <= p.N;      // every slot of the tile holds a particle
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     const int i0 = tile0 + 4 * (tid + kThreads * r);
     h4[r] = *reinterpret_cast<const float4*>(hb + i0);
     if (carry) w4[r] = *reinterpret_cast<const float4*>(p.w + i0);
-    else w4[r] = make_float4(1.f, 1.f, 1.f, 1.f);
+    else w4[r] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   if (a.ckpt) {
 #pragma unroll
@@ -139,7 +142,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
           if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
           h = propagate(h, a.mu, a.rho, a.sigma, z);
         }
-        xx = gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e);
+        xx = gauss ? obs_log2pdf_gauss_plus(y2, h, gauss_c)
+                   : __fmul_rn(obs_logpdf(obs, h), kLog2e) + carry_off;
       } else {
         const float m = propagate_mean(h, a.mu, a.rho);
         const float lm = gauss ? obs_log2pdf_gauss(y2, m) : __fmul_rn(obs_logpdf(obs, m), kLog2e);
@@ -153,7 +157,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
         }
       }
       s += step2;
-      if (carry) xx += lg2_approx(wp[e]) + carry_off;
+      if (carry) xx += wp[e];                      // carried log2-weight (offset already added)
       hh[e] = h;
       x[4 * r + e] = xx;
       hv[4 * r + e] = h;
@@ -186,12 +190,13 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int i0 = tile0 + 4 * (tid + kThreads * r);
-    float wv[4];
+    float dv[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int idx = 4 * r + e;
-      const float w = fminf(ex2_approx(x[idx] - fnk), 1.0f);
-      wv[e] = w;
+      const float d = x[idx] - fnk;
+      const float w = tile_weight(d);
+      dv[e] = d;
       fS += w;
       fQ = fmaf(w, w, fQ);
       fH = fmaf(w, hv[idx], fH);
@@ -209,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
         lF1 = fmaf(wd2, dh * dh, lF1);
       }
     }
-    *reinterpret_cast<float4*>(p.w + i0) = make_float4(wv[0], wv[1], wv[2], wv[3]);
+    *reinterpret_cast<float4*>(p.w + i0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
   }
   // tile partials: the per-thread FP32 sums are staged in shared memory and one
   // warp adds them in FP64 (and the exact masses in u64), in a fixed order
@@ -599,7 +604,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       const float4 f = wt[v];
       const float ff[4] = {f.x, f.y, f.z, f.w};
 #pragma unroll
-      for (int e = 0; e < 4; ++e) run += (tid * kPerThread + 4 * v + e < nA) ? fix_weight(ff[e]) : 0ull;
+      for (int e = 0; e < 4; ++e) run += (tid * kPerThread + 4 * v + e < nA) ? fix_weight(tile_weight(ff[e])) : 0ull;
     }
     unsigned long long tot;
     const unsigned long long excl = block_excl_scan_add<kThreads>(run, &tot, s_scan);
@@ -620,7 +625,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       if (csr && j < nA) csr[j] = q;
       if ((e & 3) == 0) f4 = wt[e >> 2];
       const float we = (e & 3) == 0 ? f4.x : (e & 3) == 1 ? f4.y : (e & 3) == 2 ? f4.z : f4.w;
-      accw += (j < nA) ? fix_weight(we) : 0ull;
+      accw += (j < nA) ? fix_weight(tile_weight(we)) : 0ull;
       const unsigned long long cj = Pk + shr64(accw, r);
       if (j < nA && q < N && tq < cj) {
         const int c = 1 + (tq + delta < cj) + (tq + 2ull * delta < cj) + (tq + 3ull * delta < cj);
@@ -696,6 +701,12 @@ __global__ void debug_pcg_kernel(int seed, int n, unsigned long long At, unsigne
   const uint32_t o = pcg_output(c.k1 + c.k2 * pcg_inc((uint32_t)i));
   if (out) out[i] = o;
   if (norm) norm[i] = icdf_normal(pcg_uniform(o));
+}
+
+// Linear tile-relative weights 2^d of the stored log2-weights (inspection API).
+__global__ void tile_weights_kernel(const float* d, float* w, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) w[i] = tile_weight(d[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -789,6 +800,11 @@ cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool p
 }
 cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s, bool pdl) {
   return launch_ex(pass2_kernel, dim3(grid), dim3(kThreads), kPass2Smem, s, pdl, p, a);
+}
+
+cudaError_t launch_tile_weights(const Plan& p, float* w_out, cudaStream_t s) {
+  tile_weights_kernel<<<(p.N + 255) / 256, 256, 0, s>>>(p.w, w_out, p.N);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s) {

@@ -4,7 +4,7 @@
 // (every particle array is padded to G*4096 floats so tile loads never
 // leave the allocation):
 //   h[2][G*4096]  f32  particle ping-pong (current buffer index in DevState)
-//   w[G*4096]     f32  tile-relative weights 2^(x_i - n_k), in [0,1]
+//   w[G*4096]     f32  tile-relative log2-weights d_i = x_i - n_k <= 0 (weight 2^d_i)
 //   tile records  rec[G] f32x4 {S=sum w, Q=sum w^2, H=sum w h, n_k bits},
 //                 nexp[G] i32 (n_k again), E[G] u64 exact fixed-point mass
 //   P[G] u64 exclusive tile prefix of the fixed-point CDF, ofirst[G+1] i32
@@ -90,6 +90,8 @@ cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_
 int pass2_grid_size(int device);
 size_t pass2_smem_bytes();
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s);
+// w_out[i] = 2^d_i of the stored tile-relative log2-weights (N floats, device).
+cudaError_t launch_tile_weights(const Plan& p, float* w_out, cudaStream_t s);
 
 }  // namespace bpf
 
