@@ -76,7 +76,9 @@ constexpr int kStWords = (int)(sizeof(DevState) / 8);
 // runs on the particles resampled by those weights, propagates them
 // (h = m + sigma eps, the same operations as a bootstrap tick) and weights them
 // by p(y | h) / p(y | m).
-template <bool TSTATE, bool LEARN, int APF>
+// GAUSS: the observation model is Gaussian (a.obs.nu == 0), fixed at compile
+// time so the per-particle code carries no model branch.
+template <bool TSTATE, bool LEARN, int APF, bool GAUSS>
 __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
   __shared__ float s_max[kThreads / 32];
   __shared__ float s_part[3][kThreads];
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   float* hb = st->cur ? p.h1 : p.h0;
 
   const float y = a.y_ptr ? __ldg(a.y_ptr) : a.obs.y;
-  const bool gauss = !(a.obs.nu > 0.0f);
+  constexpr bool gauss = GAUSS;
   ObsModel obs = a.obs;
   obs.y = y;
   const float y2 = y * y;
@@ -781,19 +783,24 @@ int pass2_grid_size(int device) {
   return sms * per_sm;
 }
 
-cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
+template <bool GAUSS>
+static cudaError_t launch_pass1_model(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
   const dim3 grid(p.G), block(kThreads);
-  if (a.apf == 1) return launch_ex(pass1_kernel<false, false, 1>, grid, block, 0, s, pdl, p, a);
+  if (a.apf == 1) return launch_ex(pass1_kernel<false, false, 1, GAUSS>, grid, block, 0, s, pdl, p, a);
   if (a.apf == 2) {
-    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 2>, grid, block, 0, s, pdl, p, a);
-    return launch_ex(pass1_kernel<false, false, 2>, grid, block, 0, s, pdl, p, a);
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 2, GAUSS>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, false, 2, GAUSS>, grid, block, 0, s, pdl, p, a);
   }
   if (a.learn && p.rec2) {
-    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, true, 0>, grid, block, 0, s, pdl, p, a);
-    return launch_ex(pass1_kernel<false, true, 0>, grid, block, 0, s, pdl, p, a);
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, true, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, true, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
   }
-  if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 0>, grid, block, 0, s, pdl, p, a);
-  return launch_ex(pass1_kernel<false, false, 0>, grid, block, 0, s, pdl, p, a);
+  if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
+  return launch_ex(pass1_kernel<false, false, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
+}
+
+cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
+  return (a.obs.nu > 0.0f) ? launch_pass1_model<false>(p, a, s, pdl) : launch_pass1_model<true>(p, a, s, pdl);
 }
 cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
   return launch_ex(plan_kernel, dim3(1), dim3(kPlanThreads), plan_smem_bytes(p.G), s, pdl, p, a);
