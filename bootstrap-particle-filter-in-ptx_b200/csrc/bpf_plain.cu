@@ -33,6 +33,7 @@
 #include "bpf_plain.cuh"
 #include "bpf_block.cuh"
 #include <cmath>
+#include <type_traits>
 
 namespace bpf {
 
@@ -127,6 +128,10 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   float x[kPerThread], hv[kPerThread];
   float hpv[LEARN ? kPerThread : 1];     // particles before this tick's propagation (learning only)
   const unsigned long long step2 = 2ull * c.k2;
+  // the per-particle loop, compiled once with and once without the propagation
+  // (tick 0 only weights the initial draw), so no particle tests the tick
+  auto particles = [&](auto prop_tag) {
+  constexpr bool PROP = decltype(prop_tag)::value;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int i0 = tile0 + 4 * (tid + kThreads * r);
@@ -139,7 +144,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
       if (LEARN) hpv[4 * r + e] = h;
       float xx;
       if (APF == 0) {
-        if (tick > 0) {
+        if (PROP) {
           float z = icdf_normal_warp(pcg_uniform(pcg_output(s)));
           if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
           h = propagate(h, a.mu, a.rho, a.sigma, z);
@@ -152,7 +157,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
         if (APF == 1) {
           xx = lm;
         } else {
-          float z = icdf_normal(pcg_uniform(pcg_output(s)));
+          float z = icdf_normal_warp(pcg_uniform(pcg_output(s)));
           if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
           h = fmaf(a.sigma, z, m);
           xx = (gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e)) - lm;
@@ -166,6 +171,9 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     }
     if (APF != 1) *reinterpret_cast<float4*>(hb + i0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
   }
+  };
+  if (APF != 0 || tick > 0) particles(std::true_type{});
+  else particles(std::false_type{});
   if (!full) {                                   // the last tile's padding slots carry no weight
 #pragma unroll
     for (int idx = 0; idx < kPerThread; ++idx)
