@@ -57,7 +57,7 @@ struct ApfImpl {
   DevState* st_pin = nullptr;
   float* y_dev = nullptr;             // [kApfChunk]
   float* y_pin = nullptr;
-  int32_t* anc_dev = nullptr;         // [2N] when recording: first stage, then second stage
+  int32_t* anc_dev = nullptr;         // when recording: first stage, then second stage at anc_stride
   bool record_anc = false;
   int ticks = 0;                      // ticks enqueued since create
   int sticky_error = BPF_OK;
@@ -69,6 +69,10 @@ struct ApfImpl {
 };
 
 inline ApfImpl* impl_of(GpuApfState* s) { return s ? reinterpret_cast<ApfImpl*>(s->impl) : nullptr; }
+
+// Offset of the second stage's ancestors in anc_dev: N rounded up to 4 slots
+// (16 bytes), so both halves start aligned.
+inline size_t anc_stride(const ApfImpl* m) { return ((size_t)m->plan.N + 3) & ~(size_t)3; }
 
 int ensure_device(ApfImpl* m) {
   int cur = -1;
@@ -107,7 +111,7 @@ cudaError_t launch3(ApfImpl* m, const TickArgs& a) {
 // the two stages. Returns the kernels launched, or -1 on a launch error.
 int enqueue_tick(const GpuApfState* s, ApfImpl* m, int t, float y, const float* y_ptr, BpfTickRecord* rec) {
   TickArgs a = make_args(s, m, y, y_ptr);
-  int32_t* anc2 = m->record_anc ? m->anc_dev + m->plan.N : nullptr;
+  int32_t* anc2 = m->record_anc ? m->anc_dev + anc_stride(m) : nullptr;
   if (t == 0) {
     a.apf = 0; a.rec = rec; a.anc = anc2;
     return launch3(m, a) == cudaSuccess ? 3 : -1;
@@ -329,8 +333,8 @@ int gpu_apf_record_ancestors(GpuApfState* s, int enable) {
   int rc = ensure_device(m);
   if (rc) return rc;
   if (enable && !m->anc_dev) {
-    ACK(cudaMalloc(&m->anc_dev, 2 * (size_t)m->plan.N * sizeof(int32_t)));
-    ACK(cudaMemsetAsync(m->anc_dev, 0xff, 2 * (size_t)m->plan.N * sizeof(int32_t), m->stream));
+    ACK(cudaMalloc(&m->anc_dev, 2 * anc_stride(m) * sizeof(int32_t)));
+    ACK(cudaMemsetAsync(m->anc_dev, 0xff, 2 * anc_stride(m) * sizeof(int32_t), m->stream));
   }
   m->record_anc = enable != 0;
   return BPF_OK;
@@ -345,7 +349,7 @@ int gpu_apf_get_ancestors(GpuApfState* s, int32_t* anc_first, int32_t* anc_secon
   ACK(cudaStreamSynchronize(m->stream));
   const size_t n = (size_t)m->plan.N;
   if (anc_first) ACK(cudaMemcpy(anc_first, m->anc_dev, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
-  if (anc_second) ACK(cudaMemcpy(anc_second, m->anc_dev + n, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (anc_second) ACK(cudaMemcpy(anc_second, m->anc_dev + anc_stride(m), n * sizeof(int32_t), cudaMemcpyDeviceToHost));
   return BPF_OK;
 }
 

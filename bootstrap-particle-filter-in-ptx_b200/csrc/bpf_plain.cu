@@ -543,7 +543,10 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
 // item has released the buffer (the other CTAs on the SM hide the latency).
 // ---------------------------------------------------------------------------
 constexpr size_t kTileBytes = (size_t)kTile * 4;
-constexpr size_t kMarkBytes = (size_t)kOutChunk * 2;      // u16 ancestor (tile-local + 1) per output
+// u16 ancestor (tile-local + 1) per output slot of a window; a window starts
+// at its item's first output rounded down to a multiple of 4 (up to 3 extra
+// slots), rounded up to whole 128-slot steps of the gather
+constexpr size_t kMarkBytes = ((size_t)kOutChunk + 128) * 2;
 constexpr size_t kMarkOffset = 2 * kTileBytes;                 // after the staged h and w tiles
 constexpr size_t kPass2Smem = kMarkOffset + kMarkBytes;         // one staged tile (h, w) + marks
 static_assert(kMarkOffset % 16 == 0 && kMarkBytes % 16 == 0, "marks are cleared with 16-byte stores");
@@ -577,6 +580,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
   const int src = st->src;
   const float* hsrc = src ? p.h1 : p.h0;
   float* hdst = src ? p.h0 : p.h1;
+  // the ancestor record takes vector stores only from a 16-byte aligned base
+  const bool anc_vec = ((reinterpret_cast<uintptr_t>(a.anc) & 15u) == 0u);
   const int tid = threadIdx.x;
   if (tid == 0) {
     s_err = 0;
@@ -592,58 +597,78 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
 
     const int4 item = p.items[it];
     const int k = item.x, oa = item.y, ob = item.z;
+    const int wa = oa & ~3;                          // window origin: 16-byte aligned output slot
     const int j0 = k * kTile;
     const int nA = min(kTile, N - j0);
-    const int nB = ob - oa;
-    const int r = nM - p.nexp[k] + kFixF - Fg;
+    const int nB = ob - wa;                          // window slots [wa, ob); [wa, oa) belong to other items
+    const int r = nM - p.nexp[k] + kFixF - Fg;       // tile frame -> global frame shift
     const unsigned long long Pk = p.P[k];
     const bool ok = mbar_wait_bounded(&mbar[0], (uint32_t)n & 1u);
     if (!ok) s_err = 1;
 
-    // clear this item's ancestor marks (the previous item's gather has finished:
+    // clear this window's ancestor marks (the previous item's gather has finished:
     // the loop ends with a barrier; the scan's barriers order this before the marks)
     const int nB128 = (nB + 127) & ~127;
     for (int x = tid; x < nB128 / 8; x += kThreads) reinterpret_cast<uint4*>(marks)[x] = make_uint4(0u, 0u, 0u, 0u);
 
-    // exact fixed-point prefix of the tile: 16 contiguous weights per thread
-    // (summed here, rebuilt element by element below from the staged tile)
+    // Exact fixed-point prefix of the tile: 16 contiguous weights per thread
+    // (summed here, rebuilt element by element below from the staged tile).
+    // A tile whose shift reaches 64 has no mass in the global frame.
     const float4* wt = reinterpret_cast<const float4*>(ws + tid * kPerThread);
+    const bool full = nA == kTile;
+    const bool massive = r < 64;
     unsigned long long run = 0ull;
+    if (massive) {
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const float4 f = wt[v];
-      const float ff[4] = {f.x, f.y, f.z, f.w};
+      for (int v = 0; v < 4; ++v) {
+        const float4 f = wt[v];
+        const float ff[4] = {f.x, f.y, f.z, f.w};
 #pragma unroll
-      for (int e = 0; e < 4; ++e) run += (tid * kPerThread + 4 * v + e < nA) ? fix_weight(tile_weight(ff[e])) : 0ull;
+        for (int e = 0; e < 4; ++e)
+          if (full || tid * kPerThread + 4 * v + e < nA) run += fix_weight(tile_weight(ff[e]));
+      }
     }
     unsigned long long tot;
     const unsigned long long excl = block_excl_scan_add<kThreads>(run, &tot, s_scan);
 
     // Element j owns the targets in [C_{j-1}, C_j), i.e. the output slots
-    // [q_j, q_{j+1}). Its child count is found without a loop (four
-    // comparisons; a division only past four children) and the element
-    // writes one start mark, at its first slot inside this item's window.
+    // [q_j, q_{j+1}). Its child count comes from one 64-bit difference against
+    // delta, 2 delta and 3 delta (a division only past four children); the
+    // element writes one start mark, at its first slot inside this window.
     const int lane = tid & 31, warp = tid >> 5;
+    const unsigned long long d2 = 2ull * delta, d3 = 3ull * delta, d4 = 4ull * delta;
     int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
     unsigned long long tq = base + (unsigned long long)q * delta;
     int32_t* csr = (a.csr && item.w) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
-    unsigned long long accw = excl;
-    float4 f4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto count_children = [&](auto full_tag) {
+      constexpr bool FULL = decltype(full_tag)::value;
+      unsigned long long accw = excl;
+      float4 f4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int e = 0; e < kPerThread; ++e) {
-      const int j = tid * kPerThread + e;
-      if (csr && j < nA) csr[j] = q;
-      if ((e & 3) == 0) f4 = wt[e >> 2];
-      const float we = (e & 3) == 0 ? f4.x : (e & 3) == 1 ? f4.y : (e & 3) == 2 ? f4.z : f4.w;
-      accw += (j < nA) ? fix_weight(tile_weight(we)) : 0ull;
-      const unsigned long long cj = Pk + shr64(accw, r);
-      if (j < nA && q < N && tq < cj) {
-        const int c = 1 + (tq + delta < cj) + (tq + 2ull * delta < cj) + (tq + 3ull * delta < cj);
-        const int q1 = (c == 4 && tq + 4ull * delta < cj) ? targets_below(cj, base, delta, magic, N) : min(q + c, N);
-        if (q < ob && q1 > oa) marks[max(q, oa) - oa] = (unsigned short)(j + 1);
-        q = q1;
-        tq = base + (unsigned long long)q * delta;
+      for (int e = 0; e < kPerThread; ++e) {
+        const int j = tid * kPerThread + e;
+        const bool in = FULL || j < nA;
+        if (csr && in) csr[j] = q;
+        if ((e & 3) == 0) f4 = wt[e >> 2];
+        const float we = (e & 3) == 0 ? f4.x : (e & 3) == 1 ? f4.y : (e & 3) == 2 ? f4.z : f4.w;
+        if (in) accw += fix_weight(tile_weight(we));
+        const unsigned long long cj = Pk + (accw >> r);
+        if (in && q < N && cj > tq) {
+          const unsigned long long diff = cj - tq;
+          const int c = 1 + (diff > delta) + (diff > d2) + (diff > d3);
+          const int q1 = (c == 4 && diff > d4) ? targets_below(cj, base, delta, magic, N) : min(q + c, N);
+          if (q < ob && q1 > oa) marks[max(q, oa) - wa] = (unsigned short)(j + 1);
+          q = q1;
+          tq = base + (unsigned long long)q * delta;
+        }
       }
+    };
+    if (massive) {
+      if (full) count_children(std::true_type{});
+      else count_children(std::false_type{});
+    } else if (csr) {
+      for (int e = 0; e < kPerThread; ++e)       // no mass: every element's children start at q
+        if (tid * kPerThread + e < nA) csr[tid * kPerThread + e] = q;
     }
     __syncthreads();
 
@@ -651,7 +676,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     // before o (marks increase along the window). Each warp takes a run of
     // slots in steps of 128 (4 per lane): the running maximum of the marks
     // is a lane-local scan, a warp max-scan and a carry from the earlier
-    // steps and warps.
+    // steps and warps. A lane's 4 slots are 16-byte aligned in the output,
+    // so whole groups are written with one vector store.
     const int chunk = ((nB + kThreads / 32 - 1) / (kThreads / 32) + 127) & ~127;
     const int cs = warp * chunk, ce = min(cs + chunk, nB);
     unsigned wmax = 0u;
@@ -665,6 +691,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     unsigned carry = 0u;
     for (int w = 0; w < warp; ++w) carry = max(carry, s_wmax[w]);
     if (ok) {
+      const int olo = oa - wa;                       // first slot of this item in the window
       for (int o0 = cs; o0 < ce; o0 += 128) {
         const uint2 m = reinterpret_cast<const uint2*>(marks + o0)[lane];
         unsigned am[4];
@@ -680,15 +707,28 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
         }
         unsigned pre = __shfl_up_sync(0xffffffffu, x, 1);
         pre = max(carry, lane == 0 ? 0u : pre);
+        const int o = o0 + 4 * lane;
+        float hv[4];
+        int av[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const int o = o0 + 4 * lane + u;
-          if (o < ce) {
-            unsigned jj = max(pre, am[u]);
-            if (jj == 0u || jj > (unsigned)nA) { jj = 1u; s_err = 1; }   // unreachable by construction
-            hdst[oa + o] = hs[jj - 1u];
-            if (a.anc) a.anc[oa + o] = j0 + (int)(jj - 1u);
-          }
+          unsigned jj = max(pre, am[u]);
+          const bool mine = o + u >= olo && o + u < ce;
+          if (mine && jj - 1u >= (unsigned)nA) { jj = 1u; s_err = 1; }   // unreachable by construction
+          if (jj == 0u) jj = 1u;                                           // a slot before the item: not written
+          hv[u] = hs[jj - 1u];
+          av[u] = j0 + (int)(jj - 1u);
+        }
+        if (o >= olo && o + 3 < ce && anc_vec) {
+          *reinterpret_cast<float4*>(hdst + wa + o) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+          if (a.anc) *reinterpret_cast<int4*>(a.anc + wa + o) = make_int4(av[0], av[1], av[2], av[3]);
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (o + u >= olo && o + u < ce) {
+              hdst[wa + o + u] = hv[u];
+              if (a.anc) a.anc[wa + o + u] = av[u];
+            }
         }
         carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
       }
