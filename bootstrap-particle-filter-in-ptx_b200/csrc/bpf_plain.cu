@@ -46,7 +46,8 @@ __global__ void init_kernel(Plan p, float mu, float std_stat, int seed) {
   const int npad = p.G * kTile;
   if (i == 0) {
     DevState d{};
-    d.At = 1ull; d.Bt = 0ull;                                   // tick 0 uses draw index 0
+    const PcgTick c0 = pcg_tick_consts(seed, 1ull, 0ull);       // tick 0 uses draw index 0
+    d.k1 = c0.k1; d.k2 = c0.k2;
     d.u_state = (unsigned long long)seed * 67890ULL + 12345ULL;  // gpu_bpf_ptx_full.cu:353
     d.logS_prev = log((double)p.N);
     d.resampled_prev = 1;                                        // gpu_bpf_ptx_full.cu:357
@@ -94,7 +95,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   const int tick = st->tick;
   const bool carry = APF == 0 && st->resampled_prev == 0;
   const int nM_prev = st->nM_prev;
-  const PcgTick c = pcg_tick_consts(st->seed, st->At, st->Bt);
+  PcgTick c;
+  c.k1 = st->k1; c.k2 = st->k2;
   float* hb = st->cur ? p.h1 : p.h0;
 
   const float y = a.y_ptr ? __ldg(a.y_ptr) : a.obs.y;
@@ -128,14 +130,19 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   float x[kPerThread], hv[kPerThread];
   float hpv[LEARN ? kPerThread : 1];     // particles before this tick's propagation (learning only)
   const unsigned long long step2 = 2ull * c.k2;
+  // state of the first particle of group r + 1 from the state after group r's
+  // four draws: inc advances by 2 * 4 * kThreads slots
+  const unsigned long long group_step = (unsigned long long)(2 * 4 * kThreads - 8) * c.k2;
+  const unsigned long long s_first = c.k1 + c.k2 * pcg_inc((uint32_t)(tile0 + 4 * tid));
   // the per-particle loop, compiled once with and once without the propagation
   // (tick 0 only weights the initial draw), so no particle tests the tick
   auto particles = [&](auto prop_tag) {
   constexpr bool PROP = decltype(prop_tag)::value;
+  unsigned long long s = s_first;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int i0 = tile0 + 4 * (tid + kThreads * r);
-    unsigned long long s = c.k1 + c.k2 * pcg_inc((uint32_t)i0);
+    if (r > 0) s += group_step;
     float hh[4] = {h4[r].x, h4[r].y, h4[r].z, h4[r].w};
     const float wp[4] = {w4[r].x, w4[r].y, w4[r].z, w4[r].w};
 #pragma unroll
@@ -419,8 +426,8 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
       *a.rec = r;
     }
     if (a.apf != 1) {
-      st->At = st->At * kPcgMult;          // next tick's jump constants
-      st->Bt = st->Bt * kPcgMult + 1ull;
+      st->k1 = st->k1 * kPcgMult;          // next tick's stream constants
+      st->k2 = st->k2 * kPcgMult + 1ull;
       st->tick = tick + 1;
     }
     st->do_resample = resample;

@@ -20,7 +20,9 @@ namespace bpf {
 
 // Scalars that live on the device from tick to tick (no host round trip).
 struct DevState {
-  uint64_t At, Bt;          // PCG jump constants A^t, sum_{k<t} A^k of the next tick
+  uint64_t k1, k2;          // PCG32 stream constants of the next tick t: slot i's state is
+                            // k1 + k2 inc_i, k1 = A^t A^2 seed, k2 = A^t (A+1) + sum_{k<t} A^k;
+                            // tick to tick k1 <- A k1, k2 <- A k2 + 1
   uint64_t u_state;         // resampling-uniform PCG32 (gpu_bpf_ptx_full.cu:353)
   uint64_t base, delta;     // systematic targets t_i = base + i*delta (fixed point)
   uint64_t delta_magic;     // floor((2^64-1)/delta)
