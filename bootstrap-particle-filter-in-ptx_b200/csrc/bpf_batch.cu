@@ -242,7 +242,11 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       const unsigned long long base = sh.base, delta = sh.delta, magic = sh.magic;
       const int j0 = tid * chunk, j1 = min(N, j0 + chunk);
       unsigned long long run = 0ull;
-      for (int j = j0; j < j1; ++j) run += fix_weight(tile_weight(Wt[swz(j)]));
+      for (int j = j0; j < j1; ++j) {            // the thread's chunk: log2-weights -> weights, in place
+        const float w = tile_weight(Wt[swz(j)]);
+        Wt[swz(j)] = w;
+        run += fix_weight(w);
+      }
       unsigned long long tot;
       const unsigned long long excl = block_excl_scan_add<NT>(run, &tot, sh.scan);
       sh.excl[tid] = excl;
@@ -263,7 +267,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
         int lo = 0, hi = 0;
         if (lst) lst[e * NT + tid] = (unsigned short)(j < j1 ? q : N);   // children of j start at slot q
         if (j < j1) {
-          loc += fix_weight(tile_weight(Wt[swz(j)]));
+          loc += fix_weight(Wt[swz(j)]);
           const unsigned long long cj = Pk + shr64(loc, r);
           if (q < N && tq < cj) {
             if (((cj - tq) >> 2) > delta) {
