@@ -24,6 +24,8 @@ one filter pass over the T=5000 series (re-seed + 5000 ticks).
          finite-difference checks
   batch_gradient  forward + backward of 256 filters x 8192 particles over a
          4000-tick regime-switching series, against the batched forward
+  extensions  Student-t noise, online learning, the auxiliary particle filter,
+         IMM and SMC^2, each on its own small workload (bench_extensions)
 
 `--impl reference` times that CPU restatement alone (rank 0) and prints the
 same metric; when oracle/_ref holds the reference's own GPU filter (built from
@@ -76,6 +78,7 @@ def parse_args():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--sweep-ticks", type=int, default=1000)
     ap.add_argument("--no-config1", action="store_true")
+    ap.add_argument("--no-extensions", action="store_true")
     ap.add_argument("--bgrad-filters", type=int, default=256)
     ap.add_argument("--bgrad-ticks", type=int, default=4000)
     return ap.parse_args()
@@ -275,6 +278,136 @@ def bench_sweep(dev, args, lib, rank, world, barrier):
         f.close()
     return {"ticks": T, "ess_threshold": args.ess, "points": out,
             "note": "device-resident CUDA-graph runs, CUDA events; hbm_frac of the measured copy peak"}
+
+
+def bench_extensions(dev, args, lib, rank):
+    """The rows beyond the plain tick, each timed on its own workload (rank 0, one GPU):
+      student_t  the plain filter with Student-t state noise (nu_state=5) and observations (nu_obs=5),
+                 N=2^24, the first --sweep-ticks ticks of the headline series, device-resident graph
+      learning   online mu learning (K=50, rho too) on the same N=2^24 run: the host update every K ticks
+                 forces tick-by-tick launches; against the same run without learning, stepped the same way
+      apf        the auxiliary particle filter (two resampling stages per tick), N=2^24 and N=4096,
+                 gpu_apf_step_many with host buffers
+      imm        8 SV models x 4096 particles, 1000 ticks through gpu_imm_step (one host round trip per
+                 tick, as the reference's API)
+      smc2       256 theta-particles x 512 state particles, 500 updates of gpu_bpf_smc2_update with one
+                 PMMH move per outer resample
+    CUDA events on the filters' streams where the work is device-resident, else wall clock around
+    synchronised calls."""
+    if rank != 0:
+        return None
+    import numpy as np
+    import torch
+    import gpubpf
+    from gpubpf import dgp
+    out = {}
+    T = args.sweep_ticks
+    N = 1 << 24
+    _, ys = dgp.matched_series(5000, RHO, SIG, MU, args.dgp_seed)
+    y_host = np.asarray(ys[:T], dtype=np.float32)
+    y = torch.tensor(y_host, device=dev)
+    rec = torch.zeros(T * RECORD_BYTES, dtype=torch.uint8, device=dev)
+
+    def timed_device(f, seed0):
+        fs = torch.cuda.ExternalStream(f.state.stream, device=dev)
+        for w in range(3):
+            f.reset(seed0 + w)
+            f.step_many_device(y.data_ptr(), T, rec.data_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, args.steps)
+        e0.record(fs)
+        for k in range(reps):
+            f.reset(seed0 + 10 + k)
+            f.step_many_device(y.data_ptr(), T, rec.data_ptr())
+        e1.record(fs)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    # Student-t state noise and observations vs Gaussian, same N and series
+    g = gpubpf.GpuBpf(N, RHO, SIG, MU, 0.0, 0.0, 7, ess_threshold=args.ess)
+    ms_g = timed_device(g, 100)
+    g.close()
+    t = gpubpf.GpuBpf(N, RHO, SIG, MU, 5.0, 5.0, 7, ess_threshold=args.ess)
+    ms_t = timed_device(t, 100)
+    t.close()
+    out["student_t"] = {"workload": f"N={N}, first {T} ticks, ESS<{args.ess}N, nu_state=5, nu_obs=5",
+                        "us_per_tick": ms_t / T * 1e3, "particle_steps_per_s": N * T / (ms_t / 1e3),
+                        "gaussian_us_per_tick": ms_g / T * 1e3, "cost_vs_gaussian": ms_t / ms_g}
+
+    # online learning: tick-by-tick stepping with and without the score sums and updates
+    Tl = min(T, 500)
+
+    def timed_host(f, learn):
+        if learn:
+            f.enable_mu_learning(1, 50, 0.1, 10.0, 0.667)
+            f.enable_rho_learning(True)
+        f.step_many(y_host[:8].tolist())
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        f.step_many(y_host[8:8 + Tl].tolist())
+        torch.cuda.synchronize(dev)
+        return (time.perf_counter() - t0) * 1e3
+    a = gpubpf.GpuBpf(N, RHO, SIG, 0.0, 0.0, 0.0, 7, ess_threshold=args.ess)
+    ms_l = timed_host(a, True)
+    mu_end = a.get_mu()
+    a.close()
+    b = gpubpf.GpuBpf(N, RHO, SIG, 0.0, 0.0, 0.0, 7, ess_threshold=args.ess)
+    ms_nl = timed_host(b, False)
+    b.close()
+    out["learning"] = {"workload": f"N={N}, {Tl} ticks stepped with gpu_bpf_step_many (host buffers), mu and rho "
+                                   f"learning from mu=0, K=50 (tick-by-tick launches), against the same call "
+                                   f"without learning (64-tick CUDA graphs)",
+                       "us_per_tick": ms_l / Tl * 1e3, "us_per_tick_without": ms_nl / Tl * 1e3,
+                       "overhead": ms_l / ms_nl, "mu_after": mu_end}
+
+    # auxiliary particle filter
+    apf = {}
+    y_all = np.asarray(ys, dtype=np.float32)
+    for n_apf, t_apf in ((N, 300), (4096, 1000)):
+        f = gpubpf.GpuApf(n_apf, RHO, SIG, MU, 0.0, 0.0, 42)
+        f.step_many(y_all[:64].tolist())
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        f.step_many(y_all[64:64 + t_apf].tolist())
+        torch.cuda.synchronize(dev)
+        ms = (time.perf_counter() - t0) * 1e3
+        f.close()
+        apf[str(n_apf)] = {"ticks": t_apf, "us_per_tick": ms / t_apf * 1e3,
+                           "particle_steps_per_s": n_apf * t_apf / (ms / 1e3)}
+    out["apf"] = {"workload": "gpu_apf_step_many (host buffers), ticks 64.. of the headline series after 64 "
+                              "warm-up ticks, two resampling stages per tick", "points": apf}
+
+    # IMM
+    grid = gpubpf.build_grid([0.95, 0.97], [0.1, 0.2], [-1.5, -1.0])
+    imm = gpubpf.Imm(grid, 4096, seed=3)
+    _, yi = dgp.matched_series(1064, RHO, SIG, MU, 42)
+    for v in yi[:64]:
+        imm.step(float(v))
+    t0 = time.perf_counter()
+    for v in yi[64:]:
+        imm.step(float(v))
+    ms = (time.perf_counter() - t0) * 1e3
+    imm.close()
+    out["imm"] = {"workload": f"{len(grid)} models x 4096 particles, 1000 ticks of gpu_imm_step",
+                  "us_per_tick": ms, "particle_steps_per_s": len(grid) * 4096 * 1000 / (ms / 1e3)}
+
+    # SMC^2
+    s2 = gpubpf.Smc2(256, 512, 600, seed=5)
+    s2.set_moves(1, 0.5, 1.0)
+    _, y2 = dgp.matched_series(600, RHO, SIG, MU, 11)
+    for v in y2[:50]:
+        s2.update(float(v))
+    t0 = time.perf_counter()
+    for v in y2[50:550]:
+        s2.update(float(v))
+    ms = (time.perf_counter() - t0) * 1e3
+    mean, sd = s2.theta()
+    st = s2.stats()
+    s2.close()
+    out["smc2"] = {"workload": "256 theta x 512 particles, 500 updates (after 50), one PMMH move per outer resample",
+                   "us_per_update": ms / 500 * 1e3, "theta_mean": [float(v) for v in mean],
+                   "theta_sd": [float(v) for v in sd], "stats": st}
+    return out
 
 
 def bench_config1(dev, args, lib, rank):
@@ -552,6 +685,11 @@ def reference_gpu(args, y):
     c1 = timed(4096, np.asarray(y1, dtype=np.float32), 0.0, 3, 1)
     out["config1"] = {"us_per_tick": c1["us_per_tick"], "value": c1["value"], "unit": c1["unit"],
                       "workload": "N=4096, T=1000, always resample, DGP seed 42"}
+    # the reference's auxiliary particle filter (gpu_apf_step), same points as the extensions section
+    _, ya = dgp.matched_series(1064, RHO, SIG, MU, args.dgp_seed)
+    ya = np.asarray(ya, dtype=np.float32)
+    out["apf"] = {str(n): {"ticks": t, "us_per_tick": refgpu.apf_time(n, RHO, SIG, MU, ya[:64 + t]) * 1e3}
+                  for n, t in ((args.n, 300), (4096, 1000))}
     return out
 
 
@@ -697,6 +835,7 @@ def main():
     batched = None if args.no_batched else bench_batched(dev, args, lib, rank, world, barrier)
     gradient = None if args.no_gradient else bench_gradient(dev, args, lib, rank, world, barrier)
     batch_gradient = None if args.no_batch_gradient else bench_batch_gradient(dev, args, lib, rank, world, barrier)
+    extensions = None if (args.no_extensions or world > 1) else bench_extensions(dev, args, lib, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -725,6 +864,7 @@ def main():
             "batched": batched,
             "gradient": gradient,
             "batch_gradient": batch_gradient,
+            "extensions": extensions,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

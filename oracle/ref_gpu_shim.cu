@@ -129,4 +129,15 @@ int refgpu_apf_run(void* sv, const float* y, int T, float* h_mean, float* log_li
   return (int)cudaGetLastError();
 }
 
+// Wall time in milliseconds of T reference APF ticks (gpu_apf_step, synchronous per tick).
+double refgpu_apf_time(void* sv, const float* y, int T) {
+  GpuApfState* s = static_cast<GpuApfState*>(sv);
+  cudaStreamSynchronize(s->stream);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int t = 0; t < T; ++t) gpu_apf_step(s, y[t]);
+  cudaStreamSynchronize(s->stream);
+  const auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
 }  // extern "C"

@@ -41,6 +41,8 @@ def lib() -> C.CDLL:
         L.refgpu_apf_create.restype = vp
         L.refgpu_apf_create.argtypes = [i32, f32, f32, f32, f32, f32, i32]
         L.refgpu_apf_destroy.argtypes = [vp]
+        L.refgpu_apf_time.restype = f64
+        L.refgpu_apf_time.argtypes = [vp, vp, i32]
         L.refgpu_apf_run.restype = i32
         L.refgpu_apf_run.argtypes = [vp, vp, i32, vp, vp]
         for name in ("refgpu_copy_rng", "refgpu_copy_h", "refgpu_copy_h2", "refgpu_copy_w"):
@@ -130,5 +132,21 @@ def apf_run(n, rho, sigma_z, mu, y, nu_state=0.0, nu_obs=0.0, seed=42):
         if rc != 0:
             raise RuntimeError(f"reference APF loop failed (CUDA error {rc})")
         return hm, ll
+    finally:
+        L.refgpu_apf_destroy(s)
+
+
+def apf_time(n, rho, sigma_z, mu, y, warmup=64, seed=42):
+    """Milliseconds per tick of the reference's APF over y[warmup:], after `warmup` untimed ticks."""
+    L = lib()
+    s = L.refgpu_apf_create(int(n), rho, sigma_z, mu, 0.0, 0.0, int(seed))
+    if not s:
+        raise RuntimeError("reference gpu_apf_create failed")
+    try:
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        L.refgpu_apf_time(s, _p(y[:warmup]), int(warmup))
+        rest = np.ascontiguousarray(y[warmup:])
+        ms = L.refgpu_apf_time(s, _p(rest), int(rest.shape[0]))
+        return ms / rest.shape[0]
     finally:
         L.refgpu_apf_destroy(s)
