@@ -122,7 +122,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
           }
           // same operation sequence as the plain filter's pass 1 (bit-identical x)
           float x = gauss ? obs_log2pdf_gauss_plus(y2, h, kGaussLog2C + coff)
-                          : __fmul_rn(obs_logpdf(obs, h), kLog2e) + coff;
+                          : obs_log2pdf_t_plus(obs, __fmul_rn(y2, obs.inv_nu), h, __fmul_rn(obs.c_obs, kLog2e) + coff);
           if (carry) x += Wt[si];                  // carried tile-relative log2-weight
           Wt[si] = x;
           m = fmaxf(m, x);
@@ -481,7 +481,7 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
           x = obs_log2pdf_gauss(y2, h);
           g = 0.5f * fmaf(y2, ex2_approx(h * -kLog2e), -1.0f);
         } else {
-          x = __fmul_rn(obs_logpdf(obs, h), kLog2e);
+          x = obs_log2pdf_t_plus(obs, __fmul_rn(y2, obs.inv_nu), h, __fmul_rn(obs.c_obs, kLog2e));
           const float q = y2 * ex2_approx(h * -kLog2e) * obs.inv_nu;
           g = fmaf(obs.nu_p1h, div_approx(q, 1.0f + q), -0.5f);
         }

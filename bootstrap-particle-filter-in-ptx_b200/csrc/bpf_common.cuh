@@ -203,6 +203,15 @@ __device__ __forceinline__ float obs_log2pdf_gauss(float y2, float h) {
 // so the fixed-point masses agree bit for bit.
 __device__ __forceinline__ float tile_weight(float d) { return fminf(ex2_approx(d), 1.0f); }
 
+// log2 p(y | h) for the Student-t model, from y2nu = y^2 / nu and
+// c = log2(e) c_obs (+ any offset):
+//   c - (nu+1)/2 log2(1 + y^2 e^{-h} / nu) - log2(e) h / 2
+__device__ __forceinline__ float obs_log2pdf_t_plus(const ObsModel& m, float y2nu, float h, float c) {
+  const float e = ex2_approx(h * -kLog2e);                       // e^{-h}
+  const float t = (y2nu > 0.0f) ? fmaf(y2nu, e, 1.0f) : 1.0f;
+  return fmaf(-m.nu_p1h, lg2_approx(t), fmaf(-0.5f * kLog2e, h, c));
+}
+
 __device__ __forceinline__ float obs_logpdf(const ObsModel& m, float h) {
   const float e = ex2_approx(h * -0.5f * kLog2e);   // exp(-h/2)
   const float eta = m.y * e;
@@ -240,6 +249,26 @@ __device__ __forceinline__ float tstate_scale(const PcgTick& pc, uint32_t i, int
   float chi2 = (-2.0f * kLn2) * l2sum;
   if (nu_int & 1) {
     const float z = icdf_normal(pcg_uniform(pcg_output(pc.k1 + pc.k2 * tstate_inc(i, pairs))));
+    chi2 = fmaf(z, z, chi2);
+  }
+  return sqrt_approx(div_approx(nu_state, chi2));
+}
+
+// The same scale from slot i's own stream state s = k1 + k2 inc_i of the tick
+// (component c's increment is inc_i + (c+1) 2^33, so its state is
+// s + (c+1) k33 with k33 = k2 2^33): no 64-bit multiply per component. For a
+// full, convergent warp (the odd component's normal uses the warp-vote form).
+// Values are identical to tstate_scale.
+__device__ __forceinline__ float tstate_scale_warp(uint64_t s, uint64_t k33, int nu_int, float nu_state) {
+  const int pairs = nu_int >> 1;
+  float l2sum = 0.0f;
+  for (int c = 0; c < pairs; ++c) {
+    s += k33;
+    l2sum += lg2_approx(pcg_uniform(pcg_output(s)));
+  }
+  float chi2 = (-2.0f * kLn2) * l2sum;
+  if (nu_int & 1) {
+    const float z = icdf_normal_warp(pcg_uniform(pcg_output(s + k33)));
     chi2 = fmaf(z, z, chi2);
   }
   return sqrt_approx(div_approx(nu_state, chi2));

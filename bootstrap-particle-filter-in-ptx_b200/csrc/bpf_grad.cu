@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_adjoint_kernel(GradAdjArgs 
         x = obs_log2pdf_gauss(y2, h);
         g = 0.5f * fmaf(y2, ex2_approx(h * -kLog2e), -1.0f);          // -1/2 + y^2 e^{-h}/2
       } else {
-        x = __fmul_rn(obs_logpdf(obs, h), kLog2e);
+        x = obs_log2pdf_t_plus(obs, __fmul_rn(y2, obs.inv_nu), h, __fmul_rn(obs.c_obs, kLog2e));
         const float q = y2 * ex2_approx(h * -kLog2e) * obs.inv_nu;     // y^2 e^{-h} / nu
         g = fmaf(obs.nu_p1h, div_approx(q, 1.0f + q), -0.5f);
       }

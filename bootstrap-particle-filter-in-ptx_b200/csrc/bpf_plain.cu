@@ -110,7 +110,10 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     const int nkp = p.nexp[k];
     carry_off = (nkp == kNkEmpty) ? -INFINITY : (float)(nkp - nM_prev);
   }
-  const float gauss_c = kGaussLog2C + carry_off;   // the carry offset folded into the Gaussian constant
+  const float gauss_c = kGaussLog2C + carry_off;   // the carry offset folded into the density's constant
+  const float t_c0 = __fmul_rn(obs.c_obs, kLog2e);
+  const float t_c = t_c0 + carry_off;
+  const float y2nu = __fmul_rn(y2, obs.inv_nu);
 
   const int tile0 = k * kTile;
   const bool full = tile0 + kTile <= p.N;      // every slot of the tile holds a particle
@@ -130,6 +133,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   float x[kPerThread], hv[kPerThread];
   float hpv[LEARN ? kPerThread : 1];     // particles before this tick's propagation (learning only)
   const unsigned long long step2 = 2ull * c.k2;
+  const unsigned long long k33 = c.k2 << 33;          // Student-t component streams (tstate_scale_warp)
   // state of the first particle of group r + 1 from the state after group r's
   // four draws: inc advances by 2 * 4 * kThreads slots
   const unsigned long long group_step = (unsigned long long)(2 * 4 * kThreads - 8) * c.k2;
@@ -153,21 +157,20 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
       if (APF == 0) {
         if (PROP) {
           float z = icdf_normal_warp(pcg_uniform(pcg_output(s)));
-          if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
+          if (TSTATE) z *= tstate_scale_warp(s, k33, a.nu_int, a.nu_state);
           h = propagate(h, a.mu, a.rho, a.sigma, z);
         }
-        xx = gauss ? obs_log2pdf_gauss_plus(y2, h, gauss_c)
-                   : __fmul_rn(obs_logpdf(obs, h), kLog2e) + carry_off;
+        xx = gauss ? obs_log2pdf_gauss_plus(y2, h, gauss_c) : obs_log2pdf_t_plus(obs, y2nu, h, t_c);
       } else {
         const float m = propagate_mean(h, a.mu, a.rho);
-        const float lm = gauss ? obs_log2pdf_gauss(y2, m) : __fmul_rn(obs_logpdf(obs, m), kLog2e);
+        const float lm = gauss ? obs_log2pdf_gauss(y2, m) : obs_log2pdf_t_plus(obs, y2nu, m, t_c0);
         if (APF == 1) {
           xx = lm;
         } else {
           float z = icdf_normal_warp(pcg_uniform(pcg_output(s)));
-          if (TSTATE) z *= tstate_scale(c, (uint32_t)(i0 + e), a.nu_int, a.nu_state);
+          if (TSTATE) z *= tstate_scale_warp(s, k33, a.nu_int, a.nu_state);
           h = fmaf(a.sigma, z, m);
-          xx = (gauss ? obs_log2pdf_gauss(y2, h) : __fmul_rn(obs_logpdf(obs, h), kLog2e)) - lm;
+          xx = (gauss ? obs_log2pdf_gauss(y2, h) : obs_log2pdf_t_plus(obs, y2nu, h, t_c0)) - lm;
         }
       }
       s += step2;
