@@ -530,7 +530,8 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   int n_items_total;
   const int it0 = block_excl_scan_add<kPlanThreads>(n_it, &n_items_total, sh.scan_i);
 
-  // 6. work items (tile, first output, end output, first item of the tile);
+  // 6. work items (tile, first output, end output, flags: 1 = first item of the
+  //    tile, 2 = the only one, holding all of the tile's outputs);
   //    heavy tiles are split
   int ib = it0;
   for (int k = k0; k < k1; ++k) {
@@ -539,7 +540,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     const int ni = max((o1 - o0 + kOutChunk - 1) / kOutChunk, min_items);
     for (int u = 0; u < ni; ++u) {
       const int oo = o0 + u * kOutChunk;
-      p.items[ib++] = make_int4(k, oo, min(o1, oo + kOutChunk), u == 0);
+      p.items[ib++] = make_int4(k, oo, min(o1, oo + kOutChunk), (u == 0 ? 1 : 0) | (ni == 1 ? 2 : 0));
     }
   }
   if (tid == 0) st->n_items = n_items_total;
@@ -649,16 +650,22 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     const unsigned long long d2 = 2ull * delta, d3 = 3ull * delta, d4 = 4ull * delta;
     int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
     unsigned long long tq = base + (unsigned long long)q * delta;
-    int32_t* csr = (a.csr && item.w) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
-    auto count_children = [&](auto full_tag) {
+    int32_t* csr = (a.csr && (item.w & 1)) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
+    // Compile-time variants: FULL (no element past N in the tile), WHOLE (the
+    // item holds every output of the tile, so each counted child lands in the
+    // window), TAPE (first-child list for the gradient tape).
+    const bool whole = (item.w & 2) != 0;
+    auto count_children = [&](auto full_tag, auto whole_tag, auto tape_tag) {
       constexpr bool FULL = decltype(full_tag)::value;
+      constexpr bool WHOLE = decltype(whole_tag)::value;
+      constexpr bool TAPE = decltype(tape_tag)::value;
       unsigned long long accw = excl;
       float4 f4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
       for (int e = 0; e < kPerThread; ++e) {
         const int j = tid * kPerThread + e;
         const bool in = FULL || j < nA;
-        if (csr && in) csr[j] = q;
+        if (TAPE && in) csr[j] = q;
         if ((e & 3) == 0) f4 = wt[e >> 2];
         const float we = (e & 3) == 0 ? f4.x : (e & 3) == 1 ? f4.y : (e & 3) == 2 ? f4.z : f4.w;
         if (in) accw += fix_weight(tile_weight(we));
@@ -666,16 +673,31 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
         if (in && q < N && cj > tq) {
           const unsigned long long diff = cj - tq;
           const int c = 1 + (diff > delta) + (diff > d2) + (diff > d3);
-          const int q1 = (c == 4 && diff > d4) ? targets_below(cj, base, delta, magic, N) : min(q + c, N);
-          if (q < ob && q1 > oa) marks[max(q, oa) - wa] = (unsigned short)(j + 1);
-          q = q1;
-          tq = base + (unsigned long long)q * delta;
+          if (c == 4 && diff > d4) {
+            const int q1 = targets_below(cj, base, delta, magic, N);
+            if (WHOLE || (q < ob && q1 > oa)) marks[(WHOLE ? q : max(q, oa)) - wa] = (unsigned short)(j + 1);
+            q = q1;
+            tq = base + (unsigned long long)q * delta;
+          } else {
+            const int q1 = min(q + c, N);
+            if (WHOLE || (q < ob && q1 > oa)) marks[(WHOLE ? q : max(q, oa)) - wa] = (unsigned short)(j + 1);
+            q = q1;
+            tq += (unsigned long long)c * delta;
+          }
         }
       }
     };
     if (massive) {
-      if (full) count_children(std::true_type{});
-      else count_children(std::false_type{});
+      if (csr) {
+        if (full) count_children(std::true_type{}, std::false_type{}, std::true_type{});
+        else count_children(std::false_type{}, std::false_type{}, std::true_type{});
+      } else if (whole) {
+        if (full) count_children(std::true_type{}, std::true_type{}, std::false_type{});
+        else count_children(std::false_type{}, std::true_type{}, std::false_type{});
+      } else {
+        if (full) count_children(std::true_type{}, std::false_type{}, std::false_type{});
+        else count_children(std::false_type{}, std::false_type{}, std::false_type{});
+      }
     } else if (csr) {
       for (int e = 0; e < kPerThread; ++e)       // no mass: every element's children start at q
         if (tid * kPerThread + e < nA) csr[tid * kPerThread + e] = q;

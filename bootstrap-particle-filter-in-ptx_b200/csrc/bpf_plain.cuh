@@ -8,7 +8,7 @@
 //   tile records  rec[G] f32x4 {S=sum w, Q=sum w^2, H=sum w h, n_k bits},
 //                 nexp[G] i32 (n_k again), E[G] u64 exact fixed-point mass
 //   P[G] u64 exclusive tile prefix of the fixed-point CDF, ofirst[G+1] i32
-//   items[G + N/12288 + 1] int4 pass-2 work items (tile, first out, end out)
+//   items[G + N/8192 + 1] int4 pass-2 work items (tile, first out, end out, flags)
 //   DevState      scalars carried from tick to tick
 #pragma once
 #include <cstdint>
