@@ -119,16 +119,24 @@ def test_ancestors_bit_exact(bpf, orc, N, thr, T):
     assert len(n_checked) >= 1
 
 
-def test_ancestors_adversarial_ties(bpf, orc):
+@pytest.mark.parametrize("N", [8192, 12388, 40000])
+def test_ancestors_adversarial_ties(bpf, orc, N):
     """A huge outlier observation concentrates the weight on few particles; the
-    resampling must still be bit-exact and every output must land on a particle."""
+    resampling must still be bit-exact and every output must land on a particle.
+    With N > 8192 the heaviest tile owns more outputs than one pass-2 work window,
+    so its outputs are split over several windows and single parents span them."""
     y = np.array([0.1, 0.2, 25.0, -0.3, 0.0, 40.0, 0.05], dtype=np.float32)
+    split = []
 
     def check(w, te, u23, anc):
         np.testing.assert_array_equal(anc, orc.resample_fixed(w, te, u23))
+        counts = np.bincount(anc // 4096, minlength=(N + 4095) // 4096)
+        split.append(int(counts.max()))
 
-    recs, flags, _ = run_recorded(bpf, 8192, y, seed=9, thr=0.0, check_anc=check)
+    recs, flags, _ = run_recorded(bpf, N, y, seed=9, thr=0.0, check_anc=check)
     assert all(math.isfinite(r.dloglik) for r in recs)
+    if N > 8192:
+        assert max(split) > 8192          # the multi-window path ran
 
 
 # ---------------------------------------------------------------------------
