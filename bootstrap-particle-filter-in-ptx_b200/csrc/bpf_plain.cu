@@ -90,8 +90,11 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
 
   griddep_wait();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int k = blockIdx.x;
   const DevState* st = p.st;
+  // Each pass walks the tiles in the order opposite to the previous pass over
+  // the particle arrays, so it starts on the tiles that pass wrote last, still
+  // in L2 (the arrays are rewritten in place every tick).
+  const int k = (st->dirs & 1) ? (p.G - 1 - (int)blockIdx.x) : (int)blockIdx.x;
   const int tick = st->tick;
   const bool carry = APF == 0 && st->resampled_prev == 0;
   const int nM_prev = st->nM_prev;
@@ -428,6 +431,12 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
       r.h_mean = (float)hm; r.ess = (float)ess; r.resampled = resample; r.tick = tick;
       *a.rec = r;
     }
+    {
+      // pass 2 runs opposite to this pass 1; the next pass 1 opposite to the
+      // last pass that wrote the particles (pass 2 on a resampling tick)
+      const int d1 = st->dirs & 1;
+      st->dirs = (resample ? d1 : (d1 ^ 1)) | ((d1 ^ 1) << 1);
+    }
     if (a.apf != 1) {
       st->k1 = st->k1 * kPcgMult;          // next tick's stream constants
       st->k2 = st->k2 * kPcgMult + 1ull;
@@ -586,6 +595,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     return;
   }
   const int n_items = st->n_items;
+  const bool rev = ((st->dirs >> 1) & 1) != 0;     // item order opposite to this tick's pass 1
   const unsigned long long base = st->base, delta = st->delta, magic = st->delta_magic;
   const int nM = st->nM, Fg = st->Fg, N = p.N;
   const int src = st->src;
@@ -597,7 +607,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
   if (tid == 0) {
     s_err = 0;
     mbar_init(&mbar[0], 1);
-    if ((int)blockIdx.x < n_items) pass2_fetch(p, hsrc, blockIdx.x, smem, &mbar[0]);
+    if ((int)blockIdx.x < n_items) pass2_fetch(p, hsrc, rev ? n_items - 1 - (int)blockIdx.x : (int)blockIdx.x, smem, &mbar[0]);
   }
   __syncthreads();
 
@@ -606,7 +616,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
   int n = 0;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x, ++n) {
 
-    const int4 item = p.items[it];
+    const int4 item = p.items[rev ? n_items - 1 - it : it];
     const int k = item.x, oa = item.y, ob = item.z;
     const int wa = oa & ~3;                          // window origin: 16-byte aligned output slot
     const int j0 = k * kTile;
@@ -766,7 +776,10 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       }
     }
     __syncthreads();   // the staged tile is free: fetch the next item's
-    if (tid == 0 && it + (int)gridDim.x < n_items) pass2_fetch(p, hsrc, it + gridDim.x, smem, &mbar[0]);
+    if (tid == 0 && it + (int)gridDim.x < n_items) {
+      const int nx = it + (int)gridDim.x;
+      pass2_fetch(p, hsrc, rev ? n_items - 1 - nx : nx, smem, &mbar[0]);
+    }
   }
   if (tid == 0 && s_err) p.st->error = BPF_ERR_STATE;
   griddep_release();

@@ -41,7 +41,7 @@ struct DevState {
   int      n_items;         // pass-2 work items of the current tick
   uint32_t u23;             // resampling uniform of the current tick
   int      resample_count;
-  int      reserved;
+  int      dirs;            // tile orders (1 = decreasing): bit 0 the next pass 1, bit 1 this tick's pass 2
   int      error;           // sticky BPF_* error code
   int      seed;            // filter seed (PCG32 streams, resampling uniform)
   double   learn[4];        // online learning sums since the last update: sum_t of
