@@ -20,9 +20,12 @@
 //           each element counts the evenly spaced targets it owns and marks
 //           the first of them, a warp max-scan over the marks gives every
 //           output its ancestor, gather of h[ancestor] from a bulk-async
-//           (TMA) copy of the tile, coalesced store. Tiles of the next item
-//           are prefetched into a second buffer. Early exit on ticks that do
-//           not resample.
+//           (TMA) copy of the tile, 16-byte vector stores. Four CTAs per SM,
+//           each staging one item's tiles at a time (the next item's copy is
+//           issued as soon as the buffer is free). Early exit on ticks that
+//           do not resample.
+// Pass 1 and pass 2 walk the tiles (items) in the order opposite to the pass
+// before them, so each starts on the tiles still in L2.
 // Consecutive kernels use programmatic dependent launch: each waits on its
 // predecessor with griddepcontrol.wait and releases its successor after its
 // last store, so launch latency overlaps the predecessor's tail.
