@@ -36,6 +36,7 @@
 #include "bpf_plain.cuh"
 #include "bpf_block.cuh"
 #include <cmath>
+#include <mutex>
 #include <type_traits>
 
 namespace bpf {
@@ -864,13 +865,22 @@ cudaError_t launch_init(const Plan& p, float mu, float std_stat, int seed, cudaS
 
 size_t pass2_smem_bytes() { return kPass2Smem; }
 
+constexpr int kMaxConfiguredDevices = 64;
+
+// Called with `device` current. The shared-memory attributes are set once per
+// device (they belong to the device's context), under a lock so filters
+// created from several threads do not race.
 int pass2_grid_size(int device) {
-  static int configured = -1;
-  if (configured != device) {
-    cudaFuncSetAttribute(pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPass2Smem);
-    cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)plan_smem_bytes(kPlanSmemTiles));
-    configured = device;
+  static std::mutex lock;
+  static bool configured[kMaxConfiguredDevices] = {};
+  {
+    std::lock_guard<std::mutex> guard(lock);
+    if (device < 0 || device >= kMaxConfiguredDevices || !configured[device]) {
+      cudaFuncSetAttribute(pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPass2Smem);
+      cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)plan_smem_bytes(kPlanSmemTiles));
+      if (device >= 0 && device < kMaxConfiguredDevices) configured[device] = true;
+    }
   }
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
