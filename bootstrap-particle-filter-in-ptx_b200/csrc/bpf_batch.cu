@@ -34,6 +34,8 @@ struct BatchShared {
   float tmax[kBatchMaxTiles][NT / 32];
   double sred[3][kBatchMaxTiles][NT / 32];
   unsigned long long ered[kBatchMaxTiles][NT / 32];
+  double tsum[3][kBatchMaxTiles];              // per-tile FP64 sums over the warps
+  unsigned long long tmass[kBatchMaxTiles];
   unsigned long long scan[NT / 32 + 1];
   unsigned long long excl[NT];
   unsigned long long Pk[kBatchMaxTiles];
@@ -168,6 +170,16 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       if (lane == 0) { sh.sred[0][k][warp] = dS; sh.sred[1][k][warp] = dQ; sh.sred[2][k][warp] = dH; sh.ered[k][warp] = E; }
     }
     __syncthreads();
+    // per-tile sums over the warps, one warp per tile (a fixed shuffle tree)
+    for (int k = warp; k < G; k += W) {
+      const bool on = lane < W;
+      const double s1 = warp_sum_d(on ? sh.sred[0][k][lane] : 0.0);
+      const double s2 = warp_sum_d(on ? sh.sred[1][k][lane] : 0.0);
+      const double s3 = warp_sum_d(on ? sh.sred[2][k][lane] : 0.0);
+      const unsigned long long e = warp_sum_u64(on ? sh.ered[k][lane] : 0ull);
+      if (lane == 0) { sh.tsum[0][k] = s1; sh.tsum[1][k] = s2; sh.tsum[2][k] = s3; sh.tmass[k] = e; }
+    }
+    __syncthreads();
 
     // 3. decision (thread 0)
     if (tid == 0) {
@@ -178,10 +190,9 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       for (int k = 0; k < kBatchMaxTiles; ++k) {
         Ek[k] = 0ull;
         if (k >= G || nk[k] == kNkEmpty) continue;
-        double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        for (int w = 0; w < W; ++w) { s1 += sh.sred[0][k][w]; s2 += sh.sred[1][k][w]; s3 += sh.sred[2][k][w]; Ek[k] += sh.ered[k][w]; }
+        Ek[k] = sh.tmass[k];
         const double sc = pow2d(nk[k] - nM);
-        S += s1 * sc; Q += s2 * sc * sc; Hm += s3 * sc;
+        S += sh.tsum[0][k] * sc; Q += sh.tsum[1][k] * sc * sc; Hm += sh.tsum[2][k] * sc;
       }
       const bool degenerate = (nM == kNkEmpty) || !(S > 0.0);
       double dll;
