@@ -8,7 +8,7 @@ directory is not importable by its hyphenated parent name; put
 from ._lib import BpfError, BpfResult, BpfTickRecord, LIB_PATH, load  # noqa: F401
 from .filter import GpuBpf, debug_normals, debug_pcg32, run_rmse  # noqa: F401
 from .batch import GpuBpfBatch  # noqa: F401
-from .grad import BpfLoglik, GradTape, ancestors_from_children, bpf_loglik  # noqa: F401
+from .grad import BpfBatchLoglik, BpfLoglik, GradTape, ancestors_from_children, bpf_batch_loglik, bpf_loglik  # noqa: F401
 from .imm import Imm, build_grid  # noqa: F401
 from .apf import GpuApf, apf_run_rmse  # noqa: F401
 from .smc2 import Smc2  # noqa: F401

@@ -43,6 +43,20 @@ class GpuBpfBatch:
     def stream(self) -> int:
         return self._lib.gpu_bpf_batch_stream(self._h)
 
+    def set_filters(self, filters: Iterable[dict]) -> None:
+        """New (mu, rho, sigma_z, nu_obs, nu_state, seed) for every filter; each n_particles must equal
+        the filter's count at creation (gpu_bpf_batch_set_filters)."""
+        fl = list(filters)
+        if len(fl) != self.n_filters:
+            raise ValueError(f"expected {self.n_filters} filters, got {len(fl)}")
+        arr = (BpfBatchFilter * len(fl))()
+        for i, f in enumerate(fl):
+            arr[i] = BpfBatchFilter(float(f["mu"]), float(f["rho"]), float(f["sigma_z"]),
+                                    float(f.get("nu_obs", 0.0)), int(f["n_particles"]), int(f["seed"]),
+                                    float(f.get("nu_state", 0.0)))
+        check(self._lib.gpu_bpf_batch_set_filters(self._h, arr), "gpu_bpf_batch_set_filters")
+        self.filters = fl
+
     def set_threads(self, size_class: int, threads: int) -> None:
         check(self._lib.gpu_bpf_batch_set_threads(self._h, int(size_class), int(threads)), "gpu_bpf_batch_set_threads")
 

@@ -204,3 +204,67 @@ def bpf_loglik(theta: torch.Tensor, y: torch.Tensor, n_particles: int, seed: int
             tape = GradTape(n_particles, int(y.shape[0]), checkpoint_every, device=dev)
             _TAPES[key] = tape
     return BpfLoglik.apply(theta, y, tape, int(seed), float(nu_obs))
+
+
+class BpfBatchLoglik(torch.autograd.Function):
+    """loglik[B] = BpfBatchLoglik.apply(theta[B, 3], y[T], batch); backward: the batched adjoint.
+
+    theta[b] = (mu, rho, sigma_z) of filter b of `batch` (a GpuBpfBatch that resamples every tick;
+    its particle counts, seeds and observation models are kept). One gpu_bpf_batch_grad_run gives
+    every filter's FP64 total log-likelihood and d loglik / d theta with the resampling ancestors
+    held fixed (tests/diff_bpf.py:35-56 semantics), so backward only scales the stored gradient.
+    """
+
+    @staticmethod
+    def forward(ctx, theta, y, batch):
+        th = theta.detach().to("cpu", torch.float64)
+        if th.dim() != 2 or th.shape[1] != 3 or th.shape[0] != batch.n_filters:
+            raise ValueError(f"theta must have shape [{batch.n_filters}, 3]")
+        batch.set_filters([dict(f, mu=float(m), rho=float(r), sigma_z=float(sg))
+                           for f, (m, r, sg) in zip(batch.filters, th.tolist())])
+        dev = y.device if y.is_cuda else torch.device("cuda", torch.cuda.current_device())
+        y_d = y.detach().to(dev, torch.float32).contiguous()
+        ll = torch.empty(batch.n_filters, dtype=torch.float64, device=dev)
+        g = torch.empty(batch.n_filters, 3, dtype=torch.float64, device=dev)
+        bs = torch.cuda.ExternalStream(batch.stream, device=dev)
+        cur = torch.cuda.current_stream(dev)
+        bs.wait_stream(cur)                       # inputs and outputs are ready before the run
+        batch.grad_run(y_d.data_ptr(), int(y_d.shape[0]), ll.data_ptr(), g.data_ptr())
+        cur.wait_stream(bs)                       # results are ready for the caller's stream
+        y_d.record_stream(bs); ll.record_stream(bs); g.record_stream(bs)
+        ctx.save_for_backward(g)
+        ctx.theta_meta = (theta.dtype, theta.device)
+        return ll
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (g,) = ctx.saved_tensors
+        dtype, device = ctx.theta_meta
+        return (grad_out.to(g.dtype)[:, None] * g).to(device=device, dtype=dtype), None, None
+
+
+_BATCHES: dict = {}
+
+
+def bpf_batch_loglik(theta: torch.Tensor, y: torch.Tensor, n_particles: Sequence[int],
+                     seeds: Optional[Sequence[int]] = None, nu_obs: float = 0.0) -> torch.Tensor:
+    """Differentiable FP64 total log-likelihoods loglik[B] of B plain filters at theta[B, 3] =
+    (mu, rho, sigma_z), filter b with n_particles[b] (<= 16384) particles and seed seeds[b]
+    (default 42 + b), resampling every tick. The batch is created on first use for
+    (device, n_particles, seeds, nu_obs) and reused."""
+    n = [int(v) for v in n_particles]
+    sd = [42 + b for b in range(len(n))] if seeds is None else [int(v) for v in seeds]
+    if len(sd) != len(n) or theta.shape[0] != len(n):
+        raise ValueError("theta, n_particles and seeds must have the same length")
+    dev = y.device if y.is_cuda else torch.device("cuda", torch.cuda.current_device())
+    key = (str(dev), tuple(n), tuple(sd), float(nu_obs))
+    batch = _BATCHES.get(key)
+    if batch is None:
+        from .batch import GpuBpfBatch
+        th = theta.detach().to("cpu", torch.float64).tolist()
+        with torch.cuda.device(dev):
+            batch = GpuBpfBatch([{"mu": m, "rho": r, "sigma_z": s, "nu_obs": nu_obs, "n_particles": k, "seed": q}
+                                 for (m, r, s), k, q in zip(th, n, sd)], ess_threshold=0.0)
+        _BATCHES[key] = batch
+    return BpfBatchLoglik.apply(theta, y, batch)
+
