@@ -273,11 +273,17 @@ def bench_sweep(dev, args, lib, rank, world, barrier):
         carry = np.zeros(T)
         carry[1:] = 1 - res[:-1]
         bytes_run = float(N) * float(np.sum(12 + 4 * carry + 12 * res))
-        out.append({"n_particles": N, "us_per_tick": ms / T * 1e3, "particle_steps_per_s": world * N * T / (ms / 1e3),
-                    "resample_rate": float(res.mean()), "hbm_frac": bytes_run / (ms / 1e3) / 1e9 / peak})
+        point = {"n_particles": N, "us_per_tick": ms / T * 1e3, "particle_steps_per_s": world * N * T / (ms / 1e3),
+                 "resample_rate": float(res.mean()), "hbm_frac": bytes_run / (ms / 1e3) / 1e9 / peak}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and N <= (1 << 22):
+            cb = cpu_baseline(N, np.asarray(ys[:T], dtype=np.float32), args.ess, 2.0)
+            point["cpu_all_cores_us_per_tick"] = cb["us_per_tick"]
+        out.append(point)
         f.close()
     return {"ticks": T, "ess_threshold": args.ess, "points": out,
-            "note": "device-resident CUDA-graph runs, CUDA events; hbm_frac of the measured copy peak"}
+            "note": "device-resident CUDA-graph runs, CUDA events; hbm_frac of the measured copy peak; "
+                    "cpu_all_cores_us_per_tick: the FP32 restatement of the reference tick loop on all host "
+                    "cores, about 2 s of ticks from the start of the same series (N <= 2^22)"}
 
 
 def bench_extensions(dev, args, lib, rank):
