@@ -46,11 +46,51 @@ struct BatchShared {
   double gred[5][NT / 32];
 };
 
-size_t batch_smem_bytes(int maxn) { return (size_t)maxn * 8 + (((size_t)maxn * 2 + 15) / 16) * 16; }
+size_t batch_smem_bytes(int maxn, bool sort_perm) {
+  const size_t u16 = (((size_t)maxn * 2 + 15) / 16) * 16;
+  return (size_t)maxn * 8 + u16 + (sort_perm ? u16 : 0);
+}
 
-template <int NT, bool RESUMABLE>
+// Sorts the particles H (keys) with their log2-weights Wt, and perm when given, into ascending
+// order of H: a bitonic network whose comparators all put the smaller key at the lower index
+// (the first step of every merge compares mirrored positions), so positions n..2^k-1 act as
+// +inf and are never touched. Deterministic for equal keys. Ends with a barrier.
+template <int NT>
+__device__ void sort_particles(float* H, float* Wt, unsigned short* perm, int n) {
+  int m = 1;
+  while (m < n) m <<= 1;
+  for (int k = 2; k <= m; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int p = threadIdx.x; p < (m >> 1); p += NT) {
+        const int off = p & (j - 1);
+        const int i = ((p - off) << 1) + off;
+        const int l = (j == (k >> 1)) ? i + (k - 1 - 2 * off) : i + j;
+        if (l < n) {
+          const int si = swz(i), sl = swz(l);
+          const float a = H[si], c = H[sl];
+          if (a > c) {
+            H[si] = c; H[sl] = a;
+            const float wa = Wt[si];
+            Wt[si] = Wt[sl]; Wt[sl] = wa;
+            if (perm) { const unsigned short q = perm[i]; perm[i] = perm[l]; perm[l] = q; }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Resampling uniform of a correlated-noise tick: the 23-bit grid point below Phi(v).
+__device__ __forceinline__ unsigned long long u23_of_normal(float v) {
+  return (unsigned long long)fminf(floorf(normcdff(v) * 8388608.0f), 8388607.0f);
+}
+
+// NOISE: a correlated-noise run (BatchArgs::nz_out set); the other instances carry none of its code.
+template <int NT, bool RESUMABLE, bool NOISE = false>
 __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, int b, float* bufA, float* bufB,
-                                 unsigned short* marks, BatchShared<NT>& sh, int maxn) {
+                                 unsigned short* marks, BatchShared<NT>& sh, int maxn,
+                                 unsigned short* perm = nullptr) {
   constexpr int W = NT / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int N = f.n;
@@ -60,6 +100,12 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
   obs.y = 0.0f; obs.nu = f.nu; obs.c_obs = f.c_obs; obs.inv_nu = f.inv_nu; obs.nu_p1h = f.nu_p1h;
   int chunk = 1;
   while (chunk * NT < N) chunk <<= 1;           // power of two: chunks never straddle a tile
+  // correlated-noise areas of this filter (null outside correlated-noise runs)
+  const int nzs = batch_noise_stride(N), npad = nzs - 4;
+  float* zo = NOISE ? a.nz_out + a.nz_out_off[b] : nullptr;
+  const float* zi = (NOISE && a.nz_in) ? a.nz_in + a.nz_in_off[b] : nullptr;
+  const float cr = a.cp_rho, cs = a.cp_scale;
+  if (!NOISE) perm = nullptr;
 
   float* H = bufA;
   float* Wt = bufB;
@@ -89,7 +135,12 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
     const PcgTick c = pcg_tick_consts(f.seed, 1ull, 0ull);
     for (int i = tid; i < N; i += NT) {
       const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
-      bufA[swz(i)] = fmaf(f.std_stat, icdf_normal(pcg_uniform(pcg_output(s))), f.mu);
+      float z = icdf_normal(pcg_uniform(pcg_output(s)));
+      if constexpr (NOISE) {
+        if (zi) z = fmaf(cr, zi[i], cs * z);
+        zo[i] = z;
+      }
+      bufA[swz(i)] = fmaf(f.std_stat, z, f.mu);
     }
     if (tid == 0) sh.carry = 0;
   }
@@ -119,6 +170,10 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
             const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
             float z = icdf_normal(pcg_uniform(pcg_output(s)));
             if (f.nu_int > 0) z *= tstate_scale(c, (uint32_t)i, f.nu_int, f.nu_state);
+            if constexpr (NOISE) {
+              if (zi) z = fmaf(cr, zi[(size_t)t * nzs + i], cs * z);
+              zo[(size_t)t * nzs + i] = z;
+            }
             h = propagate(h, f.mu, f.rho, f.sigma, z);
             H[si] = h;
           }
@@ -212,10 +267,20 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
         a.g_norm[t] = degenerate ? make_float2(0.0f, 0.0f) : make_float2((float)(1.0 / S), __int_as_float(nM));
       if (a.dll) a.dll[(size_t)b * a.T + (t - t0)] = dll;
       if (a.hmean) a.hmean[(size_t)b * a.T + (t - t0)] = hm;
+      unsigned long long u = 0ull;
+      if constexpr (NOISE) {
+        // the tick's resampling normal: slot kBatchMaxN of the filter's streams (no particle's)
+        float v = icdf_normal(pcg_uniform(pcg_output(c.k1 + c.k2 * pcg_inc((uint32_t)kBatchMaxN))));
+        if (zi) v = fmaf(cr, zi[(size_t)t * nzs + npad], cs * v);
+        zo[(size_t)t * nzs + npad] = v;
+        u = u23_of_normal(v);
+      }
       if (resample) {
-        const uint64_t old = ustate;
-        ustate = old * kPcgMult + kHostInc;
-        const unsigned long long u = pcg_output(old) >> 9;
+        if constexpr (!NOISE) {
+          const uint64_t old = ustate;
+          ustate = old * kPcgMult + kHostInc;
+          u = pcg_output(old) >> 9;
+        }
         logS_prev = log((double)N);
         ++n_res;
         const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
@@ -248,8 +313,15 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
     Bt = Bt * kPcgMult + 1ull;
     __syncthreads();
 
-    // 4. systematic resampling (fixed-point CDF, same rule as the plain filter)
+    // 4. systematic resampling (fixed-point CDF, same rule as the plain filter); correlated-noise
+    // runs first sort the particles by value (one tile: the log2-weights share one offset)
     if (sh.resample) {
+      if constexpr (NOISE) {
+        if (perm)
+          for (int i = tid; i < N; i += NT) perm[i] = (unsigned short)i;
+        __syncthreads();
+        sort_particles<NT>(H, Wt, perm, N);
+      }
       const unsigned long long base = sh.base, delta = sh.delta, magic = sh.magic;
       const int j0 = tid * chunk, j1 = min(N, j0 + chunk);
       unsigned long long run = 0ull;
@@ -304,7 +376,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       for (int i = tid; i < N; i += NT) {
         const int anc = (int)marks[i] - 1;
         Wt[swz(i)] = H[swz(anc)];
-        if (a.anc) a.anc[((size_t)b * a.T + (t - t0)) * kBatchMaxN + i] = anc;
+        if (a.anc) a.anc[((size_t)b * a.T + (t - t0)) * kBatchMaxN + i] = perm ? (int)perm[anc] : anc;
       }
       __syncthreads();
       float* tmp = H; H = Wt; Wt = tmp;
@@ -332,13 +404,14 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
   __syncthreads();
 }
 
-template <int NT>
+template <int NT, bool NOISE>
 __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_kernel(BatchArgs a, int maxn) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ BatchShared<NT> sh;
   float* bufA = reinterpret_cast<float*>(smem);
   float* bufB = bufA + maxn;
   unsigned short* marks = reinterpret_cast<unsigned short*>(bufB + maxn);
+  unsigned short* perm = (NOISE && a.anc) ? marks + ((maxn + 7) & ~7) : nullptr;
   for (;;) {
     if (threadIdx.x == 0) sh.next = atomicAdd(a.counter, 1);
     __syncthreads();
@@ -347,7 +420,7 @@ __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_ker
     if (idx >= a.n_order) break;
     const int b = a.order[idx];
     const BatchFilterDev f = a.filters[b];
-    batch_run_filter<NT, true>(a, f, b, bufA, bufB, marks, sh, maxn);
+    batch_run_filter<NT, true, NOISE>(a, f, b, bufA, bufB, marks, sh, maxn, perm);
   }
 }
 
@@ -572,6 +645,23 @@ cudaError_t launch_batch_gather(BatchFilterDev* dst_tab, BatchFilterState* dst_s
   return cudaGetLastError();
 }
 
+__global__ void noise_gather_kernel(float* nz, const long long* src_off, const long long* dst_off, long long n4) {
+  const int b = blockIdx.y;
+  const float4* src = reinterpret_cast<const float4*>(nz + src_off[b]);
+  float4* dst = reinterpret_cast<float4*>(nz + dst_off[b]);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+cudaError_t launch_noise_gather(float* nz, const long long* src_off, const long long* dst_off, long long floats,
+                                int B, cudaStream_t s) {
+  if (B <= 0 || floats <= 0) return cudaSuccess;
+  const long long n4 = floats / 4;                 // areas hold whole ticks of a multiple of 4 floats
+  const int gx = (int)((n4 + 255) / 256 < 64 ? (n4 + 255) / 256 : 64);
+  noise_gather_kernel<<<dim3(gx, B), 256, 0, s>>>(nz, src_off, dst_off, n4);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s) {
   batch_advance_kernel<<<1, 1, 0, s>>>(tick, n);
   return cudaGetLastError();
@@ -608,7 +698,10 @@ __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_gra
 // a class is configured, outside any stream capture).
 template <int NT>
 static cudaError_t launch_nt(const BatchArgs& a, int maxn, int grid, cudaStream_t s) {
-  batch_kernel<NT><<<grid, NT, batch_smem_bytes(maxn), s>>>(a, maxn);
+  if (a.nz_out)
+    batch_kernel<NT, true><<<grid, NT, batch_smem_bytes(maxn, a.anc != nullptr), s>>>(a, maxn);
+  else
+    batch_kernel<NT, false><<<grid, NT, batch_smem_bytes(maxn), s>>>(a, maxn);
   return cudaGetLastError();
 }
 
@@ -626,9 +719,11 @@ cudaError_t launch_batch_class(const BatchArgs& a, int threads, int maxn, int gr
 template <int NT>
 static int occ_nt(int maxn) {
   const size_t smem = batch_smem_bytes(maxn);
-  cudaFuncSetAttribute(batch_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(batch_kernel<NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(batch_kernel<NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)batch_smem_bytes(maxn, true));
   int per = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<NT>, NT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<NT, false>, NT, smem);
   return per;
 }
 

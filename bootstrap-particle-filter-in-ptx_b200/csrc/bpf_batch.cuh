@@ -73,10 +73,25 @@ struct BatchArgs {
   float* st_w;                // carried weights of every filter at st_off[b]
   const long long* st_off;    // [B]
   int y_abs;                  // 1: y is indexed by the absolute tick (y[t]) instead of from t0
+  // correlated-noise runs (all null otherwise): the auxiliary noise of filter b is an area at
+  // nz_out + nz_out_off[b] of batch_noise_stride(n) floats per absolute tick: the particles'
+  // standard normals (tick 0: the initial draw), then the normal of the tick's resampling
+  // uniform. With nz_in, noise = cp_rho * (nz_in + nz_in_off[b])[...] + cp_scale * fresh.
+  // Particles are sorted by value before every resampling. One tile (n <= 4096) and Gaussian
+  // state noise only.
+  const float* nz_in;
+  float* nz_out;
+  const long long* nz_in_off; // [B]
+  const long long* nz_out_off;// [B]
+  float cp_rho, cp_scale;
 };
 
-// Dynamic shared memory of the class kernel for filters of at most maxn particles.
-size_t batch_smem_bytes(int maxn);
+// Floats per tick in a correlated-noise area of a filter of n particles.
+__host__ __device__ inline int batch_noise_stride(int n) { return ((n + 3) & ~3) + 4; }
+
+// Dynamic shared memory of the class kernel for filters of at most maxn particles (with
+// sort_perm: plus the sort permutation of correlated-noise runs that record ancestors).
+size_t batch_smem_bytes(int maxn, bool sort_perm = false);
 // Launches the kernel instance with `threads` threads per CTA (64..1024, power of 2).
 cudaError_t launch_batch_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s);
 // CTAs per SM the class kernel can keep resident.
@@ -88,6 +103,10 @@ int batch_occupancy(int threads, int maxn);
 size_t batch_grad_smem_bytes(int maxn);
 cudaError_t launch_batch_grad_class(const BatchArgs& a, int threads, int maxn, int grid, cudaStream_t s);
 int batch_grad_occupancy(int threads, int maxn);
+// Filter j of a correlated-noise buffer takes the first `floats` floats (a multiple of 4) of the
+// area at src_off[j] into the area at dst_off[j] (16-byte aligned areas that do not overlap).
+cudaError_t launch_noise_gather(float* nz, const long long* src_off, const long long* dst_off, long long floats,
+                                int B, cudaStream_t s);
 // Adds n to the device tick counter of resumable runs (one thread).
 cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s);
 // Filter j of dst takes the resumable state and table entry of filter idx[j] of src (every j, or

@@ -35,6 +35,7 @@ void free_batch(GpuBpfBatch* b) {
   cudaFree(b->d_st); cudaFree(b->d_sth); cudaFree(b->d_stw); cudaFree(b->d_stoff); cudaFree(b->d_tick);
   for (int c = 0; c < kClasses; ++c) cudaFree(b->g_tape[c]);
   cudaFree(b->d_AB);
+  cudaFree(b->d_nzoff);
   cudaFree(b->d_filters); cudaFree(b->d_order); cudaFree(b->d_counters);
   cudaFree(b->d_hfinal); cudaFree(b->d_resamples); cudaFree(b->d_loglik); cudaFree(b->d_y);
   for (int c = 0; c < kClasses; ++c) {
@@ -53,8 +54,12 @@ int class_of(int n) {
 }
 
 BatchArgs class_args(GpuBpfBatch* b, int c, const float* y, int T, double* loglik, double* dll, float* hmean,
-                     int32_t* anc, float* particles) {
+                     int32_t* anc, float* particles, const NoiseArgs* nz = nullptr) {
   BatchArgs a{};
+  if (nz && nz->out) {
+    a.nz_in = nz->in; a.nz_out = nz->out; a.nz_in_off = nz->in_off; a.nz_out_off = nz->out_off;
+    a.cp_rho = nz->rho; a.cp_scale = nz->scale;
+  }
   a.filters = b->d_filters;
   a.order = b->d_order + b->class_off[c];
   a.n_order = b->class_cnt[c];
@@ -83,7 +88,7 @@ void configure_classes(GpuBpfBatch* b) {
 // Enqueue one run: zero the work counters, fork the classes (largest first),
 // join them back onto the batch stream.
 cudaError_t enqueue_run(GpuBpfBatch* b, const float* y, int T, double* loglik, double* dll, float* hmean,
-                        int32_t* anc, float* particles, int only_class = -1) {
+                        int32_t* anc, float* particles, int only_class = -1, const NoiseArgs* nz = nullptr) {
   cudaError_t e = cudaMemsetAsync(b->d_counters, 0, kClasses * sizeof(int), b->stream);
   if (e != cudaSuccess) return e;
   e = cudaEventRecord(b->fork, b->stream);
@@ -92,7 +97,7 @@ cudaError_t enqueue_run(GpuBpfBatch* b, const float* y, int T, double* loglik, d
     if (!b->class_cnt[c] || (only_class >= 0 && c != only_class)) continue;
     e = cudaStreamWaitEvent(b->cls_stream[c], b->fork, 0);
     if (e == cudaSuccess)
-      e = launch_batch_class(class_args(b, c, y, T, loglik, dll, hmean, anc, particles), b->threads[c],
+      e = launch_batch_class(class_args(b, c, y, T, loglik, dll, hmean, anc, particles, nz), b->threads[c],
                              kClassMaxN[c], b->grid[c], b->cls_stream[c]);
     if (e == cudaSuccess) e = cudaEventRecord(b->join[c], b->cls_stream[c]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[c], 0);
@@ -209,7 +214,7 @@ cudaError_t enqueue_step(GpuBpfBatch* b, const float* y, int T, double* dll, flo
   if (e != cudaSuccess) return e;
   for (int c = kClasses - 1; c >= 0; --c) {
     if (!b->class_cnt[c]) continue;
-    BatchArgs a = class_args(b, c, y, T, b->d_loglik, dll, hmean, nullptr, nullptr);
+    BatchArgs a = class_args(b, c, y, T, b->d_loglik, dll, hmean, nullptr, nullptr, &b->step_nz);
     a.t0_dev = b->d_tick;
     a.st = b->d_st;
     a.st_h = b->d_sth;
@@ -292,6 +297,13 @@ int batch_set_filters(GpuBpfBatch* b, const BpfBatchFilter* filters) {
   BCK(cudaMemcpyAsync(b->d_filters, tab.data(), (size_t)b->B * sizeof(BatchFilterDev), cudaMemcpyHostToDevice,
                       b->stream));
   BCK(cudaStreamSynchronize(b->stream));   // the host table goes out of scope
+  for (int i = 0; i < b->B; ++i) b->nus_of[i] = filters[i].nu_state;
+  return BPF_OK;
+}
+
+int batch_check_correlated(const GpuBpfBatch* b) {
+  for (int i = 0; i < b->B; ++i)
+    if (b->n_of[i] > kTile || b->nus_of[i] != 0.0f) return bpf_record_error(BPF_ERR_UNSUPPORTED);
   return BPF_OK;
 }
 
@@ -323,6 +335,8 @@ GpuBpfBatch* gpu_bpf_batch_create(const BpfBatchFilter* filters, int n_filters, 
   std::copy(kDefaultThreads, kDefaultThreads + kClasses, b->threads);
   b->n_of.resize(n_filters);
   for (int i = 0; i < n_filters; ++i) b->n_of[i] = tab[i].n;
+  b->nus_of.resize(n_filters);
+  for (int i = 0; i < n_filters; ++i) b->nus_of[i] = filters[i].nu_state;
   // LPT order inside each class: largest N first
   std::vector<int> order(n_filters);
   for (int i = 0; i < n_filters; ++i) order[i] = i;
@@ -455,6 +469,7 @@ static int step_common(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* 
   if (rc) return rc;
   GraphKey k;
   k.y = y_dev; k.T = n_ticks; k.dll = dll_dev; k.hmean = hmean_dev; k.y_abs = y_abs;
+  k.nz = b->step_nz;
   std::copy(b->threads, b->threads + kClasses, k.threads);
   if (!b->sgraph || !(k == b->skey)) {
     if (b->sgraph) { cudaGraphExecDestroy(b->sgraph); b->sgraph = nullptr; }
@@ -548,6 +563,44 @@ int gpu_bpf_batch_run_debug(GpuBpfBatch* b, const float* y_dev, int n_ticks, dou
   int rc = ensure_device_b(b);
   if (rc) return rc;
   BCK(enqueue_run(b, y_dev, n_ticks, loglik_dev, dll_dev, nullptr, anc_dev, particles_dev));
+  bpf_note_launches(kClasses);
+  return BPF_OK;
+}
+
+long long gpu_bpf_batch_noise_offset(GpuBpfBatch* b, int filter, int n_ticks) {
+  if (!b || filter < 0 || filter > b->B || n_ticks <= 0) return -bpf_record_error(BPF_ERR_ARG);
+  long long off = 0;
+  for (int i = 0; i < filter; ++i) off += (long long)n_ticks * batch_noise_stride(b->n_of[i]);
+  return off;
+}
+
+int gpu_bpf_batch_run_correlated(GpuBpfBatch* b, const float* y_dev, int n_ticks, const float* noise_in_dev,
+                                 float* noise_out_dev, float rho, double* loglik_dev, double* dll_dev,
+                                 int32_t* anc_dev) {
+  if (!b) return bpf_record_error(BPF_ERR_STATE);
+  if (n_ticks <= 0 || !y_dev || !loglik_dev || !noise_out_dev || noise_in_dev == noise_out_dev ||
+      !(rho >= 0.0f && rho <= 1.0f))
+    return bpf_record_error(BPF_ERR_ARG);
+  int rc = batch_check_correlated(b);
+  if (rc) return rc;
+  rc = ensure_device_b(b);
+  if (rc) return rc;
+  if (b->nz_T != n_ticks) {
+    BCK(cudaStreamSynchronize(b->stream));           // the old offsets may be in use
+    std::vector<long long> off(b->B);
+    for (int i = 0; i < b->B; ++i) off[i] = gpu_bpf_batch_noise_offset(b, i, n_ticks);
+    if (!b->d_nzoff) BCK(cudaMalloc(&b->d_nzoff, (size_t)b->B * sizeof(long long)));
+    BCK(cudaMemcpy(b->d_nzoff, off.data(), (size_t)b->B * sizeof(long long), cudaMemcpyHostToDevice));
+    b->nz_T = n_ticks;
+  }
+  NoiseArgs nz;
+  nz.in = noise_in_dev;
+  nz.out = noise_out_dev;
+  nz.in_off = b->d_nzoff;
+  nz.out_off = b->d_nzoff;
+  nz.rho = rho;
+  nz.scale = sqrtf(fmaxf(0.0f, 1.0f - rho * rho));
+  BCK(enqueue_run(b, y_dev, n_ticks, loglik_dev, dll_dev, nullptr, anc_dev, nullptr, -1, &nz));
   bpf_note_launches(kClasses);
   return BPF_OK;
 }

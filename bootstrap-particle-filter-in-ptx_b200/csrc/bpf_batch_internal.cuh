@@ -26,6 +26,19 @@ constexpr int kThreadChoices[] = {64, 128, 256, 512, 1024};
     }                                                                         \
   } while (0)
 
+// Correlated-noise fields of a run (BatchArgs::nz_*); out == nullptr: none.
+struct NoiseArgs {
+  const float* in = nullptr;
+  float* out = nullptr;
+  const long long* in_off = nullptr;
+  const long long* out_off = nullptr;
+  float rho = 0.0f, scale = 1.0f;
+  bool operator==(const NoiseArgs& o) const {
+    return in == o.in && out == o.out && in_off == o.in_off && out_off == o.out_off && rho == o.rho &&
+           scale == o.scale;
+  }
+};
+
 struct GraphKey {
   const float* y = nullptr;
   int T = 0;
@@ -36,10 +49,11 @@ struct GraphKey {
   int32_t* anc = nullptr;
   float* particles = nullptr;
   int threads[kClasses] = {0, 0, 0, 0, 0};
+  NoiseArgs nz;
   bool operator==(const GraphKey& o) const {
     return y == o.y && T == o.T && y_abs == o.y_abs && loglik == o.loglik && dll == o.dll && hmean == o.hmean &&
            anc == o.anc &&
-           particles == o.particles && std::equal(threads, threads + kClasses, o.threads);
+           particles == o.particles && std::equal(threads, threads + kClasses, o.threads) && nz == o.nz;
   }
 };
 
@@ -70,6 +84,13 @@ struct GpuBpfBatch {
   cudaGraphExec_t graph = nullptr;
   GraphKey key;
   std::vector<int> n_of;      // particle count per filter
+  std::vector<float> nus_of;  // Student-t state noise dof per filter (0 = Gaussian)
+
+  // correlated-noise runs: per-filter area offsets of gpu_bpf_batch_run_correlated (for nz_T
+  // ticks), and the noise fields resumable steps run with (NoiseArgs::out null: none)
+  long long* d_nzoff = nullptr;
+  int nz_T = 0;
+  NoiseArgs step_nz;
 
   // gradient runs: per-class tape for the class's CTA slots, PCG jump table, graph
   unsigned char* g_tape[kClasses] = {};
@@ -101,3 +122,5 @@ int batch_step_abs(GpuBpfBatch* b, const float* y_base, int n, double* dll_dev);
 int batch_set_tick(GpuBpfBatch* b, int tick);
 // Replace every filter's parameters and seed (particle counts unchanged); waits.
 int batch_set_filters(GpuBpfBatch* b, const BpfBatchFilter* filters);
+// BPF_OK if every filter can run with correlated noise (one tile, Gaussian state noise).
+int batch_check_correlated(const GpuBpfBatch* b);

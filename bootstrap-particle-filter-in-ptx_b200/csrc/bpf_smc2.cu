@@ -15,9 +15,20 @@
 // theta-particles, each scored by a fresh inner filter run over the whole
 // history (a second batch, one launch), accepted with probability
 // min(1, p^(y|theta') p(theta') / p^(y|theta) p(theta)); accepted proposals'
-// filter states are gathered into the current batch. The reference's
-// correlated-noise (CPMMH) variant and its regime-switching RBPF inner model
-// are not part of this driver.
+// filter states are gathered into the current batch.
+//
+// Correlated-noise moves (CPMMH, Deligiannidis, Doucet & Pitt 2018; the
+// reference's kernel_cpmmh_rejuvenate_fused, smc2/smc2_rbpf_batch.cu:651-935):
+// with cpmmh_rho > 0 every theta-particle's auxiliary noise (its inner filter's
+// normals and resampling normals, gpu_bpf_batch_run_correlated's layout) is
+// kept on the device in one of two areas; par[j] names theta-particle j's
+// current area. The forward ticks record into the current area, a proposal is
+// scored with noise rho * current + sqrt(1 - rho^2) * fresh written into the
+// other area, and acceptance flips par[j] (no copy; the reference copies the
+// accepted noise back, kernel_commit_accepted_noise :959-985). Outer
+// resampling copies the ancestors' areas into the other areas and flips every
+// par[j]. The reference's regime-switching RBPF inner model is not part of
+// this driver.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -87,6 +98,20 @@ struct GpuBpfSmc2 {
   int n_rejuv = 0;
   long long n_prop = 0, n_acc = 0;
   float last_ess = 0.0f;
+  // correlated-noise moves
+  float cp_rho = 0.0f;
+  float* d_nz = nullptr;               // 2 areas per theta-particle, each `area` floats
+  long long area = 0;
+  long long* d_off_cur = nullptr;      // [M] current areas
+  long long* d_off_oth = nullptr;      // [M] the other areas
+  long long* d_off_src = nullptr;      // [M] outer resampling: the ancestors' current areas
+  long long* off_pin = nullptr;        // [3M] staging
+  std::vector<int> par;
+  // the last PMMH move
+  bool have_move = false;
+  std::vector<float> lm_theta_prop, lm_theta_cur;
+  std::vector<double> lm_ll_prop, lm_ll_cur;
+  std::vector<int> lm_acc;
 };
 
 namespace {
@@ -115,6 +140,8 @@ void free_smc2(GpuBpfSmc2* s) {
   cudaFree(s->s_tab); cudaFree(s->s_st); cudaFree(s->s_h); cudaFree(s->s_w);
   cudaFreeHost(s->y_pin); cudaFreeHost(s->dll_pin); cudaFreeHost(s->i_pin); cudaFreeHost(s->st_pin);
   cudaFreeHost(s->ll_pin);
+  cudaFree(s->d_nz); cudaFree(s->d_off_cur); cudaFree(s->d_off_oth); cudaFree(s->d_off_src);
+  cudaFreeHost(s->off_pin);
   delete s;
 }
 
@@ -124,6 +151,19 @@ double outer_ess(const std::vector<double>& lw) {
   double a = 0.0, b = 0.0;
   for (double v : lw) { const double e = std::exp(v - m); a += e; b += e * e; }
   return a * a / b;
+}
+
+// Uploads the current / other area offsets of par[] (and waits: off_pin is reused).
+int upload_noise_offsets(GpuBpfSmc2* s) {
+  const int M = s->n_theta;
+  for (int j = 0; j < M; ++j) {
+    s->off_pin[j] = (2LL * j + s->par[j]) * s->area;
+    s->off_pin[M + j] = (2LL * j + 1 - s->par[j]) * s->area;
+  }
+  BCK(cudaMemcpyAsync(s->d_off_cur, s->off_pin, M * sizeof(long long), cudaMemcpyHostToDevice, s->stream));
+  BCK(cudaMemcpyAsync(s->d_off_oth, s->off_pin + M, M * sizeof(long long), cudaMemcpyHostToDevice, s->stream));
+  BCK(cudaStreamSynchronize(s->stream));
+  return BPF_OK;
 }
 
 // Outer systematic resampling and PMMH rejuvenation at tick count s->t + 1.
@@ -155,6 +195,17 @@ int resample_move(GpuBpfSmc2* s) {
   BCK(cudaMemcpyAsync(cur->d_st, s->s_st, M * sizeof(BatchFilterState), cudaMemcpyDeviceToDevice, s->stream));
   BCK(cudaMemcpyAsync(cur->d_sth, s->s_h, nh * sizeof(float), cudaMemcpyDeviceToDevice, s->stream));
   BCK(cudaMemcpyAsync(cur->d_stw, s->s_w, nh * sizeof(float), cudaMemcpyDeviceToDevice, s->stream));
+  const bool cp = s->cp_rho > 0.0f;
+  const long long used = (long long)T * batch_noise_stride(s->n);   // floats of ticks 0..T-1
+  if (cp) {
+    // the copies take their ancestors' noise (into their other areas), then those become current
+    for (int j = 0; j < M; ++j) s->off_pin[2 * M + j] = (2LL * idx[j] + s->par[idx[j]]) * s->area;
+    BCK(cudaMemcpyAsync(s->d_off_src, s->off_pin + 2 * M, M * sizeof(long long), cudaMemcpyHostToDevice, s->stream));
+    BCK(launch_noise_gather(s->d_nz, s->d_off_src, s->d_off_oth, used, M, s->stream));
+    for (int j = 0; j < M; ++j) s->par[j] ^= 1;
+    const int rc = upload_noise_offsets(s);
+    if (rc) return rc;
+  }
   std::vector<Theta> th(M);
   for (int j = 0; j < M; ++j) th[j] = s->theta[idx[j]];
   s->theta = th;
@@ -197,6 +248,18 @@ int resample_move(GpuBpfSmc2* s) {
     }
     int rc = batch_set_filters(s->prop, fl.data());
     if (rc) return rc;
+    if (cp) {
+      NoiseArgs nz;
+      nz.in = s->d_nz;
+      nz.out = s->d_nz;
+      nz.in_off = s->d_off_cur;
+      nz.out_off = s->d_off_oth;
+      nz.rho = s->cp_rho;
+      nz.scale = sqrtf(fmaxf(0.0f, 1.0f - s->cp_rho * s->cp_rho));
+      s->prop->step_nz = nz;
+    } else {
+      s->prop->step_nz = NoiseArgs{};
+    }
     rc = batch_set_tick(s->prop, 0);
     if (rc) return rc;
     rc = batch_step_abs(s->prop, s->d_y, T, nullptr);
@@ -205,18 +268,32 @@ int resample_move(GpuBpfSmc2* s) {
     BCK(cudaStreamSynchronize(s->prop->stream));
     BCK(cudaMemcpyAsync(s->st_pin, cur->d_st, M * sizeof(BatchFilterState), cudaMemcpyDeviceToHost, s->stream));
     BCK(cudaStreamSynchronize(s->stream));
+    s->lm_theta_prop.resize(3 * M); s->lm_theta_cur.resize(3 * M);
+    s->lm_ll_prop.resize(M); s->lm_ll_cur.resize(M); s->lm_acc.resize(M);
     for (int j = 0; j < M; ++j) {
       const double la = s->ll_pin[j] + lpn[j] - s->st_pin[j].ll_total - lp[j];
       const bool ok = std::isfinite(lpn[j]) && std::isfinite(s->ll_pin[j]) && std::log(s->rng.uniform()) < la;
       s->i_pin[j] = ok ? 1 : 0;
-      if (ok) { s->theta[j] = pr[j]; ++s->n_acc; }
+      s->lm_theta_prop[3 * j] = fl[j].mu; s->lm_theta_prop[3 * j + 1] = fl[j].rho; s->lm_theta_prop[3 * j + 2] = fl[j].sigma_z;
+      s->lm_theta_cur[3 * j] = (float)s->theta[j].mu; s->lm_theta_cur[3 * j + 1] = (float)s->theta[j].rho;
+      s->lm_theta_cur[3 * j + 2] = (float)s->theta[j].sigma;
+      s->lm_ll_prop[j] = s->ll_pin[j]; s->lm_ll_cur[j] = s->st_pin[j].ll_total; s->lm_acc[j] = ok ? 1 : 0;
+      if (ok) {
+        s->theta[j] = pr[j]; ++s->n_acc;
+        if (cp) s->par[j] ^= 1;                             // the proposal's noise becomes current
+      }
       ++s->n_prop;
     }
+    s->have_move = true;
     BCK(cudaMemcpyAsync(s->d_mask, s->i_pin, M * sizeof(int), cudaMemcpyHostToDevice, s->stream));
     BCK(launch_batch_gather(cur->d_filters, cur->d_st, cur->d_sth, cur->d_stw, s->prop->d_filters, s->prop->d_st,
                             s->prop->d_sth, s->prop->d_stw, cur->d_stoff, nullptr, s->d_mask, nullptr, s->n, M,
                             s->stream));
     BCK(cudaStreamSynchronize(s->stream));
+    if (cp) {
+      rc = upload_noise_offsets(s);
+      if (rc) return rc;
+    }
   }
   return BPF_OK;
 }
@@ -366,6 +443,74 @@ int gpu_bpf_smc2_get_particles(GpuBpfSmc2* s, float* theta, double* logw, double
       return bpf_record_error(BPF_ERR_CUDA);
     }
     for (int j = 0; j < s->n_theta; ++j) loglik[j] = s->st_pin[j].ll_total;
+  }
+  return BPF_OK;
+}
+
+int gpu_bpf_smc2_set_cpmmh_rho(GpuBpfSmc2* s, float rho) {
+  if (!s) return bpf_record_error(BPF_ERR_STATE);
+  if (!(rho >= 0.0f && rho <= 1.0f)) return bpf_record_error(BPF_ERR_ARG);
+  const bool on = rho > 0.0f;
+  if (on != (s->cp_rho > 0.0f) && s->t > 0) return bpf_record_error(BPF_ERR_STATE);
+  if (on && s->n > kTile) return bpf_record_error(BPF_ERR_UNSUPPORTED);
+  int cur_dev = -1;
+  if (cudaGetDevice(&cur_dev) != cudaSuccess || (cur_dev != s->cur->device && cudaSetDevice(s->cur->device) != cudaSuccess))
+    return bpf_record_error(BPF_ERR_CUDA);
+  const int M = s->n_theta;
+  if (on && !s->d_nz) {
+    s->area = (long long)s->max_ticks * batch_noise_stride(s->n);
+    cudaError_t e = cudaMalloc(&s->d_nz, (size_t)(2LL * M * s->area) * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_off_cur, M * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_off_oth, M * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_off_src, M * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->off_pin, 3 * M * sizeof(long long));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(s->d_nz); cudaFree(s->d_off_cur); cudaFree(s->d_off_oth); cudaFree(s->d_off_src);
+      cudaFreeHost(s->off_pin);
+      s->d_nz = nullptr; s->d_off_cur = s->d_off_oth = s->d_off_src = nullptr; s->off_pin = nullptr;
+      return bpf_record_error(BPF_ERR_ALLOC);
+    }
+    s->par.assign(M, 0);
+    const int rc = upload_noise_offsets(s);
+    if (rc) return rc;
+  }
+  s->cp_rho = rho;
+  if (on) {
+    NoiseArgs nz;                                            // forward ticks: fresh noise, recorded
+    nz.out = s->d_nz;
+    nz.out_off = s->d_off_cur;
+    s->cur->step_nz = nz;
+  } else {
+    s->cur->step_nz = NoiseArgs{};
+  }
+  return BPF_OK;
+}
+
+int gpu_bpf_smc2_get_last_move(GpuBpfSmc2* s, float* theta_prop, float* theta_cur, double* loglik_prop,
+                               double* loglik_cur, int* accepted) {
+  if (!s || !s->have_move) return bpf_record_error(BPF_ERR_STATE);
+  const int M = s->n_theta;
+  if (theta_prop) std::copy(s->lm_theta_prop.begin(), s->lm_theta_prop.end(), theta_prop);
+  if (theta_cur) std::copy(s->lm_theta_cur.begin(), s->lm_theta_cur.end(), theta_cur);
+  if (loglik_prop) std::copy(s->lm_ll_prop.begin(), s->lm_ll_prop.begin() + M, loglik_prop);
+  if (loglik_cur) std::copy(s->lm_ll_cur.begin(), s->lm_ll_cur.begin() + M, loglik_cur);
+  if (accepted) std::copy(s->lm_acc.begin(), s->lm_acc.begin() + M, accepted);
+  return BPF_OK;
+}
+
+int gpu_bpf_smc2_get_noise(GpuBpfSmc2* s, int j, int n_ticks, float* out) {
+  if (!s) return bpf_record_error(BPF_ERR_STATE);
+  if (!(s->cp_rho > 0.0f) || !s->d_nz) return bpf_record_error(BPF_ERR_STATE);
+  if (j < 0 || j >= s->n_theta || n_ticks <= 0 || n_ticks > s->t || !out) return bpf_record_error(BPF_ERR_ARG);
+  int cur_dev = -1;
+  if (cudaGetDevice(&cur_dev) != cudaSuccess || (cur_dev != s->cur->device && cudaSetDevice(s->cur->device) != cudaSuccess))
+    return bpf_record_error(BPF_ERR_CUDA);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(out, s->d_nz + (2LL * j + s->par[j]) * s->area,
+                 (size_t)n_ticks * batch_noise_stride(s->n) * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return bpf_record_error(BPF_ERR_CUDA);
   }
   return BPF_OK;
 }

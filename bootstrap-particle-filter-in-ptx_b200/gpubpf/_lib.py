@@ -156,6 +156,8 @@ SIGNATURES = {
     "gpu_bpf_batch_tick": (_i, [_vp]),
     "gpu_bpf_batch_loglik_device": (_vp, [_vp]),
     "gpu_bpf_batch_grad_tape_bytes": (C.c_size_t, [_vp, _i]),
+    "gpu_bpf_batch_run_correlated": (_i, [_vp, _vp, _i, _vp, _vp, _f, _vp, _vp, _vp]),
+    "gpu_bpf_batch_noise_offset": (C.c_longlong, [_vp, _i, _i]),
     # APF (gpu_bpf/gpu_bpf.cuh:114-126)
     "gpu_apf_create": (P_APF, [_i, _f, _f, _f, _f, _f, _i]),
     "gpu_apf_destroy": (None, [P_APF]),
@@ -184,6 +186,9 @@ SIGNATURES = {
     "gpu_bpf_smc2_get_theta": (_i, [_vp, C.POINTER(_f), C.POINTER(_f)]),
     "gpu_bpf_smc2_get_particles": (_i, [_vp, _vp, _vp, _vp]),
     "gpu_bpf_smc2_stats": (_i, [_vp, C.POINTER(_i), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "gpu_bpf_smc2_set_cpmmh_rho": (_i, [_vp, _f]),
+    "gpu_bpf_smc2_get_last_move": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "gpu_bpf_smc2_get_noise": (_i, [_vp, _i, _i, _vp]),
     # gradient
     "gpu_bpf_grad_create": (_vp, [_i, _i, _i]),
     "gpu_bpf_grad_destroy": (None, [_vp]),

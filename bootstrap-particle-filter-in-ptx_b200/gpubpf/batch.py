@@ -89,6 +89,23 @@ class GpuBpfBatch:
                                                 C.c_void_p(dll_ptr or None), C.c_void_p(anc_ptr or None),
                                                 C.c_void_p(particles_ptr or None)), "gpu_bpf_batch_run_debug")
 
+    def run_correlated(self, y_ptr: int, n_ticks: int, noise_in_ptr: int, noise_out_ptr: int, rho: float,
+                       loglik_ptr: int, dll_ptr: int = 0, anc_ptr: int = 0) -> None:
+        """Correlated-noise run from tick 0 (device pointers, batch stream): noise_out receives the
+        noise used, rho * noise_in + sqrt(1 - rho^2) * fresh (noise_in 0: fresh only). Areas start
+        at noise_offset(f, n_ticks) floats; see gpu_bpf_batch_run_correlated."""
+        check(self._lib.gpu_bpf_batch_run_correlated(self._h, C.c_void_p(y_ptr), int(n_ticks),
+                                                     C.c_void_p(noise_in_ptr or None), C.c_void_p(noise_out_ptr),
+                                                     float(rho), C.c_void_p(loglik_ptr), C.c_void_p(dll_ptr or None),
+                                                     C.c_void_p(anc_ptr or None)), "gpu_bpf_batch_run_correlated")
+
+    def noise_offset(self, f: int, n_ticks: int) -> int:
+        """First float of filter f's noise area (f = n_filters: the buffers' length)."""
+        v = int(self._lib.gpu_bpf_batch_noise_offset(self._h, int(f), int(n_ticks)))
+        if v < 0:
+            raise BpfError(-v, "gpu_bpf_batch_noise_offset")
+        return v
+
     def grad_run(self, y_ptr: int, n_ticks: int, loglik_ptr: int, grad_ptr: int) -> None:
         """Forward + adjoint backward of every filter: loglik[B] (FP64) and grad[B, 3] = d loglik /
         d(mu, rho, sigma_z), enqueued on the batch stream (device pointers)."""

@@ -63,6 +63,33 @@ class Smc2:
               "gpu_bpf_smc2_get_particles")
         return th, lw, ll
 
+    def set_cpmmh_rho(self, rho: float) -> None:
+        """Correlated-noise PMMH moves with correlation rho (0 = fresh inner filters, the default;
+        ~ smc2_cuda_set_cpmmh_rho). Switch on or off before the first update."""
+        check(self._lib.gpu_bpf_smc2_set_cpmmh_rho(self._h, float(rho)), "gpu_bpf_smc2_set_cpmmh_rho")
+
+    def last_move(self):
+        """The last PMMH move: dict of theta_prop, theta_cur [M, 3] (float32, as the inner filters
+        use them), loglik_prop, loglik_cur [M] and accepted [M]."""
+        M = self.n_theta
+        tp = np.zeros((M, 3), dtype=np.float32)
+        tc = np.zeros((M, 3), dtype=np.float32)
+        lp = np.zeros(M)
+        lc = np.zeros(M)
+        acc = np.zeros(M, dtype=np.int32)
+        check(self._lib.gpu_bpf_smc2_get_last_move(self._h, tp.ctypes.data, tc.ctypes.data, lp.ctypes.data,
+                                                   lc.ctypes.data, acc.ctypes.data), "gpu_bpf_smc2_get_last_move")
+        return {"theta_prop": tp, "theta_cur": tc, "loglik_prop": lp, "loglik_cur": lc, "accepted": acc}
+
+    def noise(self, j: int, n_ticks: int, n_particles: int):
+        """Theta-particle j's current auxiliary noise: (normals [n_ticks, n_particles], resampling
+        normals [n_ticks])."""
+        stride = ((n_particles + 3) & ~3) + 4
+        out = np.zeros((n_ticks, stride), dtype=np.float32)
+        check(self._lib.gpu_bpf_smc2_get_noise(self._h, int(j), int(n_ticks), out.ctypes.data),
+              "gpu_bpf_smc2_get_noise")
+        return out[:, :n_particles].copy(), out[:, stride - 4].copy()
+
     def stats(self):
         r, p, a = C.c_int(0), C.c_longlong(0), C.c_longlong(0)
         check(self._lib.gpu_bpf_smc2_stats(self._h, C.byref(r), C.byref(p), C.byref(a)), "gpu_bpf_smc2_stats")

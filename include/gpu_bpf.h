@@ -389,6 +389,29 @@ int          gpu_bpf_batch_grad_run(GpuBpfBatch* batch, const float* y_dev, int 
 /* Device memory the gradient tape of gpu_bpf_batch_grad_run takes for n_ticks ticks (it is sized
  * for the CTAs in flight, not for the number of filters). */
 size_t       gpu_bpf_batch_grad_tape_bytes(GpuBpfBatch* batch, int n_ticks);
+/* Correlated-noise runs: the building block of correlated pseudo-marginal MCMC (CPMMH,
+ * Deligiannidis, Doucet & Pitt 2018), as the reference's CPMMH rejuvenation kernel uses it
+ * (smc2/smc2_rbpf_batch.cu:651-935). Every filter runs ticks 0..n_ticks-1 from a fresh start
+ * with its auxiliary noise exposed: filter f's noise is an area of
+ * n_ticks * (n_pad + 4) floats, n_pad = n_particles rounded up to a multiple of 4, starting at
+ * element gpu_bpf_batch_noise_offset(f) of the noise buffers. Per tick: floats [0, n_particles)
+ * are the particles' standard normals (tick 0: the initial draw), float n_pad is the normal v
+ * whose Phi(v) is the tick's resampling uniform, the rest are unused. With noise_in_dev NULL the
+ * normals are the filters' own PCG32 draws (as an ordinary run); otherwise
+ * noise = rho * noise_in + sqrt(1 - rho^2) * the filter's own draw (rho in [0, 1]; rho = 1
+ * replays noise_in exactly). The noise used is written to noise_out_dev (which must not be
+ * noise_in_dev). Before every resampling the particles are sorted by value, so that nearby
+ * noise gives nearby resampling. Filters must have at most 4096 particles and Gaussian state
+ * noise (BPF_ERR_UNSUPPORTED otherwise). loglik_dev[n_filters] and dll_dev[n_filters*n_ticks]
+ * (or NULL) as in gpu_bpf_batch_run_device; anc_dev (or NULL, a testing aid) as in
+ * gpu_bpf_batch_run_debug, each ancestor the particle's slot before the sort. Enqueued on the
+ * batch stream. */
+int          gpu_bpf_batch_run_correlated(GpuBpfBatch* batch, const float* y_dev, int n_ticks,
+                                          const float* noise_in_dev, float* noise_out_dev, float rho,
+                                          double* loglik_dev, double* dll_dev, int32_t* anc_dev);
+/* First element of filter f's area in the noise buffers of n_ticks-tick correlated-noise runs;
+ * with f = n_filters, the buffers' length in floats. */
+long long    gpu_bpf_batch_noise_offset(GpuBpfBatch* batch, int filter, int n_ticks);
 
 /* ---- Gradient (addition) ---------------------------------------------------
  * d loglik / d(mu, rho, sigma_z) of the plain filter with the resampling ancestors held fixed.
@@ -436,8 +459,9 @@ int gpu_bpf_grad_get_children(GpuBpfGrad* grad, int tick, int32_t* first_child);
  * Metropolis-Hastings moves whose proposals are scored by fresh inner filters over the whole
  * history. The outer loop of the reference's smc2_cuda_update
  * (smc2/smc2_rbpf_batch.cu:1329-1502, host API smc2/smc2_rbpf_batch.cuh:461-489) on this build's
- * SV model; the reference's regime-switching RBPF inner model and correlated-noise moves are not
- * part of it. Prior: mu ~ N(mu_mean, mu_sd^2), rho ~ U(rho_lo, rho_hi), sigma_z ~ U(sigma_lo,
+ * SV model, with the reference's correlated-noise (CPMMH) moves as an option
+ * (gpu_bpf_smc2_set_cpmmh_rho); the reference's regime-switching RBPF inner model is not part
+ * of it. Prior: mu ~ N(mu_mean, mu_sd^2), rho ~ U(rho_lo, rho_hi), sigma_z ~ U(sigma_lo,
  * sigma_hi) (NULL = N(-1, 0.5^2), U(0.85, 0.995), U(0.05, 0.4)). Deterministic given the seed. */
 typedef struct {
     float mu_mean, mu_sd, rho_lo, rho_hi, sigma_lo, sigma_hi;
@@ -463,6 +487,24 @@ int         gpu_bpf_smc2_get_theta(GpuBpfSmc2* smc2, float* mean3, float* std3);
 int         gpu_bpf_smc2_get_particles(GpuBpfSmc2* smc2, float* theta, double* logw, double* loglik);
 int         gpu_bpf_smc2_stats(GpuBpfSmc2* smc2, int* n_rejuvenations, long long* n_proposed,
                                long long* n_accepted);
+/* ~ smc2_cuda_set_cpmmh_rho (smc2/smc2_rbpf_batch.cu:1238-1240): correlated-noise PMMH moves.
+ * rho in (0, 1] keeps every theta-particle's auxiliary noise (its inner filter's normals and
+ * resampling normals, as in gpu_bpf_batch_run_correlated) on the device and scores each proposal
+ * with noise rho * current + sqrt(1 - rho^2) * fresh; accepted proposals' noise becomes current,
+ * outer resampling copies it with the filter. rho = 0 (the default) scores proposals with fresh
+ * inner filters. Switching between 0 and > 0 is allowed only before the first update; the noise
+ * takes 8 * n_theta * max_ticks * (n_particles + 8) bytes; n_particles must be at most 4096. The
+ * reference's default is 0.99. */
+int         gpu_bpf_smc2_set_cpmmh_rho(GpuBpfSmc2* smc2, float rho);
+/* The last PMMH move (host arrays, each may be NULL): proposed and current theta [3*n_theta]
+ * (as the inner filters use them), the proposals' and the current inner log-likelihoods
+ * [n_theta] and the acceptance flags [n_theta]. BPF_ERR_STATE before the first move. */
+int         gpu_bpf_smc2_get_last_move(GpuBpfSmc2* smc2, float* theta_prop, float* theta_cur,
+                                       double* loglik_prop, double* loglik_cur, int* accepted);
+/* Theta-particle j's current auxiliary noise for ticks 0..n_ticks-1 (n_ticks at most the ticks
+ * seen; layout of gpu_bpf_batch_run_correlated's areas) into the host array out. Needs
+ * rho > 0. */
+int         gpu_bpf_smc2_get_noise(GpuBpfSmc2* smc2, int j, int n_ticks, float* out);
 
 /* Number of kernel launches this library has issued (all filters). */
 long long gpu_bpf_launch_count(void);

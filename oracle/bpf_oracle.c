@@ -15,6 +15,9 @@
  *                        (erfc-based): the FP64 oracle's inverse normal CDF
  *   orc_filter_f64       FP64 filter in this build's semantics, optionally
  *                        replaying resampling decisions and ancestors
+ *   orc_filter_noise_f64 FP64 filter driven by given auxiliary noise, sorting the
+ *                        particles before every resampling (the correlated-noise runs
+ *                        of the reference's CPMMH moves, smc2/smc2_rbpf_batch.cu:651-935)
  *   orc_apf_f64          FP64 auxiliary particle filter (gpu_bpf_ptx_full.cu:990-1175)
  *                        with the PCG32 streams, optionally replaying ancestors
  *   orc_grad_f64         d loglik / d(mu, rho, sigma) of the FP64 filter with the
@@ -323,6 +326,113 @@ int orc_filter_f64(const OrcConfig* c, const float* y, int T,
         }
     }
     free(h); free(hn); free(lw); free(lwc); free(cdf);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP64 filter driven by given auxiliary noise (correlated-noise runs)         */
+/* ------------------------------------------------------------------------- */
+/*
+ * The auxiliary noise of a correlated pseudo-marginal run (the reference's
+ * CPMMH replay, smc2/smc2_rbpf_batch.cu:741-860, which stores the noise per
+ * tick and particle and draws the resampling offset from a stored normal):
+ * z[t*stride + i] (i < N) are the particles' standard normals at tick t
+ * (tick 0: h_0 = mu + s_stat z), z[t*stride + npad] (npad = N rounded up to 4)
+ * is the normal v_t of the tick's resampling offset u = Phi(v_t), taken on the
+ * 23-bit grid (floor(Phi(v_t) 2^23) 2^-23). Before every resampling the
+ * particles are put in ascending order (ties by slot), so resampling maps
+ * nearby noise to nearby ancestors (the reference sorts the resampled
+ * particles, cpmmh_sort, :836-845). anc_replay: [T][N] slot ancestors (the
+ * slot before the sort) the run follows; NULL = its own FP64 systematic
+ * resampling. flags_replay as orc_filter_f64. Outputs (each may be NULL): dll,
+ * hmean, ess [T], flags_out [T], anc_out [T][N]: on resampling ticks the
+ * oracle's own slot ancestors from that tick's particles (with anc_replay, a
+ * lock-step check of the replayed ancestors).
+ */
+static const double* g_sort_key;
+static int cmp_slot(const void* a, const void* b) {
+    const int i = *(const int*)a, j = *(const int*)b;
+    const double x = g_sort_key[i], y = g_sort_key[j];
+    if (x < y) return -1;
+    if (x > y) return 1;
+    return (i > j) - (i < j);
+}
+
+int orc_filter_noise_f64(const OrcConfig* c, const float* y, int T, const float* z, int stride,
+                         const int32_t* anc_replay, const int32_t* flags_replay,
+                         double* dll, double* hmean, double* ess, int32_t* flags_out, int32_t* anc_out) {
+    const int N = c->n_particles, npad = (N + 3) & ~3;
+    if (N <= 0 || T < 0 || stride < npad + 1 || !z) return 1;
+    double* h = (double*)malloc(sizeof(double) * N);
+    double* hn = (double*)malloc(sizeof(double) * N);
+    double* lw = (double*)malloc(sizeof(double) * N);
+    double* lwc = (double*)malloc(sizeof(double) * N);
+    double* cdf = (double*)malloc(sizeof(double) * N);
+    int* ord = (int*)malloc(sizeof(int) * N);
+    if (!h || !hn || !lw || !lwc || !cdf || !ord) {
+        free(h); free(hn); free(lw); free(lwc); free(cdf); free(ord);
+        return 2;
+    }
+    const double mu = c->mu, rho = c->rho, sig = c->sigma_z, nu = c->nu_obs, cobs = c_obs_of(nu);
+    const double sstat = sqrt(sig * sig / fmax(1.0 - rho * rho, 1e-6));
+    for (int i = 0; i < N; ++i) { h[i] = mu + sstat * (double)z[i]; lwc[i] = 0.0; }
+    int prev_res = 1;
+    double lse_prev = log((double)N);
+    for (int t = 0; t < T; ++t) {
+        const float* zt = z + (size_t)t * stride;
+        if (t > 0)
+            for (int i = 0; i < N; ++i) h[i] = mu + rho * (h[i] - mu) + sig * (double)zt[i];
+        double M = -INFINITY;
+        for (int i = 0; i < N; ++i) {
+            lw[i] = (prev_res ? 0.0 : lwc[i]) + obs_logpdf_f64((double)y[t], h[i], nu, cobs);
+            if (lw[i] > M) M = lw[i];
+        }
+        double S = 0.0, Q = 0.0, H = 0.0;
+        for (int i = 0; i < N; ++i) {
+            const double e = exp(lw[i] - M);
+            S += e; Q += e * e; H += e * h[i];
+        }
+        const double lse = M + log(S);
+        const double es = S * S / Q;
+        if (dll) dll[t] = lse - (prev_res ? log((double)N) : lse_prev);
+        if (hmean) hmean[t] = H / S;
+        if (ess) ess[t] = es;
+        const int res = flags_replay ? (flags_replay[t] != 0)
+                                     : ((c->ess_threshold <= 0.0f) || (es / (double)N < (double)c->ess_threshold));
+        if (flags_out) flags_out[t] = res;
+        if (res) {
+            int32_t* ao = anc_out ? anc_out + (size_t)t * N : NULL;
+            if (!anc_replay || ao) {
+                for (int i = 0; i < N; ++i) ord[i] = i;
+                g_sort_key = h;
+                qsort(ord, (size_t)N, sizeof(int), cmp_slot);
+                double acc = 0.0;
+                for (int p = 0; p < N; ++p) { acc += exp(lw[ord[p]] - M); cdf[p] = acc; }
+                double u = 0.5 * erfc(-(double)zt[npad] * 0.70710678118654752440);
+                double u23 = floor(u * 8388608.0);
+                if (u23 > 8388607.0) u23 = 8388607.0;
+                const double step = acc / (double)N, u0 = u23 * 1.1920928955078125e-07;
+                int j = 0;
+                for (int i = 0; i < N; ++i) {
+                    const double target = (u0 + (double)i) * step;
+                    while (j < N - 1 && !(cdf[j] > target)) ++j;
+                    if (!anc_replay) hn[i] = h[ord[j]];
+                    if (ao) ao[i] = ord[j];
+                }
+            }
+            if (anc_replay) {
+                const int32_t* a = anc_replay + (size_t)t * N;
+                for (int i = 0; i < N; ++i) hn[i] = h[a[i]];
+            }
+            double* tmp = h; h = hn; hn = tmp;
+            prev_res = 1;
+        } else {
+            memcpy(lwc, lw, sizeof(double) * N);
+            lse_prev = lse;
+            prev_res = 0;
+        }
+    }
+    free(h); free(hn); free(lw); free(lwc); free(cdf); free(ord);
     return 0;
 }
 

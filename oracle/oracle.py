@@ -75,6 +75,9 @@ def lib(native: bool = False) -> C.CDLL:
     L.orc_ref_run.restype = C.c_int
     L.orc_ref_run.argtypes = [C.c_int, f32, f32, f32, f32, C.c_int, f32, C.c_void_p, C.c_int,
                               C.c_void_p, C.c_void_p, C.c_int, P(C.c_int)]
+    L.orc_filter_noise_f64.restype = C.c_int
+    L.orc_filter_noise_f64.argtypes = [P(OrcConfig), C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_apf_f64.restype = C.c_int
     L.orc_apf_f64.argtypes = [P(OrcConfig), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -133,6 +136,32 @@ def filter_f64(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.0, nu_
     if rc != 0:
         raise RuntimeError(f"orc_filter_f64 failed ({rc})")
     out["resampled"] = flags
+    return out
+
+
+def filter_noise_f64(n_particles, rho, sigma_z, mu, y, z, ess_threshold=0.0, nu_obs=0.0, anc_replay=None,
+                     flags_replay=None):
+    """FP64 filter driven by the auxiliary noise z [T, stride] of a correlated-noise run (particles'
+    normals in z[t, :N], the resampling normal in z[t, stride - 4]), sorting before every
+    resampling. Returns dict of per-tick dll, hmean, ess, resampled and anc [T, N] (slot ancestors)."""
+    L = lib()
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    z = np.ascontiguousarray(z, dtype=np.float32)
+    T = y.shape[0]
+    assert z.shape[0] >= T
+    N = int(n_particles)
+    cfg = OrcConfig(N, rho, sigma_z, mu, nu_obs, 0, ess_threshold, 0.0)
+    out = {k: np.zeros(T, dtype=np.float64) for k in ("dll", "hmean", "ess")}
+    flags = np.zeros(T, dtype=np.int32)
+    anc = np.zeros((T, N), dtype=np.int32)
+    ar = None if anc_replay is None else np.ascontiguousarray(anc_replay, dtype=np.int32)
+    fr = None if flags_replay is None else np.ascontiguousarray(flags_replay, dtype=np.int32)
+    rc = L.orc_filter_noise_f64(C.byref(cfg), _ptr(y), T, _ptr(z), int(z.shape[1]), _ptr(ar), _ptr(fr),
+                                _ptr(out["dll"]), _ptr(out["hmean"]), _ptr(out["ess"]), _ptr(flags), _ptr(anc))
+    if rc != 0:
+        raise RuntimeError(f"orc_filter_noise_f64 failed ({rc})")
+    out["resampled"] = flags
+    out["anc"] = anc
     return out
 
 
