@@ -2,8 +2,8 @@
 
 Restates ``generate_matched_series`` and its PCG32 helpers from the reference
 test ``tests/test_bpf_matched_dgp.cu`` (seeding :69-76, doubles :78-80,
-Box-Muller :82-87, series :141-175) for the Gaussian case (nu_state =
-nu_obs = 0), plus the series used by the benchmark configurations.
+Box-Muller :82-87, Student-t :89-99, series :141-175), plus the series used by
+the benchmark configurations.
 """
 from __future__ import annotations
 
@@ -42,19 +42,33 @@ class Pcg32:
         u2 = self.next_double()
         return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * 3.14159265358979323846 * u2)
 
+    def student_t(self, nu: float) -> float:  # :89-99: z / sqrt(chi2 / nu), chi2 with int(nu) dof
+        if nu > 100.0:
+            return self.gaussian()
+        z = self.gaussian()
+        chi_sq = 0.0
+        for _ in range(int(nu)):
+            g = self.gaussian()
+            chi_sq += g * g
+        return z / math.sqrt(chi_sq / nu)
 
-def matched_series(T: int, rho: float, sigma_z: float, mu: float, seed: int):
-    """(true_h[T], y[T]) from generate_matched_series with Gaussian noises."""
+
+def matched_series(T: int, rho: float, sigma_z: float, mu: float, seed: int, nu_state: float = 0.0,
+                   nu_obs: float = 0.0):
+    """(true_h[T], y[T]) from generate_matched_series; nu_state / nu_obs > 0 draw the state /
+    observation noise from Student-t laws (0 = Gaussian)."""
     rng = Pcg32(seed)
     var_stat = (sigma_z * sigma_z) / max(1.0 - rho * rho, 1e-6)
     h = mu + math.sqrt(var_stat) * rng.gaussian()
     hs, ys = [], []
     for t in range(T):
         if t > 0:
-            h = mu + rho * (h - mu) + sigma_z * rng.gaussian()
+            eps = rng.student_t(nu_state) if nu_state > 0.0 else rng.gaussian()
+            h = mu + rho * (h - mu) + sigma_z * eps
         h = min(max(h, -12.0), 4.0)
         hs.append(h)
-        ys.append(math.exp(h / 2.0) * rng.gaussian())
+        eta = rng.student_t(nu_obs) if nu_obs > 0.0 else rng.gaussian()
+        ys.append(math.exp(h / 2.0) * eta)
     return hs, ys
 
 

@@ -16,6 +16,11 @@ Fixtures
   dgp_series.json        generate_matched_series of tests/test_bpf_matched_dgp.cu
                          (:59-99 helpers, :105-127 data struct, :141-175) for the
                          benchmark inputs, compiled from the reference lines
+  dgp_scenarios.json     the nine matched-DGP scenarios of tests/test_bpf_matched_dgp.cu:181-285
+                         (parameters parsed from the gen_* functions) and, for each, the
+                         head and sums of generate_matched_series with Student-t noises
+                         (:88-99) at the suite's seeds (base 42 + scenario index, T = 5000),
+                         compiled from the reference lines
   systematic_resample.json  tests/diff_bpf.py:35-56 systematic_resample run on
                          seeded log-weights (imports the reference module)
 
@@ -148,6 +153,51 @@ def dgp(tmp: str) -> dict:
     return res
 
 
+def dgp_scenarios(tmp: str) -> dict:
+    rel = "tests/test_bpf_matched_dgp.cu"
+    src = ref_lines(rel, 181, 285)
+    pat = re.compile(r'scenario_id\s*=\s*(\d+);\s*d->scenario_name\s*=\s*"([^"]+)";.*?'
+                     r'generate_matched_series\(d,\s*([-0-9.]+),\s*([-0-9.]+),\s*([-0-9.]+),\s*([-0-9.]+),'
+                     r'\s*([-0-9.]+),\s*&rng\)', re.S)
+    scen = [(int(m.group(1)), m.group(2), *(float(m.group(k)) for k in range(3, 8))) for m in pat.finditer(src)]
+    assert len(scen) == 9, scen
+    helpers = ref_lines(rel, 59, 99)
+    data = ref_lines(rel, 105, 127)
+    free_ = ref_lines(rel, 129, 135)
+    gen = ref_lines(rel, 141, 175)
+    T, base_seed = 5000, 42                      # the suite's defaults (:739-742)
+    drv = ["#include <stdio.h>", "#include <stdlib.h>", "#include <stdint.h>", "#include <math.h>",
+           helpers, data, free_, gen, "int main(void) {"]
+    for i, (sid, name, rho, sig, mu, nus, nuo) in enumerate(scen):
+        drv.append(f'  {{ pcg32_dgp_t rng; pcg32_dgp_seed(&rng, {base_seed + i}ULL);'
+                   f' MatchedTestData* d = alloc_matched_data({T});'
+                   f' generate_matched_series(d, {rho!r}, {sig!r}, {mu!r}, {nus!r}, {nuo!r}, &rng);'
+                   f' printf("case {sid}\\n");'
+                   f' for (int t = 0; t < {T}; ++t) printf("%.17g %.17g\\n", d->true_h[t], d->returns[t]);'
+                   f' free_matched_data(d); }}')
+    drv.append("  return 0;\n}\n")
+    out = compile_run("\n".join(drv), tmp, "dgp_scen")
+    series, cur = {}, None
+    for line in out.splitlines():
+        if line.startswith("case "):
+            cur = int(line.split()[1])
+            series[cur] = ([], [])
+        else:
+            h, y = line.split()
+            series[cur][0].append(float(h))
+            series[cur][1].append(float(y))
+    res = {"source": f"{rel}:59-99,105-135,141-175,181-285 (parsed, compiled and run); suite defaults T = 5000, "
+                     f"base seed 42, scenario i (0-based) generated with seed 42 + i (:462-464)",
+           "T": T, "base_seed": base_seed, "scenarios": []}
+    for i, (sid, name, rho, sig, mu, nus, nuo) in enumerate(scen):
+        hs, ys = series[sid]
+        res["scenarios"].append({
+            "id": sid, "name": name, "seed": base_seed + i, "rho": rho, "sigma_z": sig, "mu": mu,
+            "nu_state": nus, "nu_obs": nuo, "true_h_head": hs[:300], "y_head": ys[:300],
+            "sum_h": sum(hs), "sum_y2": sum(v * v for v in ys)})
+    return res
+
+
 def systematic() -> dict:
     import torch
     spec = importlib.util.spec_from_file_location("ref_diff_bpf", os.path.join(REF, "tests", "diff_bpf.py"))
@@ -176,6 +226,7 @@ def main():
             "rng_diag_seed42.json": rng_diag(tmp),
             "host_u_stream.json": host_u(tmp),
             "dgp_series.json": dgp(tmp),
+            "dgp_scenarios.json": dgp_scenarios(tmp),
         }
     fixtures["systematic_resample.json"] = systematic()
     for name, obj in fixtures.items():

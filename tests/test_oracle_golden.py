@@ -61,6 +61,21 @@ def test_dgp_matches_reference_generator(golden):
             pytest.skip("libm differs in the last ulp from the fixture host")
 
 
+def test_dgp_scenarios_match_reference_generator(golden):
+    """The nine matched-DGP scenarios (test_bpf_matched_dgp.cu:181-285), Student-t noises included:
+    gpubpf.dgp.matched_series == generate_matched_series at the suite's seeds, T = 5000."""
+    from gpubpf import dgp
+    g = golden("dgp_scenarios.json")
+    assert len(g["scenarios"]) == 9
+    for c in g["scenarios"]:
+        hs, ys = dgp.matched_series(g["T"], c["rho"], c["sigma_z"], c["mu"], c["seed"], c["nu_state"], c["nu_obs"])
+        n = len(c["y_head"])
+        np.testing.assert_allclose(hs[:n], c["true_h_head"], rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(ys[:n], c["y_head"], rtol=1e-12, atol=1e-12)
+        assert abs(sum(hs) - c["sum_h"]) < 1e-9 * max(1.0, abs(c["sum_h"])), c["name"]
+        assert abs(sum(v * v for v in ys) - c["sum_y2"]) < 1e-9 * max(1.0, c["sum_y2"]), c["name"]
+
+
 def test_acklam_f64_accuracy(orc):
     """Acklam's rational approximation: relative error below 1.15e-9 (his published bound)."""
     from scipy.special import ndtri
