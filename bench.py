@@ -296,6 +296,8 @@ def bench_extensions(dev, args, lib, rank):
                  gpu_apf_step_many with host buffers
       imm        8 SV models x 4096 particles, 1000 ticks through gpu_imm_step (one host round trip per
                  tick, as the reference's API)
+      step_api   gpu_bpf_step per tick on the reference suite's throughput workload (matched-DGP
+                 Student-t scenario, N = 1K / 4K / 16K / 64K, 2000 ticks)
       smc2       256 theta-particles x 512 state particles, 500 updates of gpu_bpf_smc2_update with one
                  PMMH move per outer resample; smc2_cpmmh the same with correlated-noise moves (rho 0.99)
     CUDA events on the filters' streams where the work is device-resident, else wall clock around
@@ -397,6 +399,25 @@ def bench_extensions(dev, args, lib, rank):
     out["imm"] = {"workload": f"{len(grid)} models x 4096 particles, 1000 ticks of gpu_imm_step",
                   "us_per_tick": ms, "particle_steps_per_s": len(grid) * 4096 * 1000 / (ms / 1e3)}
 
+    # the synchronous per-tick API on the matched-DGP Student-t scenario (the reference suite's
+    # throughput test, tests/test_bpf_matched_dgp.cu:560-603): 100 warm-up ticks, then 2000 ticks
+    # of gpu_bpf_step, one Python call each (the reference arm times its filter in a C loop)
+    ys4 = np.asarray(step_api_series(), dtype=np.float32)
+    rows = {}
+    for n in STEP_API_N:
+        f = gpubpf.GpuBpf(n, 0.97, 0.15, -4.5, 5.0, 5.0, 42 + 900)
+        for t in range(100):
+            f.step(float(ys4[t % len(ys4)]))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for v in ys4.tolist():
+            f.step(v)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        f.close()
+        rows[str(n)] = {"us_per_tick": ms * 1e3 / len(ys4), "ticks_per_s": len(ys4) / (ms / 1e3)}
+    out["step_api"] = {"workload": STEP_API_WORKLOAD, "points": rows}
+
     # SMC^2, with fresh inner filters scoring the proposals and with correlated-noise (CPMMH) moves
     _, y2 = dgp.matched_series(600, RHO, SIG, MU, 11)
     for key, cp in (("smc2", 0.0), ("smc2_cpmmh", 0.99)):
@@ -418,6 +439,16 @@ def bench_extensions(dev, args, lib, rank):
                     "theta_sd": [float(v) for v in sd], "stats": st,
                     "acceptance": st["accepted"] / max(1, st["proposed"])}
     return out
+
+
+STEP_API_N = (1024, 4096, 16384, 65536)
+STEP_API_WORKLOAD = ("gpu_bpf_step per tick, matched-DGP Student-t scenario (rho 0.97, sigma_z 0.15, mu -4.5, "
+                     "nu_state 5, nu_obs 5, DGP seed 42, 2000 ticks after 100 warm-up), filter seed 942, ESS<0.5N")
+
+
+def step_api_series():
+    from gpubpf import dgp
+    return dgp.matched_series(2000, 0.97, 0.15, -4.5, 42, 5.0, 5.0)[1]
 
 
 def bench_config1(dev, args, lib, rank):
@@ -700,6 +731,15 @@ def reference_gpu(args, y):
     ya = np.asarray(ya, dtype=np.float32)
     out["apf"] = {str(n): {"ticks": t, "us_per_tick": refgpu.apf_time(n, RHO, SIG, MU, ya[:64 + t]) * 1e3}
                   for n, t in ((args.n, 300), (4096, 1000))}
+    # its synchronous per-tick API on the suite's throughput workload (same points as the extensions)
+    ys4 = np.asarray(step_api_series(), dtype=np.float32)
+    rows = {}
+    for n in STEP_API_N:
+        f = refgpu.RefGpuFilter(n, 0.97, 0.15, -4.5, 5.0, 5.0, seed=42 + 900)
+        ms = f.time_steps(ys4, warmup=100)
+        f.close()
+        rows[str(n)] = {"us_per_tick": ms * 1e3 / len(ys4), "ticks_per_s": len(ys4) / (ms / 1e3)}
+    out["step_api"] = {"workload": STEP_API_WORKLOAD + "; gpu_bpf_step in a C loop", "points": rows}
     return out
 
 

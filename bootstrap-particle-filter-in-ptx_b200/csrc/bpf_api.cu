@@ -52,6 +52,13 @@ struct Impl {
   BpfTickRecord* rec_dev = nullptr;     // [1 + kGraphChunk]: slot 0 single step, 1.. graph ticks
   BpfTickRecord* rec_pin = nullptr;     // pinned mirror
   DevState* st_pin = nullptr;           // pinned DevState snapshot
+  // single ticks (gpu_bpf_step / step_async) write their record and outcome straight into
+  // host-mapped memory, so reading the result back is one stream synchronise and no copy
+  BpfTickRecord* rec_map = nullptr;     // host view
+  BpfTickRecord* rec_map_dev = nullptr; // device view of the same memory
+  TickMirror* mir_map = nullptr;
+  TickMirror* mir_map_dev = nullptr;
+  bool last_in_map = false;             // the last enqueued tick wrote rec_map (not rec_dev[0])
   float* y_dev = nullptr;               // [kGraphChunk]
   float* y_pin = nullptr;               // [kGraphChunk]
   int32_t* anc_dev = nullptr;           // [N] when recording
@@ -209,6 +216,17 @@ int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
 }
 
 int read_back(GpuBpfState* s, Impl* m, int slot, BpfTickRecord* out) {
+  if (slot == 0 && m->last_in_map) {
+    CK(cudaStreamSynchronize(m->stream));
+    *out = *m->rec_map;                    // written by this tick's kernels, complete after the synchronise
+    const TickMirror mm = *m->mir_map;
+    s->did_resample = out->resampled;
+    s->resample_count = mm.resample_count;
+    s->timestep = mm.tick;
+    s->last_h_est = out->h_mean;
+    if (mm.error != BPF_OK) m->sticky_error = mm.error;
+    return BPF_OK;
+  }
   CK(cudaMemcpyAsync(m->rec_pin + slot, m->rec_dev + slot, sizeof(BpfTickRecord), cudaMemcpyDeviceToHost, m->stream));
   CK(cudaMemcpyAsync(m->st_pin, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost, m->stream));
   CK(cudaStreamSynchronize(m->stream));
@@ -237,6 +255,7 @@ int free_impl(Impl* m) {
   plan_free(m->plan);
   cudaFree(m->rec_dev); cudaFree(m->y_dev); cudaFree(m->anc_dev);
   cudaFreeHost(m->rec_pin); cudaFreeHost(m->st_pin); cudaFreeHost(m->y_pin);
+  cudaFreeHost(m->rec_map); cudaFreeHost(m->mir_map);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   return BPF_OK;
@@ -329,6 +348,12 @@ static int create_impl(GpuBpfState* s, Impl* m, int n, float rho, float sigma_z,
   CK(cudaMallocHost(&m->rec_pin, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
   CK(cudaMallocHost(&m->st_pin, sizeof(DevState)));
   CK(cudaMallocHost(&m->y_pin, kGraphChunk * sizeof(float)));
+  CK(cudaHostAlloc(&m->rec_map, sizeof(BpfTickRecord), cudaHostAllocMapped));
+  CK(cudaHostAlloc(&m->mir_map, sizeof(TickMirror), cudaHostAllocMapped));
+  CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->rec_map_dev), m->rec_map, 0));
+  CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->mir_map_dev), m->mir_map, 0));
+  std::memset(m->rec_map, 0, sizeof(BpfTickRecord));
+  std::memset(m->mir_map, 0, sizeof(TickMirror));
   CK(cudaMemsetAsync(m->rec_dev, 0, (1 + kGraphChunk) * sizeof(BpfTickRecord), m->stream));
   m->pass2_grid = pass2_grid_size(m->device);
   if (const char* v = std::getenv("BPF_DISABLE_PDL")) m->pdl = (v[0] == '0');
@@ -397,7 +422,11 @@ static int step_async_rc(GpuBpfState* s, float y_t) {
   if (rc) return rc;
   rc = ensure_device(m);
   if (rc) return rc;
-  return enqueue_tick(s, m, make_args(s, m, y_t, nullptr, m->rec_dev));
+  TickArgs a = make_args(s, m, y_t, nullptr, m->rec_map_dev ? m->rec_map_dev : m->rec_dev);
+  a.mirror = m->mir_map_dev;
+  rc = enqueue_tick(s, m, a);
+  if (rc == BPF_OK) m->last_in_map = m->rec_map_dev != nullptr;
+  return rc;
 }
 
 void gpu_bpf_step_async(GpuBpfState* s, float y_t) { step_async_rc(s, y_t); }
@@ -565,6 +594,7 @@ int gpu_bpf_step_many(GpuBpfState* s, const float* y, int n_ticks, BpfResult* ou
   }
   // keep slot 0 = last tick so get_result/get_record see it
   if (n_ticks > 0) {
+    m->last_in_map = false;
     const int last = (n_ticks - 1) % kGraphChunk;
     const BpfTickRecord& lr = m->rec_pin[1 + last];
     CK(cudaMemcpyAsync(m->rec_dev, m->rec_dev + 1 + last, sizeof(BpfTickRecord), cudaMemcpyDeviceToDevice, m->stream));
@@ -601,8 +631,10 @@ int gpu_bpf_step_many_device(GpuBpfState* s, const float* y_dev, int n_ticks, Bp
       if (rc) return rc;
     }
   }
-  if (n_ticks > 0)
+  if (n_ticks > 0) {
     CK(cudaMemcpyAsync(m->rec_dev, rec_dev + n_ticks - 1, sizeof(BpfTickRecord), cudaMemcpyDeviceToDevice, m->stream));
+    m->last_in_map = false;
+  }
   return BPF_OK;
 }
 
@@ -618,6 +650,7 @@ int gpu_bpf_reset(GpuBpfState* s, int seed) {
   CK(launch_init(m->plan, s->mu, std_stat, seed, m->stream));   // also resets the DevState
   g_launches += 1;
   m->ticks_enqueued = 0;
+  m->last_in_map = false;
   m->grad_count = 0;                               // the init kernel zeroes the device sums
   s->timestep = 0; s->did_resample = 1; s->resample_count = 0; s->last_h_est = s->mu;
   return BPF_OK;

@@ -321,6 +321,11 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     __syncthreads();
     if (tid < kStWords)
       reinterpret_cast<unsigned long long*>(p.st)[tid] = reinterpret_cast<const unsigned long long*>(&s_st)[tid];
+    if (tid == 0 && a.mirror) {
+      TickMirror mm;
+      mm.resample_count = st->resample_count; mm.tick = st->tick; mm.error = st->error; mm.pad = 0;
+      *a.mirror = mm;
+    }
   };
 
   // 1. FP64 combine of the tile partials (one 16-byte record per tile, eight in
@@ -785,7 +790,10 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       pass2_fetch(p, hsrc, rev ? n_items - 1 - nx : nx, smem, &mbar[0]);
     }
   }
-  if (tid == 0 && s_err) p.st->error = BPF_ERR_STATE;
+  if (tid == 0 && s_err) {
+    p.st->error = BPF_ERR_STATE;
+    if (a.mirror) a.mirror->error = BPF_ERR_STATE;
+  }
   griddep_release();
 }
 

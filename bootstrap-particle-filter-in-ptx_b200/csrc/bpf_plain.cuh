@@ -58,6 +58,15 @@ struct Plan {
   DevState* st;
 };
 
+// Host-mapped mirror of the state a synchronous tick reads back (zero-copy): written by the
+// plan kernel at the end of every tick it is given to, and by pass 2 when it records an error.
+struct TickMirror {
+  int resample_count;
+  int tick;                  // ticks completed
+  int error;                 // DevState::error
+  int pad;
+};
+
 struct TickArgs {
   float mu, rho, sigma;
   float ess_threshold;
@@ -76,6 +85,7 @@ struct TickArgs {
   float* ckpt;               // copy of the particles pass 1 reads this tick (G*4096 floats) or null
   int32_t* csr;              // on resampling ticks: first child slot of every parent (N ints) or null
   float2* aux;               // {1/S, nM}: normalised weight W_i = 2^(x_i - nM) / S of this tick, or null
+  TickMirror* mirror;        // host-mapped mirror of this tick's outcome, or null
 };
 
 // Device buffers of a plan for N particles (G, max_items set; DevState included).

@@ -82,6 +82,20 @@ double refgpu_time_run(void* sv, const float* y, int T, float* last) {
   return std::chrono::duration<double, std::milli>(t1 - t0).count();
 }
 
+// Wall time in milliseconds of `warmup` untimed then T timed ticks of the synchronous per-tick
+// API gpu_bpf_step (gpu_bpf_ptx_full.cu:764-775), the loop of the reference's matched-DGP
+// throughput test (tests/test_bpf_matched_dgp.cu:560-603): warm-up ticks take y[t % T].
+double refgpu_time_steps(void* sv, const float* y, int T, int warmup) {
+  GpuBpfState* s = static_cast<GpuBpfState*>(sv);
+  for (int t = 0; t < warmup; ++t) gpu_bpf_step(s, y[t % T]);
+  cudaDeviceSynchronize();
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int t = 0; t < T; ++t) gpu_bpf_step(s, y[t]);
+  cudaDeviceSynchronize();
+  const auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
 // Device state read-back: the PCG32 states [state, inc] per particle
 // (gpu_bpf_full.cuh:87), the particles and the normalised weights of the last tick.
 int refgpu_copy_rng(void* sv, unsigned long long* out, int n) {

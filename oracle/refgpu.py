@@ -38,6 +38,8 @@ def lib() -> C.CDLL:
         L.refgpu_run.argtypes = [vp, vp, i32, vp, vp]
         L.refgpu_time_run.restype = f64
         L.refgpu_time_run.argtypes = [vp, vp, i32, vp]
+        L.refgpu_time_steps.restype = f64
+        L.refgpu_time_steps.argtypes = [vp, vp, i32, i32]
         L.refgpu_apf_create.restype = vp
         L.refgpu_apf_create.argtypes = [i32, f32, f32, f32, f32, f32, i32]
         L.refgpu_apf_destroy.argtypes = [vp]
@@ -83,6 +85,11 @@ class RefGpuFilter:
         last = np.zeros(2, dtype=np.float32)
         ms = self.L.refgpu_time_run(self.s, _p(y), int(y.shape[0]), _p(last))
         return ms, float(last[0]), float(last[1])
+
+    def time_steps(self, y, warmup=100):
+        """warmup untimed then len(y) timed ticks of gpu_bpf_step in a C loop: milliseconds."""
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        return float(self.L.refgpu_time_steps(self.s, _p(y), int(y.shape[0]), int(warmup)))
 
     def _copy(self, name, dtype, count):
         out = np.zeros(count, dtype=dtype)
