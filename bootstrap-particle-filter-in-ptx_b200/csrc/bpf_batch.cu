@@ -54,13 +54,46 @@ size_t batch_smem_bytes(int maxn, bool sort_perm) {
 // Sorts the particles H (keys) with their log2-weights Wt, and perm when given, into ascending
 // order of H: a bitonic network whose comparators all put the smaller key at the lower index
 // (the first step of every merge compares mirrored positions), so positions n..2^k-1 act as
-// +inf and are never touched. Deterministic for equal keys. Ends with a barrier.
+// +inf and are never stored. Steps whose partners are less than 32 apart run on 32-element
+// segments held in registers (one element per lane, partners by warp shuffle); only the wider
+// steps go through shared memory with a barrier each. Deterministic for equal keys. Ends with a
+// barrier.
 template <int NT>
-__device__ void sort_particles(float* H, float* Wt, unsigned short* perm, int n) {
-  int m = 1;
+__device__ __noinline__ void sort_particles(float* H, float* Wt, unsigned short* perm, int n) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int m = 32;
   while (m < n) m <<= 1;
-  for (int k = 2; k <= m; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
+  // merges k = k_lo..k_hi, each from its step min(k/2, 16) down to 1, segment by segment
+  auto warp_steps = [&](int k_lo, int k_hi) {
+    for (int sg = warp; sg < (m >> 5); sg += W) {
+      const int i = (sg << 5) + lane;
+      const bool in = i < n;
+      float key = in ? H[swz(i)] : INFINITY;
+      float w = in ? Wt[swz(i)] : 0.0f;
+      unsigned pm = (perm && in) ? (unsigned)perm[i] : 0u;
+      for (int k = k_lo; k <= k_hi; k <<= 1) {
+        for (int j = min(k >> 1, 16); j > 0; j >>= 1) {
+          const bool mirror = j == (k >> 1);                  // k <= 32: the merge's first step
+          const int x = mirror ? k - 1 : j;
+          const bool lower = (lane & j) == 0;
+          const float pk = __shfl_xor_sync(0xffffffffu, key, x);
+          const float pw = __shfl_xor_sync(0xffffffffu, w, x);
+          const unsigned pp = perm ? __shfl_xor_sync(0xffffffffu, pm, x) : 0u;
+          if (lower ? (key > pk) : (pk > key)) { key = pk; w = pw; pm = pp; }
+        }
+      }
+      if (in) {
+        H[swz(i)] = key;
+        Wt[swz(i)] = w;
+        if (perm) perm[i] = (unsigned short)pm;
+      }
+    }
+    __syncthreads();
+  };
+  warp_steps(2, 32);
+  for (int k = 64; k <= m; k <<= 1) {
+    for (int j = k >> 1; j >= 32; j >>= 1) {
       for (int p = threadIdx.x; p < (m >> 1); p += NT) {
         const int off = p & (j - 1);
         const int i = ((p - off) << 1) + off;
@@ -78,6 +111,7 @@ __device__ void sort_particles(float* H, float* Wt, unsigned short* perm, int n)
       }
       __syncthreads();
     }
+    warp_steps(k, k);
   }
 }
 
