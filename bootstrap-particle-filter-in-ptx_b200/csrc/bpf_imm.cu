@@ -41,6 +41,9 @@ double lse(const double* x, int n) {
   return m + std::log(s);
 }
 
+// The tick's observation and the models' increments and means live in host-mapped memory: the
+// batched kernel reads y and writes its outputs there directly (the *_dev pointers are device
+// views of the *_pin allocations), so a tick is one graph launch and one synchronise, no copies.
 struct ImmImpl {
   int device = 0;
   GpuBpfBatch* batch = nullptr;
@@ -56,7 +59,6 @@ struct ImmImpl {
 void free_impl(ImmImpl* m) {
   if (!m) return;
   if (m->batch) gpu_bpf_batch_destroy(m->batch);
-  cudaFree(m->y_dev); cudaFree(m->dll_dev); cudaFree(m->hm_dev);
   cudaFreeHost(m->y_pin); cudaFreeHost(m->dll_pin); cudaFreeHost(m->hm_pin);
   delete m;
 }
@@ -108,14 +110,17 @@ GpuImmState* gpu_imm_create(const ImmModelParams* models, int n_models, int n_pa
     if (!m->batch) return fail(gpu_bpf_last_error());
     if (cudaGetDevice(&m->device) != cudaSuccess) return fail(BPF_ERR_CUDA);
     m->stream = (cudaStream_t)gpu_bpf_batch_stream(m->batch);
-    if (cudaMalloc(&m->y_dev, sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&m->dll_dev, K * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&m->hm_dev, K * sizeof(float)) != cudaSuccess ||
-        cudaMallocHost(&m->y_pin, sizeof(float)) != cudaSuccess ||
-        cudaMallocHost(&m->dll_pin, K * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&m->hm_pin, K * sizeof(float)) != cudaSuccess) {
+    if (cudaHostAlloc(&m->y_pin, sizeof(float), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostAlloc(&m->dll_pin, K * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostAlloc(&m->hm_pin, K * sizeof(float), cudaHostAllocMapped) != cudaSuccess) {
       cudaGetLastError();
       return fail(BPF_ERR_ALLOC);
+    }
+    if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->y_dev), m->y_pin, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->dll_dev), m->dll_pin, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->hm_dev), m->hm_pin, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(BPF_ERR_CUDA);
     }
   } else {
     s->filters = (GpuBpfState**)calloc(K, sizeof(GpuBpfState*));
@@ -162,15 +167,9 @@ ImmResult gpu_imm_step(GpuImmState* s, float y_t) {
       bpf_record_error(BPF_ERR_CUDA);
       return bad;
     }
-    *m->y_pin = y_t;
-    if (cudaMemcpyAsync(m->y_dev, m->y_pin, sizeof(float), cudaMemcpyHostToDevice, m->stream) != cudaSuccess) {
-      bpf_record_error(BPF_ERR_CUDA);
-      return bad;
-    }
+    *m->y_pin = y_t;                       // the previous tick has completed: nothing reads it now
     if (gpu_bpf_batch_step_device(m->batch, m->y_dev, 1, m->dll_dev, m->hm_dev) != BPF_OK) return bad;
-    if (cudaMemcpyAsync(m->dll_pin, m->dll_dev, K * sizeof(double), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
-        cudaMemcpyAsync(m->hm_pin, m->hm_dev, K * sizeof(float), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
-        cudaStreamSynchronize(m->stream) != cudaSuccess) {
+    if (cudaStreamSynchronize(m->stream) != cudaSuccess) {
       cudaGetLastError();
       bpf_record_error(BPF_ERR_CUDA);
       return bad;
