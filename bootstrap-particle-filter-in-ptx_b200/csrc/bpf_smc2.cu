@@ -78,7 +78,7 @@ struct GpuBpfSmc2 {
   cudaStream_t stream = nullptr;
   float* d_y = nullptr;
   float* y_pin = nullptr;
-  double* d_dll = nullptr;
+  double* d_dll = nullptr;                 // device view of dll_pin (host-mapped): the forward tick's increments
   double* dll_pin = nullptr;
   int* d_idx = nullptr;
   int* d_mask = nullptr;
@@ -136,7 +136,7 @@ void free_smc2(GpuBpfSmc2* s) {
   if (!s) return;
   if (s->cur) gpu_bpf_batch_destroy(s->cur);
   if (s->prop) gpu_bpf_batch_destroy(s->prop);
-  cudaFree(s->d_y); cudaFree(s->d_dll); cudaFree(s->d_idx); cudaFree(s->d_mask); cudaFree(s->d_seed);
+  cudaFree(s->d_y); cudaFree(s->d_idx); cudaFree(s->d_mask); cudaFree(s->d_seed);
   cudaFree(s->s_tab); cudaFree(s->s_st); cudaFree(s->s_h); cudaFree(s->s_w);
   cudaFreeHost(s->y_pin); cudaFreeHost(s->dll_pin); cudaFreeHost(s->i_pin); cudaFreeHost(s->st_pin);
   cudaFreeHost(s->ll_pin);
@@ -339,7 +339,6 @@ GpuBpfSmc2* gpu_bpf_smc2_create(int n_theta, int n_particles, int max_ticks, con
   auto al = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(ptr, bytes); };
   auto ah = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = cudaMallocHost(ptr, bytes); };
   al(&s->d_y, (size_t)max_ticks * sizeof(float));
-  al(&s->d_dll, n_theta * sizeof(double));
   al(&s->d_idx, n_theta * sizeof(int));
   al(&s->d_mask, n_theta * sizeof(int));
   al(&s->d_seed, n_theta * sizeof(int));
@@ -348,7 +347,8 @@ GpuBpfSmc2* gpu_bpf_smc2_create(int n_theta, int n_particles, int max_ticks, con
   al(&s->s_h, nh * sizeof(float));
   al(&s->s_w, nh * sizeof(float));
   ah(&s->y_pin, sizeof(float));
-  ah(&s->dll_pin, n_theta * sizeof(double));
+  if (e == cudaSuccess) e = cudaHostAlloc(&s->dll_pin, n_theta * sizeof(double), cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_dll), s->dll_pin, 0);
   ah(&s->i_pin, 2 * n_theta * sizeof(int));
   ah(&s->st_pin, n_theta * sizeof(BatchFilterState));
   ah(&s->ll_pin, n_theta * sizeof(double));
@@ -388,8 +388,7 @@ float gpu_bpf_smc2_update(GpuBpfSmc2* s, float y) {
     return NAN;
   }
   if (batch_step_abs(s->cur, s->d_y, 1, s->d_dll) != BPF_OK) return NAN;
-  if (cudaMemcpyAsync(s->dll_pin, s->d_dll, s->n_theta * sizeof(double), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
-      cudaStreamSynchronize(s->stream) != cudaSuccess) {
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
     cudaGetLastError();
     bpf_record_error(BPF_ERR_CUDA);
     return NAN;
