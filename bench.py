@@ -84,13 +84,21 @@ def parse_args():
     return ap.parse_args()
 
 
+FALLBACK_HBM_GBS = 6650.0   # an earlier STREAM-style copy measurement on this pool's B200s
+
+
 def load_peaks():
+    """(HBM GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json when it holds a
+    usable `hbm_gbs`, else the fallback figure."""
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
+    try:
         with open(p) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+            v = float(json.load(f)["hbm_gbs"])
+        if v > 0.0:
+            return v, "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
+    return FALLBACK_HBM_GBS, f"fallback {FALLBACK_HBM_GBS:.0f} GB/s (MEASURED_PEAKS.json absent or without hbm_gbs)"
 
 
 def load_traffic():
@@ -836,7 +844,7 @@ def main():
     roofline = {
         "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
         "traffic": (tr * N if tr is not None else None),
-        "kernel": dominant + "_kernel", "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+        "kernel": dominant + "_kernel", "peak_source": peak_kind,
         "algorithmic_bytes_per_launch": (bytes_p1 if dominant == "pass1" else bytes_p2) / max(1, nl),
         "avg_launch_us": tms / max(1, nl) * 1e3,
         "pass1": {"ms": p1_ms, "launches": n1, "GBps": ach1, "frac": ach1 / peak},
