@@ -72,6 +72,20 @@ struct Impl {
   float g_mu = NAN, g_rho = NAN, g_sigma = NAN, g_thr = NAN, g_nus = NAN;
   bool g_anc = false;
 
+  // graph of one tick for single steps (gpu_bpf_step / step_async), keyed likewise: pass 1's
+  // node gets the tick's observation by a parameter update of the instantiated graph, so a tick
+  // is one graph launch instead of three kernel launches. t_g (the captured graph) stays alive
+  // because the update names pass 1's node in it; t_params points at t_plan / t_args.
+  cudaGraph_t t_g = nullptr;
+  cudaGraphExec_t tgraph = nullptr;
+  cudaGraphNode_t t_pass1 = nullptr;
+  cudaKernelNodeParams t_params{};
+  Plan t_plan{};
+  TickArgs t_args{};
+  void* t_argv[2] = {nullptr, nullptr};
+  float t_mu = NAN, t_rho = NAN, t_sigma = NAN, t_thr = NAN, t_nus = NAN;
+  bool t_anc = false;
+
   // graph of a whole device-resident run (step_many_device), keyed likewise
   cudaGraphExec_t dgraph = nullptr;
   const float* dg_y = nullptr;
@@ -250,6 +264,8 @@ int free_impl(Impl* m) {
   if (!m) return BPF_OK;
   if (m->graph) cudaGraphExecDestroy(m->graph);
   if (m->dgraph) cudaGraphExecDestroy(m->dgraph);
+  if (m->tgraph) cudaGraphExecDestroy(m->tgraph);
+  if (m->t_g) cudaGraphDestroy(m->t_g);
   for (cudaEvent_t e : m->ev_pending) cudaEventDestroy(e);
   for (cudaEvent_t e : m->ev_pool) cudaEventDestroy(e);
   plan_free(m->plan);
@@ -302,6 +318,50 @@ int build_device_graph(GpuBpfState* s, Impl* m, const float* y_dev, int n, BpfTi
   m->dg_mu = s->mu; m->dg_rho = s->rho; m->dg_sigma = s->sigma_z; m->dg_thr = s->ess_threshold;
   m->dg_nus = s->nu_state;
   m->dg_anc = m->record_anc;
+  return BPF_OK;
+}
+
+bool tick_graph_stale(GpuBpfState* s, Impl* m) {
+  return !m->tgraph || m->t_mu != s->mu || m->t_rho != s->rho || m->t_sigma != s->sigma_z ||
+         m->t_thr != s->ess_threshold || m->t_nus != s->nu_state || m->t_anc != m->record_anc;
+}
+
+// Captures one tick (pass 1, plan, pass 2 with their programmatic dependencies) writing its
+// record and outcome into the host-mapped slot, and finds pass 1's node: the graph's only root.
+int build_tick_graph(GpuBpfState* s, Impl* m) {
+  if (m->tgraph) { cudaGraphExecDestroy(m->tgraph); m->tgraph = nullptr; }
+  if (m->t_g) { cudaGraphDestroy(m->t_g); m->t_g = nullptr; }
+  m->t_pass1 = nullptr;
+  TickArgs a = make_args(s, m, 0.0f, nullptr, m->rec_map_dev);
+  a.mirror = m->mir_map_dev;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t err = launch_tick3(m, a);
+  const cudaError_t e2 = cudaStreamEndCapture(m->stream, &g);
+  if (err != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return set_err(BPF_ERR_CUDA); }
+  size_t nroot = 0;
+  cudaGraphNode_t root = nullptr;
+  cudaGraphNodeType type = cudaGraphNodeTypeEmpty;
+  if (cudaGraphGetRootNodes(g, nullptr, &nroot) != cudaSuccess || nroot != 1 ||
+      cudaGraphGetRootNodes(g, &root, &nroot) != cudaSuccess || cudaGraphNodeGetType(root, &type) != cudaSuccess ||
+      type != cudaGraphNodeTypeKernel || cudaGraphKernelNodeGetParams(root, &m->t_params) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    cudaGetLastError();
+    return set_err(BPF_ERR_CUDA);
+  }
+  cudaGraphExec_t ex = nullptr;
+  if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) { cudaGraphDestroy(g); cudaGetLastError(); return set_err(BPF_ERR_CUDA); }
+  m->t_g = g;
+  m->tgraph = ex;
+  m->t_pass1 = root;
+  m->t_plan = m->plan;                     // pass 1's arguments, as launch_pass1 passed them
+  m->t_args = a;
+  m->t_argv[0] = &m->t_plan;
+  m->t_argv[1] = &m->t_args;
+  m->t_params.kernelParams = m->t_argv;
+  m->t_params.extra = nullptr;
+  m->t_mu = s->mu; m->t_rho = s->rho; m->t_sigma = s->sigma_z; m->t_thr = s->ess_threshold; m->t_nus = s->nu_state;
+  m->t_anc = m->record_anc;
   return BPF_OK;
 }
 
@@ -414,7 +474,10 @@ void gpu_bpf_destroy(GpuBpfState* s) {
   free(s);
 }
 
-static int step_async_rc(GpuBpfState* s, float y_t) {
+// One tick enqueued. A synchronous step (one_shot) launches the single-tick graph (less host
+// time per tick); consecutive asynchronous steps launch the kernels directly, so each tick's
+// pass 1 overlaps the previous tick's pass 2 through programmatic dependent launch.
+static int step_async_rc(GpuBpfState* s, float y_t, bool one_shot) {
   Impl* m = impl_of(s);
   if (!m) return set_err(BPF_ERR_STATE);
   if (!std::isfinite(y_t)) return set_err(BPF_ERR_ARG);
@@ -422,14 +485,24 @@ static int step_async_rc(GpuBpfState* s, float y_t) {
   if (rc) return rc;
   rc = ensure_device(m);
   if (rc) return rc;
-  TickArgs a = make_args(s, m, y_t, nullptr, m->rec_map_dev ? m->rec_map_dev : m->rec_dev);
+  if (one_shot && !m->profiling && !m->learn_mode) {  // learning updates need the host every K ticks
+    if (tick_graph_stale(s, m)) { rc = build_tick_graph(s, m); if (rc) return rc; }
+    m->t_args.obs.y = y_t;
+    CK(cudaGraphExecKernelNodeSetParams(m->tgraph, m->t_pass1, &m->t_params));
+    CK(cudaGraphLaunch(m->tgraph, m->stream));
+    g_launches += 3;
+    m->ticks_enqueued += 1;
+    m->last_in_map = true;
+    return BPF_OK;
+  }
+  TickArgs a = make_args(s, m, y_t, nullptr, m->rec_map_dev);
   a.mirror = m->mir_map_dev;
   rc = enqueue_tick(s, m, a);
-  if (rc == BPF_OK) m->last_in_map = m->rec_map_dev != nullptr;
+  if (rc == BPF_OK) m->last_in_map = true;
   return rc;
 }
 
-void gpu_bpf_step_async(GpuBpfState* s, float y_t) { step_async_rc(s, y_t); }
+void gpu_bpf_step_async(GpuBpfState* s, float y_t) { step_async_rc(s, y_t, false); }
 
 BpfResult gpu_bpf_get_result(GpuBpfState* s) {
   BpfResult bad; bad.h_mean = NAN; bad.log_lik = NAN;
@@ -444,7 +517,7 @@ BpfResult gpu_bpf_get_result(GpuBpfState* s) {
 
 BpfResult gpu_bpf_step(GpuBpfState* s, float y_t) {
   BpfResult bad; bad.h_mean = NAN; bad.log_lik = NAN;
-  if (step_async_rc(s, y_t) != BPF_OK) return bad;
+  if (step_async_rc(s, y_t, true) != BPF_OK) return bad;
   return gpu_bpf_get_result(s);
 }
 

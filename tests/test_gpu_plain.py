@@ -268,6 +268,37 @@ def test_parameters_change_between_ticks(bpf, orc):
     a.close(); b.close()
 
 
+def test_single_tick_graph_matches_direct_launches(bpf):
+    """gpu_bpf_step (one captured tick graph, pass 1's observation updated per call) against
+    gpu_bpf_step_async + get_record (direct launches), with mu, the ESS threshold and ancestor
+    recording changed between ticks (each change re-captures the graph): identical records and
+    ancestors."""
+    _, y = series(90, 7)
+    a = bpf.GpuBpf(5000, RHO, SIG, MU, seed=12, ess_threshold=0.5)
+    b = bpf.GpuBpf(5000, RHO, SIG, MU, seed=12, ess_threshold=0.5)
+    for t, v in enumerate(y):
+        if t == 30:
+            a.set_mu(-0.6); b.set_mu(-0.6)
+        if t == 50:
+            a.set_ess_threshold(0.0); b.set_ess_threshold(0.0)
+        if t == 70:
+            a.record_ancestors(True); b.record_ancestors(True)
+        ra = a.step(float(v))
+        rec_a = a.get_record()
+        b.step_async(float(v))
+        rec_b = b.get_record()
+        assert (rec_a.dloglik, rec_a.h_mean, rec_a.ess, rec_a.resampled, rec_a.tick) == \
+               (rec_b.dloglik, rec_b.h_mean, rec_b.ess, rec_b.resampled, rec_b.tick), t
+        assert ra.h_mean == rec_a.h_mean
+        if t >= 70:
+            fa, aa = a.get_ancestors()
+            fb, ab = b.get_ancestors()
+            assert fa == fb and bytes(aa) == bytes(ab), t
+    assert a.state.resample_count == b.state.resample_count and a.state.timestep == b.state.timestep == len(y)
+    assert bytes(a.get_particles()) == bytes(b.get_particles())
+    a.close(); b.close()
+
+
 def test_independent_filters_do_not_interact(bpf):
     _, y = series(50, 42)
     solo = bpf.GpuBpf(10_000, RHO, SIG, MU, seed=21, ess_threshold=0.5)
