@@ -2,7 +2,8 @@
 correlated-noise PMMH moves (gpu_bpf_smc2_set_cpmmh_rho; the reference's CPMMH rejuvenation,
 smc2/smc2_rbpf_batch.cu:651-935, and smc2_cuda_set_cpmmh_rho :1238-1240).
 
-  fresh run (no input noise)            recorded normals equal the filters' PCG32 draws bit for bit
+  fresh run (no input noise; Gaussian    recorded normals equal the filters' PCG32 draws bit for bit
+  and Student-t observations)
                                         (slot kBatchMaxN = 16384 for the resampling normal); the
                                         FP64 oracle driven by the recorded noise, the GPU's
                                         resampling decisions and slot ancestors: per-tick dll <= 2e-4
@@ -44,12 +45,13 @@ def _series(T, theta=(MU, RHO, SIG), seed=42):
     return np.asarray(ys, dtype=np.float32)
 
 
-def _filters(ns, seed0=100):
+def _filters(ns, seed0=100, nu_obs=None):
     rng = np.random.default_rng(4)
     out = []
     for j, n in enumerate(ns):
         out.append({"mu": float(rng.normal(-1.0, 0.3)), "rho": float(rng.uniform(0.9, 0.99)),
-                    "sigma_z": float(rng.uniform(0.1, 0.3)), "n_particles": int(n), "seed": seed0 + j})
+                    "sigma_z": float(rng.uniform(0.1, 0.3)), "n_particles": int(n), "seed": seed0 + j,
+                    "nu_obs": float(nu_obs[j]) if nu_obs is not None else 0.0})
     return out
 
 
@@ -79,9 +81,9 @@ def _area(b, nz, f, T, n):
 def test_fresh_run_records_pcg_noise_and_matches_oracle(bpf, orc):
     import torch
     lib = bpf.load()
-    ns = [512, 1000, 4096, 37]
+    ns = [512, 1000, 4096, 37, 800]
     T = 60
-    fl = _filters(ns)
+    fl = _filters(ns, nu_obs=[0.0, 0.0, 0.0, 0.0, 5.0])        # the last one: Student-t observations
     y = _series(T)
     b = bpf.GpuBpfBatch(fl, ess_threshold=0.5)
     nfl = b.noise_offset(len(ns), T)
@@ -105,7 +107,7 @@ def test_fresh_run_records_pcg_noise_and_matches_oracle(bpf, orc):
         flags = (anc[:, 0] >= 0).astype(np.int32)          # resampling ticks wrote their ancestors
         assert flags.sum() > 0
         o = orc.filter_noise_f64(n, fd["rho"], fd["sigma_z"], fd["mu"], y, z, ess_threshold=0.5,
-                                 anc_replay=np.maximum(anc, 0), flags_replay=flags)
+                                 nu_obs=fd["nu_obs"], anc_replay=np.maximum(anc, 0), flags_replay=flags)
         np.testing.assert_array_equal(o["resampled"], flags)
         np.testing.assert_allclose(r["dll"][f], o["dll"], atol=2e-4, rtol=0)
         assert abs(r["dll"][f].sum() - o["dll"].sum()) <= 1e-4 * abs(o["dll"].sum())
