@@ -221,17 +221,21 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
       }
       tmax[k] = m;
     }
+    // the reductions run for the filter's G tiles only (G is the same for the whole CTA)
 #pragma unroll
     for (int k = 0; k < kBatchMaxTiles; ++k) {
-      const float v = warp_max_f(tmax[k]);
-      if (lane == 0) sh.tmax[k][warp] = v;
+      if (k < G) {
+        const float v = warp_max_f(tmax[k]);
+        if (lane == 0) sh.tmax[k][warp] = v;
+      }
     }
     __syncthreads();
     int nk[kBatchMaxTiles];
 #pragma unroll
     for (int k = 0; k < kBatchMaxTiles; ++k) {
       float m = -INFINITY;
-      for (int w = 0; w < W; ++w) m = fmaxf(m, sh.tmax[k][w]);
+      if (k < G)
+        for (int w = 0; w < W; ++w) m = fmaxf(m, sh.tmax[k][w]);
       nk[k] = (m == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(m, -1.0e9f));
     }
 
@@ -254,18 +258,20 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
           E += fix_weight(w);
         }
       }
-      const double dS = warp_sum_d((double)fS), dQ = warp_sum_d((double)fQ), dH = warp_sum_d((double)fH);
-      E = warp_sum_u64(E);
-      if (lane == 0) { sh.sred[0][k][warp] = dS; sh.sred[1][k][warp] = dQ; sh.sred[2][k][warp] = dH; sh.ered[k][warp] = E; }
+      if (k < G) {
+        const double dS = warp_sum_d((double)fS), dQ = warp_sum_d((double)fQ), dH = warp_sum_d((double)fH);
+        E = warp_sum_u64(E);
+        if (lane == 0) { sh.sred[0][k][warp] = dS; sh.sred[1][k][warp] = dQ; sh.sred[2][k][warp] = dH; sh.ered[k][warp] = E; }
+      }
     }
     __syncthreads();
-    // per-tile sums over the warps, one warp per tile (a fixed shuffle tree)
+    // per-tile sums over the warps, one warp per tile (a fixed shuffle tree over its W lanes)
     for (int k = warp; k < G; k += W) {
       const bool on = lane < W;
-      const double s1 = warp_sum_d(on ? sh.sred[0][k][lane] : 0.0);
-      const double s2 = warp_sum_d(on ? sh.sred[1][k][lane] : 0.0);
-      const double s3 = warp_sum_d(on ? sh.sred[2][k][lane] : 0.0);
-      const unsigned long long e = warp_sum_u64(on ? sh.ered[k][lane] : 0ull);
+      const double s1 = warp_sum_d_w<W>(on ? sh.sred[0][k][lane] : 0.0);
+      const double s2 = warp_sum_d_w<W>(on ? sh.sred[1][k][lane] : 0.0);
+      const double s3 = warp_sum_d_w<W>(on ? sh.sred[2][k][lane] : 0.0);
+      const unsigned long long e = warp_sum_u64_w<W>(on ? sh.ered[k][lane] : 0ull);
       if (lane == 0) { sh.tsum[0][k] = s1; sh.tsum[1][k] = s2; sh.tsum[2][k] = s3; sh.tmass[k] = e; }
     }
     __syncthreads();

@@ -14,7 +14,7 @@ namespace bpf_batch_detail {
 
 constexpr int kClasses = 5;
 constexpr int kClassMaxN[kClasses] = {1024, 2048, 4096, 8192, 16384};
-constexpr int kDefaultThreads[kClasses] = {128, 256, 256, 512, 1024};
+constexpr int kDefaultThreads[kClasses] = {256, 256, 512, 512, 1024};
 constexpr int kThreadChoices[] = {64, 128, 256, 512, 1024};
 
 #define BCK(call)                                                             \

@@ -79,6 +79,21 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Sums over lanes 0..WIDTH-1 (WIDTH a power of two <= 32), complete in those lanes. When the
+// other lanes hold zeros, lane 0 gets the same value as warp_sum_d / warp_sum_u64 (their extra
+// steps only add exact zeros).
+template <int WIDTH>
+__device__ __forceinline__ double warp_sum_d_w(double v) {
+#pragma unroll
+  for (int o = WIDTH / 2; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int WIDTH>
+__device__ __forceinline__ unsigned long long warp_sum_u64_w(unsigned long long v) {
+#pragma unroll
+  for (int o = WIDTH / 2; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan_add(T v, int lane) {
 #pragma unroll

@@ -116,7 +116,9 @@ def test_batch_cta_shape_does_not_change_results(bpf):
     b = _run_debug(bpf, fl, y, 0.5, threads={0: 256, 2: 512, 3: 1024, 4: 1024})
     np.testing.assert_array_equal(a[2], b[2])          # ancestors
     np.testing.assert_array_equal(a[3], b[3])          # particles
-    np.testing.assert_allclose(a[0], b[0], rtol=1e-9)  # log-likelihood (sum order only)
+    # log-likelihood: the per-thread FP32 partial sums take other particles under another CTA
+    # shape (FP32 rounding of S, sum W^2, sum W h), so totals agree to about 1e-8 relative
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-7)
 
 
 def test_batch_graph_run_and_autotune(bpf, tmp_path):
@@ -137,7 +139,7 @@ def test_batch_graph_run_and_autotune(bpf, tmp_path):
     chosen = [b.get_threads(c) for c in range(5)]
     assert all(t in (64, 128, 256, 512, 1024) for t in chosen)
     ll2, _ = b.run(y.tolist())
-    np.testing.assert_allclose(ll2, ll_host, rtol=1e-9)
+    np.testing.assert_allclose(ll2, ll_host, rtol=1e-7)  # the autotuned shapes regroup the FP32 partials
     lines = open(cache).read().split()
     assert len(lines) % 3 == 0 and len(lines) >= 3
     b2 = bpf.GpuBpfBatch(fl, ess_threshold=0.0)
