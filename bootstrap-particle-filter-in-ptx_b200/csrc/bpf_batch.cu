@@ -44,7 +44,12 @@ struct BatchShared {
   unsigned long long base, delta, magic;
   int resample, carry, next;
   double gred[5][NT / 32];
+  double fin_ll, fin_logS;                     // the log-likelihood keeper's state at the end of a run
 };
+
+// The tick's decision runs on thread 0; the FP64 logarithm of the weight sum, the increment and
+// the running log-likelihood on the first lane of the second warp (kLogTid), concurrently.
+constexpr int kLogTid = 32;
 
 size_t batch_smem_bytes(int maxn, bool sort_perm) {
   const size_t u16 = (((size_t)maxn * 2 + 15) / 16) * 16;
@@ -145,7 +150,8 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
   float* Wt = bufB;
   uint64_t At = 1ull, Bt = 0ull;
   // thread-0 filter state
-  double logS_prev = log((double)N), ll_total = 0.0;
+  const double logN = log((double)N);
+  double logS_prev = logN, ll_total = 0.0;     // kept by thread kLogTid
   uint64_t ustate = (unsigned long long)f.seed * 67890ULL + 12345ULL;
   int n_res = 0;
   float hm_last = 0.0f;
@@ -276,8 +282,8 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
     }
     __syncthreads();
 
-    // 3. decision (thread 0)
-    if (tid == 0) {
+    // 3. decision (thread 0) and log-likelihood (thread kLogTid), from the same sums
+    if (tid == 0 || tid == kLogTid) {
       int nM = kNkEmpty;
       for (int k = 0; k < G; ++k) nM = max(nM, nk[k]);
       double S = 0.0, Q = 0.0, Hm = 0.0;
@@ -290,64 +296,63 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
         S += sh.tsum[0][k] * sc; Q += sh.tsum[1][k] * sc * sc; Hm += sh.tsum[2][k] * sc;
       }
       const bool degenerate = (nM == kNkEmpty) || !(S > 0.0);
-      double dll;
       int resample = 0;
-      float hm = __int_as_float(0x7fc00000);
-      if (degenerate) {
-        dll = -INFINITY;
-      } else {
-        dll = (double)nM * 0.693147180559945309417232121458 + log(S) - logS_prev;
+      if (!degenerate) {
         const double ess = S * S / Q;
-        hm = (float)(Hm / S);
         resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
       }
-      ll_total += dll;
-      hm_last = hm;
-      if (a.g_norm)
-        a.g_norm[t] = degenerate ? make_float2(0.0f, 0.0f) : make_float2((float)(1.0 / S), __int_as_float(nM));
-      if (a.dll) a.dll[(size_t)b * a.T + (t - t0)] = dll;
-      if (a.hmean) a.hmean[(size_t)b * a.T + (t - t0)] = hm;
-      unsigned long long u = 0ull;
-      if constexpr (NOISE) {
-        // the tick's resampling normal: slot kBatchMaxN of the filter's streams (no particle's)
-        float v = icdf_normal(pcg_uniform(pcg_output(c.k1 + c.k2 * pcg_inc((uint32_t)kBatchMaxN))));
-        if (zi) v = fmaf(cr, zi[(size_t)t * nzs + npad], cs * v);
-        zo[(size_t)t * nzs + npad] = v;
-        u = u23_of_normal(v);
-      }
-      if (resample) {
-        if constexpr (!NOISE) {
-          const uint64_t old = ustate;
-          ustate = old * kPcgMult + kHostInc;
-          u = pcg_output(old) >> 9;
-        }
-        logS_prev = log((double)N);
-        ++n_res;
-        const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
-        unsigned long long P = 0ull;
-        for (int k = 0; k < kBatchMaxTiles; ++k) {
-          const int r = (k < G && nk[k] != kNkEmpty) ? nM - nk[k] + kFixF - Fg : 64;
-          sh.rk[k] = r;
-          sh.Pk[k] = P;
-          P += shr64(Ek[k], r);
-        }
-        unsigned long long delta = udiv_fp64(P, (unsigned long long)N);
-        if (delta == 0ull) delta = 1ull;
-        const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
-        sh.base = (hi << 41) | (lo >> 23);
-        sh.delta = delta;
-        sh.magic = udiv_magic_of(delta);
-        sh.carry = 0;
-      } else if (degenerate) {
-        logS_prev = log((double)N);
-        sh.carry = 0;
+      if (tid == kLogTid) {
+        const double lS = degenerate ? 0.0 : log(S);
+        const double dll = degenerate ? -INFINITY
+                                      : (double)nM * 0.693147180559945309417232121458 + lS - logS_prev;
+        ll_total += dll;
+        if (a.dll) a.dll[(size_t)b * a.T + (t - t0)] = dll;
+        logS_prev = (resample || degenerate) ? logN : lS;
       } else {
-        logS_prev = log(S);
-        for (int k = 0; k < kBatchMaxTiles; ++k)
-          sh.carry_off[k] = (k < G && nk[k] != kNkEmpty) ? (float)(nk[k] - nM) : -INFINITY;
-        sh.carry = 1;
+        const float hm = degenerate ? __int_as_float(0x7fc00000) : (float)(Hm / S);
+        hm_last = hm;
+        if (a.g_norm)
+          a.g_norm[t] = degenerate ? make_float2(0.0f, 0.0f) : make_float2((float)(1.0 / S), __int_as_float(nM));
+        if (a.hmean) a.hmean[(size_t)b * a.T + (t - t0)] = hm;
+        unsigned long long u = 0ull;
+        if constexpr (NOISE) {
+          // the tick's resampling normal: slot kBatchMaxN of the filter's streams (no particle's)
+          float v = icdf_normal(pcg_uniform(pcg_output(c.k1 + c.k2 * pcg_inc((uint32_t)kBatchMaxN))));
+          if (zi) v = fmaf(cr, zi[(size_t)t * nzs + npad], cs * v);
+          zo[(size_t)t * nzs + npad] = v;
+          u = u23_of_normal(v);
+        }
+        if (resample) {
+          if constexpr (!NOISE) {
+            const uint64_t old = ustate;
+            ustate = old * kPcgMult + kHostInc;
+            u = pcg_output(old) >> 9;
+          }
+          ++n_res;
+          const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
+          unsigned long long P = 0ull;
+          for (int k = 0; k < kBatchMaxTiles; ++k) {
+            const int r = (k < G && nk[k] != kNkEmpty) ? nM - nk[k] + kFixF - Fg : 64;
+            sh.rk[k] = r;
+            sh.Pk[k] = P;
+            P += shr64(Ek[k], r);
+          }
+          unsigned long long delta = udiv_fp64(P, (unsigned long long)N);
+          if (delta == 0ull) delta = 1ull;
+          const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
+          sh.base = (hi << 41) | (lo >> 23);
+          sh.delta = delta;
+          sh.magic = udiv_magic_of(delta);
+          sh.carry = 0;
+        } else if (degenerate) {
+          sh.carry = 0;
+        } else {
+          for (int k = 0; k < kBatchMaxTiles; ++k)
+            sh.carry_off[k] = (k < G && nk[k] != kNkEmpty) ? (float)(nk[k] - nM) : -INFINITY;
+          sh.carry = 1;
+        }
+        sh.resample = resample;
       }
-      sh.resample = resample;
     }
     At = At * kPcgMult;
     Bt = Bt * kPcgMult + 1ull;
@@ -429,13 +434,15 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
     if (sh.carry)
       for (int i = tid; i < N; i += NT) a.st_w[soff + i] = Wt[swz(i)];
   }
+  if (tid == kLogTid) { sh.fin_ll = ll_total; sh.fin_logS = logS_prev; }
+  __syncthreads();
   if (tid == 0) {
-    a.loglik[b] = ll_total;
+    a.loglik[b] = sh.fin_ll;
     a.h_final[b] = hm_last;
     a.resamples[b] = n_res;
     if (fs) {
       BatchFilterState r;
-      r.logS_prev = logS_prev; r.ll_total = ll_total; r.ustate = ustate;
+      r.logS_prev = sh.fin_logS; r.ll_total = sh.fin_ll; r.ustate = ustate;
       r.carry = sh.carry; r.n_res = n_res; r.hm_last = hm_last; r.pad = 0;
       for (int k = 0; k < kBatchMaxTiles; ++k) r.carry_off[k] = sh.carry_off[k];
       *fs = r;
