@@ -149,3 +149,18 @@ def test_apf_host_side(lib):
         lib.gpu_apf_destroy(s)
         pytest.skip("GPU present")
     assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_NODEVICE
+
+
+def test_correlated_noise_and_smc2_host_side(lib):
+    """The correlated-noise and SMC^2 entry points reject NULL handles and bad arguments on the
+    host, before any CUDA call."""
+    from gpubpf import _lib
+    assert lib.gpu_bpf_smc2_set_cpmmh_rho(None, 0.5) == _lib.BPF_ERR_STATE
+    assert lib.gpu_bpf_smc2_get_last_move(None, None, None, None, None, None) == _lib.BPF_ERR_STATE
+    assert lib.gpu_bpf_smc2_get_noise(None, 0, 1, None) == _lib.BPF_ERR_STATE
+    assert lib.gpu_bpf_batch_run_correlated(None, None, 1, None, None, 0.5, None, None, None) == _lib.BPF_ERR_STATE
+    assert lib.gpu_bpf_batch_noise_offset(None, 0, 10) < 0
+    assert not lib.gpu_bpf_smc2_create(1, 512, 100, None, 1)                 # fewer than 2 theta-particles
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_ARG
+    assert not lib.gpu_bpf_smc2_create(64, 20000, 100, None, 1)              # above 16384 particles
+    assert lib.gpu_bpf_last_error() == _lib.BPF_ERR_ARG
