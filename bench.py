@@ -306,6 +306,8 @@ def bench_extensions(dev, args, lib, rank):
                  tick, as the reference's API)
       step_api   gpu_bpf_step per tick on the reference suite's throughput workload (matched-DGP
                  Student-t scenario, N = 1K / 4K / 16K / 64K, 2000 ticks)
+      particle_scaling  gpu_bpf_step per tick on the reference's particle-scaling benchmark
+                 (N = 50K .. 1M, nu_obs 5)
       smc2       256 theta-particles x 512 state particles, 500 updates of gpu_bpf_smc2_update with one
                  PMMH move per outer resample; smc2_cpmmh the same with correlated-noise moves (rho 0.99)
     CUDA events on the filters' streams where the work is device-resident, else wall clock around
@@ -426,6 +428,23 @@ def bench_extensions(dev, args, lib, rank):
         rows[str(n)] = {"us_per_tick": ms * 1e3 / len(ys4), "ticks_per_s": len(ys4) / (ms / 1e3)}
     out["step_api"] = {"workload": STEP_API_WORKLOAD, "points": rows}
 
+    # the reference's particle-scaling benchmark, same calls
+    ysc = np.asarray(scaling_series(), dtype=np.float32)
+    rows = {}
+    for n in SCALING_N:
+        f = gpubpf.GpuBpf(n, 0.98, 0.15, -1.0, 0.0, 5.0, 42)
+        for t in range(200):
+            f.step(float(ysc[t]))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for v in ysc[200:].tolist():
+            f.step(v)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        f.close()
+        rows[str(n)] = {"us_per_tick": ms * 1e3 / (len(ysc) - 200)}
+    out["particle_scaling"] = {"workload": SCALING_WORKLOAD, "points": rows}
+
     # SMC^2, with fresh inner filters scoring the proposals and with correlated-noise (CPMMH) moves
     _, y2 = dgp.matched_series(600, RHO, SIG, MU, 11)
     for key, cp in (("smc2", 0.0), ("smc2_cpmmh", 0.99)):
@@ -446,6 +465,32 @@ def bench_extensions(dev, args, lib, rank):
                     "us_per_update": ms / 500 * 1e3, "theta_mean": [float(v) for v in mean],
                     "theta_sd": [float(v) for v in sd], "stats": st,
                     "acceptance": st["accepted"] / max(1, st["proposed"])}
+    return out
+
+
+SCALING_N = (50000, 100000, 200000, 300000, 400000, 500000, 1000000)
+SCALING_WORKLOAD = ("the reference's particle-scaling benchmark (tests/bench_particle_scaling.cu): gpu_bpf_step "
+                    "per tick, rho 0.98, sigma_z 0.15, mu -1, nu_obs 5, seed 42, LCG + Box-Muller series (state "
+                    "123456789), 200 warm-up then 1800 timed ticks")
+
+
+def scaling_series(n=2000):
+    """The series of tests/bench_particle_scaling.cu:29-38,54-63 (FP64, as there)."""
+    import math
+    st = 123456789
+
+    def normal():
+        nonlocal st
+        st = (st * 6364136223846793005 + 1442695040888963407) & ((1 << 64) - 1)
+        u1 = max((st >> 11) / float(1 << 53), 1e-15)
+        st = (st * 6364136223846793005 + 1442695040888963407) & ((1 << 64) - 1)
+        u2 = (st >> 11) / float(1 << 53)
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * 3.14159265358979323846 * u2)
+
+    h, out = -1.0, []
+    for _ in range(n):
+        h = -1.0 + 0.98 * (h + 1.0) + 0.15 * normal()
+        out.append(math.exp(h / 2.0) * normal())
     return out
 
 
@@ -748,6 +793,15 @@ def reference_gpu(args, y):
         f.close()
         rows[str(n)] = {"us_per_tick": ms * 1e3 / len(ys4), "ticks_per_s": len(ys4) / (ms / 1e3)}
     out["step_api"] = {"workload": STEP_API_WORKLOAD + "; gpu_bpf_step in a C loop", "points": rows}
+    ysc = np.asarray(scaling_series(), dtype=np.float32)
+    rows = {}
+    for n in SCALING_N:
+        f = refgpu.RefGpuFilter(n, 0.98, 0.15, -1.0, 0.0, 5.0, seed=42)
+        f.run(ysc[:200])                                  # warm-up ticks, as the benchmark's
+        ms = f.time_steps(ysc[200:], warmup=0)
+        f.close()
+        rows[str(n)] = {"us_per_tick": ms * 1e3 / (len(ysc) - 200)}
+    out["particle_scaling"] = {"workload": SCALING_WORKLOAD + "; gpu_bpf_step in a C loop", "points": rows}
     return out
 
 
