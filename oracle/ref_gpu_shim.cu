@@ -96,6 +96,17 @@ double refgpu_time_steps(void* sv, const float* y, int T, int warmup) {
   return std::chrono::duration<double, std::milli>(t1 - t0).count();
 }
 
+// Online mu / rho learning of the reference (gpu_bpf_full.cuh:197-210, gpu_bpf_ptx_full.cu:469-544,
+// 777-828).
+void refgpu_enable_mu_learning(void* s, int mode, int K, float c, float t0, float gamma) {
+  gpu_bpf_enable_mu_learning(static_cast<GpuBpfState*>(s), mode, K, c, t0, gamma);
+}
+void refgpu_enable_rho_learning(void* s, int enable) {
+  gpu_bpf_enable_rho_learning(static_cast<GpuBpfState*>(s), enable);
+}
+float refgpu_get_mu(void* s) { return gpu_bpf_get_mu(static_cast<GpuBpfState*>(s)); }
+float refgpu_get_rho(void* s) { return gpu_bpf_get_rho(static_cast<GpuBpfState*>(s)); }
+
 // Device state read-back: the PCG32 states [state, inc] per particle
 // (gpu_bpf_full.cuh:87), the particles and the normalised weights of the last tick.
 int refgpu_copy_rng(void* sv, unsigned long long* out, int n) {

@@ -38,6 +38,12 @@ def lib() -> C.CDLL:
         L.refgpu_run.argtypes = [vp, vp, i32, vp, vp]
         L.refgpu_time_run.restype = f64
         L.refgpu_time_run.argtypes = [vp, vp, i32, vp]
+        L.refgpu_enable_mu_learning.argtypes = [vp, i32, i32, f32, f32, f32]
+        L.refgpu_enable_rho_learning.argtypes = [vp, i32]
+        L.refgpu_get_mu.restype = f32
+        L.refgpu_get_mu.argtypes = [vp]
+        L.refgpu_get_rho.restype = f32
+        L.refgpu_get_rho.argtypes = [vp]
         L.refgpu_time_steps.restype = f64
         L.refgpu_time_steps.argtypes = [vp, vp, i32, i32]
         L.refgpu_apf_create.restype = vp
@@ -85,6 +91,18 @@ class RefGpuFilter:
         last = np.zeros(2, dtype=np.float32)
         ms = self.L.refgpu_time_run(self.s, _p(y), int(y.shape[0]), _p(last))
         return ms, float(last[0]), float(last[1])
+
+    def enable_mu_learning(self, mode=1, K=50, c=0.1, t0=10.0, gamma=0.667):
+        self.L.refgpu_enable_mu_learning(self.s, int(mode), int(K), float(c), float(t0), float(gamma))
+
+    def enable_rho_learning(self, enable=True):
+        self.L.refgpu_enable_rho_learning(self.s, int(enable))
+
+    def mu(self):
+        return float(self.L.refgpu_get_mu(self.s))
+
+    def rho_value(self):
+        return float(self.L.refgpu_get_rho(self.s))
 
     def time_steps(self, y, warmup=100):
         """warmup untimed then len(y) timed ticks of gpu_bpf_step in a C loop: milliseconds."""

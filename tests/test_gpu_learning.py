@@ -6,6 +6,9 @@
   update rule vs a host restatement     <= 1e-5 relative on mu and rho (the reference's formulas,
   (gpu_bpf_ptx_full.cu:489-543)         fed the same sums)
   learning from a wrong mu              moves mu most of the way to the generating value
+  the reference's mu-regime head-to-head  learning lowers the phase-2 RMSE; learnt mu and phase-2
+  (smc2/test_mu_learning.cu:232-290)      RMSE within 0.1 / 0.02 of the reference's own learning
+                                          filter on the same series
 """
 from __future__ import annotations
 
@@ -111,3 +114,73 @@ def test_mu_learning_moves_to_the_generating_value(bpf):
     f.disable_mu_learning()
     f.close()
     assert abs(mu - (-1.0)) < 0.4, mu
+
+
+def _mu_regime_series(T=5000, t_switch=2500, mu1=-1.0, mu2=-2.5, rho=0.98, sigma_z=0.15, nu_obs=5.0, seed=42):
+    """generate_sv_mu_regime of smc2/test_mu_learning.cu:70-108 (FP64, its host PCG32 + Box-Muller:
+    all state draws first, then all observation draws)."""
+    rng = seed
+
+    def randn():
+        nonlocal rng
+        s = (rng * 6364136223846793005 + 1442695040888963407) & ((1 << 64) - 1)
+        u1 = (s >> 11) * (1.0 / 9007199254740992.0)
+        s = (s * 6364136223846793005 + 1442695040888963407) & ((1 << 64) - 1)
+        u2 = (s >> 11) * (1.0 / 9007199254740992.0)
+        rng = s
+        u1 = max(u1, 1e-15)
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * 3.14159265358979323846 * u2)
+
+    def sample_t(nu):
+        z = randn()
+        chi2 = 0.0
+        for _ in range(int(nu)):
+            g = randn()
+            chi2 += g * g
+        return z / math.sqrt(chi2 / nu)
+
+    h = np.zeros(T)
+    h[0] = mu1 + sigma_z / math.sqrt(max(1.0 - rho * rho, 1e-10)) * randn()
+    for t in range(1, T):
+        mu = mu1 if t < t_switch else mu2
+        h[t] = mu + rho * (h[t - 1] - mu) + sigma_z * randn()
+    y = np.array([math.exp(h[t] / 2.0) * sample_t(nu_obs) for t in range(T)], dtype=np.float32)
+    return h, y
+
+
+def test_mu_regime_head_to_head_with_reference(bpf):
+    """The reference's head-to-head test (smc2/test_mu_learning.cu:232-290): mu shifts from -1.0
+    to -2.5 at t = 2500 (rho 0.98, sigma_z 0.15, nu_obs 5, N = 4096, T = 5000); both filters start
+    at mu = -1.0, one without learning, one with natural-gradient learning (K 50, c 0.1, t0 10,
+    gamma 2/3). Learning lowers the phase-2 RMSE; the learnt mu ends near -2.5, as the
+    reference's own learning filter's does on the same series."""
+    T, ts = 5000, 2500
+    h, y = _mu_regime_series()
+
+    def rmse(hm, lo, hi):
+        e = np.asarray(hm[lo:hi], dtype=np.float64) - h[lo:hi]
+        return float(np.sqrt(np.mean(e * e)))
+
+    res = {}
+    for learn in (False, True):
+        f = bpf.GpuBpf(4096, 0.98, 0.15, -1.0, 0.0, 5.0, 42)
+        if learn:
+            f.enable_mu_learning(1, 50, 0.1, 10.0, 0.667)
+        hm = [f.step(float(v)).h_mean for v in y]
+        res[learn] = (rmse(hm, 50, ts), rmse(hm, ts, T), f.get_mu())
+        f.close()
+    ref = None
+    from oracle import refgpu
+    if refgpu.available():
+        g = refgpu.RefGpuFilter(4096, 0.98, 0.15, -1.0, 0.0, 5.0, seed=42)
+        g.enable_mu_learning(1, 50, 0.1, 10.0, 0.667)
+        hm_r, _ = g.run(y)
+        ref = (rmse(hm_r, 50, ts), rmse(hm_r, ts, T), g.mu())
+        g.close()
+    print(f"\n  vanilla: P1 {res[False][0]:.4f} P2 {res[False][1]:.4f}; learning: P1 {res[True][0]:.4f} "
+          f"P2 {res[True][1]:.4f} mu {res[True][2]:+.4f}; reference learning: {ref}")
+    assert res[True][1] < res[False][1] - 0.05, res
+    assert abs(res[True][2] - (-2.5)) < 0.5, res
+    if ref is not None:                      # measured: mu -2.787 vs -2.791, phase-2 RMSE 0.4622 vs 0.4623
+        assert abs(res[True][2] - ref[2]) < 0.1, (res, ref)
+        assert abs(res[True][1] - ref[1]) < 0.02, (res, ref)
