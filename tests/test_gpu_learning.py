@@ -9,6 +9,8 @@
   the reference's mu-regime head-to-head  learning lowers the phase-2 RMSE; learnt mu and phase-2
   (smc2/test_mu_learning.cu:232-290)      RMSE within 0.1 / 0.02 of the reference's own learning
                                           filter on the same series
+  the reference's rho-regime test         mu + rho learning: learnt rho within 0.02, mu within 0.1,
+  (smc2/test_mu_learning.cu:468-525)      phase-2 RMSE within 0.02 of the reference's
 """
 from __future__ import annotations
 
@@ -116,9 +118,11 @@ def test_mu_learning_moves_to_the_generating_value(bpf):
     assert abs(mu - (-1.0)) < 0.4, mu
 
 
-def _mu_regime_series(T=5000, t_switch=2500, mu1=-1.0, mu2=-2.5, rho=0.98, sigma_z=0.15, nu_obs=5.0, seed=42):
+def _mu_regime_series(T=5000, t_switch=2500, mu1=-1.0, mu2=-2.5, rho=0.98, sigma_z=0.15, nu_obs=5.0, seed=42,
+                      rho2=None):
     """generate_sv_mu_regime of smc2/test_mu_learning.cu:70-108 (FP64, its host PCG32 + Box-Muller:
-    all state draws first, then all observation draws)."""
+    all state draws first, then all observation draws); with rho2, generate_sv_rho_regime
+    (:110-140): mu1 throughout, rho -> rho2 at t_switch."""
     rng = seed
 
     def randn():
@@ -142,8 +146,11 @@ def _mu_regime_series(T=5000, t_switch=2500, mu1=-1.0, mu2=-2.5, rho=0.98, sigma
     h = np.zeros(T)
     h[0] = mu1 + sigma_z / math.sqrt(max(1.0 - rho * rho, 1e-10)) * randn()
     for t in range(1, T):
-        mu = mu1 if t < t_switch else mu2
-        h[t] = mu + rho * (h[t - 1] - mu) + sigma_z * randn()
+        if rho2 is None:
+            mu, r = (mu1 if t < t_switch else mu2), rho
+        else:
+            mu, r = mu1, (rho if t < t_switch else rho2)
+        h[t] = mu + r * (h[t - 1] - mu) + sigma_z * randn()
     y = np.array([math.exp(h[t] / 2.0) * sample_t(nu_obs) for t in range(T)], dtype=np.float32)
     return h, y
 
@@ -184,3 +191,36 @@ def test_mu_regime_head_to_head_with_reference(bpf):
     if ref is not None:                      # measured: mu -2.787 vs -2.791, phase-2 RMSE 0.4622 vs 0.4623
         assert abs(res[True][2] - ref[2]) < 0.1, (res, ref)
         assert abs(res[True][1] - ref[1]) < 0.02, (res, ref)
+
+
+def test_rho_regime_learning_with_reference(bpf):
+    """The reference's rho-regime test (smc2/test_mu_learning.cu:468-525, its first seed): rho falls
+    from 0.98 to 0.90 at t = 2500 (mu -1.0, sigma_z 0.15, nu_obs 5, N = 4096, T = 5000); mu and rho
+    learning from (mu, rho) = (-1.0, 0.98), this build against the reference's own learning filter
+    on the same series: learnt rho, mu and phase-2 RMSE."""
+    T, ts = 5000, 2500
+    h, y = _mu_regime_series(rho2=0.90)
+
+    def rmse(hm):
+        e = np.asarray(hm[ts:T], dtype=np.float64) - h[ts:T]
+        return float(np.sqrt(np.mean(e * e)))
+
+    f = bpf.GpuBpf(4096, 0.98, 0.15, -1.0, 0.0, 5.0, 42)
+    f.enable_mu_learning(1, 50, 0.1, 10.0, 0.667)
+    f.enable_rho_learning(True)
+    hm = [f.step(float(v)).h_mean for v in y]
+    ours = (rmse(hm), f.get_rho(), f.get_mu())
+    f.close()
+    from oracle import refgpu
+    if not refgpu.available():
+        pytest.skip("oracle/_ref not built")
+    g = refgpu.RefGpuFilter(4096, 0.98, 0.15, -1.0, 0.0, 5.0, seed=42)
+    g.enable_mu_learning(1, 50, 0.1, 10.0, 0.667)
+    g.enable_rho_learning(True)
+    hm_r, _ = g.run(y)
+    ref = (rmse(hm_r), g.rho_value(), g.mu())
+    g.close()
+    print(f"\n  mu+rho learning, phase-2 RMSE / rho / mu: ours {ours}, reference {ref}")
+    assert abs(ours[0] - ref[0]) < 0.02, (ours, ref)
+    assert abs(ours[1] - ref[1]) < 0.02, (ours, ref)
+    assert abs(ours[2] - ref[2]) < 0.1, (ours, ref)
