@@ -17,6 +17,11 @@ where it lies, together with oracle/ref_gpu_shim.cu (C-linkage wrappers), into
 oracle/_ref/librefgpu.so. Nothing else of the reference is built; it needs the
 CUDA driver library, cuRAND and thrust from the toolkit only.
 
+A second library, oracle/_ref/librefcuda.so, is the reference's CUDA-C edition
+(gpu_bpf/gpu_bpf.cu behind gpu_bpf/gpu_bpf.cuh, which holds the reference's
+IMM) compiled from where it lies with oracle/ref_cuda_shim.cu. The two
+editions export the same C++ names, so each gets its own library.
+
 The output is git-ignored and travels with the repository snapshot to a GPU
 machine; the reference tree itself is only read here, at build time.
 """
@@ -33,15 +38,40 @@ OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "librefgpu.so")
 PTX = os.path.join(OUT, "bpf_kernels_full.ptx")
 SHIM = os.path.join(HERE, "ref_gpu_shim.cu")
+LIB_C = os.path.join(OUT, "librefcuda.so")
+SHIM_C = os.path.join(HERE, "ref_cuda_shim.cu")
 
 REF_ROOT = os.environ.get("BPF_REFERENCE_ROOT", "/root/reference")
 REF_DRIVER = os.path.join(REF_ROOT, "gpu_bpf", "gpu_bpf_ptx_full.cu")
 REF_PTX = os.path.join(REF_ROOT, "ptx_assembly", "bpf_kernels_full.ptx")
+REF_CUDA = os.path.join(REF_ROOT, "gpu_bpf", "gpu_bpf.cu")
 
 
 def available() -> bool:
     """True when the library and its PTX module are built."""
     return os.path.exists(LIB) and os.path.exists(PTX)
+
+
+def available_cuda() -> bool:
+    """True when the CUDA-C edition's library is built."""
+    return os.path.exists(LIB_C)
+
+
+def build_cuda(force: bool = False) -> str | None:
+    """Build oracle/_ref/librefcuda.so (the CUDA-C edition) when the reference tree is present."""
+    if not os.path.exists(REF_CUDA):
+        return LIB_C if available_cuda() else None
+    inputs = [REF_CUDA, SHIM_C, os.path.join(os.path.dirname(REF_CUDA), "gpu_bpf.cuh")]
+    if not force and available_cuda() and os.path.getmtime(LIB_C) >= max(os.path.getmtime(p) for p in inputs):
+        return LIB_C
+    os.makedirs(OUT, exist_ok=True)
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    cmd = [nvcc, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-shared", "-Xcompiler", "-fPIC", "-I", os.path.dirname(REF_CUDA),
+           REF_CUDA, SHIM_C, "-o", LIB_C + ".tmp", "-lcurand"]
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+    os.replace(LIB_C + ".tmp", LIB_C)
+    return LIB_C
 
 
 def _retarget(src: bytes) -> bytes:
@@ -77,3 +107,4 @@ def build(force: bool = False) -> str | None:
 if __name__ == "__main__":
     path = build(force="--force" in sys.argv)
     print(path or "reference tree absent; oracle/_ref not built")
+    print(build_cuda(force="--force" in sys.argv) or "reference tree absent; CUDA-C edition not built")

@@ -175,3 +175,78 @@ def apf_time(n, rho, sigma_z, mu, y, warmup=64, seed=42):
         return ms / rest.shape[0]
     finally:
         L.refgpu_apf_destroy(s)
+
+
+# ---------------------------------------------------------------------------
+# The reference's CUDA-C edition (oracle/_ref/librefcuda.so): plain filter and IMM
+# ---------------------------------------------------------------------------
+_LIBC = None
+
+
+def available_cuda() -> bool:
+    return build_ref.available_cuda()
+
+
+def lib_cuda() -> C.CDLL:
+    global _LIBC
+    if _LIBC is None:
+        if not build_ref.available_cuda():
+            raise RuntimeError("oracle/_ref/librefcuda.so is not built")
+        L = C.CDLL(build_ref.LIB_C)
+        vp, f32, i32 = C.c_void_p, C.c_float, C.c_int
+        L.refc_create.restype = vp
+        L.refc_create.argtypes = [i32, f32, f32, f32, f32, f32, i32, f32, f32]
+        L.refc_destroy.argtypes = [vp]
+        L.refc_resample_count.restype = i32
+        L.refc_resample_count.argtypes = [vp]
+        L.refc_run.restype = i32
+        L.refc_run.argtypes = [vp, vp, i32, vp, vp]
+        L.refc_imm_create.restype = vp
+        L.refc_imm_create.argtypes = [vp, i32, i32, vp, i32, f32, f32]
+        L.refc_imm_destroy.argtypes = [vp]
+        L.refc_imm_run.restype = i32
+        L.refc_imm_run.argtypes = [vp, vp, i32, vp, vp, vp, vp]
+        _LIBC = L
+    return _LIBC
+
+
+def cuda_run(n, rho, sigma_z, mu, y, nu_state=0.0, nu_obs=0.0, seed=42, ess_threshold=0.5, silverman=0.0):
+    """The CUDA-C edition's plain filter over y (gpu_bpf_step per tick): (h_mean[T], log_lik[T],
+    resample count)."""
+    L = lib_cuda()
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    s = L.refc_create(int(n), rho, sigma_z, mu, nu_state, nu_obs, int(seed), silverman, ess_threshold)
+    if not s:
+        raise RuntimeError("CUDA-C edition gpu_bpf_create failed")
+    hm = np.zeros(y.shape[0], dtype=np.float32)
+    ll = np.zeros(y.shape[0], dtype=np.float32)
+    rc = L.refc_run(s, _p(y), int(y.shape[0]), _p(hm), _p(ll))
+    cnt = L.refc_resample_count(s)
+    L.refc_destroy(s)
+    if rc != 0:
+        raise RuntimeError(f"CUDA-C edition tick loop failed (CUDA error {rc})")
+    return hm, ll, cnt
+
+
+def cuda_imm_run(models, n, y, transition=None, seed=42, silverman=0.0, ess_threshold=0.5):
+    """The CUDA-C edition's IMM over y: (h_mean[T], log_lik[T], best_model[T], final probs[K]).
+    ess_threshold applies to every model's filter (its default is 0.5)."""
+    L = lib_cuda()
+    K = len(models)
+    m = np.array([[d["rho"], d["sigma_z"], d["mu"], d.get("nu_state", 0.0), d.get("nu_obs", 0.0)] for d in models],
+                 dtype=np.float32).ravel()
+    tm = None if transition is None else np.ascontiguousarray(transition, dtype=np.float32)
+    s = L.refc_imm_create(_p(m), K, int(n), _p(tm) if tm is not None else None, int(seed), silverman,
+                          ess_threshold)
+    if not s:
+        raise RuntimeError("CUDA-C edition gpu_imm_create failed")
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    hm = np.zeros(y.shape[0], dtype=np.float32)
+    ll = np.zeros(y.shape[0], dtype=np.float32)
+    best = np.zeros(y.shape[0], dtype=np.int32)
+    pr = np.zeros(K, dtype=np.float32)
+    rc = L.refc_imm_run(s, _p(y), int(y.shape[0]), _p(hm), _p(ll), _p(best), _p(pr))
+    L.refc_imm_destroy(s)
+    if rc != 0:
+        raise RuntimeError(f"CUDA-C edition IMM failed (CUDA error {rc})")
+    return hm, ll, best, pr
