@@ -308,6 +308,8 @@ def bench_extensions(dev, args, lib, rank):
                  Student-t scenario, N = 1K / 4K / 16K / 64K, 2000 ticks)
       particle_scaling  gpu_bpf_step per tick on the reference's particle-scaling benchmark
                  (N = 50K .. 1M, nu_obs 5)
+      cond_resample  the reference's conditional-resampling workload (N = 300K, 3000 ticks of
+                 gpu_bpf_step, always and ESS < 0.5N), beside its published RTX 5080 figures
       smc2       256 theta-particles x 512 state particles, 500 updates of gpu_bpf_smc2_update with one
                  PMMH move per outer resample; smc2_cpmmh the same with correlated-noise moves (rho 0.99)
     CUDA events on the filters' streams where the work is device-resident, else wall clock around
@@ -445,6 +447,23 @@ def bench_extensions(dev, args, lib, rank):
         rows[str(n)] = {"us_per_tick": ms * 1e3 / (len(ysc) - 200)}
     out["particle_scaling"] = {"workload": SCALING_WORKLOAD, "points": rows}
 
+    # the reference's conditional-resampling workload, the one per-tick figure it publishes with a
+    # harness (760 ms always resampling, 448 ms with ESS < 0.5N, RTX 5080, its CUDA-C path)
+    _, ycr = dgp.cond_resample_series(lambda t: 0.15)
+    rows = {}
+    for thr in (0.0, 0.5):
+        f = gpubpf.GpuBpf(300000, 0.98, 0.15, -4.5, 0.0, 0.0, 42, ess_threshold=thr)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for v in ycr.tolist():
+            f.step(v)
+        torch.cuda.synchronize()
+        rows["always" if thr == 0.0 else "ess0.5"] = {"ms_3000_ticks": (time.perf_counter() - t0) * 1e3,
+                                                       "resamples": f.state.resample_count}
+        f.close()
+    out["cond_resample"] = {"workload": COND_WORKLOAD, "points": rows,
+                            "published_rtx5080_ms": {"always": 760.0, "ess0.5": 448.0}}
+
     # SMC^2, with fresh inner filters scoring the proposals and with correlated-noise (CPMMH) moves
     _, y2 = dgp.matched_series(600, RHO, SIG, MU, 11)
     for key, cp in (("smc2", 0.0), ("smc2_cpmmh", 0.99)):
@@ -468,6 +487,9 @@ def bench_extensions(dev, args, lib, rank):
     return out
 
 
+COND_WORKLOAD = ("the reference's conditional-resampling workload (tests/test_cond_resample.cu): N = 300000, "
+                 "3000 ticks of gpu_bpf_step, rho 0.98, sigma_z 0.15, mu -4.5, seed 42, resampling every tick "
+                 "and at ESS < 0.5N")
 SCALING_N = (50000, 100000, 200000, 300000, 400000, 500000, 1000000)
 SCALING_WORKLOAD = ("the reference's particle-scaling benchmark (tests/bench_particle_scaling.cu): gpu_bpf_step "
                     "per tick, rho 0.98, sigma_z 0.15, mu -1, nu_obs 5, seed 42, LCG + Box-Muller series (state "
@@ -802,6 +824,14 @@ def reference_gpu(args, y):
         f.close()
         rows[str(n)] = {"us_per_tick": ms * 1e3 / (len(ysc) - 200)}
     out["particle_scaling"] = {"workload": SCALING_WORKLOAD + "; gpu_bpf_step in a C loop", "points": rows}
+    _, ycr = dgp.cond_resample_series(lambda t: 0.15)
+    rows = {}
+    for thr in (0.0, 0.5):
+        f = refgpu.RefGpuFilter(300000, 0.98, 0.15, -4.5, seed=42, ess_threshold=thr)
+        rows["always" if thr == 0.0 else "ess0.5"] = {"ms_3000_ticks": f.time_steps(ycr, warmup=0),
+                                                       "resamples": f.resample_count}
+        f.close()
+    out["cond_resample"] = {"workload": COND_WORKLOAD + "; gpu_bpf_step in a C loop", "points": rows}
     return out
 
 

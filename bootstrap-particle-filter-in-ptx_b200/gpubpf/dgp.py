@@ -88,3 +88,35 @@ def regime_series(T: int, mus=(-1.5, 0.0), period: int = 500, rho: float = 0.97,
         hs.append(h)
         ys.append(math.exp(h / 2.0) * rng.gaussian())
     return hs, ys
+
+
+def cond_resample_series(sigma_of_t, T: int = 3000, rho: float = 0.98, mu: float = -4.5, seed: int = 42):
+    """(true_h[T], y[T]) of the reference's conditional-resampling study (tests/test_cond_resample.cu:
+    25-57): its host PCG32 (fixed increment) and FP32 Box-Muller, h_0 = mu, sigma_z = sigma_of_t(t)
+    (the regime scenario changes it mid-series). Restated in numpy FP32; the same law as the C
+    build, not pinned to it bit for bit."""
+    import numpy as np
+    f32 = np.float32
+    state = seed
+
+    def u23():
+        nonlocal state
+        old = state
+        state = (old * PCG_MULT + 1442695040888963407) & MASK64
+        xsh = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        r = ((xsh >> rot) | (xsh << ((-rot) & 31))) & 0xFFFFFFFF
+        return f32(r >> 9) * f32(1.0 / 8388608.0)
+
+    def randn():
+        u1 = u23() + f32(1e-10)
+        u2 = u23()
+        return f32(np.sqrt(f32(-2.0) * np.log(f32(u1)))) * f32(np.cos(f32(2.0) * f32(3.14159265358979) * u2))
+
+    h = f32(mu)
+    ys, hs = [], []
+    for t in range(T):
+        h = f32(mu) + f32(rho) * (h - f32(mu)) + f32(sigma_of_t(t)) * randn()
+        ys.append(float(f32(np.exp(h * f32(0.5))) * randn()))
+        hs.append(float(h))
+    return np.array(hs), np.array(ys, dtype=np.float32)

@@ -5,15 +5,15 @@ own GPU filter (the PTX edition, whose Silverman jitter is off, as in this build
   scenarios (:124-200)     N = 300000, T = 3000, rho 0.98, sigma_z 0.15, mu -4.5, filter seed 42:
                            oracle parameters; filter sigma_z 0.08 (misspecified); a regime change
                            (sigma_z 0.15 -> 0.40 at t = 1500); high volatility (sigma_z 0.40)
-  series                   the suite's host PCG32 + Box-Muller generator restated in numpy FP32
-                           (seed 42, :25-57); the same law, not pinned bit for bit to the C build
+  series                   gpubpf.dgp.cond_resample_series: the suite's host PCG32 + Box-Muller
+                           generator restated in numpy FP32 (seed 42, :25-57); the same law, not
+                           pinned bit for bit to the C build
   checks                   per scenario and threshold: resampling counts within 2% (+3) of the
                            reference's, RMSE of the filtered mean after 100 ticks within 0.01;
                            this build's count falls as the threshold falls
 """
 from __future__ import annotations
 
-import math
 
 import numpy as np
 import pytest
@@ -22,37 +22,12 @@ pytestmark = pytest.mark.gpu
 
 T, N, SKIP = 3000, 300000, 100
 RHO, SZ, MU = 0.98, 0.15, -4.5
-A, C_INC = 6364136223846793005, 1442695040888963407
-M64 = (1 << 64) - 1
 
 
 def _series(sigma_of_t):
-    """Returns and true h of the suite's DGP (test_cond_resample.cu:25-57), FP32 as there."""
-    state = 42
-    f32 = np.float32
-
-    def u23():
-        nonlocal state
-        old = state
-        state = (old * A + C_INC) & M64
-        xsh = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
-        rot = old >> 59
-        r = ((xsh >> rot) | (xsh << ((-rot) & 31))) & 0xFFFFFFFF
-        return f32(r >> 9) * f32(1.0 / 8388608.0)
-
-    def randn():
-        u1 = u23() + f32(1e-10)
-        u2 = u23()
-        return f32(np.sqrt(f32(-2.0) * np.log(f32(u1)))) * f32(np.cos(f32(2.0) * f32(3.14159265358979) * u2))
-
-    h = f32(MU)
-    ys, hs = [], []
-    for t in range(T):
-        sz = f32(sigma_of_t(t))
-        h = f32(MU) + f32(RHO) * (h - f32(MU)) + sz * randn()
-        ys.append(float(f32(np.exp(h * f32(0.5))) * randn()))
-        hs.append(float(h))
-    return np.array(ys, dtype=np.float32), np.array(hs)
+    from gpubpf import dgp
+    h, y = dgp.cond_resample_series(sigma_of_t, T, RHO, MU, 42)
+    return y, h
 
 
 def _rmse(hm, h):
