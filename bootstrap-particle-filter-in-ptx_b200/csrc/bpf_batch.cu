@@ -469,6 +469,17 @@ __global__ void __launch_bounds__(NT, (1024 / NT > 0 ? 1024 / NT : 1)) batch_ker
     const BatchFilterDev f = a.filters[b];
     batch_run_filter<NT, true, NOISE>(a, f, b, bufA, bufB, marks, sh, maxn, perm);
   }
+  // every CTA has taken its last work item and read the tick before it counts
+  // itself done, so the last one may reset the counters and advance the tick
+  if (a.ep_done && threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(a.ep_done, 1) == a.ep_total - 1) {
+      for (int c = 0; c < a.ep_n; ++c) a.ep_counters[c] = 0;
+      if (a.ep_tick) *a.ep_tick += a.ep_add;
+      *a.ep_done = 0;
+      __threadfence();
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -657,8 +668,6 @@ __device__ void batch_run_backward(const BatchArgs& a, const BatchFilterDev& f, 
 
 size_t batch_grad_smem_bytes(int maxn) { return (size_t)maxn * 12; }
 
-__global__ void batch_advance_kernel(int* tick, int n) { *tick += n; }
-
 __global__ void batch_gather_kernel(BatchFilterDev* dst_tab, BatchFilterState* dst_st, float* dst_h, float* dst_w,
                                     const BatchFilterDev* src_tab, const BatchFilterState* src_st,
                                     const float* __restrict__ src_h, const float* __restrict__ src_w,
@@ -706,11 +715,6 @@ cudaError_t launch_noise_gather(float* nz, const long long* src_off, const long 
   const long long n4 = floats / 4;                 // areas hold whole ticks of a multiple of 4 floats
   const int gx = (int)((n4 + 255) / 256 < 64 ? (n4 + 255) / 256 : 64);
   noise_gather_kernel<<<dim3(gx, B), 256, 0, s>>>(nz, src_off, dst_off, n4);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s) {
-  batch_advance_kernel<<<1, 1, 0, s>>>(tick, n);
   return cudaGetLastError();
 }
 

@@ -84,6 +84,14 @@ struct BatchArgs {
   const long long* nz_in_off; // [B]
   const long long* nz_out_off;// [B]
   float cp_rho, cp_scale;
+  // Launch epilogue of resumable steps (null ep_done: none, the host zeroes the
+  // counter before the launch): the CTA that finishes last of the ep_total CTAs
+  // launched over all classes zeroes the ep_n work counters and ep_done and
+  // adds ep_add to *ep_tick, so a step is one kernel node per class.
+  int* ep_done;
+  int* ep_counters;
+  int* ep_tick;
+  int ep_total, ep_n, ep_add;
 };
 
 // Floats per tick in a correlated-noise area of a filter of n particles.
@@ -107,8 +115,6 @@ int batch_grad_occupancy(int threads, int maxn);
 // area at src_off[j] into the area at dst_off[j] (16-byte aligned areas that do not overlap).
 cudaError_t launch_noise_gather(float* nz, const long long* src_off, const long long* dst_off, long long floats,
                                 int B, cudaStream_t s);
-// Adds n to the device tick counter of resumable runs (one thread).
-cudaError_t launch_batch_advance(int* tick, int n, cudaStream_t s);
 // Filter j of dst takes the resumable state and table entry of filter idx[j] of src (every j, or
 // those with mask[j] != 0); with new_seed, filter j continues with seed new_seed[j] (fresh noise
 // streams and resampling uniforms). Filters have n particles each at offsets off[]; src and dst

@@ -33,6 +33,7 @@ void free_batch(GpuBpfBatch* b) {
   if (b->ggraph) cudaGraphExecDestroy(b->ggraph);
   if (b->sgraph) cudaGraphExecDestroy(b->sgraph);
   cudaFree(b->d_st); cudaFree(b->d_sth); cudaFree(b->d_stw); cudaFree(b->d_stoff); cudaFree(b->d_tick);
+  cudaFree(b->d_scounters);
   for (int c = 0; c < kClasses; ++c) cudaFree(b->g_tape[c]);
   cudaFree(b->d_AB);
   cudaFree(b->d_nzoff);
@@ -198,8 +199,10 @@ int batch_prepare_steps(GpuBpfBatch* b) {
   BCK(cudaMalloc(&b->d_stw, (size_t)tot * sizeof(float)));
   BCK(cudaMalloc(&b->d_stoff, (size_t)b->B * sizeof(long long)));
   BCK(cudaMalloc(&b->d_tick, sizeof(int)));
+  BCK(cudaMalloc(&b->d_scounters, (kClasses + 1) * sizeof(int)));
   BCK(cudaMemcpy(b->d_stoff, off.data(), (size_t)b->B * sizeof(long long), cudaMemcpyHostToDevice));
   BCK(cudaMemset(b->d_tick, 0, sizeof(int)));
+  BCK(cudaMemset(b->d_scounters, 0, (kClasses + 1) * sizeof(int)));
   b->host_tick = 0;
   return BPF_OK;
 }
@@ -207,11 +210,14 @@ int batch_prepare_steps(GpuBpfBatch* b) {
 namespace {
 
 // Advance every filter by T ticks from its saved state (tick 0 = fresh start).
+// The step path has its own work counters, left at zero by every step launch
+// (the last CTA resets them and advances the device tick), so the captured step
+// holds the class kernels alone.
 cudaError_t enqueue_step(GpuBpfBatch* b, const float* y, int T, double* dll, float* hmean, int y_abs) {
-  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, kClasses * sizeof(int), b->stream);
+  cudaError_t e = cudaEventRecord(b->fork, b->stream);
   if (e != cudaSuccess) return e;
-  e = cudaEventRecord(b->fork, b->stream);
-  if (e != cudaSuccess) return e;
+  int ctas = 0;
+  for (int c = 0; c < kClasses; ++c) if (b->class_cnt[c]) ctas += b->grid[c];
   for (int c = kClasses - 1; c >= 0; --c) {
     if (!b->class_cnt[c]) continue;
     BatchArgs a = class_args(b, c, y, T, b->d_loglik, dll, hmean, nullptr, nullptr, &b->step_nz);
@@ -221,13 +227,20 @@ cudaError_t enqueue_step(GpuBpfBatch* b, const float* y, int T, double* dll, flo
     a.st_w = b->d_stw;
     a.st_off = b->d_stoff;
     a.y_abs = y_abs;
+    a.counter = b->d_scounters + c;
+    a.ep_done = b->d_scounters + kClasses;
+    a.ep_counters = b->d_scounters;
+    a.ep_tick = b->d_tick;
+    a.ep_total = ctas;
+    a.ep_n = kClasses;
+    a.ep_add = T;
     e = cudaStreamWaitEvent(b->cls_stream[c], b->fork, 0);
     if (e == cudaSuccess) e = launch_batch_class(a, b->threads[c], kClassMaxN[c], b->grid[c], b->cls_stream[c]);
     if (e == cudaSuccess) e = cudaEventRecord(b->join[c], b->cls_stream[c]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[c], 0);
     if (e != cudaSuccess) return e;
   }
-  return launch_batch_advance(b->d_tick, T, b->stream);
+  return cudaSuccess;
 }
 
 int ensure_device_b(GpuBpfBatch* b) {
@@ -484,7 +497,9 @@ static int step_common(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* 
     b->skey = k;
   }
   BCK(cudaGraphLaunch(b->sgraph, b->stream));
-  bpf_note_launches(kClasses + 1);
+  int launched = 0;
+  for (int c = 0; c < kClasses; ++c) launched += b->class_cnt[c] ? 1 : 0;
+  bpf_note_launches(launched);
   b->host_tick += n_ticks;
   return BPF_OK;
 }

@@ -109,6 +109,8 @@ struct GpuBpfBatch {
   float* d_stw = nullptr;
   long long* d_stoff = nullptr;
   int* d_tick = nullptr;
+  int* d_scounters = nullptr;       // work counters of the step path ([kClasses]) and its done counter;
+                                    // zero between step launches (reset by each launch's last CTA)
   int host_tick = 0;
   cudaGraphExec_t sgraph = nullptr;
   GraphKey skey;
