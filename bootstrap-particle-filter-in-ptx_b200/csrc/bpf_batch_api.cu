@@ -484,19 +484,32 @@ static int step_common(GpuBpfBatch* b, const float* y_dev, int n_ticks, double* 
   k.y = y_dev; k.T = n_ticks; k.dll = dll_dev; k.hmean = hmean_dev; k.y_abs = y_abs;
   k.nz = b->step_nz;
   std::copy(b->threads, b->threads + kClasses, k.threads);
-  if (!b->sgraph || !(k == b->skey)) {
-    if (b->sgraph) { cudaGraphExecDestroy(b->sgraph); b->sgraph = nullptr; }
-    cudaGraph_t g = nullptr;
-    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = enqueue_step(b, y_dev, n_ticks, dll_dev, hmean_dev, y_abs);
-    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
-    if (e != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
-    e = cudaGraphInstantiate(&b->sgraph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) { b->sgraph = nullptr; cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
-    b->skey = k;
+  // Only the observation / output pointers differ from the captured step (a caller
+  // walking a device series tick by tick): launch the step directly instead of
+  // capturing and instantiating a graph for every call.
+  GraphKey shape = k;
+  shape.y = b->skey.y; shape.dll = b->skey.dll; shape.hmean = b->skey.hmean;
+  if (b->sgraph && !(k == b->skey) && shape == b->skey) {
+    BCK(enqueue_step(b, y_dev, n_ticks, dll_dev, hmean_dev, y_abs));
+  } else {
+    if (!b->sgraph || !(k == b->skey)) {
+      if (b->sgraph) { cudaGraphExecDestroy(b->sgraph); b->sgraph = nullptr; }
+      cudaGraph_t g = nullptr;
+      BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = enqueue_step(b, y_dev, n_ticks, dll_dev, hmean_dev, y_abs);
+      cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+      if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return bpf_record_error(BPF_ERR_CUDA);
+      }
+      e = cudaGraphInstantiate(&b->sgraph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { b->sgraph = nullptr; cudaGetLastError(); return bpf_record_error(BPF_ERR_CUDA); }
+      b->skey = k;
+    }
+    BCK(cudaGraphLaunch(b->sgraph, b->stream));
   }
-  BCK(cudaGraphLaunch(b->sgraph, b->stream));
   int launched = 0;
   for (int c = 0; c < kClasses; ++c) launched += b->class_cnt[c] ? 1 : 0;
   bpf_note_launches(launched);

@@ -67,7 +67,8 @@ def test_batch_steps_equal_one_run(bpf, thr):
     torch.cuda.synchronize()
     ll_full, dll_full, hm_full = ll.cpu().numpy(), dll.cpu().numpy().reshape(B, T), hm.cpu().numpy().reshape(B, T)
     for rep in range(2):                                  # the second pass starts again after reset
-        pieces, t0 = [1, 1, 5, 13, 1, 26], 0
+        # runs of equal lengths at moving pointers take the direct launch, new lengths a new graph
+        pieces, t0 = [1, 1, 1, 5, 13, 1, 1, 24], 0
         dll_s = np.zeros((B, T))
         hm_s = np.zeros((B, T), dtype=np.float32)
         for n in pieces:
