@@ -364,7 +364,9 @@ int          gpu_bpf_batch_run_debug(GpuBpfBatch* batch, const float* y_dev, int
 int          gpu_bpf_batch_resample_counts(GpuBpfBatch* batch, int* counts, float* hmean_last);
 /* Resumable stepping: advance every filter by n_ticks from where the previous step left it
  * (the first step after create or gpu_bpf_batch_reset starts at tick 0), enqueued on the batch
- * stream as one CUDA graph. Device buffers: y_dev[n_ticks]; dll_dev[n_filters*n_ticks] and
+ * stream as one CUDA graph (captured on the first call and whenever n_ticks or the CTA shapes
+ * change; a call that differs only in y_dev / dll_dev / hmean_dev launches the same kernels
+ * directly, so walking a device series one tick at a time captures nothing). Device buffers: y_dev[n_ticks]; dll_dev[n_filters*n_ticks] and
  * hmean_dev[n_filters*n_ticks] (either may be NULL) receive this step's per-tick increments and
  * filtered means. The filters' state lives on the device between steps (8 B per particle). A
  * batch stepped in pieces is bit-identical to one run over the whole series. */
