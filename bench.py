@@ -81,6 +81,10 @@ def parse_args():
     ap.add_argument("--no-extensions", action="store_true")
     ap.add_argument("--bgrad-filters", type=int, default=256)
     ap.add_argument("--bgrad-ticks", type=int, default=4000)
+    ap.add_argument("--parity-ticks", type=int, default=20,
+                    help="ticks of the headline run followed by the FP64 oracle in lock step (0 = off)")
+    ap.add_argument("--plumbing-check", action="store_true",
+                    help="CPU-only check of the multi-rank path (gloo): rank launch, shard, gather, max-reduce")
     return ap.parse_args()
 
 
@@ -213,6 +217,28 @@ def bench_batched(dev, args, lib, rank, world, barrier):
     finite = bool(torch.isfinite(ll).all().item())
     b.close()
 
+    # several ranks: every filter's log-likelihood gathered from the shards must equal one GPU running
+    # all filters (both with the default CTA shapes: a filter's result depends on its class's shape,
+    # never on the other filters in the launch)
+    shard_check = None
+    if world > 1:
+        bd = gpubpf.GpuBpfBatch(fl, ess_threshold=0.0)
+        ll_d = torch.zeros(len(fl), dtype=torch.float64, device=dev)
+        bd.run_device(y_d.data_ptr(), T, ll_d.data_ptr())
+        torch.cuda.synchronize(dev)
+        bd.close()
+        full = parallel.gather_results(idx, ll_d.cpu().tolist(), B)
+        if rank == 0:
+            ba = gpubpf.GpuBpfBatch(allf, ess_threshold=0.0)
+            ll_a = torch.zeros(B, dtype=torch.float64, device=dev)
+            ba.run_device(y_d.data_ptr(), T, ll_a.data_ptr())
+            one = ll_a.cpu().tolist()
+            ba.close()
+            diffs = [abs(a - b_) for a, b_ in zip(full, one)]
+            shard_check = {"filters": B, "ranks": world, "bit_identical": all(a == b_ for a, b_ in zip(full, one)),
+                           "max_abs_diff": max(diffs),
+                           "method": "per-filter loglik gathered from the LPT shards vs one GPU running all filters"}
+
     # comparator: per-filter plain launches (graph per filter, one stream each)
     sub = fl[::16]
     filt = [gpubpf.GpuBpf(f["n_particles"], f["rho"], f["sigma_z"], f["mu"], 0.0, 0.0, f["seed"], ess_threshold=0.0)
@@ -236,7 +262,7 @@ def bench_batched(dev, args, lib, rank, world, barrier):
             "per_filter_plain": {"value": per_filter, "unit": "particle-steps/s", "filters_timed": len(sub),
                                  "method": "gpu_bpf_step_many_device per filter, own stream, CUDA graph"},
             "speedup_vs_per_filter": value / per_filter if world == 1 else None,
-            "loglik_finite": finite}
+            "loglik_finite": finite, "shard_check": shard_check}
 
 
 def bench_sweep(dev, args, lib, rank, world, barrier):
@@ -726,6 +752,107 @@ def bench_batch_gradient(dev, args, lib, rank, world, barrier):
             "shard": f"LPT on N over {world} rank(s)"}
 
 
+def headline_config(args, world):
+    """The `config` of the headline line, identical in both arms (same workload, same keys)."""
+    return {"workload": f"plain SV BPF, N={args.n}, T={args.ticks}, ESS<{args.ess}N, theta=(mu={MU}, phi={RHO}, "
+                        f"sigma_eta={SIG}), DGP seed {args.dgp_seed}",
+            "n_particles": args.n, "ticks": args.ticks, "ess_threshold": args.ess, "l2": L2_NOTE,
+            "parallelism": f"replicas x{world}" if world > 1 else "single filter"}
+
+
+def _free_port():
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def spawn_ranks(n):
+    """`bench.py --gpus N` started without a launcher: start N ranks of this same command line (one
+    process per GPU) through torch.distributed.run on 127.0.0.1 and return its exit status. Rank 0
+    prints the JSON line."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={_free_port()}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def plumbing_check(args):
+    """The multi-rank path of this bench without a GPU (gloo): every rank takes its LPT shard of the
+    configuration-4 filters, produces one stand-in value per filter (a function of the filter alone),
+    the values are gathered with gpubpf.parallel.gather_results and a per-rank time is max-reduced,
+    as the GPU path does. Rank 0 prints one JSON line saying whether every filter came back once and
+    unchanged."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from gpubpf import configs, parallel
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    allf = configs.config4(args.batch_filters)
+
+    def stand_in(f):
+        return f["n_particles"] * 1e-3 + f["mu"] + 10.0 * f["rho"] + 100.0 * f["sigma_z"] + f["seed"] * 1e-6
+
+    idx, mine = parallel.shard(allf, rank, world)
+    vals = [stand_in(f) for f in mine]
+    full = parallel.gather_results(idx, vals, len(allf)) if world > 1 else vals
+    t = torch.tensor([float(rank + 1)], dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        ok = len(full) == len(allf) and all(a == stand_in(f) for a, f in zip(full, allf))
+        print(json.dumps({"plumbing_check": True, "n_ranks": world, "filters": len(allf), "gathered_ok": ok,
+                          "max_over_ranks": float(t.item()), "shard_sizes": [len(p) for p in parallel.lpt_partition(
+                              [f["n_particles"] for f in allf], world)]}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def headline_parity(N, y, ess, ticks, seed=42):
+    """The headline workload's first `ticks` ticks followed by the FP64 oracle in lock step: the
+    device filter runs tick by tick through the C ABI with its ancestors recorded, the oracle
+    replays each tick's resampling decision and ancestors, and each resampling tick's ancestors are
+    recomputed by the oracle's fixed-point mirror from the device's weights. Checker only: nothing
+    here is timed."""
+    import numpy as np
+    import gpubpf
+    from oracle import oracle
+    f = gpubpf.GpuBpf(N, RHO, SIG, MU, 0.0, 0.0, seed, ess_threshold=ess)
+    f.record_ancestors(True)
+    o = oracle.F64Filter(N, RHO, SIG, MU, seed=seed, ess_threshold=ess)
+    gd, od, n_res, n_exact = [], [], 0, 0
+    try:
+        for t in range(ticks):
+            f.step(float(y[t]))
+            r = f.get_record()
+            anc = None
+            if r.resampled:
+                anc = np.frombuffer(f.get_ancestors()[1], dtype=np.int32)
+                w, te, u23 = f.get_resample_inputs()
+                ref = oracle.resample_fixed(np.frombuffer(w, dtype=np.float32), np.frombuffer(te, dtype=np.int32), u23)
+                n_res += 1
+                n_exact += int(np.array_equal(anc, ref))
+            q = o.tick(y[t], anc=anc, flag=int(r.resampled))
+            gd.append(r.dloglik)
+            od.append(q["dll"])
+    finally:
+        f.close()
+        o.close()
+    gd, od = np.asarray(gd), np.asarray(od)
+    return {"n_particles": N, "ticks": ticks, "filter_seed": seed,
+            "loglik": float(gd.sum()), "loglik_oracle_fp64": float(od.sum()),
+            "loglik_rel_err": float(abs(gd.sum() - od.sum()) / abs(od.sum())),
+            "max_abs_increment_err": float(np.max(np.abs(gd - od))),
+            "resampling_ticks": n_res, "ancestors_bit_exact_ticks": n_exact,
+            "method": "FP64 oracle (oracle/bpf_oracle.c orc_f64_tick) in lock step on the device's ancestors; "
+                      "ancestors vs orc_resample_fixed on the device's weights"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -749,9 +876,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": wall / max(1, args.steps) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plain SV BPF (N={args.n}, T={args.ticks}, ESS<{args.ess}N, DGP seed {args.dgp_seed})",
-                   "n_particles": args.n, "ticks": args.ticks, "ess_threshold": args.ess,
-                   "parallelism": "host cores"},
+        "config": headline_config(args, int(os.environ.get("WORLD_SIZE", "1"))),
         "us_per_tick": statistics.mean(uspt),
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": "port",
                          "sample": r["sample"]},
@@ -837,6 +962,10 @@ def reference_gpu(args, y):
 
 def main():
     args = parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args.gpus)
+    if args.plumbing_check:
+        return plumbing_check(args)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -980,9 +1109,12 @@ def main():
     extensions = None if (args.no_extensions or world > 1) else bench_extensions(dev, args, lib, rank)
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(N, y_host, args.ess, args.cpu_seconds)
         cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if args.parity_ticks > 0:
+            parity = headline_parity(N, y_host, args.ess, min(args.parity_ticks, T))
 
     if rank == 0:
         line = {
@@ -990,15 +1122,13 @@ def main():
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (reference matched DGP, seed 7)",
-            "config": {"workload": f"plain SV BPF, N={N}, T={T}, ESS<{args.ess}N, theta=(mu={MU}, phi={RHO}, "
-                                   f"sigma_eta={SIG}), DGP seed {args.dgp_seed}",
-                       "n_particles": N, "ticks": T, "ess_threshold": args.ess, "l2": L2_NOTE,
-                       "parallelism": f"replicas x{world}" if world > 1 else "single filter"},
+            "config": headline_config(args, world),
             "us_per_tick": ms_max / (args.steps * T) * 1e3,
             "resample_rate": resample_rate,
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": e2e,
             "clocks": clocks,
             "sweep": sweep,

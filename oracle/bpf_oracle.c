@@ -242,6 +242,146 @@ static int nu_int_of(double nu_state) { return nu_state > 0.0 ? (int)(nu_state +
 static int ceil_log2_u(unsigned n) { int c = 0; while ((1ull << c) < (unsigned long long)n) ++c; return c; }
 
 /*
+ * The FP64 filter as an object stepped one tick at a time, so a checker can
+ * follow a device run of any length in lock step (replaying each resampling
+ * tick's ancestors as it comes) without holding T x N ancestors. The
+ * per-particle loops run on OpenMP threads; every sum runs over the
+ * particles in index order on one thread, so results do not depend on the
+ * thread count.
+ */
+typedef struct {
+    OrcConfig c;
+    int N, nu_int, t, prev_res;
+    double mu, rho, sig, nu, cobs, lse_prev, llr;
+    uint64_t ustate;
+    double *h, *hn, *lw, *lwc, *cdf;
+} OrcF64;
+
+void orc_f64_destroy(OrcF64* s) {
+    if (!s) return;
+    free(s->h); free(s->hn); free(s->lw); free(s->lwc); free(s->cdf);
+    free(s);
+}
+
+OrcF64* orc_f64_create(const OrcConfig* c) {
+    const int N = c->n_particles;
+    if (N <= 0) return NULL;
+    OrcF64* s = (OrcF64*)calloc(1, sizeof(OrcF64));
+    if (!s) return NULL;
+    s->c = *c;
+    s->N = N;
+    s->h = (double*)malloc(sizeof(double) * N);
+    s->hn = (double*)malloc(sizeof(double) * N);
+    s->lw = (double*)malloc(sizeof(double) * N);
+    s->lwc = (double*)malloc(sizeof(double) * N);
+    s->cdf = (double*)malloc(sizeof(double) * N);
+    if (!s->h || !s->hn || !s->lw || !s->lwc || !s->cdf) { orc_f64_destroy(s); return NULL; }
+    s->mu = c->mu; s->rho = c->rho; s->sig = c->sigma_z; s->nu = c->nu_obs; s->cobs = c_obs_of(s->nu);
+    s->nu_int = nu_int_of((double)c->nu_state);
+    const double sstat = sqrt(s->sig * s->sig / fmax(1.0 - s->rho * s->rho, 1e-6));
+    double* h = s->h;
+    double* lwc = s->lwc;
+    const double mu = s->mu;
+    const int seed = c->seed;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N; ++i) {
+        float u = orc_uniform(orc_pcg32_draw_jump(seed, (uint32_t)i, 0));
+        h[i] = mu + sstat * orc_icdf_f64((double)u);
+        lwc[i] = 0.0;
+    }
+    s->ustate = orc_host_seed(seed);
+    s->prev_res = 1;
+    s->lse_prev = log((double)N);
+    s->llr = 0.0;
+    s->t = 0;
+    return s;
+}
+
+/*
+ * One tick on observation y. anc: this tick's ancestors [N] used if the tick
+ * resamples (NULL = own FP64 systematic resampling); flag: the resampling
+ * decision to replay (-1 = own). out5 (may be NULL) receives
+ * {dll, ll_ref, hmean, ess, resampled}.
+ */
+int orc_f64_tick(OrcF64* s, float y, const int32_t* anc, int flag, double* out5) {
+    if (!s) return 1;
+    const int N = s->N, t = s->t;
+    const double mu = s->mu, rho = s->rho, sig = s->sig, nu = s->nu, cobs = s->cobs;
+    double* h = s->h;
+    double* lw = s->lw;
+    double* lwc = s->lwc;
+    double* cdf = s->cdf;
+    const int seed = s->c.seed, nu_int = s->nu_int, prev_res = s->prev_res;
+    const double nu_state = (double)s->c.nu_state;
+    if (t > 0) {
+        uint64_t At, Bt;
+        orc_pcg32_jump((uint64_t)t, &At, &Bt);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < N; ++i) {
+            uint64_t s0, inc;
+            orc_pcg32_init(seed, (uint32_t)i, &s0, &inc);
+            float u = orc_uniform(orc_pcg32_output(At * s0 + Bt * inc));
+            double eps = orc_icdf_f64((double)u);
+            if (nu_int > 0) eps *= orc_tstate_scale(seed, (uint32_t)i, t, nu_int, nu_state);
+            h[i] = mu + rho * (h[i] - mu) + sig * eps;
+        }
+    }
+    double M = -INFINITY;
+#pragma omp parallel for schedule(static) reduction(max : M)
+    for (int i = 0; i < N; ++i) {
+        lw[i] = (prev_res ? 0.0 : lwc[i]) + obs_logpdf_f64((double)y, h[i], nu, cobs);
+        if (lw[i] > M) M = lw[i];
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N; ++i) cdf[i] = exp(lw[i] - M);
+    double S = 0.0, Q = 0.0, H = 0.0;
+    for (int i = 0; i < N; ++i) {
+        const double e = cdf[i];
+        S += e; Q += e * e; H += e * h[i];
+        cdf[i] = S;
+    }
+    const double lse = M + log(S);
+    const double d = lse - (prev_res ? log((double)N) : s->lse_prev);
+    s->llr = (prev_res ? 0.0 : s->llr) + d;
+    const double es = S * S / Q;
+    const int res = flag >= 0 ? (flag != 0)
+                              : ((s->c.ess_threshold <= 0.0f) || (es / (double)N < (double)s->c.ess_threshold));
+    if (out5) { out5[0] = d; out5[1] = s->llr; out5[2] = H / S; out5[3] = es; out5[4] = (double)res; }
+    if (res) {
+        const uint32_t u23 = orc_host_pcg32(&s->ustate) >> 9;
+        double* hn = s->hn;
+        if (anc) {
+            for (int i = 0; i < N; ++i) if (anc[i] < 0 || anc[i] >= N) return 3;
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < N; ++i) hn[i] = h[anc[i]];
+        } else {
+            const double step = S / (double)N, u0 = (double)u23 * 1.1920928955078125e-07;
+            int j = 0;
+            for (int i = 0; i < N; ++i) {
+                double target = (u0 + (double)i) * step;
+                while (j < N - 1 && !(cdf[j] > target)) ++j;
+                hn[i] = h[j];
+            }
+        }
+        s->hn = h; s->h = hn;
+        s->prev_res = 1;
+    } else {
+        double* tmp = s->lwc; s->lwc = s->lw; s->lw = tmp;   /* the carried log-weights */
+        s->lse_prev = lse;
+        s->prev_res = 0;
+    }
+    s->t = t + 1;
+    return 0;
+}
+
+/* Current particles h[0..N) of the object (after its last tick's resampling). */
+int orc_f64_particles(const OrcF64* s, double* out) {
+    if (!s || !out) return 1;
+    memcpy(out, s->h, sizeof(double) * s->N);
+    return 0;
+}
+
+/*
  * y[T]; anc_replay: [T][N] ancestors used on resampling ticks (NULL = own FP64
  * systematic resampling); flags_replay: [T] decisions to replay (NULL = own).
  * Outputs (each may be NULL): dll[T], ll_ref[T], hmean[T], ess[T], flags_out[T].
@@ -249,83 +389,22 @@ static int ceil_log2_u(unsigned n) { int c = 0; while ((1ull << c) < (unsigned l
 int orc_filter_f64(const OrcConfig* c, const float* y, int T,
                    const int32_t* anc_replay, const int32_t* flags_replay,
                    double* dll, double* ll_ref, double* hmean, double* ess, int32_t* flags_out) {
+    if (c->n_particles <= 0 || T < 0) return 1;
+    OrcF64* s = orc_f64_create(c);
+    if (!s) return 2;
     const int N = c->n_particles;
-    if (N <= 0 || T < 0) return 1;
-    double* h = (double*)malloc(sizeof(double) * N);
-    double* hn = (double*)malloc(sizeof(double) * N);
-    double* lw = (double*)malloc(sizeof(double) * N);
-    double* lwc = (double*)malloc(sizeof(double) * N);
-    double* cdf = (double*)malloc(sizeof(double) * N);
-    if (!h || !hn || !lw || !lwc || !cdf) { free(h); free(hn); free(lw); free(lwc); free(cdf); return 2; }
-    const double mu = c->mu, rho = c->rho, sig = c->sigma_z, nu = c->nu_obs, cobs = c_obs_of(nu);
-    const int nu_int = nu_int_of((double)c->nu_state);
-    const double sstat = sqrt(sig * sig / fmax(1.0 - rho * rho, 1e-6));
-    for (int i = 0; i < N; ++i) {
-        float u = orc_uniform(orc_pcg32_draw_jump(c->seed, (uint32_t)i, 0));
-        h[i] = mu + sstat * orc_icdf_f64((double)u);
-        lwc[i] = 0.0;
-    }
-    uint64_t ustate = orc_host_seed(c->seed);
-    int prev_res = 1;
-    double lse_prev = log((double)N), llr = 0.0;
     for (int t = 0; t < T; ++t) {
-        if (t > 0) {
-            uint64_t At, Bt;
-            orc_pcg32_jump((uint64_t)t, &At, &Bt);
-            for (int i = 0; i < N; ++i) {
-                uint64_t s0, inc;
-                orc_pcg32_init(c->seed, (uint32_t)i, &s0, &inc);
-                float u = orc_uniform(orc_pcg32_output(At * s0 + Bt * inc));
-                double eps = orc_icdf_f64((double)u);
-                if (nu_int > 0) eps *= orc_tstate_scale(c->seed, (uint32_t)i, t, nu_int, (double)c->nu_state);
-                h[i] = mu + rho * (h[i] - mu) + sig * eps;
-            }
-        }
-        double M = -INFINITY;
-        for (int i = 0; i < N; ++i) {
-            lw[i] = (prev_res ? 0.0 : lwc[i]) + obs_logpdf_f64((double)y[t], h[i], nu, cobs);
-            if (lw[i] > M) M = lw[i];
-        }
-        double S = 0.0, Q = 0.0, H = 0.0;
-        for (int i = 0; i < N; ++i) {
-            double e = exp(lw[i] - M);
-            S += e; Q += e * e; H += e * h[i];
-            cdf[i] = S;
-        }
-        const double lse = M + log(S);
-        const double d = lse - (prev_res ? log((double)N) : lse_prev);
-        llr = (prev_res ? 0.0 : llr) + d;
-        const double es = S * S / Q;
-        if (dll) dll[t] = d;
-        if (ll_ref) ll_ref[t] = llr;
-        if (hmean) hmean[t] = H / S;
-        if (ess) ess[t] = es;
-        int res = flags_replay ? (flags_replay[t] != 0)
-                               : ((c->ess_threshold <= 0.0f) || (es / (double)N < (double)c->ess_threshold));
-        if (flags_out) flags_out[t] = res;
-        if (res) {
-            uint32_t u23 = orc_host_pcg32(&ustate) >> 9;
-            if (anc_replay) {
-                const int32_t* a = anc_replay + (size_t)t * N;
-                for (int i = 0; i < N; ++i) hn[i] = h[a[i]];
-            } else {
-                const double step = S / (double)N, u0 = (double)u23 * 1.1920928955078125e-07;
-                int j = 0;
-                for (int i = 0; i < N; ++i) {
-                    double target = (u0 + (double)i) * step;
-                    while (j < N - 1 && !(cdf[j] > target)) ++j;
-                    hn[i] = h[j];
-                }
-            }
-            double* tmp = h; h = hn; hn = tmp;
-            prev_res = 1;
-        } else {
-            memcpy(lwc, lw, sizeof(double) * N);
-            lse_prev = lse;
-            prev_res = 0;
-        }
+        double o[5];
+        const int rc = orc_f64_tick(s, y[t], anc_replay ? anc_replay + (size_t)t * N : NULL,
+                                    flags_replay ? (flags_replay[t] != 0) : -1, o);
+        if (rc) { orc_f64_destroy(s); return rc; }
+        if (dll) dll[t] = o[0];
+        if (ll_ref) ll_ref[t] = o[1];
+        if (hmean) hmean[t] = o[2];
+        if (ess) ess[t] = o[3];
+        if (flags_out) flags_out[t] = (int32_t)o[4];
     }
-    free(h); free(hn); free(lw); free(lwc); free(cdf);
+    orc_f64_destroy(s);
     return 0;
 }
 

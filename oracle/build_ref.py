@@ -41,7 +41,8 @@ SHIM = os.path.join(HERE, "ref_gpu_shim.cu")
 LIB_C = os.path.join(OUT, "librefcuda.so")
 SHIM_C = os.path.join(HERE, "ref_cuda_shim.cu")
 
-REF_ROOT = os.environ.get("BPF_REFERENCE_ROOT", "/root/reference")
+# The reference tree: $BPF_REFERENCE_ROOT, else a checkout named `reference` beside this repository.
+REF_ROOT = os.environ.get("BPF_REFERENCE_ROOT") or os.path.join(os.path.dirname(HERE), os.pardir, "reference")
 REF_DRIVER = os.path.join(REF_ROOT, "gpu_bpf", "gpu_bpf_ptx_full.cu")
 REF_PTX = os.path.join(REF_ROOT, "ptx_assembly", "bpf_kernels_full.ptx")
 REF_CUDA = os.path.join(REF_ROOT, "gpu_bpf", "gpu_bpf.cu")

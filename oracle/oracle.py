@@ -70,6 +70,11 @@ def lib(native: bool = False) -> C.CDLL:
     L.orc_filter_f64.restype = C.c_int
     L.orc_filter_f64.argtypes = [P(OrcConfig), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_f64_create.restype = C.c_void_p; L.orc_f64_create.argtypes = [P(OrcConfig)]
+    L.orc_f64_destroy.restype = None; L.orc_f64_destroy.argtypes = [C.c_void_p]
+    L.orc_f64_tick.restype = C.c_int
+    L.orc_f64_tick.argtypes = [C.c_void_p, f32, C.c_void_p, C.c_int, C.c_void_p]
+    L.orc_f64_particles.restype = C.c_int; L.orc_f64_particles.argtypes = [C.c_void_p, C.c_void_p]
     L.orc_resample_fixed.restype = C.c_int
     L.orc_resample_fixed.argtypes = [C.c_int, C.c_void_p, C.c_void_p, u32, C.c_void_p]
     L.orc_ref_run.restype = C.c_int
@@ -137,6 +142,47 @@ def filter_f64(n_particles, rho, sigma_z, mu, y, seed=42, ess_threshold=0.0, nu_
         raise RuntimeError(f"orc_filter_f64 failed ({rc})")
     out["resampled"] = flags
     return out
+
+
+class F64Filter:
+    """The FP64 oracle filter stepped one tick at a time (orc_f64_*): follows a device run of any
+    length in lock step, replaying each resampling tick's ancestors as it comes."""
+
+    def __init__(self, n_particles, rho, sigma_z, mu, seed=42, ess_threshold=0.0, nu_obs=0.0, nu_state=0.0):
+        self._L = lib()
+        self.N = int(n_particles)
+        self._cfg = OrcConfig(self.N, rho, sigma_z, mu, nu_obs, int(seed), ess_threshold, nu_state)
+        self._s = self._L.orc_f64_create(C.byref(self._cfg))
+        if not self._s:
+            raise MemoryError("orc_f64_create failed")
+
+    def tick(self, y, anc=None, flag=None):
+        """One tick; anc [N] int32 replays the ancestors if the tick resamples, flag replays the
+        decision. Returns dict dll, ll_ref, hmean, ess, resampled."""
+        a = None if anc is None else np.ascontiguousarray(anc, dtype=np.int32)
+        if a is not None and a.shape[0] != self.N:
+            raise ValueError("anc must hold N ancestors")
+        out = np.zeros(5, dtype=np.float64)
+        rc = self._L.orc_f64_tick(self._s, float(y), _ptr(a), -1 if flag is None else int(bool(flag)), _ptr(out))
+        if rc != 0:
+            raise RuntimeError(f"orc_f64_tick failed ({rc})")
+        return {"dll": out[0], "ll_ref": out[1], "hmean": out[2], "ess": out[3], "resampled": int(out[4])}
+
+    def particles(self):
+        out = np.zeros(self.N, dtype=np.float64)
+        self._L.orc_f64_particles(self._s, _ptr(out))
+        return out
+
+    def close(self):
+        if self._s:
+            self._L.orc_f64_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def filter_noise_f64(n_particles, rho, sigma_z, mu, y, z, ess_threshold=0.0, nu_obs=0.0, anc_replay=None,

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container where the reference checkout is mounted (default
-/root/reference, or $BPF_REFERENCE). Nothing at test time reads the
+Run where the reference checkout is readable ($BPF_REFERENCE, else a directory
+named `reference` beside this repository). Nothing at test time reads the
 reference; only the JSON files written here are committed.
 
 Fixtures
@@ -39,7 +39,9 @@ import subprocess
 import sys
 import tempfile
 
-REF = os.environ.get("BPF_REFERENCE", "/root/reference")
+# The reference tree: $BPF_REFERENCE, else a checkout named `reference` beside this repository.
+REF = os.environ.get("BPF_REFERENCE") or os.path.join(os.path.dirname(os.path.abspath(__file__)), os.pardir,
+                                                      os.pardir, os.pardir, "reference")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -80,3 +80,25 @@ def test_sharded_batch_gathers_every_filter():
     ref = [oracle.filter_f64(f["n_particles"], f["rho"], f["sigma_z"], f["mu"], y, seed=f["seed"])["dll"].sum()
            for f in fl]
     np.testing.assert_allclose(full, ref, rtol=0, atol=0)
+
+
+def test_bench_spawns_ranks_and_gathers():
+    """`bench.py --gpus 2` started without a launcher starts its own two ranks (torch.distributed.run
+    on 127.0.0.1); with --plumbing-check they run on CPU over gloo: LPT shards of the
+    configuration-4 filters, the gather of per-filter values and the max over ranks, as the GPU
+    path does."""
+    import json
+    import subprocess
+    import sys
+    env = dict(os.environ)
+    env.pop("WORLD_SIZE", None)
+    env.pop("RANK", None)
+    env.pop("LOCAL_RANK", None)
+    out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--gpus", "2", "--plumbing-check"],
+                         cwd=REPO, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["n_ranks"] == 2 and d["filters"] == 1024 and d["gathered_ok"]
+    assert d["max_over_ranks"] == 2.0 and sum(d["shard_sizes"]) == 1024
