@@ -22,6 +22,12 @@ A second library, oracle/_ref/librefcuda.so, is the reference's CUDA-C edition
 IMM) compiled from where it lies with oracle/ref_cuda_shim.cu. The two
 editions export the same C++ names, so each gets its own library.
 
+The drop-in check (build_dropin) compiles some of the reference's own caller
+programs (its tests and benchmarks that use the host API) from where they lie,
+unchanged, against this repository's include/ directory (which answers to the
+reference header names gpu_bpf.cuh and gpu_bpf_full.cuh) and links them to
+libgpubpf.so, into oracle/_ref/dropin/. tests/test_gpu_dropin.py runs them.
+
 The output is git-ignored and travels with the repository snapshot to a GPU
 machine; the reference tree itself is only read here, at build time.
 """
@@ -75,6 +81,55 @@ def build_cuda(force: bool = False) -> str | None:
     return LIB_C
 
 
+REPO = os.path.dirname(HERE)
+INCLUDE = os.path.join(REPO, "include")
+PKG_LIB_DIR = os.path.join(REPO, "bootstrap-particle-filter-in-ptx_b200", "gpubpf")
+DROPIN = os.path.join(OUT, "dropin")
+# reference caller programs built unchanged against include/ + libgpubpf.so: (output name, source, defines)
+DROPIN_PROGRAMS = [
+    ("bench_particle_scaling", os.path.join("tests", "bench_particle_scaling.cu"), []),
+    ("bench_particle_scaling_ptx_full", os.path.join("tests", "bench_particle_scaling.cu"), ["-DUSE_PTX_FULL=1"]),
+    ("test_cond_resample", os.path.join("tests", "test_cond_resample.cu"), []),
+    ("test_bpf_matched_dgp", os.path.join("tests", "test_bpf_matched_dgp.cu"), []),
+    ("test_mu_learning", os.path.join("smc2", "test_mu_learning.cu"), []),
+    ("bench_grad_overhead", os.path.join("tests", "bench_grad_overhead.cu"), []),
+]
+
+
+def dropin_path(name: str) -> str:
+    return os.path.join(DROPIN, name)
+
+
+def build_dropin(force: bool = False) -> list:
+    """Compile the reference caller programs of DROPIN_PROGRAMS, unmodified, against include/ and
+    libgpubpf.so (run-time search path relative to the executable). Returns the names built or up
+    to date; nothing when the reference tree is absent."""
+    lib = os.path.join(PKG_LIB_DIR, "libgpubpf.so")
+    if not os.path.exists(lib):
+        return []
+    headers = [os.path.join(INCLUDE, h) for h in ("gpu_bpf.h", "gpu_bpf.cuh", "gpu_bpf_full.cuh")]
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    rpath = "$ORIGIN/" + os.path.relpath(PKG_LIB_DIR, DROPIN)
+    done = []
+    for name, rel, defs in DROPIN_PROGRAMS:
+        src = os.path.join(REF_ROOT, rel)
+        out = dropin_path(name)
+        if not os.path.exists(src):
+            if os.path.exists(out):
+                done.append(name)
+            continue
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(p) for p in [src] + headers):
+            done.append(name)
+            continue
+        os.makedirs(DROPIN, exist_ok=True)
+        cmd = [nvcc, "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", *defs, "-I", INCLUDE, src,
+               "-o", out + ".tmp", "-L", PKG_LIB_DIR, "-lgpubpf", "-Xlinker", "-rpath", "-Xlinker", rpath]
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        os.replace(out + ".tmp", out)
+        done.append(name)
+    return done
+
+
 def _retarget(src: bytes) -> bytes:
     text = bytes(b for b in src if b < 0x80).decode("ascii")
     text, n = re.subn(r"^\.target\s+sm_\w+", ".target sm_100a", text, count=1, flags=re.M)
@@ -109,3 +164,4 @@ if __name__ == "__main__":
     path = build(force="--force" in sys.argv)
     print(path or "reference tree absent; oracle/_ref not built")
     print(build_cuda(force="--force" in sys.argv) or "reference tree absent; CUDA-C edition not built")
+    print("drop-in programs:", build_dropin(force="--force" in sys.argv))
