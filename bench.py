@@ -50,7 +50,7 @@ for _p in (REPO, PKG_DIR):
         sys.path.insert(0, _p)
 
 RHO, SIG, MU = 0.97, 0.15, -1.0
-DEVSTATE_BYTES = 168          # sizeof(bpf::DevState), read back once after a host-buffer run
+DEVSTATE_BYTES = 200          # sizeof(bpf::DevState), read back once after a host-buffer run
 RECORD_BYTES = 40             # sizeof(BpfTickRecord)
 L2_NOTE = "working set h 4B + w 4B per particle = 128 MiB per tick at N=2^24 (> 126 MB L2); 256 MiB L2 flush between steps"
 

@@ -69,7 +69,7 @@ struct Impl {
 
   // graph of kGraphChunk ticks, keyed by the launch arguments baked into it
   cudaGraphExec_t graph = nullptr;
-  float g_mu = NAN, g_rho = NAN, g_sigma = NAN, g_thr = NAN, g_nus = NAN;
+  float g_mu = NAN, g_rho = NAN, g_sigma = NAN, g_thr = NAN, g_nus = NAN, g_silv = NAN;
   bool g_anc = false;
 
   // graph of one tick for single steps (gpu_bpf_step / step_async), keyed likewise: pass 1's
@@ -83,7 +83,7 @@ struct Impl {
   Plan t_plan{};
   TickArgs t_args{};
   void* t_argv[2] = {nullptr, nullptr};
-  float t_mu = NAN, t_rho = NAN, t_sigma = NAN, t_thr = NAN, t_nus = NAN;
+  float t_mu = NAN, t_rho = NAN, t_sigma = NAN, t_thr = NAN, t_nus = NAN, t_silv = NAN;
   bool t_anc = false;
 
   // graph of a whole device-resident run (step_many_device), keyed likewise
@@ -91,7 +91,7 @@ struct Impl {
   const float* dg_y = nullptr;
   BpfTickRecord* dg_rec = nullptr;
   int dg_n = 0;
-  float dg_mu = NAN, dg_rho = NAN, dg_sigma = NAN, dg_thr = NAN, dg_nus = NAN;
+  float dg_mu = NAN, dg_rho = NAN, dg_sigma = NAN, dg_thr = NAN, dg_nus = NAN, dg_silv = NAN;
   bool dg_anc = false;
 
   // programmatic dependent launch between consecutive kernels (off while profiling)
@@ -120,10 +120,14 @@ int ensure_device(Impl* m) {
   return BPF_OK;
 }
 
+// Kernels one tick launches: pass 1, plan, pass 2, and the two Silverman jitter kernels when on.
+int tick_launches(const TickArgs& a) { return a.silverman > 0.0f ? 5 : 3; }
+
 cudaError_t launch_tick3(Impl* m, const TickArgs& a) {
   cudaError_t e = launch_pass1(m->plan, a, m->stream, m->pdl);
   if (e == cudaSuccess) e = launch_plan(m->plan, a, m->stream, m->pdl);
   if (e == cudaSuccess) e = launch_pass2(m->plan, a, m->pass2_grid, m->stream, m->pdl);
+  if (e == cudaSuccess && a.silverman > 0.0f) e = launch_jitter(m->plan, a, m->stream, m->pdl);
   return e;
 }
 
@@ -140,13 +144,14 @@ TickArgs make_args(GpuBpfState* s, Impl* m, float y, const float* y_ptr, BpfTick
   a.nu_int = (s->nu_state > 0.0f) ? (int)(s->nu_state + 0.5f) : 0;   // gpu_bpf_ptx_full.cu:392
   a.nu_state = s->nu_state;
   a.learn = m->learn_mode ? 1 : 0;
+  a.silverman = s->silverman_shrink > 0.0f ? s->silverman_shrink : 0.0f;   // gpu_bpf_ptx_full.cu:709
   return a;
 }
 
 int check_options(GpuBpfState* s) {
   if (!std::isfinite(s->mu) || !std::isfinite(s->rho) || !std::isfinite(s->sigma_z)) return set_err(BPF_ERR_ARG);
   if (!(std::fabs(s->rho) < 1.0f) || !(s->sigma_z > 0.0f)) return set_err(BPF_ERR_ARG);
-  if (s->silverman_shrink != 0.0f) return set_err(BPF_ERR_UNSUPPORTED);
+  if (!std::isfinite(s->silverman_shrink)) return set_err(BPF_ERR_ARG);
   if (!(s->nu_state == 0.0f || (s->nu_state >= 0.5f && std::isfinite(s->nu_state)))) return set_err(BPF_ERR_ARG);
   if (std::isnan(s->ess_threshold)) return set_err(BPF_ERR_ARG);
   return BPF_OK;
@@ -216,13 +221,14 @@ int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
     CK(launch_plan(m->plan, a, m->stream, false));
     CK(cudaEventRecord(ev[2], m->stream));
     CK(launch_pass2(m->plan, a, m->pass2_grid, m->stream, false));
+    if (a.silverman > 0.0f) CK(launch_jitter(m->plan, a, m->stream, false));   // timed with pass 2
     CK(cudaEventRecord(ev[3], m->stream));
     for (cudaEvent_t e : ev) m->ev_pending.push_back(e);
     if (m->ev_pending.size() >= 4 * 4096) { int rc = drain_profile(m); if (rc) return rc; }
   } else {
     CK(launch_tick3(m, a));
   }
-  g_launches += 3;
+  g_launches += tick_launches(a);
   const int tick = m->ticks_enqueued;
   m->ticks_enqueued += 1;
   if (m->learn_mode && tick > 0 && ++m->grad_count >= m->update_K) return learning_update(s, m);
@@ -294,6 +300,7 @@ int build_graph(GpuBpfState* s, Impl* m) {
   cudaGraphDestroy(g);
   if (e3 != cudaSuccess) { m->graph = nullptr; return set_err(BPF_ERR_CUDA); }
   m->g_mu = s->mu; m->g_rho = s->rho; m->g_sigma = s->sigma_z; m->g_thr = s->ess_threshold; m->g_nus = s->nu_state;
+  m->g_silv = s->silverman_shrink;
   m->g_anc = m->record_anc;
   return BPF_OK;
 }
@@ -317,13 +324,15 @@ int build_device_graph(GpuBpfState* s, Impl* m, const float* y_dev, int n, BpfTi
   m->dg_y = y_dev; m->dg_rec = rec_dev; m->dg_n = n;
   m->dg_mu = s->mu; m->dg_rho = s->rho; m->dg_sigma = s->sigma_z; m->dg_thr = s->ess_threshold;
   m->dg_nus = s->nu_state;
+  m->dg_silv = s->silverman_shrink;
   m->dg_anc = m->record_anc;
   return BPF_OK;
 }
 
 bool tick_graph_stale(GpuBpfState* s, Impl* m) {
   return !m->tgraph || m->t_mu != s->mu || m->t_rho != s->rho || m->t_sigma != s->sigma_z ||
-         m->t_thr != s->ess_threshold || m->t_nus != s->nu_state || m->t_anc != m->record_anc;
+         m->t_thr != s->ess_threshold || m->t_nus != s->nu_state || m->t_silv != s->silverman_shrink ||
+         m->t_anc != m->record_anc;
 }
 
 // Captures one tick (pass 1, plan, pass 2 with their programmatic dependencies) writing its
@@ -361,13 +370,15 @@ int build_tick_graph(GpuBpfState* s, Impl* m) {
   m->t_params.kernelParams = m->t_argv;
   m->t_params.extra = nullptr;
   m->t_mu = s->mu; m->t_rho = s->rho; m->t_sigma = s->sigma_z; m->t_thr = s->ess_threshold; m->t_nus = s->nu_state;
+  m->t_silv = s->silverman_shrink;
   m->t_anc = m->record_anc;
   return BPF_OK;
 }
 
 bool graph_stale(GpuBpfState* s, Impl* m) {
   return !m->graph || m->g_mu != s->mu || m->g_rho != s->rho || m->g_sigma != s->sigma_z ||
-         m->g_thr != s->ess_threshold || m->g_nus != s->nu_state || m->g_anc != m->record_anc;
+         m->g_thr != s->ess_threshold || m->g_nus != s->nu_state || m->g_silv != s->silverman_shrink ||
+         m->g_anc != m->record_anc;
 }
 
 }  // namespace
@@ -490,7 +501,7 @@ static int step_async_rc(GpuBpfState* s, float y_t, bool one_shot) {
     m->t_args.obs.y = y_t;
     CK(cudaGraphExecKernelNodeSetParams(m->tgraph, m->t_pass1, &m->t_params));
     CK(cudaGraphLaunch(m->tgraph, m->stream));
-    g_launches += 3;
+    g_launches += tick_launches(m->t_args);
     m->ticks_enqueued += 1;
     m->last_in_map = true;
     return BPF_OK;
@@ -641,7 +652,7 @@ int gpu_bpf_step_many(GpuBpfState* s, const float* y, int n_ticks, BpfResult* ou
       std::memcpy(m->y_pin, y + t, kGraphChunk * sizeof(float));
       CK(cudaGraphLaunch(m->graph, m->stream));
       CK(cudaStreamSynchronize(m->stream));
-      g_launches += 3 * kGraphChunk;
+      g_launches += (long long)tick_launches(make_args(s, m, 0.0f, nullptr, nullptr)) * kGraphChunk;
       m->ticks_enqueued += kGraphChunk;
       for (int k = 0; k < kGraphChunk; ++k) {
         if (out) out[t + k] = to_result(m, m->rec_pin[1 + k]);
@@ -693,10 +704,11 @@ int gpu_bpf_step_many_device(GpuBpfState* s, const float* y_dev, int n_ticks, Bp
   if (!m->profiling && !m->learn_mode && n_ticks > 0 && n_ticks <= kMaxGraphTicks) {
     const bool stale = !m->dgraph || m->dg_y != y_dev || m->dg_rec != rec_dev || m->dg_n != n_ticks ||
                        m->dg_mu != s->mu || m->dg_rho != s->rho || m->dg_sigma != s->sigma_z ||
-                       m->dg_thr != s->ess_threshold || m->dg_nus != s->nu_state || m->dg_anc != m->record_anc;
+                       m->dg_thr != s->ess_threshold || m->dg_nus != s->nu_state ||
+                       m->dg_silv != s->silverman_shrink || m->dg_anc != m->record_anc;
     if (stale) { rc = build_device_graph(s, m, y_dev, n_ticks, rec_dev); if (rc) return rc; }
     CK(cudaGraphLaunch(m->dgraph, m->stream));
-    g_launches += 3LL * n_ticks;
+    g_launches += (long long)tick_launches(make_args(s, m, 0.0f, nullptr, nullptr)) * n_ticks;
     m->ticks_enqueued += n_ticks;
   } else {
     for (int t = 0; t < n_ticks; ++t) {

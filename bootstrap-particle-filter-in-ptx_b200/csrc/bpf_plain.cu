@@ -431,6 +431,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
       ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
     }
     st->ll_ref = ll_ref;
+    st->hm = degenerate ? 0.0 : hm;
     if (a.apf != 1) st->ll_total += rec_dll;
     if (a.aux) *a.aux = degenerate ? make_float2(0.0f, __int_as_float(0))
                                    : make_float2((float)(1.0 / tS), __int_as_float(nM));
@@ -574,12 +575,24 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
 constexpr size_t kTileBytes = (size_t)kTile * 4;
 // u16 ancestor (tile-local + 1) per output slot of a window; a window starts
 // at its item's first output rounded down to a multiple of 4 (up to 3 extra
-// slots), rounded up to whole 128-slot steps of the gather
-constexpr size_t kMarkBytes = ((size_t)kOutChunk + 128) * 2;
+// slots), rounded up to whole 256-slot steps of the gather (8 slots a lane)
+constexpr int kGatherStep = 256;
+constexpr size_t kMarkBytes = ((size_t)kOutChunk + kGatherStep) * 2;
 constexpr size_t kMarkOffset = 2 * kTileBytes;                 // after the staged h and w tiles
 constexpr size_t kPass2Smem = kMarkOffset + kMarkBytes;         // one staged tile (h, w) + marks
 static_assert(kMarkOffset % 16 == 0 && kMarkBytes % 16 == 0, "marks are cleared with 16-byte stores");
-static_assert((size_t)kOutChunk % 128 == 0, "the gather reads marks in steps of 128 slots");
+static_assert((size_t)kOutChunk % kGatherStep == 0, "the gather reads marks in steps of 256 slots");
+
+// Tile-frame thresholds of the child count are kept relative to the thread's first
+// element and capped here: a thread's 16 fixed-point weights sum to at most 16 * 2^50
+// < kThCap, so a capped threshold is never reached, and threshold + c * spacing stays
+// below 2^57 for every count c the loop forms.
+constexpr unsigned long long kThCap = 1ull << 55;
+
+// floor(a / d) for 1 <= d, a < 2^62: the rare path of a parent with more than four children.
+__device__ __noinline__ unsigned long long udiv_slow(unsigned long long a, unsigned long long d) {
+  return udiv_fp64(a, d);
+}
 
 __device__ __forceinline__ void pass2_fetch(const Plan& p, const float* hsrc, int it, unsigned char* buf,
                                             uint64_t* bar) {
@@ -633,13 +646,22 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     const int nB = ob - wa;                          // window slots [wa, ob); [wa, oa) belong to other items
     const int r = nM - p.nexp[k] + kFixF - Fg;       // tile frame -> global frame shift
     const unsigned long long Pk = p.P[k];
-    const bool ok = mbar_wait_bounded(&mbar[0], (uint32_t)n & 1u);
-    if (!ok) s_err = 1;
+    // A staged copy that does not land within the wait's limit ends the CTA's work: the error is
+    // recorded, thread 0 waits once more (bounded) for that copy, and no further copy is issued
+    // into the buffer, so the CTA never reads a partial tile or leaves with its own copy in flight
+    // unless the second wait gives up too.
+    if (__syncthreads_or(!mbar_wait_bounded(&mbar[0], (uint32_t)n & 1u))) {
+      if (tid == 0) {
+        s_err = 1;
+        mbar_wait_bounded(&mbar[0], (uint32_t)n & 1u);
+      }
+      break;
+    }
 
     // clear this window's ancestor marks (the previous item's gather has finished:
     // the loop ends with a barrier; the scan's barriers order this before the marks)
-    const int nB128 = (nB + 127) & ~127;
-    for (int x = tid; x < nB128 / 8; x += kThreads) reinterpret_cast<uint4*>(marks)[x] = make_uint4(0u, 0u, 0u, 0u);
+    const int nBs = (nB + kGatherStep - 1) & ~(kGatherStep - 1);
+    for (int x = tid; x < nBs / 8; x += kThreads) reinterpret_cast<uint4*>(marks)[x] = make_uint4(0u, 0u, 0u, 0u);
 
     // Exact fixed-point prefix of the tile: 16 contiguous weights per thread
     // (summed here, rebuilt element by element below from the staged tile).
@@ -661,14 +683,21 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     unsigned long long tot;
     const unsigned long long excl = block_excl_scan_add<kThreads>(run, &tot, s_scan);
 
-    // Element j owns the targets in [C_{j-1}, C_j), i.e. the output slots
-    // [q_j, q_{j+1}). Its child count comes from one 64-bit difference against
-    // delta, 2 delta and 3 delta (a division only past four children); the
-    // element writes one start mark, at its first slot inside this window.
+    // Element j owns the output slots [q_{j-1}, q_j): the targets t_q below its CDF value
+    // C_j = P_k + (A_j >> r) (A_j its tile-local inclusive prefix) and not below the previous
+    // element's. In the tile's own frame, C_j > t_q  <=>  A_j >= ((t_q - P_k + 1) << r), and
+    // consecutive targets are delta << r apart there, so the count needs neither the shift nor
+    // P_k per element: each thread tracks its next target's threshold relative to its first
+    // element's exclusive prefix (capped, see kThCap). The element writes one start mark, at its
+    // first slot inside this window.
     const int lane = tid & 31, warp = tid >> 5;
-    const unsigned long long d2 = 2ull * delta, d3 = 3ull * delta, d4 = 4ull * delta;
     int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
-    unsigned long long tq = base + (unsigned long long)q * delta;
+    unsigned long long th = kThCap, D = kThCap;
+    if (massive && q < N) {
+      const unsigned long long m = base + (unsigned long long)q * delta - Pk + 1ull;   // t_q >= P_k
+      if (m <= (~0ull >> r)) th = min((m << r) - excl, kThCap);                           // (m << r) > excl
+      if (delta <= (kThCap >> r)) D = delta << r;
+    }
     int32_t* csr = (a.csr && (item.w & 1)) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
     // Compile-time variants: FULL (no element past N in the tile), WHOLE (the
     // item holds every output of the tile, so each counted child lands in the
@@ -678,30 +707,26 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       constexpr bool FULL = decltype(full_tag)::value;
       constexpr bool WHOLE = decltype(whole_tag)::value;
       constexpr bool TAPE = decltype(tape_tag)::value;
-      unsigned long long accw = excl;
-      float4 f4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      const unsigned long long D2 = 2ull * D, D3 = 3ull * D, D4 = 4ull * D;
+      unsigned long long acc = 0ull;
+#pragma unroll 1
+      for (int g = 0; g < 4; ++g) {
+        const float4 f4 = wt[g];
+        const float ff[4] = {f4.x, f4.y, f4.z, f4.w};
 #pragma unroll
-      for (int e = 0; e < kPerThread; ++e) {
-        const int j = tid * kPerThread + e;
-        const bool in = FULL || j < nA;
-        if (TAPE && in) csr[j] = q;
-        if ((e & 3) == 0) f4 = wt[e >> 2];
-        const float we = (e & 3) == 0 ? f4.x : (e & 3) == 1 ? f4.y : (e & 3) == 2 ? f4.z : f4.w;
-        if (in) accw += fix_weight(tile_weight(we));
-        const unsigned long long cj = Pk + (accw >> r);
-        if (in && q < N && cj > tq) {
-          const unsigned long long diff = cj - tq;
-          const int c = 1 + (diff > delta) + (diff > d2) + (diff > d3);
-          if (c == 4 && diff > d4) {
-            const int q1 = targets_below(cj, base, delta, magic, N);
-            if (WHOLE || (q < ob && q1 > oa)) marks[(WHOLE ? q : max(q, oa)) - wa] = (unsigned short)(j + 1);
-            q = q1;
-            tq = base + (unsigned long long)q * delta;
-          } else {
+        for (int e = 0; e < 4; ++e) {
+          const int j = tid * kPerThread + 4 * g + e;
+          const bool in = FULL || j < nA;
+          if (TAPE && in) csr[j] = q;
+          if (in) acc += fix_weight(tile_weight(ff[e]));
+          if (in && acc >= th) {
+            const unsigned long long diff = acc - th;
+            int c = 1 + (diff >= D) + (diff >= D2) + (diff >= D3);
+            if (c == 4 && diff >= D4) c = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
             const int q1 = min(q + c, N);
             if (WHOLE || (q < ob && q1 > oa)) marks[(WHOLE ? q : max(q, oa)) - wa] = (unsigned short)(j + 1);
+            th = (q1 >= N) ? kThCap : th + (unsigned long long)c * D;
             q = q1;
-            tq += (unsigned long long)c * delta;
           }
         }
       }
@@ -725,32 +750,39 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
 
     // Gather: the ancestor of window slot o is the last start mark at or
     // before o (marks increase along the window). Each warp takes a run of
-    // slots in steps of 128 (4 per lane): the running maximum of the marks
+    // slots in steps of 256 (8 per lane): the running maximum of the marks
     // is a lane-local scan, a warp max-scan and a carry from the earlier
-    // steps and warps. A lane's 4 slots are 16-byte aligned in the output,
-    // so whole groups are written with one vector store.
-    const int chunk = ((nB + kThreads / 32 - 1) / (kThreads / 32) + 127) & ~127;
+    // steps and warps. A lane's 8 slots are 16-byte aligned in the output,
+    // so whole groups are written with two vector stores; every slot from
+    // the item's first one on has a mark at or before it, so a group that
+    // lies inside the item needs no per-slot test.
+    const int chunk = ((nB + kThreads / 32 - 1) / (kThreads / 32) + kGatherStep - 1) & ~(kGatherStep - 1);
     const int cs = warp * chunk, ce = min(cs + chunk, nB);
     unsigned wmax = 0u;
-    for (int o0 = cs; o0 < ce; o0 += 128) {
-      const uint2 m = reinterpret_cast<const uint2*>(marks + o0)[lane];
-      wmax = max(wmax, max(max(m.x & 0xffffu, m.x >> 16), max(m.y & 0xffffu, m.y >> 16)));
+    for (int o0 = cs; o0 < ce; o0 += kGatherStep) {
+      const uint4 m = reinterpret_cast<const uint4*>(marks + o0)[lane];
+      const unsigned v = __vmaxu2(__vmaxu2(m.x, m.y), __vmaxu2(m.z, m.w));
+      wmax = max(wmax, max(v & 0xffffu, v >> 16));
     }
     wmax = __reduce_max_sync(0xffffffffu, wmax);
     if (lane == 0) s_wmax[warp] = wmax;
     __syncthreads();
     unsigned carry = 0u;
     for (int w = 0; w < warp; ++w) carry = max(carry, s_wmax[w]);
-    if (ok) {
+    {
       const int olo = oa - wa;                       // first slot of this item in the window
-      for (int o0 = cs; o0 < ce; o0 += 128) {
-        const uint2 m = reinterpret_cast<const uint2*>(marks + o0)[lane];
-        unsigned am[4];
+      for (int o0 = cs; o0 < ce; o0 += kGatherStep) {
+        const uint4 m = reinterpret_cast<const uint4*>(marks + o0)[lane];
+        unsigned am[8];
         am[0] = m.x & 0xffffu;
         am[1] = max(am[0], m.x >> 16);
         am[2] = max(am[1], m.y & 0xffffu);
         am[3] = max(am[2], m.y >> 16);
-        unsigned x = am[3];
+        am[4] = max(am[3], m.z & 0xffffu);
+        am[5] = max(am[4], m.z >> 16);
+        am[6] = max(am[5], m.w & 0xffffu);
+        am[7] = max(am[6], m.w >> 16);
+        unsigned x = am[7];
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
           const unsigned t = __shfl_up_sync(0xffffffffu, x, off);
@@ -758,28 +790,34 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
         }
         unsigned pre = __shfl_up_sync(0xffffffffu, x, 1);
         pre = max(carry, lane == 0 ? 0u : pre);
-        const int o = o0 + 4 * lane;
-        float hv[4];
-        int av[4];
+        const int o = o0 + 8 * lane;
+        if (o >= olo && o + 7 < ce) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          unsigned jj = max(pre, am[u]);
-          const bool mine = o + u >= olo && o + u < ce;
-          if (mine && jj - 1u >= (unsigned)nA) { jj = 1u; s_err = 1; }   // unreachable by construction
-          if (jj == 0u) jj = 1u;                                           // a slot before the item: not written
-          hv[u] = hs[jj - 1u];
-          av[u] = j0 + (int)(jj - 1u);
-        }
-        if (o >= olo && o + 3 < ce && anc_vec) {
-          *reinterpret_cast<float4*>(hdst + wa + o) = make_float4(hv[0], hv[1], hv[2], hv[3]);
-          if (a.anc) *reinterpret_cast<int4*>(a.anc + wa + o) = make_int4(av[0], av[1], av[2], av[3]);
+          for (int hf = 0; hf < 2; ++hf) {
+            float hv[4];
+            int av[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const unsigned jj = max(pre, am[4 * hf + u]);
+              hv[u] = hs[jj - 1u];
+              av[u] = j0 + (int)(jj - 1u);
+            }
+            *reinterpret_cast<float4*>(hdst + wa + o + 4 * hf) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+            if (a.anc) {
+              if (anc_vec) *reinterpret_cast<int4*>(a.anc + wa + o + 4 * hf) = make_int4(av[0], av[1], av[2], av[3]);
+              else for (int u = 0; u < 4; ++u) a.anc[wa + o + 4 * hf + u] = av[u];
+            }
+          }
         } else {
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+          for (int u = 0; u < 8; ++u) {
             if (o + u >= olo && o + u < ce) {
-              hdst[wa + o + u] = hv[u];
-              if (a.anc) a.anc[wa + o + u] = av[u];
+              unsigned jj = max(pre, am[u]);
+              if (jj - 1u >= (unsigned)nA) { jj = 1u; s_err = 1; }   // unreachable by construction
+              hdst[wa + o + u] = hs[jj - 1u];
+              if (a.anc) a.anc[wa + o + u] = j0 + (int)(jj - 1u);
             }
+          }
         }
         carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
       }
@@ -790,9 +828,105 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       pass2_fetch(p, hsrc, rev ? n_items - 1 - nx : nx, smem, &mbar[0]);
     }
   }
+  __syncthreads();
   if (tid == 0 && s_err) {
     p.st->error = BPF_ERR_STATE;
     if (a.mirror) a.mirror->error = BPF_ERR_STATE;
+  }
+  griddep_release();
+}
+
+// ---------------------------------------------------------------------------
+// Silverman jitter after a resampling tick (the reference's legacy option,
+// gpu_bpf/gpu_bpf_ptx_full.cu:708-738 with kernels ptx_assembly/
+// bpf_kernels_full.ptx:846-1060): bandwidth
+//   bw = shrink * sigma_hat * 1.05922 * N^-0.2,  sigma_hat^2 = sum_i (h'_i - hm)^2 / N
+// over the resampled particles h', hm the tick's filtered mean; then
+//   h'_i = clamp(h'_i + bw z_i, mu - 8, mu + 8)
+// with z_i the normal of particle slot i's next PCG32 draw. The reference
+// draws z from the slot's own stream (bpf_gen_noise steps it), so each jitter
+// takes one draw and the next propagation the one after it: here the draw's
+// stream constants are the device state's current ones, and the variance
+// kernel's last CTA advances them once more.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) jitter_var_kernel(Plan p, float shrink) {
+  __shared__ float s_part[kThreads];
+  __shared__ double s_red[kThreads / 32];
+  __shared__ int s_last;
+  griddep_wait();
+  DevState* st = p.st;
+  if (!st->do_resample) { griddep_release(); return; }
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int k = blockIdx.x, tile0 = k * kTile;
+  const float* h = st->cur ? p.h1 : p.h0;           // the resampled particles
+  const float hmf = (float)st->hm;
+  float acc = 0.0f;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i0 = tile0 + 4 * (tid + kThreads * r);
+    const float4 v = *reinterpret_cast<const float4*>(h + i0);
+    const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (i0 + u < p.N) { const float d = e[u] - hmf; acc = fmaf(d, d, acc); }
+  }
+  s_part[tid] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) t += (double)s_part[lane + 32 * w];
+    t = warp_sum_d(t);
+    if (lane == 0) {
+      p.jpart[k] = t;
+      __threadfence();
+      s_last = (atomicAdd(p.jticket, 1u) == (unsigned)(p.G - 1));
+    }
+  }
+  __syncthreads();
+  if (s_last) {
+    // every tile's sum is visible (each was fenced before its ticket); fixed-order FP64 combine
+    __threadfence();
+    double v = 0.0;
+    for (int j = tid; j < p.G; j += kThreads) v += __ldcg(p.jpart + j);
+    v = warp_sum_d(v);
+    if (lane == 0) s_red[warp] = v;
+    __syncthreads();
+    if (tid == 0) {
+      double V = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w) V += s_red[w];
+      const double n = (double)p.N;
+      st->bw = (float)((double)shrink * sqrt(V / n) * 1.05922 * pow(n, -0.2));
+      st->jk1 = st->k1;                              // the jitter takes the next draw
+      st->jk2 = st->k2;
+      st->k1 = st->k1 * kPcgMult;                    // the next propagation the one after it
+      st->k2 = st->k2 * kPcgMult + 1ull;
+      *p.jticket = 0u;
+    }
+  }
+  griddep_release();
+}
+
+__global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu) {
+  griddep_wait();
+  const DevState* st = p.st;
+  if (!st->do_resample) { griddep_release(); return; }
+  const int tid = threadIdx.x;
+  const int tile0 = blockIdx.x * kTile;
+  float* h = st->cur ? p.h1 : p.h0;
+  const float bw = st->bw, lo = mu - 8.0f, hi = mu + 8.0f;
+  const uint64_t k1 = st->jk1, k2 = st->jk2;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i0 = tile0 + 4 * (tid + kThreads * r);
+    float4 v = *reinterpret_cast<const float4*>(h + i0);
+    float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const float z = icdf_normal_warp(pcg_uniform(pcg_output(k1 + k2 * pcg_inc((uint32_t)(i0 + u)))));
+      if (i0 + u < p.N) e[u] = fminf(fmaxf(fmaf(bw, z, e[u]), lo), hi);
+    }
+    *reinterpret_cast<float4*>(h + i0) = make_float4(e[0], e[1], e[2], e[3]);
   }
   griddep_release();
 }
@@ -852,8 +986,11 @@ cudaError_t plan_alloc(Plan& p, int N) {
   al(&p.P, p.G * sizeof(unsigned long long));
   al(&p.ofirst, (p.G + 1) * sizeof(int));
   al(&p.items, p.max_items * sizeof(int4));
+  al(&p.jpart, p.G * sizeof(double));
+  al(&p.jticket, sizeof(unsigned));
   al(&p.st, sizeof(DevState));
   if (e == cudaSuccess) e = cudaMemset(p.nexp, 0, p.G * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(p.jticket, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaDeviceSynchronize();   // visible to every stream before first use
   return e;
 }
@@ -862,6 +999,7 @@ void plan_free(Plan& p) {
   cudaFree(p.h0); cudaFree(p.h1); cudaFree(p.w);
   cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.rec); cudaFree(p.rec2);
   cudaFree(p.P); cudaFree(p.ofirst); cudaFree(p.items); cudaFree(p.st);
+  cudaFree(p.jpart); cudaFree(p.jticket);
   p = Plan{};
 }
 
@@ -921,6 +1059,13 @@ cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool p
 }
 cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s, bool pdl) {
   return launch_ex(pass2_kernel, dim3(grid), dim3(kThreads), kPass2Smem, s, pdl, p, a);
+}
+
+cudaError_t launch_jitter(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
+  if (!p.jpart || !p.jticket) return cudaErrorInvalidValue;
+  cudaError_t e = launch_ex(jitter_var_kernel, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a.silverman);
+  if (e == cudaSuccess) e = launch_ex(jitter_apply_kernel, dim3(p.G), dim3(kThreads), 0, s, pdl, p, a.mu);
+  return e;
 }
 
 cudaError_t launch_tile_weights(const Plan& p, float* w_out, cudaStream_t s) {

@@ -46,8 +46,12 @@ struct DevState {
   int      seed;            // filter seed (PCG32 streams, resampling uniform)
   double   learn[4];        // online learning sums since the last update: sum_t of
                             // sum W dlw, sum W dlw^2, sum W dlw (h_prev-mu), sum W dlw^2 (h_prev-mu)^2
+  double   hm;              // filtered mean of the current tick (FP64): the centre of Silverman jitter
+  uint64_t jk1, jk2;        // PCG32 stream constants of the current tick's jitter draw
+  float    bw;              // Silverman jitter bandwidth of the current tick
+  int      pad_;
 };
-static_assert(sizeof(DevState) == 168, "DevState layout");
+static_assert(sizeof(DevState) == 200, "DevState layout");
 
 struct Plan {
   int N, G, max_items;
@@ -55,6 +59,8 @@ struct Plan {
   int* nexp; unsigned long long* E; float4* rec;
   float4* rec2;              // per tile, online learning only: tile-frame sums of w dlw, w dlw^2, w dlw dh, w dlw^2 dh^2
   unsigned long long* P; int* ofirst; int4* items;
+  double* jpart;             // per tile, Silverman jitter only: sum of (h - hm)^2 over the tile's particles
+  unsigned* jticket;         // CTAs of the jitter-variance kernel done this tick (the last one resets it)
   DevState* st;
 };
 
@@ -86,6 +92,7 @@ struct TickArgs {
   int32_t* csr;              // on resampling ticks: first child slot of every parent (N ints) or null
   float2* aux;               // {1/S, nM}: normalised weight W_i = 2^(x_i - nM) / S of this tick, or null
   TickMirror* mirror;        // host-mapped mirror of this tick's outcome, or null
+  float silverman;           // Silverman jitter shrink after resampling (0 = off; needs p.jpart)
 };
 
 // Device buffers of a plan for N particles (G, max_items set; DevState included).
@@ -99,6 +106,10 @@ cudaError_t launch_init(const Plan& p, float mu, float std_stat, int seed, cudaS
 cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
 cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
 cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s, bool pdl);
+// Silverman jitter of a resampling tick (both kernels exit at once on other ticks): the bandwidth
+// from the resampled particles' spread about the tick's filtered mean, then h += bw z clamped to
+// [mu - 8, mu + 8], z from the particle slot's next PCG32 draw.
+cudaError_t launch_jitter(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
 int pass2_grid_size(int device);
 size_t pass2_smem_bytes();
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s);

@@ -29,7 +29,7 @@ extern "C" {
 #define BPF_ERR_ARG          1  /* invalid argument (N<=0, |rho|>=1, sigma<=0, non-finite y, NULL) */
 #define BPF_ERR_CUDA         2  /* a CUDA runtime call failed                                       */
 #define BPF_ERR_ALLOC        3  /* device or pinned allocation failed                               */
-#define BPF_ERR_UNSUPPORTED  4  /* option outside this build (bands, Silverman jitter)               */
+#define BPF_ERR_UNSUPPORTED  4  /* option outside this build (multi-band proposals)                   */
 #define BPF_ERR_STATE        5  /* call not valid in the filter's current state                     */
 #define BPF_ERR_DEGENERATE   6  /* every particle weight underflowed on a tick                      */
 #define BPF_ERR_NODEVICE     7  /* no CUDA device / kernel image for this GPU                       */
@@ -58,7 +58,13 @@ typedef struct {
  * buffers live behind `impl`.
  *   rho, sigma_z, mu   may be changed between ticks (read at every step)
  *   ess_threshold      0 = always resample, else resample iff ESS/N < it
- *   silverman_shrink   must stay 0 (jitter is not part of this build)
+ *   silverman_shrink   > 0: Silverman jitter after every resampling, as the
+ *                      reference's PTX edition (gpu_bpf_ptx_full.cu:708-738):
+ *                      h += bw z clamped to [mu-8, mu+8], bw = shrink * 1.05922
+ *                      * N^-0.2 * std of the resampled particles about the
+ *                      tick's filtered mean, z from each slot's next PCG32
+ *                      draw (so the next propagation takes the draw after
+ *                      it, as in the reference); 0 (default) = off
  *   did_resample, resample_count, timestep, last_h_est: refreshed whenever a
  *                      result is read back (gpu_bpf_step / get_result)
  */
@@ -232,7 +238,12 @@ int gpu_bpf_profile_read(GpuBpfState* state, double* pass1_ms, double* plan_ms, 
  * re-initialises the whole state, and all calls share the one scratch area:
  * calls whose GPU work overlaps (other streams or host threads) race and
  * corrupt each other, so serialise them. Enqueued on `stream` (a
- * cudaStream_t, NULL = the legacy default stream); does not synchronise. */
+ * cudaStream_t, NULL = the legacy default stream); does not synchronise.
+ * The return value covers the arguments and the launches only: the run's
+ * device-side outcome is in the records (a tick whose every weight underflowed
+ * has dloglik = -inf and h_mean = NaN), and a resampling copy that failed to
+ * complete on the device, which gpu_bpf_step reports as BPF_ERR_STATE, is not
+ * reported by this entry point. */
 #define BPF_STATIC_MAX_PARTICLES 262144
 int gpu_bpf_run_static(int n_particles, float rho, float sigma_z, float mu, float nu_obs, int seed,
                        float ess_threshold, const float* y_dev, int n_ticks, BpfTickRecord* rec_dev,

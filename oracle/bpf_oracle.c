@@ -13,6 +13,9 @@
  *   orc_acklam_f64       Acklam inverse normal CDF in FP64 (PTX :166-205 in FP32)
  *   orc_icdf_f64         the same plus Acklam's published Halley refinement step
  *                        (erfc-based): the FP64 oracle's inverse normal CDF
+ *   orc_f64_*            the same filter stepped one tick at a time (lock-step checks
+ *                        of runs of any length), with the reference's Silverman
+ *                        jitter after resampling (gpu_bpf_ptx_full.cu:708-738)
  *   orc_filter_f64       FP64 filter in this build's semantics, optionally
  *                        replaying resampling decisions and ancestors
  *   orc_filter_noise_f64 FP64 filter driven by given auxiliary noise, sorting the
@@ -207,6 +210,7 @@ typedef struct {
     int seed;
     float ess_threshold;
     float nu_state;        /* Student-t state noise, 0 = Gaussian */
+    float silverman;       /* Silverman jitter shrink after resampling, 0 = off (orc_f64_* only) */
 } OrcConfig;
 
 /*
@@ -252,6 +256,7 @@ static int ceil_log2_u(unsigned n) { int c = 0; while ((1ull << c) < (unsigned l
 typedef struct {
     OrcConfig c;
     int N, nu_int, t, prev_res;
+    int draw;              /* index of the next draw of every slot's PCG32 stream */
     double mu, rho, sig, nu, cobs, lse_prev, llr;
     uint64_t ustate;
     double *h, *hn, *lw, *lwc, *cdf;
@@ -294,6 +299,7 @@ OrcF64* orc_f64_create(const OrcConfig* c) {
     s->lse_prev = log((double)N);
     s->llr = 0.0;
     s->t = 0;
+    s->draw = 1;           /* draw 0 is the initial particle */
     return s;
 }
 
@@ -314,15 +320,16 @@ int orc_f64_tick(OrcF64* s, float y, const int32_t* anc, int flag, double* out5)
     const int seed = s->c.seed, nu_int = s->nu_int, prev_res = s->prev_res;
     const double nu_state = (double)s->c.nu_state;
     if (t > 0) {
+        const int draw = s->draw++;
         uint64_t At, Bt;
-        orc_pcg32_jump((uint64_t)t, &At, &Bt);
+        orc_pcg32_jump((uint64_t)draw, &At, &Bt);
 #pragma omp parallel for schedule(static)
         for (int i = 0; i < N; ++i) {
             uint64_t s0, inc;
             orc_pcg32_init(seed, (uint32_t)i, &s0, &inc);
             float u = orc_uniform(orc_pcg32_output(At * s0 + Bt * inc));
             double eps = orc_icdf_f64((double)u);
-            if (nu_int > 0) eps *= orc_tstate_scale(seed, (uint32_t)i, t, nu_int, nu_state);
+            if (nu_int > 0) eps *= orc_tstate_scale(seed, (uint32_t)i, draw, nu_int, nu_state);
             h[i] = mu + rho * (h[i] - mu) + sig * eps;
         }
     }
@@ -365,6 +372,25 @@ int orc_f64_tick(OrcF64* s, float y, const int32_t* anc, int flag, double* out5)
         }
         s->hn = h; s->h = hn;
         s->prev_res = 1;
+        if (s->c.silverman > 0.0f) {
+            /* Silverman jitter (gpu_bpf_ptx_full.cu:708-738, PTX :846-1060): bandwidth from the
+             * resampled particles' spread about this tick's filtered mean, noise from every slot's
+             * next PCG32 draw, clamp to [mu - 8, mu + 8] */
+            const double hm = H / S;
+            double V = 0.0;
+            for (int i = 0; i < N; ++i) V += (hn[i] - hm) * (hn[i] - hm);
+            const double bw = (double)s->c.silverman * sqrt(V / (double)N) * 1.05922 * pow((double)N, -0.2);
+            const int draw = s->draw++;
+            uint64_t At, Bt;
+            orc_pcg32_jump((uint64_t)draw, &At, &Bt);
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < N; ++i) {
+                uint64_t s0, inc;
+                orc_pcg32_init(seed, (uint32_t)i, &s0, &inc);
+                const double z = orc_icdf_f64((double)orc_uniform(orc_pcg32_output(At * s0 + Bt * inc)));
+                hn[i] = fmin(fmax(hn[i] + bw * z, mu - 8.0), mu + 8.0);
+            }
+        }
     } else {
         double* tmp = s->lwc; s->lwc = s->lw; s->lw = tmp;   /* the carried log-weights */
         s->lse_prev = lse;

@@ -42,6 +42,7 @@ class OrcConfig(C.Structure):
         ("seed", C.c_int),
         ("ess_threshold", C.c_float),
         ("nu_state", C.c_float),
+        ("silverman", C.c_float),
     ]
 
 
@@ -148,10 +149,11 @@ class F64Filter:
     """The FP64 oracle filter stepped one tick at a time (orc_f64_*): follows a device run of any
     length in lock step, replaying each resampling tick's ancestors as it comes."""
 
-    def __init__(self, n_particles, rho, sigma_z, mu, seed=42, ess_threshold=0.0, nu_obs=0.0, nu_state=0.0):
+    def __init__(self, n_particles, rho, sigma_z, mu, seed=42, ess_threshold=0.0, nu_obs=0.0, nu_state=0.0,
+                 silverman=0.0):
         self._L = lib()
         self.N = int(n_particles)
-        self._cfg = OrcConfig(self.N, rho, sigma_z, mu, nu_obs, int(seed), ess_threshold, nu_state)
+        self._cfg = OrcConfig(self.N, rho, sigma_z, mu, nu_obs, int(seed), ess_threshold, nu_state, silverman)
         self._s = self._L.orc_f64_create(C.byref(self._cfg))
         if not self._s:
             raise MemoryError("orc_f64_create failed")

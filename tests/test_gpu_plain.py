@@ -242,10 +242,10 @@ def test_errors_are_reported(bpf):
     with pytest.raises(bpf.BpfError) as e:
         f.step(float("nan"))
     assert e.value.code == _lib.BPF_ERR_ARG
-    f.state.silverman_shrink = 0.5
+    f.state.silverman_shrink = float("nan")
     with pytest.raises(bpf.BpfError) as e:
         f.step(0.1)
-    assert e.value.code == _lib.BPF_ERR_UNSUPPORTED
+    assert e.value.code == _lib.BPF_ERR_ARG
     f.state.silverman_shrink = 0.0
     f.step(0.1)
     f.set_rho(1.5)
