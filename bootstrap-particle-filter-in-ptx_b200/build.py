@@ -42,12 +42,33 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+OBJ_DIR = os.path.join(HERE, "_build")
+
+
 def build_library(force: bool = False, verbose: bool = False) -> str:
-    """Compile libgpubpf.so if any source is newer than it; return its path."""
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "gpu_bpf.h")]
+    """Compile libgpubpf.so if any source is newer than it; return its path. The sources are
+    compiled to objects in parallel (one nvcc per source) and linked into the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
+    headers = [os.path.join(CSRC, f) for f in HEADERS] + [os.path.join(INCLUDE, "gpu_bpf.h")]
+    deps = [os.path.join(CSRC, f) for f in SOURCES] + headers
     if not force and not _stale(OUT, deps):
         return OUT
-    cmd = [_nvcc(), *NVCC_FLAGS, *[os.path.join(CSRC, f) for f in SOURCES], "-o", OUT + ".tmp"]
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src: str) -> str:
+        obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+        if force or _stale(obj, [os.path.join(CSRC, src)] + headers):
+            cmd = [_nvcc(), *compile_flags, "-c", os.path.join(CSRC, src), "-o", obj + ".tmp"]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+            os.replace(obj + ".tmp", obj)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", OUT + ".tmp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

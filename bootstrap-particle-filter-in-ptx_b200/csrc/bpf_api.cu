@@ -82,7 +82,8 @@ struct Impl {
   cudaKernelNodeParams t_params{};
   Plan t_plan{};
   TickArgs t_args{};
-  void* t_argv[2] = {nullptr, nullptr};
+  int t_n = 1;                          // the fused kernel's tick count
+  void* t_argv[3] = {nullptr, nullptr, nullptr};
   float t_mu = NAN, t_rho = NAN, t_sigma = NAN, t_thr = NAN, t_nus = NAN, t_silv = NAN;
   bool t_anc = false;
 
@@ -96,6 +97,10 @@ struct Impl {
 
   // programmatic dependent launch between consecutive kernels (off while profiling)
   bool pdl = true;
+
+  // filters of at most kSmallMaxN particles run each tick (or each captured run of ticks) as one
+  // fused launch (gpu_bpf_set_fused_small)
+  bool fused_small = true;
 
   // profiling
   bool profiling = false;
@@ -120,10 +125,22 @@ int ensure_device(Impl* m) {
   return BPF_OK;
 }
 
-// Kernels one tick launches: pass 1, plan, pass 2, and the two Silverman jitter kernels when on.
-int tick_launches(const TickArgs& a) { return a.silverman > 0.0f ? 5 : 3; }
+// A tick runs as the fused small-filter kernel when the filter is small enough and the tick
+// needs nothing that only the three-kernel path provides (learning, Silverman jitter, per-kernel
+// profiling); the two give bit-identical results.
+bool use_small(const Impl* m, const TickArgs& a) {
+  return m->fused_small && !m->profiling && small_eligible(m->plan, a);
+}
+
+// Kernels one tick launches: the fused kernel alone, or pass 1, plan, pass 2 and the two
+// Silverman jitter kernels when on.
+int tick_launches(const Impl* m, const TickArgs& a) {
+  if (use_small(m, a)) return 1;
+  return a.silverman > 0.0f ? 5 : 3;
+}
 
 cudaError_t launch_tick3(Impl* m, const TickArgs& a) {
+  if (use_small(m, a)) return launch_small(m->plan, a, 1, m->stream, m->pdl);
   cudaError_t e = launch_pass1(m->plan, a, m->stream, m->pdl);
   if (e == cudaSuccess) e = launch_plan(m->plan, a, m->stream, m->pdl);
   if (e == cudaSuccess) e = launch_pass2(m->plan, a, m->pass2_grid, m->stream, m->pdl);
@@ -228,7 +245,7 @@ int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
   } else {
     CK(launch_tick3(m, a));
   }
-  g_launches += tick_launches(a);
+  g_launches += tick_launches(m, a);
   const int tick = m->ticks_enqueued;
   m->ticks_enqueued += 1;
   if (m->learn_mode && tick > 0 && ++m->grad_count >= m->update_K) return learning_update(s, m);
@@ -288,9 +305,14 @@ int build_graph(GpuBpfState* s, Impl* m) {
   cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t err = cudaMemcpyAsync(m->y_dev, m->y_pin, kGraphChunk * sizeof(float), cudaMemcpyHostToDevice, m->stream);
-  for (int k = 0; k < kGraphChunk && err == cudaSuccess; ++k) {
-    TickArgs a = make_args(s, m, 0.0f, m->y_dev + k, m->rec_dev + 1 + k);
-    err = launch_tick3(m, a);
+  const TickArgs a0 = make_args(s, m, 0.0f, m->y_dev, m->rec_dev + 1);
+  if (err == cudaSuccess && use_small(m, a0)) {
+    err = launch_small(m->plan, a0, kGraphChunk, m->stream, m->pdl);     // the chunk as one launch
+  } else {
+    for (int k = 0; k < kGraphChunk && err == cudaSuccess; ++k) {
+      TickArgs a = make_args(s, m, 0.0f, m->y_dev + k, m->rec_dev + 1 + k);
+      err = launch_tick3(m, a);
+    }
   }
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(m->rec_pin + 1, m->rec_dev + 1, kGraphChunk * sizeof(BpfTickRecord), cudaMemcpyDeviceToHost, m->stream);
@@ -312,9 +334,14 @@ int build_device_graph(GpuBpfState* s, Impl* m, const float* y_dev, int n, BpfTi
   cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t err = cudaSuccess;
-  for (int k = 0; k < n && err == cudaSuccess; ++k) {
-    TickArgs a = make_args(s, m, 0.0f, y_dev + k, rec_dev + k);
-    err = launch_tick3(m, a);
+  const TickArgs a0 = make_args(s, m, 0.0f, y_dev, rec_dev);
+  if (use_small(m, a0)) {
+    err = launch_small(m->plan, a0, n, m->stream, m->pdl);              // the whole run as one launch
+  } else {
+    for (int k = 0; k < n && err == cudaSuccess; ++k) {
+      TickArgs a = make_args(s, m, 0.0f, y_dev + k, rec_dev + k);
+      err = launch_tick3(m, a);
+    }
   }
   cudaError_t e2 = cudaStreamEndCapture(m->stream, &g);
   if (err != cudaSuccess || e2 != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return set_err(BPF_ERR_CUDA); }
@@ -363,10 +390,12 @@ int build_tick_graph(GpuBpfState* s, Impl* m) {
   m->t_g = g;
   m->tgraph = ex;
   m->t_pass1 = root;
-  m->t_plan = m->plan;                     // pass 1's arguments, as launch_pass1 passed them
+  m->t_plan = m->plan;                     // the root kernel's arguments, as its launcher passed them
+  m->t_n = 1;
   m->t_args = a;
   m->t_argv[0] = &m->t_plan;
   m->t_argv[1] = &m->t_args;
+  m->t_argv[2] = &m->t_n;                  // read only by the fused kernel (three parameters)
   m->t_params.kernelParams = m->t_argv;
   m->t_params.extra = nullptr;
   m->t_mu = s->mu; m->t_rho = s->rho; m->t_sigma = s->sigma_z; m->t_thr = s->ess_threshold; m->t_nus = s->nu_state;
@@ -501,7 +530,7 @@ static int step_async_rc(GpuBpfState* s, float y_t, bool one_shot) {
     m->t_args.obs.y = y_t;
     CK(cudaGraphExecKernelNodeSetParams(m->tgraph, m->t_pass1, &m->t_params));
     CK(cudaGraphLaunch(m->tgraph, m->stream));
-    g_launches += tick_launches(m->t_args);
+    g_launches += tick_launches(m, m->t_args);
     m->ticks_enqueued += 1;
     m->last_in_map = true;
     return BPF_OK;
@@ -652,7 +681,8 @@ int gpu_bpf_step_many(GpuBpfState* s, const float* y, int n_ticks, BpfResult* ou
       std::memcpy(m->y_pin, y + t, kGraphChunk * sizeof(float));
       CK(cudaGraphLaunch(m->graph, m->stream));
       CK(cudaStreamSynchronize(m->stream));
-      g_launches += (long long)tick_launches(make_args(s, m, 0.0f, nullptr, nullptr)) * kGraphChunk;
+      g_launches += use_small(m, make_args(s, m, 0.0f, nullptr, nullptr))
+                        ? 1 : (long long)tick_launches(m, make_args(s, m, 0.0f, nullptr, nullptr)) * kGraphChunk;
       m->ticks_enqueued += kGraphChunk;
       for (int k = 0; k < kGraphChunk; ++k) {
         if (out) out[t + k] = to_result(m, m->rec_pin[1 + k]);
@@ -708,7 +738,8 @@ int gpu_bpf_step_many_device(GpuBpfState* s, const float* y_dev, int n_ticks, Bp
                        m->dg_silv != s->silverman_shrink || m->dg_anc != m->record_anc;
     if (stale) { rc = build_device_graph(s, m, y_dev, n_ticks, rec_dev); if (rc) return rc; }
     CK(cudaGraphLaunch(m->dgraph, m->stream));
-    g_launches += (long long)tick_launches(make_args(s, m, 0.0f, nullptr, nullptr)) * n_ticks;
+    g_launches += use_small(m, make_args(s, m, 0.0f, nullptr, nullptr))
+                      ? 1 : (long long)tick_launches(m, make_args(s, m, 0.0f, nullptr, nullptr)) * n_ticks;
     m->ticks_enqueued += n_ticks;
   } else {
     for (int t = 0; t < n_ticks; ++t) {
@@ -830,6 +861,23 @@ int gpu_bpf_get_resample_inputs(GpuBpfState* s, float* w_out, int32_t* tile_exp_
   }
   if (tile_exp_out) CK(cudaMemcpy(tile_exp_out, m->plan.nexp, (size_t)m->plan.G * sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (u23_out) *u23_out = m->st_pin->u23;
+  return BPF_OK;
+}
+
+int gpu_bpf_set_fused_small(GpuBpfState* s, int enable) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  const bool on = enable != 0;
+  if (on != m->fused_small) {              // captured graphs hold the other path's launches
+    int rc = ensure_device(m);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(m->stream));
+    if (m->graph) { cudaGraphExecDestroy(m->graph); m->graph = nullptr; }
+    if (m->dgraph) { cudaGraphExecDestroy(m->dgraph); m->dgraph = nullptr; }
+    if (m->tgraph) { cudaGraphExecDestroy(m->tgraph); m->tgraph = nullptr; }
+    if (m->t_g) { cudaGraphDestroy(m->t_g); m->t_g = nullptr; }
+    m->fused_small = on;
+  }
   return BPF_OK;
 }
 

@@ -94,6 +94,14 @@ __device__ __forceinline__ unsigned long long warp_sum_u64_w(unsigned long long 
   for (int o = WIDTH / 2; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Barrier of a block-level helper run by NT threads: the whole CTA, or, for NT = 32, the one
+// warp that runs it while the rest of the CTA does something else.
+template <int NT>
+__device__ __forceinline__ void nt_sync() {
+  if constexpr (NT == 32) __syncwarp();
+  else __syncthreads();
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan_add(T v, int lane) {
 #pragma unroll
@@ -111,7 +119,7 @@ __device__ T block_excl_scan_add(T v, T* total, T* sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T inc = warp_incl_scan_add(v, lane);
   if (lane == 31) sh[warp] = inc;
-  __syncthreads();
+  nt_sync<NT>();
   if (warp == 0) {
     const T t = lane < W ? sh[lane] : T(0);
     const T ti = warp_incl_scan_add(t, lane);
@@ -119,10 +127,10 @@ __device__ T block_excl_scan_add(T v, T* total, T* sh) {
     if (lane < W) sh[lane] = ti - t;
     if (lane == W - 1) sh[W] = ti;
   }
-  __syncthreads();
+  nt_sync<NT>();
   const T r = sh[warp] + inc - v;
   *total = sh[W];
-  __syncthreads();
+  nt_sync<NT>();
   return r;
 }
 template <int NT>
@@ -130,11 +138,11 @@ __device__ int block_max_i(int v, int* sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   v = warp_max_i(v);
   if (lane == 0) sh[warp] = v;
-  __syncthreads();
+  nt_sync<NT>();
   int m = sh[0];
 #pragma unroll
   for (int w = 1; w < NT / 32; ++w) m = max(m, sh[w]);
-  __syncthreads();
+  nt_sync<NT>();
   return m;
 }
 

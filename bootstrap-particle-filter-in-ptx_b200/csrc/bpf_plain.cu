@@ -76,6 +76,22 @@ constexpr int kStWords = (int)(sizeof(DevState) / 8);
 // ---------------------------------------------------------------------------
 // Pass 1
 // ---------------------------------------------------------------------------
+// Shared memory of one tile's pass 1 (one group of kThreads threads).
+struct Pass1Shared {
+  float s_max[kThreads / 32];
+  float s_part[3][kThreads];
+  unsigned long long s_E[kThreads];
+  double s_red[3][kThreads / 32];          // online-learning sums
+  unsigned long long s_redE[kThreads / 32];
+  double s_red4[kThreads / 32];
+};
+
+// Barrier of one group of kThreads threads: barrier 0 is the whole CTA of the
+// pass-1 kernel; the fused small-filter kernel gives each tile's group its own.
+__device__ __forceinline__ void group_sync(int bar) {
+  asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(kThreads) : "memory");
+}
+
 // APF = 0: bootstrap tick; 1 / 2: the two stages of an auxiliary-particle-filter
 // tick (gpu_bpf_ptx_full.cu:990-1047): stage 1 weights each particle by
 // p(y | m), m = mu + rho (h - mu), and leaves the particles in place; stage 2
@@ -84,21 +100,17 @@ constexpr int kStWords = (int)(sizeof(DevState) / 8);
 // by p(y | h) / p(y | m).
 // GAUSS: the observation model is Gaussian (a.obs.nu == 0), fixed at compile
 // time so the per-particle code carries no model branch.
+// Pass 1 of tile k by one group of kThreads threads (tid = 0..kThreads-1 inside
+// the group, `bar` its barrier), reading the tick's state from st.
 template <bool TSTATE, bool LEARN, int APF, bool GAUSS>
-__global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
-  __shared__ float s_max[kThreads / 32];
-  __shared__ float s_part[3][kThreads];
-  __shared__ unsigned long long s_E[kThreads];
-  __shared__ double s_red[3][kThreads / 32];          // online-learning sums
-  __shared__ unsigned long long s_redE[kThreads / 32];
-
-  griddep_wait();
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const DevState* st = p.st;
-  // Each pass walks the tiles in the order opposite to the previous pass over
-  // the particle arrays, so it starts on the tiles that pass wrote last, still
-  // in L2 (the arrays are rewritten in place every tick).
-  const int k = (st->dirs & 1) ? (p.G - 1 - (int)blockIdx.x) : (int)blockIdx.x;
+__device__ __forceinline__ void pass1_tile(const Plan& p, const TickArgs& a, const DevState* st, int k, int tid,
+                                           int bar, Pass1Shared& sh) {
+  float* s_max = sh.s_max;
+  float (*s_part)[kThreads] = sh.s_part;
+  unsigned long long* s_E = sh.s_E;
+  double (*s_red)[kThreads / 32] = sh.s_red;
+  unsigned long long* s_redE = sh.s_redE;
+  const int lane = tid & 31, warp = tid >> 5;
   const int tick = st->tick;
   const bool carry = APF == 0 && st->resampled_prev == 0;
   const int nM_prev = st->nM_prev;
@@ -203,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   for (int e = 1; e < kPerThread; ++e) mx = fmaxf(mx, x[e]);
   mx = warp_max_f(mx);
   if (lane == 0) s_max[warp] = mx;
-  __syncthreads();
+  group_sync(bar);
   mx = s_max[0];
 #pragma unroll
   for (int w = 1; w < kThreads / 32; ++w) mx = fmaxf(mx, s_max[w]);
@@ -246,7 +258,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   // tile partials: the per-thread FP32 sums are staged in shared memory and one
   // warp adds them in FP64 (and the exact masses in u64), in a fixed order
   s_part[0][tid] = fS; s_part[1][tid] = fQ; s_part[2][tid] = fH; s_E[tid] = E;
-  __syncthreads();
+  group_sync(bar);
   if (warp == 0) {
     double tS = 0.0, tQ = 0.0, tH = 0.0;
     unsigned long long tE = 0ull;
@@ -266,13 +278,13 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
     }
   }
   if (LEARN) {
-    __syncthreads();                                 // s_red is reused
+    group_sync(bar);                                 // s_red is reused
     const double g0 = warp_sum_d((double)lG0), f0 = warp_sum_d((double)lF0);
     const double g1 = warp_sum_d((double)lG1), f1 = warp_sum_d((double)lF1);
     if (lane == 0) { s_red[0][warp] = g0; s_red[1][warp] = f0; s_red[2][warp] = g1; s_redE[warp] = 0ull; }
-    __shared__ double s_red4[kThreads / 32];
+    double* s_red4 = sh.s_red4;
     if (lane == 0) s_red4[warp] = f1;
-    __syncthreads();
+    group_sync(bar);
     if (tid == 0) {
       double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
 #pragma unroll
@@ -280,6 +292,18 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
       p.rec2[k] = make_float4((float)t0, (float)t1, (float)t2, (float)t3);
     }
   }
+}
+
+template <bool TSTATE, bool LEARN, int APF, bool GAUSS>
+__global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
+  __shared__ Pass1Shared sh;
+  griddep_wait();
+  const DevState* st = p.st;
+  // Each pass walks the tiles in the order opposite to the previous pass over
+  // the particle arrays, so it starts on the tiles that pass wrote last, still
+  // in L2 (the arrays are rewritten in place every tick).
+  const int k = (st->dirs & 1) ? (p.G - 1 - (int)blockIdx.x) : (int)blockIdx.x;
+  pass1_tile<TSTATE, LEARN, APF, GAUSS>(p, a, st, k, (int)threadIdx.x, 0, sh);
   griddep_release();
 }
 
@@ -289,36 +313,34 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
 // the tile exponents and fixed-point masses in shared memory with coalesced
 // loads and builds the prefix, the target spacing and the work list there.
 // ---------------------------------------------------------------------------
+template <int NT>
 struct PlanShared {
-  int red_i[kPlanThreads / 32];
-  double red[3][kPlanThreads / 32];
-  double learn3[kPlanThreads / 32];
+  int red_i[NT / 32];
+  double red[3][NT / 32];
+  double learn3[NT / 32];
   double tot[3];
   double res[4];
-  unsigned long long scan_u[kPlanThreads / 32 + 1];
-  int scan_i[kPlanThreads / 32 + 1];
+  unsigned long long scan_u[NT / 32 + 1];
+  int scan_i[NT / 32 + 1];
   unsigned long long b_base, b_delta, b_magic;
   int b_resample, b_Fg;
 };
 
-size_t plan_smem_bytes(int G) {
+__host__ __device__ constexpr size_t plan_smem_bytes(int G) {
   return G <= kPlanSmemTiles ? (size_t)G * 8 + (size_t)(2 * G + 1) * 4 : 0;
 }
 
-__global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs a) {
-  __shared__ PlanShared sh;
-  __shared__ __align__(16) DevState s_st;
-  extern __shared__ __align__(16) unsigned char plan_smem[];
-  griddep_wait();
+// The plan of one tick by a CTA of NT threads on the device state s_st held in
+// shared memory (the body's first barrier comes before its first read of s_st);
+// it ends by writing s_st back to p.st. ITEMS: also write pass 2's work items.
+template <int NT, bool ITEMS>
+__device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevState& s_st, PlanShared<NT>& sh,
+                                          unsigned char* plan_smem) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = p.G, N = p.N;
-  // the device state lives in shared memory for the whole kernel (one load, one store)
-  if (tid < kStWords)
-    reinterpret_cast<unsigned long long*>(&s_st)[tid] =
-        __ldcg(reinterpret_cast<const unsigned long long*>(p.st) + tid);
   DevState* st = &s_st;
   auto store_state = [&]() {
-    __syncthreads();
+    nt_sync<NT>();
     if (tid < kStWords)
       reinterpret_cast<unsigned long long*>(p.st)[tid] = reinterpret_cast<const unsigned long long*>(&s_st)[tid];
     if (tid == 0 && a.mirror) {
@@ -332,11 +354,11 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   //    flight per thread), per thread in a running frame 2^nrun
   int nrun = kNkEmpty;
   double S = 0.0, Q = 0.0, H = 0.0;
-  for (int k0 = 0; k0 < G; k0 += 8 * kPlanThreads) {
+  for (int k0 = 0; k0 < G; k0 += 8 * NT) {
     float4 r8[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const int k = k0 + u * kPlanThreads + tid;
+      const int k = k0 + u * NT + tid;
       r8[u] = (k < G) ? __ldcg(p.rec + k) : make_float4(0.f, 0.f, 0.f, __int_as_float(kNkEmpty));
     }
 #pragma unroll
@@ -353,7 +375,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     }
   }
   // 2. global frame 2^nM, FP64 block sums
-  const int nM = block_max_i<kPlanThreads>(nrun, sh.red_i);   // barrier: s_st loaded
+  const int nM = block_max_i<NT>(nrun, sh.red_i);   // barrier: s_st loaded
   if (nrun != kNkEmpty) {
     const double sc = pow2d(nrun - nM);
     S *= sc; Q *= sc * sc; H *= sc;
@@ -362,29 +384,32 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   }
   S = warp_sum_d(S); Q = warp_sum_d(Q); H = warp_sum_d(H);
   if (lane == 0) { sh.red[0][warp] = S; sh.red[1][warp] = Q; sh.red[2][warp] = H; }
-  __syncthreads();
+  nt_sync<NT>();
 
   // 3. tick statistics: the three FP64 transcendental/division chains run on
   //    different warps, then thread 0 takes the decision
-  if (lane == 0 && warp < 3) {
+  // one thread per chain: lane 0 of warps 0..3 (lanes 0..3 of the single warp when NT = 32)
+  const int slot = (NT >= 128) ? warp : lane;
+  const bool slot_lead = (NT >= 128) ? (lane == 0) : true;
+  if (slot_lead && slot < 3) {
     double v = 0.0;
-    for (int w = 0; w < kPlanThreads / 32; ++w) v += sh.red[warp][w];
-    sh.tot[warp] = v;
+    for (int w = 0; w < NT / 32; ++w) v += sh.red[slot][w];
+    sh.tot[slot] = v;
   }
-  __syncthreads();
+  nt_sync<NT>();
   const double tS = sh.tot[0], tQ = sh.tot[1], tH = sh.tot[2];
   const bool degenerate = (nM == kNkEmpty) || !(tS > 0.0);
-  if (lane == 0 && !degenerate) {
-    if (warp == 0) sh.res[0] = (double)nM * 0.693147180559945309417232121458 + log(tS);   // log-sum in the carry frame
-    if (warp == 1) sh.res[1] = tS * tS / tQ;                                                // ESS
-    if (warp == 2) sh.res[2] = tH / tS;                                                     // filtered mean
-    if (warp == 3) sh.res[3] = log(tS);
+  if (slot_lead && !degenerate) {
+    if (slot == 0) sh.res[0] = (double)nM * 0.693147180559945309417232121458 + log(tS);   // log-sum in the carry frame
+    if (slot == 1) sh.res[1] = tS * tS / tQ;                                                // ESS
+    if (slot == 2) sh.res[2] = tH / tS;                                                     // filtered mean
+    if (slot == 3) sh.res[3] = log(tS);
   }
-  __syncthreads();
+  nt_sync<NT>();
   // online learning: normalised score sums of this tick, FP64 in the global frame
   if (a.learn && p.rec2 && st->tick > 0 && !degenerate) {
     double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k = tid; k < G; k += kPlanThreads) {
+    for (int k = tid; k < G; k += NT) {
       const int nk = __float_as_int(__ldcg(p.rec + k).w);
       if (nk == kNkEmpty) continue;
       const float4 r2 = __ldcg(p.rec2 + k);
@@ -393,16 +418,16 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) v[q] = warp_sum_d(v[q]);
-    __syncthreads();                                  // sh.red is free again
+    nt_sync<NT>();                                  // sh.red is free again
     if (lane == 0) { sh.red[0][warp] = v[0]; sh.red[1][warp] = v[1]; sh.red[2][warp] = v[2]; }
     if (lane == 0) sh.learn3[warp] = v[3];
-    __syncthreads();
+    nt_sync<NT>();
     if (tid < 4) {
       double t = 0.0;
-      for (int w = 0; w < kPlanThreads / 32; ++w) t += (tid < 3) ? sh.red[tid][w] : sh.learn3[w];
+      for (int w = 0; w < NT / 32; ++w) t += (tid < 3) ? sh.red[tid][w] : sh.learn3[w];
       st->learn[tid] += t / tS;
     }
-    __syncthreads();
+    nt_sync<NT>();
   }
   if (tid == 0) {
     const int tick = st->tick, cur = st->cur;
@@ -474,10 +499,9 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     sh.b_resample = resample;
     sh.b_Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
   }
-  __syncthreads();
+  nt_sync<NT>();
   if (!sh.b_resample) {
     store_state();
-    griddep_release();
     return;
   }
 
@@ -487,26 +511,26 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   int* n_s = in_smem ? reinterpret_cast<int*>(plan_smem + (size_t)G * 8) : p.nexp;
   int* o_s = in_smem ? n_s + G : p.ofirst;
   if (in_smem) {
-    for (int k0 = 0; k0 < G; k0 += 4 * kPlanThreads) {
+    for (int k0 = 0; k0 < G; k0 += 4 * NT) {
       int nk[4]; unsigned long long e4[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const int k = k0 + u * kPlanThreads + tid;
+        const int k = k0 + u * NT + tid;
         if (k < G) { nk[u] = __ldcg(p.nexp + k); e4[u] = __ldcg(p.E + k); }
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const int k = k0 + u * kPlanThreads + tid;
+        const int k = k0 + u * NT + tid;
         if (k < G) { n_s[k] = nk[u]; e_s[k] = e4[u]; }
       }
     }
   }
-  __syncthreads();
+  nt_sync<NT>();
 
   // 4. fixed-point CDF over contiguous runs of tiles: masses in the global
   //    frame, prefix and total
   const int Fg = sh.b_Fg;
-  const int C = (G + kPlanThreads - 1) / kPlanThreads;
+  const int C = (G + NT - 1) / NT;
   const int k0 = min(tid * C, G), k1 = min(k0 + C, G);
   auto ehat = [&](int k) -> unsigned long long {
     const int nk = n_s[k];
@@ -516,7 +540,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   unsigned long long part = 0ull;
   for (int k = k0; k < k1; ++k) part += ehat(k);
   unsigned long long total;
-  const unsigned long long excl = block_excl_scan_add<kPlanThreads>(part, &total, sh.scan_u);
+  const unsigned long long excl = block_excl_scan_add<NT>(part, &total, sh.scan_u);
   if (tid == 0) {
     unsigned long long delta = udiv_fp64(total, (unsigned long long)N);
     if (delta == 0ull) { delta = 1ull; st->error = BPF_ERR_DEGENERATE; }
@@ -528,7 +552,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
     st->base = sh.b_base; st->delta = delta; st->delta_magic = sh.b_magic; st->total = total;
     st->Fg = Fg;
   }
-  __syncthreads();
+  nt_sync<NT>();
   const unsigned long long base = sh.b_base, delta = sh.b_delta, magic = sh.b_magic;
 
   // 5. per tile: prefix, first output index, number of work items (a taped
@@ -547,13 +571,13 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   }
   const int o_end = o;     // first output of the next thread's first tile (N for the last)
   int n_items_total;
-  const int it0 = block_excl_scan_add<kPlanThreads>(n_it, &n_items_total, sh.scan_i);
+  const int it0 = block_excl_scan_add<NT>(n_it, &n_items_total, sh.scan_i);
 
   // 6. work items (tile, first output, end output, flags: 1 = first item of the
   //    tile, 2 = the only one, holding all of the tile's outputs);
   //    heavy tiles are split
   int ib = it0;
-  for (int k = k0; k < k1; ++k) {
+  for (int k = k0; ITEMS && k < k1; ++k) {
     const int o0 = o_s[k];
     const int o1 = (k + 1 < k1) ? o_s[k + 1] : o_end;
     const int ni = max((o1 - o0 + kOutChunk - 1) / kOutChunk, min_items);
@@ -564,6 +588,18 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   }
   if (tid == 0) st->n_items = n_items_total;
   store_state();
+}
+
+__global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs a) {
+  __shared__ PlanShared<kPlanThreads> sh;
+  __shared__ __align__(16) DevState s_st;
+  extern __shared__ __align__(16) unsigned char plan_smem[];
+  griddep_wait();
+  // the device state lives in shared memory for the whole kernel (one load, one store)
+  if (threadIdx.x < kStWords)
+    reinterpret_cast<unsigned long long*>(&s_st)[threadIdx.x] =
+        __ldcg(reinterpret_cast<const unsigned long long*>(p.st) + threadIdx.x);
+  plan_body<kPlanThreads, true>(p, a, s_st, sh, plan_smem);
   griddep_release();
 }
 
@@ -665,19 +701,17 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
 
     // Exact fixed-point prefix of the tile: 16 contiguous weights per thread
     // (summed here, rebuilt element by element below from the staged tile).
-    // A tile whose shift reaches 64 has no mass in the global frame.
+    // A tile whose shift reaches 64 has no mass in the global frame. Slots past N
+    // hold the log2-weight -inf (weight 0), so they need no test here or below.
     const float4* wt = reinterpret_cast<const float4*>(ws + tid * kPerThread);
-    const bool full = nA == kTile;
     const bool massive = r < 64;
     unsigned long long run = 0ull;
     if (massive) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const float4 f = wt[v];
-        const float ff[4] = {f.x, f.y, f.z, f.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (full || tid * kPerThread + 4 * v + e < nA) run += fix_weight(tile_weight(ff[e]));
+        run += fix_weight(tile_weight(f.x)) + fix_weight(tile_weight(f.y));
+        run += fix_weight(tile_weight(f.z)) + fix_weight(tile_weight(f.w));
       }
     }
     unsigned long long tot;
@@ -688,8 +722,9 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     // element's. In the tile's own frame, C_j > t_q  <=>  A_j >= ((t_q - P_k + 1) << r), and
     // consecutive targets are delta << r apart there, so the count needs neither the shift nor
     // P_k per element: each thread tracks its next target's threshold relative to its first
-    // element's exclusive prefix (capped, see kThCap). The element writes one start mark, at its
-    // first slot inside this window.
+    // element's exclusive prefix (capped, see kThCap). The count has no branch per element (a
+    // warp vote guards the division of parents with more than four children); each element
+    // with children writes one start mark, at its first slot inside this window.
     const int lane = tid & 31, warp = tid >> 5;
     int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
     unsigned long long th = kThCap, D = kThCap;
@@ -699,12 +734,10 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       if (delta <= (kThCap >> r)) D = delta << r;
     }
     int32_t* csr = (a.csr && (item.w & 1)) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
-    // Compile-time variants: FULL (no element past N in the tile), WHOLE (the
-    // item holds every output of the tile, so each counted child lands in the
-    // window), TAPE (first-child list for the gradient tape).
+    // Compile-time variants: WHOLE (the item holds every output of the tile, so each
+    // counted child lands in the window), TAPE (first-child list for the gradient tape).
     const bool whole = (item.w & 2) != 0;
-    auto count_children = [&](auto full_tag, auto whole_tag, auto tape_tag) {
-      constexpr bool FULL = decltype(full_tag)::value;
+    auto count_children = [&](auto whole_tag, auto tape_tag) {
       constexpr bool WHOLE = decltype(whole_tag)::value;
       constexpr bool TAPE = decltype(tape_tag)::value;
       const unsigned long long D2 = 2ull * D, D3 = 3ull * D, D4 = 4ull * D;
@@ -716,32 +749,26 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int j = tid * kPerThread + 4 * g + e;
-          const bool in = FULL || j < nA;
-          if (TAPE && in) csr[j] = q;
-          if (in) acc += fix_weight(tile_weight(ff[e]));
-          if (in && acc >= th) {
-            const unsigned long long diff = acc - th;
-            int c = 1 + (diff >= D) + (diff >= D2) + (diff >= D3);
-            if (c == 4 && diff >= D4) c = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
-            const int q1 = min(q + c, N);
-            if (WHOLE || (q < ob && q1 > oa)) marks[(WHOLE ? q : max(q, oa)) - wa] = (unsigned short)(j + 1);
-            th = (q1 >= N) ? kThCap : th + (unsigned long long)c * D;
-            q = q1;
+          if (TAPE && j < nA) csr[j] = q;
+          acc += fix_weight(tile_weight(ff[e]));
+          const bool ge = acc >= th;
+          const unsigned long long diff = acc - th;
+          int c = ge ? 1 + (int)(diff >= D) + (int)(diff >= D2) + (int)(diff >= D3) : 0;
+          const bool slow = ge && diff >= D4;
+          if (__any_sync(0xffffffffu, slow)) {
+            if (slow) c = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
           }
+          const int q1 = min(q + c, N);
+          if (c > 0 && (WHOLE || (q < ob && q1 > oa))) marks[(WHOLE ? q : max(q, oa)) - wa] = (unsigned short)(j + 1);
+          th = (q1 >= N) ? kThCap : th + (unsigned long long)c * D;
+          q = q1;
         }
       }
     };
     if (massive) {
-      if (csr) {
-        if (full) count_children(std::true_type{}, std::false_type{}, std::true_type{});
-        else count_children(std::false_type{}, std::false_type{}, std::true_type{});
-      } else if (whole) {
-        if (full) count_children(std::true_type{}, std::true_type{}, std::false_type{});
-        else count_children(std::false_type{}, std::true_type{}, std::false_type{});
-      } else {
-        if (full) count_children(std::true_type{}, std::false_type{}, std::false_type{});
-        else count_children(std::false_type{}, std::false_type{}, std::false_type{});
-      }
+      if (csr) count_children(std::false_type{}, std::true_type{});
+      else if (whole) count_children(std::true_type{}, std::false_type{});
+      else count_children(std::false_type{}, std::false_type{});
     } else if (csr) {
       for (int e = 0; e < kPerThread; ++e)       // no mass: every element's children start at q
         if (tid * kPerThread + e < nA) csr[tid * kPerThread + e] = q;
@@ -932,6 +959,297 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 }
 
 // ---------------------------------------------------------------------------
+// Fused tick for small filters (N <= kSmallMaxN, at most kSmallTiles tiles):
+// one CTA runs n consecutive ticks, each as pass 1, the plan and the
+// resampling, without leaving the SM, so a tick costs one launch (or a run of
+// ticks one launch) instead of three dependent launches.
+//   pass 1    group g of kThreads threads runs tile g with the pass-1 code and
+//             its own barrier, so every tile record is bit for bit pass 1's;
+//   plan      the plan code on warp 0 alone (warp barriers only; with at most
+//             four tiles it forms the same FP64 sums), device state in shared memory;
+//   resample  the whole filter at once: the same fixed-point rule (integer
+//             exact, so the ancestors do not depend on how the work is split),
+//             a per-output start mark in shared memory and the max-scan gather.
+// Results equal the three-kernel tick's bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kSmallThreads = kSmallTiles * kThreads;
+constexpr size_t kSmallMarkBytes = ((size_t)kSmallMaxN + kGatherStep) * 2;
+static_assert(kSmallMaxN % kGatherStep == 0, "the small gather reads marks in 256-slot steps");
+
+// Pass 1 of tile k for a filter of one or two tiles, spread over SPLIT times as many
+// threads as pass 1 uses (group barrier `bar`, rt = 0..SPLIT*kThreads-1 inside the group).
+// Pass-1 thread v's sixteen particles (four float4 groups r) go to SPLIT adjacent threads,
+// 4/SPLIT groups each, with the per-particle arithmetic of pass1_tile; the FP32 tile
+// partials are then accumulated in pass 1's order by handing the running sums from one of
+// those threads to the next, so every tile record is bit for bit pass 1's.
+struct SplitShared {
+  float s_max[kSmallThreads / 32];
+  float s_part[3][kThreads];
+  unsigned long long s_E[kThreads];
+};
+
+template <bool TSTATE, bool GAUSS, int SPLIT>
+__device__ __forceinline__ void pass1_split(const Plan& p, const TickArgs& a, const DevState* st, int k, int rt,
+                                            int bar, SplitShared& sh) {
+  constexpr int R = 4 / SPLIT;                 // float4 groups of this thread
+  constexpr int NTG = kThreads * SPLIT;        // threads of the tile's group
+  const int v = rt / SPLIT, sidx = rt % SPLIT;
+  const int lane = rt & 31, warp = rt >> 5;
+  auto gsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(NTG) : "memory"); };
+  const int tick = st->tick;
+  const bool carry = st->resampled_prev == 0;
+  const int nM_prev = st->nM_prev;
+  const uint64_t k1 = st->k1, k2 = st->k2;
+  float* hb = st->cur ? p.h1 : p.h0;
+  const float y = a.y_ptr ? __ldg(a.y_ptr) : a.obs.y;
+  ObsModel obs = a.obs;
+  obs.y = y;
+  const float y2 = y * y;
+  float carry_off = 0.0f;
+  if (carry) {
+    const int nkp = p.nexp[k];
+    carry_off = (nkp == kNkEmpty) ? -INFINITY : (float)(nkp - nM_prev);
+  }
+  const float gauss_c = kGaussLog2C + carry_off;
+  const float t_c = __fmul_rn(obs.c_obs, kLog2e) + carry_off;
+  const float y2nu = __fmul_rn(y2, obs.inv_nu);
+  const unsigned long long k33 = k2 << 33;
+  const int tile0 = k * kTile;
+
+  float x[4 * R], hv[4 * R];
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) {
+    const int i0 = tile0 + 4 * (v + kThreads * (sidx * R + rr));
+    const float4 h4 = *reinterpret_cast<const float4*>(hb + i0);
+    const float4 w4 = carry ? *reinterpret_cast<const float4*>(p.w + i0) : make_float4(0.f, 0.f, 0.f, 0.f);
+    float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+    const float wp[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float h = hh[e];
+      if (tick > 0) {
+        const uint64_t sst = k1 + k2 * pcg_inc((uint32_t)(i0 + e));
+        float z = icdf_normal_warp(pcg_uniform(pcg_output(sst)));
+        if (TSTATE) z *= tstate_scale_warp(sst, k33, a.nu_int, a.nu_state);
+        h = propagate(h, a.mu, a.rho, a.sigma, z);
+      }
+      float xx = GAUSS ? obs_log2pdf_gauss_plus(y2, h, gauss_c) : obs_log2pdf_t_plus(obs, y2nu, h, t_c);
+      if (carry) xx += wp[e];
+      if (i0 + e >= p.N) xx = -INFINITY;          // padding slots carry no weight
+      hh[e] = h;
+      x[4 * rr + e] = xx;
+      hv[4 * rr + e] = h;
+    }
+    *reinterpret_cast<float4*>(hb + i0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
+  }
+  float mx = x[0];
+#pragma unroll
+  for (int e = 1; e < 4 * R; ++e) mx = fmaxf(mx, x[e]);
+  mx = warp_max_f(mx);
+  if (lane == 0) sh.s_max[warp] = mx;
+  gsync();
+  mx = sh.s_max[0];
+  for (int w = 1; w < NTG / 32; ++w) mx = fmaxf(mx, sh.s_max[w]);
+  const int nk = (mx == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(mx, -1.0e9f));
+  const float fnk = (nk == kNkEmpty) ? INFINITY : (float)nk;
+
+  float wv[4 * R];
+  unsigned long long E = 0ull;
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) {
+    const int i0 = tile0 + 4 * (v + kThreads * (sidx * R + rr));
+    float dv[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      dv[e] = x[4 * rr + e] - fnk;
+      wv[4 * rr + e] = tile_weight(dv[e]);
+      E += fix_weight(wv[4 * rr + e]);
+    }
+    *reinterpret_cast<float4*>(p.w + i0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+  }
+  // pass 1's per-thread FP32 sums, in its element order, handed along the SPLIT threads
+  float aS = 0.f, aQ = 0.f, aH = 0.f;
+#pragma unroll
+  for (int step = 0; step < SPLIT; ++step) {
+    if (sidx == step) {
+#pragma unroll
+      for (int e = 0; e < 4 * R; ++e) {
+        aS += wv[e];
+        aQ = fmaf(wv[e], wv[e], aQ);
+        aH = fmaf(wv[e], hv[e], aH);
+      }
+    }
+    const float nS = __shfl_up_sync(0xffffffffu, aS, 1);
+    const float nQ = __shfl_up_sync(0xffffffffu, aQ, 1);
+    const float nH = __shfl_up_sync(0xffffffffu, aH, 1);
+    if (step + 1 < SPLIT && sidx == step + 1) { aS = nS; aQ = nQ; aH = nH; }
+  }
+#pragma unroll
+  for (int o = 1; o < SPLIT; o <<= 1) E += __shfl_xor_sync(0xffffffffu, E, o);
+  if (sidx == SPLIT - 1) { sh.s_part[0][v] = aS; sh.s_part[1][v] = aQ; sh.s_part[2][v] = aH; }
+  if (sidx == 0) sh.s_E[v] = E;
+  gsync();
+  if (warp == 0) {                              // pass 1's FP64 tile combine, same order
+    double tS = 0.0, tQ = 0.0, tH = 0.0;
+    unsigned long long tE = 0ull;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+      tS += (double)sh.s_part[0][lane + 32 * w];
+      tQ += (double)sh.s_part[1][lane + 32 * w];
+      tH += (double)sh.s_part[2][lane + 32 * w];
+      tE += sh.s_E[lane + 32 * w];
+    }
+    tS = warp_sum_d(tS); tQ = warp_sum_d(tQ); tH = warp_sum_d(tH);
+    tE = warp_sum_u64(tE);
+    if (lane == 0) {
+      p.nexp[k] = nk;
+      p.E[k] = tE;
+      p.rec[k] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
+    }
+  }
+}
+
+struct SmallShared {
+  Pass1Shared p1[kSmallTiles];
+  PlanShared<32> pl;
+  __align__(16) DevState st;
+  __align__(16) unsigned char plan_stage[(plan_smem_bytes(kSmallTiles) + 15) & ~(size_t)15];
+  unsigned long long scan[kSmallThreads / 32 + 1];
+  unsigned long long tstart[kSmallTiles];   // block-scan value at each tile's first element
+  unsigned wmax[kSmallThreads / 32];
+  SplitShared sp[2];
+};
+
+__device__ __forceinline__ void small_resample(const Plan& p, const TickArgs& a, SmallShared& sh,
+                                               unsigned short* marks) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N = p.N;
+  const DevState& st = sh.st;
+  const unsigned long long base = st.base, delta = st.delta, magic = st.delta_magic;
+  const int nM = st.nM, Fg = st.Fg;
+  const float* hsrc = st.src ? p.h1 : p.h0;
+  float* hdst = st.src ? p.h0 : p.h1;
+  const int Ns = (N + kGatherStep - 1) & ~(kGatherStep - 1);
+  for (int x = tid; x < Ns / 8; x += kSmallThreads) reinterpret_cast<uint4*>(marks)[x] = make_uint4(0u, 0u, 0u, 0u);
+
+  // each thread a power-of-two chunk of consecutive elements (chunks never straddle a tile)
+  int chunk = 1;
+  while (chunk * kSmallThreads < N) chunk <<= 1;
+  const int j0 = tid * chunk, j1 = min(N, j0 + chunk);
+  const int k = min(j0, N - 1) >> 12;
+  const int nk = p.nexp[k];
+  const int r = (nk == kNkEmpty) ? 64 : nM - nk + kFixF - Fg;
+  const unsigned long long Pk = p.P[k];
+  unsigned long long run = 0ull;
+  if (r < 64)
+    for (int j = j0; j < j1; ++j) run += fix_weight(tile_weight(p.w[j]));
+  unsigned long long tot;
+  const unsigned long long excl = block_excl_scan_add<kSmallThreads>(run, &tot, sh.scan);
+  if (j0 < N && (j0 & (kTile - 1)) == 0) sh.tstart[k] = excl;
+  __syncthreads();
+  const unsigned long long loc = excl - sh.tstart[k];   // tile-local exclusive prefix
+
+  // child counts against tile-frame thresholds, as pass 2 (every output is in the window)
+  int q = targets_below(Pk + shr64(loc, r), base, delta, magic, N);
+  unsigned long long th = kThCap, D = kThCap;
+  if (r < 64 && q < N && j0 < N) {
+    const unsigned long long m = base + (unsigned long long)q * delta - Pk + 1ull;
+    if (m <= (~0ull >> r)) th = min((m << r) - loc, kThCap);
+    if (delta <= (kThCap >> r)) D = delta << r;
+  }
+  unsigned long long acc = 0ull;
+  for (int j = j0; j < j1; ++j) {
+    acc += fix_weight(tile_weight(p.w[j]));
+    if (acc >= th) {
+      const unsigned long long diff = acc - th;
+      int c = 1 + (diff >= D) + (diff >= 2ull * D) + (diff >= 3ull * D);
+      if (c == 4 && diff >= 4ull * D) c = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
+      const int q1 = min(q + c, N);
+      marks[q] = (unsigned short)(j + 1);
+      th = (q1 >= N) ? kThCap : th + (unsigned long long)c * D;
+      q = q1;
+    }
+  }
+  __syncthreads();
+
+  // gather: the ancestor of output o is the last start mark at or before o
+  constexpr int W = kSmallThreads / 32;
+  const int wchunk = ((N + W - 1) / W + kGatherStep - 1) & ~(kGatherStep - 1);
+  const int cs = warp * wchunk, ce = min(cs + wchunk, N);
+  unsigned wmax = 0u;
+  for (int o0 = cs; o0 < ce; o0 += kGatherStep) {
+    const uint4 m = reinterpret_cast<const uint4*>(marks + o0)[lane];
+    const unsigned v = __vmaxu2(__vmaxu2(m.x, m.y), __vmaxu2(m.z, m.w));
+    wmax = max(wmax, max(v & 0xffffu, v >> 16));
+  }
+  wmax = __reduce_max_sync(0xffffffffu, wmax);
+  if (lane == 0) sh.wmax[warp] = wmax;
+  __syncthreads();
+  unsigned carry = 0u;
+  for (int w = 0; w < warp; ++w) carry = max(carry, sh.wmax[w]);
+  for (int o0 = cs; o0 < ce; o0 += kGatherStep) {
+    const uint4 m = reinterpret_cast<const uint4*>(marks + o0)[lane];
+    unsigned am[8];
+    am[0] = m.x & 0xffffu;
+    am[1] = max(am[0], m.x >> 16);
+    am[2] = max(am[1], m.y & 0xffffu);
+    am[3] = max(am[2], m.y >> 16);
+    am[4] = max(am[3], m.z & 0xffffu);
+    am[5] = max(am[4], m.z >> 16);
+    am[6] = max(am[5], m.w & 0xffffu);
+    am[7] = max(am[6], m.w >> 16);
+    unsigned x = am[7];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= off) x = max(x, t);
+    }
+    unsigned pre = __shfl_up_sync(0xffffffffu, x, 1);
+    pre = max(carry, lane == 0 ? 0u : pre);
+    const int o = o0 + 8 * lane;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      if (o + u < ce) {
+        const unsigned jj = max(max(pre, am[u]), 1u);    // output 0 has the first mark: jj >= 1
+        hdst[o + u] = hsrc[jj - 1u];
+        if (a.anc) a.anc[o + u] = (int)(jj - 1u);
+      }
+    }
+    carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
+  }
+}
+
+template <bool TSTATE, bool GAUSS>
+__global__ void __launch_bounds__(kSmallThreads, 1) small_kernel(Plan p, TickArgs a, int n_ticks) {
+  __shared__ SmallShared sh;
+  extern __shared__ __align__(16) unsigned char small_smem[];
+  unsigned short* marks = reinterpret_cast<unsigned short*>(small_smem);
+  griddep_wait();
+  const int tid = threadIdx.x, g = tid / kThreads;
+  if (tid < kStWords)
+    reinterpret_cast<unsigned long long*>(&sh.st)[tid] = __ldcg(reinterpret_cast<const unsigned long long*>(p.st) + tid);
+  __syncthreads();
+  for (int t = 0; t < n_ticks; ++t) {
+    TickArgs at = a;
+    at.y_ptr = a.y_ptr ? a.y_ptr + t : nullptr;
+    at.rec = a.rec ? a.rec + t : nullptr;
+    if (p.G == 1) {                          // one tile: four threads per pass-1 thread
+      pass1_split<TSTATE, GAUSS, 4>(p, at, &sh.st, 0, tid, 1, sh.sp[0]);
+    } else if (p.G == 2) {                   // two tiles: two threads per pass-1 thread
+      pass1_split<TSTATE, GAUSS, 2>(p, at, &sh.st, tid >> 9, tid & 511, 1 + (tid >> 9), sh.sp[tid >> 9]);
+    } else if (g < p.G) {
+      pass1_tile<TSTATE, false, 0, GAUSS>(p, at, &sh.st, g, tid & (kThreads - 1), 1 + g, sh.p1[g]);
+    }
+    __syncthreads();                       // the tile records are visible to the plan
+    if (tid < 32) plan_body<32, false>(p, at, sh.st, sh.pl, sh.plan_stage);   // warp 0, warp barriers
+    __syncthreads();
+    if (sh.st.do_resample) small_resample(p, at, sh, marks);
+    __syncthreads();
+  }
+  griddep_release();
+}
+
+// ---------------------------------------------------------------------------
 // Debug probe: raw PCG32 output and the derived normal for draw t
 // ---------------------------------------------------------------------------
 __global__ void debug_pcg_kernel(int seed, int n, unsigned long long At, unsigned long long Bt,
@@ -1025,6 +1343,10 @@ int pass2_grid_size(int device) {
       cudaFuncSetAttribute(pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPass2Smem);
       cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)plan_smem_bytes(kPlanSmemTiles));
+      cudaFuncSetAttribute(small_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
+      cudaFuncSetAttribute(small_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
+      cudaFuncSetAttribute(small_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
+      cudaFuncSetAttribute(small_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
       if (device >= 0 && device < kMaxConfiguredDevices) configured[device] = true;
     }
   }
@@ -1059,6 +1381,21 @@ cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool p
 }
 cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s, bool pdl) {
   return launch_ex(pass2_kernel, dim3(grid), dim3(kThreads), kPass2Smem, s, pdl, p, a);
+}
+
+bool small_eligible(const Plan& p, const TickArgs& a) {
+  return p.N <= kSmallMaxN && !a.learn && a.apf == 0 && !(a.silverman > 0.0f) && !a.ckpt && !a.csr && !a.aux;
+}
+
+cudaError_t launch_small(const Plan& p, const TickArgs& a, int n_ticks, cudaStream_t s, bool pdl) {
+  if (p.N > kSmallMaxN || n_ticks < 1) return cudaErrorInvalidValue;
+  const dim3 grid(1), block(kSmallThreads);
+  if (a.obs.nu > 0.0f) {
+    if (a.nu_int > 0) return launch_ex(small_kernel<true, false>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
+    return launch_ex(small_kernel<false, false>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
+  }
+  if (a.nu_int > 0) return launch_ex(small_kernel<true, true>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
+  return launch_ex(small_kernel<false, true>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
 }
 
 cudaError_t launch_jitter(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {

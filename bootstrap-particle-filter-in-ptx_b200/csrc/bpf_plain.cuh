@@ -110,6 +110,12 @@ cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_
 // from the resampled particles' spread about the tick's filtered mean, then h += bw z clamped to
 // [mu - 8, mu + 8], z from the particle slot's next PCG32 draw.
 cudaError_t launch_jitter(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
+// Fused small-filter tick (N <= kSmallMaxN): one launch of one CTA runs n_ticks consecutive
+// ticks (pass 1, plan and resampling), bit-identical to the three-kernel tick. a.y_ptr and
+// a.rec point at the run's first tick (a.obs.y is the observation when y_ptr is null and
+// n_ticks is 1). Not for learning, auxiliary-filter, Silverman or taped ticks.
+bool small_eligible(const Plan& p, const TickArgs& a);
+cudaError_t launch_small(const Plan& p, const TickArgs& a, int n_ticks, cudaStream_t s, bool pdl);
 int pass2_grid_size(int device);
 size_t pass2_smem_bytes();
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s);

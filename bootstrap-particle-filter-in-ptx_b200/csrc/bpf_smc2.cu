@@ -56,7 +56,11 @@ struct HostPcg {
     const uint32_t xs = (uint32_t)(((old >> 18) ^ old) >> 27), rot = (uint32_t)(old >> 59);
     return (xs >> rot) | (xs << ((32u - rot) & 31u));
   }
-  double uniform() { return ((double)(next() >> 5) * 67108864.0 + (double)(next() >> 6) + 0.5) / 9007199254740992.0; }
+  double uniform() {   // 53 bits: the first draw's top 27, then the second's top 26
+    const uint32_t a = next() >> 5;
+    const uint32_t b = next() >> 6;
+    return ((double)a * 67108864.0 + (double)b + 0.5) / 9007199254740992.0;
+  }
   double normal() {   // Box-Muller
     const double u1 = uniform(), u2 = uniform();
     return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586476925286766559 * u2);
@@ -107,6 +111,11 @@ struct GpuBpfSmc2 {
   long long* d_off_src = nullptr;      // [M] outer resampling: the ancestors' current areas
   long long* off_pin = nullptr;        // [3M] staging
   std::vector<int> par;
+  // the last update: forward increments, whether it resampled, the outer ancestors
+  bool have_update = false;
+  std::vector<double> lu_dll;
+  std::vector<int> lu_idx;
+  int lu_res = 0;
   // the last PMMH move
   bool have_move = false;
   std::vector<float> lm_theta_prop, lm_theta_cur;
@@ -184,6 +193,7 @@ int resample_move(GpuBpfSmc2* s) {
     while (k < M - 1 && cdf[k] <= tgt) ++k;
     idx[j] = k;
   }
+  s->lu_idx = idx;
   for (int j = 0; j < M; ++j) s->i_pin[j] = idx[j];
   for (int j = 0; j < M; ++j) s->i_pin[M + j] = s->next_seed++;
   BCK(cudaMemcpyAsync(s->d_idx, s->i_pin, M * sizeof(int), cudaMemcpyHostToDevice, s->stream));
@@ -394,8 +404,12 @@ float gpu_bpf_smc2_update(GpuBpfSmc2* s, float y) {
     return NAN;
   }
   for (int j = 0; j < s->n_theta; ++j) s->logw[j] += s->dll_pin[j];
+  s->lu_dll.assign(s->dll_pin, s->dll_pin + s->n_theta);
+  s->lu_res = 0;
+  s->have_update = true;
   double ess = outer_ess(s->logw);
   if (ess < (double)s->ess_frac * s->n_theta) {
+    s->lu_res = 1;
     if (resample_move(s) != BPF_OK) return NAN;
     ess = (double)s->n_theta;
   }
@@ -495,6 +509,15 @@ int gpu_bpf_smc2_get_last_move(GpuBpfSmc2* s, float* theta_prop, float* theta_cu
   if (loglik_prop) std::copy(s->lm_ll_prop.begin(), s->lm_ll_prop.begin() + M, loglik_prop);
   if (loglik_cur) std::copy(s->lm_ll_cur.begin(), s->lm_ll_cur.begin() + M, loglik_cur);
   if (accepted) std::copy(s->lm_acc.begin(), s->lm_acc.begin() + M, accepted);
+  return BPF_OK;
+}
+
+int gpu_bpf_smc2_get_last_update(GpuBpfSmc2* s, double* dll, int* resampled, int* ancestors) {
+  if (!s || !s->have_update) return bpf_record_error(BPF_ERR_STATE);
+  const int M = s->n_theta;
+  if (dll) std::copy(s->lu_dll.begin(), s->lu_dll.begin() + M, dll);
+  if (resampled) *resampled = s->lu_res;
+  if (ancestors && s->lu_res) std::copy(s->lu_idx.begin(), s->lu_idx.begin() + M, ancestors);
   return BPF_OK;
 }
 

@@ -132,6 +132,7 @@ SIGNATURES = {
     "gpu_bpf_get_ancestors": (_i, [P_STATE, C.POINTER(C.c_int32)]),
     "gpu_bpf_get_resample_inputs": (_i, [P_STATE, C.POINTER(_f), C.POINTER(C.c_int32), C.POINTER(C.c_uint32)]),
     "gpu_bpf_profile": (_i, [P_STATE, _i]),
+    "gpu_bpf_set_fused_small": (_i, [P_STATE, _i]),
     "gpu_bpf_profile_read": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), C.POINTER(_i),
                                   C.POINTER(_i)]),
     "gpu_bpf_launch_count": (C.c_longlong, []),
@@ -188,6 +189,7 @@ SIGNATURES = {
     "gpu_bpf_smc2_stats": (_i, [_vp, C.POINTER(_i), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "gpu_bpf_smc2_set_cpmmh_rho": (_i, [_vp, _f]),
     "gpu_bpf_smc2_get_last_move": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "gpu_bpf_smc2_get_last_update": (_i, [_vp, _vp, _vp, _vp]),
     "gpu_bpf_smc2_get_noise": (_i, [_vp, _i, _i, _vp]),
     # gradient
     "gpu_bpf_grad_create": (_vp, [_i, _i, _i]),

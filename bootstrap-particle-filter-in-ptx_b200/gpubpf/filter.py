@@ -163,6 +163,10 @@ class GpuBpf:
         check(self._lib.gpu_bpf_get_resample_inputs(self._s, w, te, C.byref(u)), "gpu_bpf_get_resample_inputs")
         return w, te, u.value
 
+    def set_fused_small(self, enable: bool = True) -> None:
+        """Fused one-launch ticks for filters of at most 16384 particles (default on)."""
+        check(self._lib.gpu_bpf_set_fused_small(self._s, int(bool(enable))), "gpu_bpf_set_fused_small")
+
     def profile(self, enable: bool = True) -> None:
         check(self._lib.gpu_bpf_profile(self._s, int(enable)), "gpu_bpf_profile")
 

@@ -81,6 +81,17 @@ class Smc2:
                                                    lc.ctypes.data, acc.ctypes.data), "gpu_bpf_smc2_get_last_move")
         return {"theta_prop": tp, "theta_cur": tc, "loglik_prop": lp, "loglik_cur": lc, "accepted": acc}
 
+    def last_update(self):
+        """The last update: dict of dll [M] (the forward tick's inner log-likelihood increments),
+        resampled (bool) and ancestors [M] (the outer ancestors when resampled, else None)."""
+        M = self.n_theta
+        dll = np.zeros(M)
+        res = C.c_int(0)
+        anc = np.zeros(M, dtype=np.int32)
+        check(self._lib.gpu_bpf_smc2_get_last_update(self._h, dll.ctypes.data, C.addressof(res), anc.ctypes.data),
+              "gpu_bpf_smc2_get_last_update")
+        return {"dll": dll, "resampled": bool(res.value), "ancestors": anc if res.value else None}
+
     def noise(self, j: int, n_ticks: int, n_particles: int):
         """Theta-particle j's current auxiliary noise: (normals [n_ticks, n_particles], resampling
         normals [n_ticks])."""

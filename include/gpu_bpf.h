@@ -212,6 +212,15 @@ int gpu_bpf_get_ancestors(GpuBpfState* state, int32_t* anc_out);
 int gpu_bpf_get_resample_inputs(GpuBpfState* state, float* w_out, int32_t* tile_exp_out,
                                 uint32_t* u23_out);
 
+/* Fused small-filter ticks (addition): a filter of at most 16384 particles runs
+ * each tick as one launch of one CTA (pass 1, the resampling decision and the
+ * resampling without leaving the SM), and a captured run of ticks
+ * (gpu_bpf_step_many, gpu_bpf_step_many_device) as one launch for the whole
+ * run, with results bit-identical to the three-kernel tick. On by default;
+ * enable = 0 selects the three-kernel tick. Learning filters, Silverman jitter
+ * and profiled ticks always take the three-kernel path. */
+int gpu_bpf_set_fused_small(GpuBpfState* state, int enable);
+
 /* Kernel profiling: when enabled, every tick's three kernels (pass 1, plan,
  * pass 2) are timed with CUDA events on state->stream (launched without
  * programmatic dependent launch so the events bracket each kernel). read
@@ -514,6 +523,10 @@ int         gpu_bpf_smc2_set_cpmmh_rho(GpuBpfSmc2* smc2, float rho);
  * [n_theta] and the acceptance flags [n_theta]. BPF_ERR_STATE before the first move. */
 int         gpu_bpf_smc2_get_last_move(GpuBpfSmc2* smc2, float* theta_prop, float* theta_cur,
                                        double* loglik_prop, double* loglik_cur, int* accepted);
+/* The last update (host arrays, each may be NULL): the forward tick's inner log-likelihood
+ * increments [n_theta] (the outer log-weights' increments), whether the theta-particles were
+ * resampled, and then their outer ancestors [n_theta]. BPF_ERR_STATE before the first update. */
+int         gpu_bpf_smc2_get_last_update(GpuBpfSmc2* smc2, double* dll, int* resampled, int* ancestors);
 /* Theta-particle j's current auxiliary noise for ticks 0..n_ticks-1 (n_ticks at most the ticks
  * seen; layout of gpu_bpf_batch_run_correlated's areas) into the host array out. Needs
  * rho > 0. */

@@ -313,3 +313,66 @@ def test_independent_filters_do_not_interact(bpf):
         b.get_result()
     assert r_a == r_solo
     a.close(); b.close()
+
+
+# ---------------------------------------------------------------------------
+# fused small-filter tick (N <= 16384): bit-identical to the three-kernel tick
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("N,thr,nu_obs,nu_state", [(1, 0.0, 0.0, 0.0), (31, 0.5, 0.0, 0.0), (4096, 0.0, 0.0, 0.0),
+                                                   (4097, 0.5, 5.0, 0.0), (12388, 0.5, 0.0, 5.0),
+                                                   (16384, 0.3, 5.0, 5.0)])
+def test_fused_small_matches_three_kernel_path(bpf, N, thr, nu_obs, nu_state):
+    """Records, ancestors and particles of the fused one-launch tick equal the three-kernel
+    tick's bit for bit: through step_many (a captured run of 64 ticks as one launch), the
+    single-tick graph of gpu_bpf_step, and direct gpu_bpf_step_async launches."""
+    _, y = series(150, 7)
+
+    def run(fused, mode):
+        f = bpf.GpuBpf(N, RHO, SIG, MU, nu_state, nu_obs, 17, ess_threshold=thr)
+        f.set_fused_small(fused)
+        f.record_ancestors(True)
+        recs, ancs = [], []
+        if mode == "many":
+            recs = f.step_many(y[:128].tolist(), records=True)
+            for v in y[128:]:
+                f.step(float(v))
+                recs.append(f.get_record())
+                ancs.append(bytes(f.get_ancestors()[1]))
+        else:
+            for v in y:
+                if mode == "step":
+                    f.step(float(v))
+                else:
+                    f.step_async(float(v))
+                recs.append(f.get_record())
+                ancs.append(bytes(f.get_ancestors()[1]))
+        parts = bytes(f.get_particles())
+        w, te, u23 = f.get_resample_inputs()
+        total = f.get_loglik_total()
+        count = f.get_resample_count()
+        f.close()
+        key = [(r.dloglik, r.loglik_ref, r.loglik_total, r.h_mean, r.ess, r.resampled, r.tick) for r in recs]
+        return key, ancs, parts, bytes(w), bytes(te), u23, total, count
+
+    for mode in ("many", "step", "async"):
+        a = run(True, mode)
+        b = run(False, mode)
+        assert a[0] == b[0], mode
+        assert a[1] == b[1] and a[2] == b[2] and a[3:] == b[3:], mode
+
+
+def test_fused_small_long_device_run(bpf):
+    """A whole device-resident run of 1000 ticks as one fused launch equals the three-kernel run."""
+    import torch
+    _, y = series(1000, 42)
+    yd = torch.tensor(y, device="cuda")
+    out = []
+    for fused in (True, False):
+        f = bpf.GpuBpf(4096, RHO, SIG, MU, seed=42, ess_threshold=0.0)
+        f.set_fused_small(fused)
+        rec = torch.zeros(1000 * 40, dtype=torch.uint8, device="cuda")
+        f.step_many_device(yd.data_ptr(), 1000, rec.data_ptr())
+        torch.cuda.synchronize()
+        out.append((rec.cpu().numpy().tobytes(), bytes(f.get_particles())))
+        f.close()
+    assert out[0] == out[1]

@@ -75,3 +75,47 @@ def test_smc2_posterior_contracts_around_the_truth(bpf):
     assert sd[0] < 0.35                          # the N(-1, 0.5^2) prior on mu has contracted
     assert abs(mean[2] - truth[2]) < 3 * sd[2] + 0.05, (mean, sd)
     assert 0.85 < mean[1] < 0.995
+
+
+@pytest.mark.parametrize("cp_rho", [0.0, 0.99])
+def test_smc2_outer_loop_matches_host_restatement(bpf, cp_rho):
+    """Every outer step of a real update sequence against the host restatement of the outer loop
+    (oracle/smc2_outer.py, the reference's smc2_cuda_update outer step on this SV model) fed the
+    device's inner log-likelihoods: the prior draws, each tick's outer ESS, whether it resamples,
+    the outer ancestors, every proposal and acceptance flag bit for bit, and the outer log-weights
+    exactly (within 1e-12)."""
+    from oracle.smc2_outer import Smc2Outer
+    M, N, T, seed = 48, 256, 120, 11
+    y = _series(T, seed=6)
+    s = bpf.Smc2(M, N, T, seed=seed)
+    s.set_moves(1, 0.5, 1.0)
+    if cp_rho > 0:
+        s.set_cpmmh_rho(cp_rho)
+    ref = Smc2Outer(M, seed)
+    th, _, _ = s.particles()
+    np.testing.assert_array_equal(th, ref.theta_f32())
+    n_res = n_acc = 0
+    for t, v in enumerate(y):
+        ess = s.update(float(v))
+        lu = s.last_update()
+        ess_ref, res_ref = ref.observe(lu["dll"])
+        assert res_ref == lu["resampled"], t
+        if res_ref:
+            n_res += 1
+            assert ess == np.float32(M)
+            assert list(lu["ancestors"]) == ref.resample(), t
+            scored, cur = ref.propose()
+            mv = s.last_move()
+            np.testing.assert_array_equal(mv["theta_prop"], scored)
+            np.testing.assert_array_equal(mv["theta_cur"], cur)
+            flags = ref.accept(mv["loglik_prop"], mv["loglik_cur"])
+            assert list(mv["accepted"]) == flags, t
+            n_acc += sum(flags)
+        else:
+            assert ess == np.float32(ess_ref), t
+        th, lw, _ = s.particles()
+        np.testing.assert_array_equal(th, ref.theta_f32())
+        assert np.max(np.abs(lw - np.asarray(ref.logw))) <= 1e-12
+    st = s.stats()
+    s.close()
+    assert n_res >= 2 and st["rejuvenations"] == n_res and st["accepted"] == n_acc
