@@ -15,9 +15,9 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "gpubpf", "libgpubpf.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["bpf_plain.cu", "bpf_api.cu", "bpf_static.cu", "bpf_batch.cu", "bpf_batch_api.cu", "bpf_grad.cu",
+SOURCES = ["bpf_alloc.cu", "bpf_plain.cu", "bpf_api.cu", "bpf_static.cu", "bpf_batch.cu", "bpf_batch_api.cu", "bpf_grad.cu",
            "bpf_grad_api.cu", "bpf_imm.cu", "bpf_smc2.cu", "bpf_apf.cu"]
-HEADERS = ["bpf_common.cuh", "bpf_plain.cuh", "bpf_block.cuh", "bpf_batch.cuh", "bpf_grad.cuh",
+HEADERS = ["bpf_alloc.cuh", "bpf_common.cuh", "bpf_plain.cuh", "bpf_block.cuh", "bpf_batch.cuh", "bpf_grad.cuh",
            "bpf_batch_internal.cuh"]
 
 NVCC_FLAGS = [

@@ -128,8 +128,8 @@ int free_impl(ApfImpl* m) {
   if (!m) return BPF_OK;
   if (m->graph) cudaGraphExecDestroy(m->graph);
   plan_free(m->plan);
-  cudaFree(m->rec_dev); cudaFree(m->y_dev); cudaFree(m->anc_dev);
-  cudaFreeHost(m->rec_pin); cudaFreeHost(m->st_pin); cudaFreeHost(m->y_pin);
+  bpf_free(m->rec_dev); bpf_free(m->y_dev); bpf_free(m->anc_dev);
+  bpf_free_host(m->rec_pin); bpf_free_host(m->st_pin); bpf_free_host(m->y_pin);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   return BPF_OK;
@@ -141,11 +141,11 @@ int create_impl(GpuApfState* s, ApfImpl* m, int seed) {
   ACK(cudaGetDevice(&m->device));
   ACK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
   ACK(plan_alloc(m->plan, s->n_particles));
-  ACK(cudaMalloc(&m->rec_dev, (1 + kApfChunk) * sizeof(BpfTickRecord)));
-  ACK(cudaMalloc(&m->y_dev, kApfChunk * sizeof(float)));
-  ACK(cudaMallocHost(&m->rec_pin, (1 + kApfChunk) * sizeof(BpfTickRecord)));
-  ACK(cudaMallocHost(&m->st_pin, sizeof(DevState)));
-  ACK(cudaMallocHost(&m->y_pin, kApfChunk * sizeof(float)));
+  ACK(bpf_malloc(&m->rec_dev, (1 + kApfChunk) * sizeof(BpfTickRecord)));
+  ACK(bpf_malloc(&m->y_dev, kApfChunk * sizeof(float)));
+  ACK(bpf_malloc_host(&m->rec_pin, (1 + kApfChunk) * sizeof(BpfTickRecord)));
+  ACK(bpf_malloc_host(&m->st_pin, sizeof(DevState)));
+  ACK(bpf_malloc_host(&m->y_pin, kApfChunk * sizeof(float)));
   ACK(cudaMemsetAsync(m->rec_dev, 0, (1 + kApfChunk) * sizeof(BpfTickRecord), m->stream));
   m->pass2_grid = pass2_grid_size(m->device);
   if (const char* v = std::getenv("BPF_DISABLE_PDL")) m->pdl = (v[0] == '0');
@@ -333,7 +333,7 @@ int gpu_apf_record_ancestors(GpuApfState* s, int enable) {
   int rc = ensure_device(m);
   if (rc) return rc;
   if (enable && !m->anc_dev) {
-    ACK(cudaMalloc(&m->anc_dev, 2 * anc_stride(m) * sizeof(int32_t)));
+    ACK(bpf_malloc(&m->anc_dev, 2 * anc_stride(m) * sizeof(int32_t)));
     ACK(cudaMemsetAsync(m->anc_dev, 0xff, 2 * anc_stride(m) * sizeof(int32_t), m->stream));
   }
   m->record_anc = enable != 0;

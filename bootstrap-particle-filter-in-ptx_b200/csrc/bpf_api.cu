@@ -292,9 +292,9 @@ int free_impl(Impl* m) {
   for (cudaEvent_t e : m->ev_pending) cudaEventDestroy(e);
   for (cudaEvent_t e : m->ev_pool) cudaEventDestroy(e);
   plan_free(m->plan);
-  cudaFree(m->rec_dev); cudaFree(m->y_dev); cudaFree(m->anc_dev);
-  cudaFreeHost(m->rec_pin); cudaFreeHost(m->st_pin); cudaFreeHost(m->y_pin);
-  cudaFreeHost(m->rec_map); cudaFreeHost(m->mir_map);
+  bpf_free(m->rec_dev); bpf_free(m->y_dev); bpf_free(m->anc_dev);
+  bpf_free_host(m->rec_pin); bpf_free_host(m->st_pin); bpf_free_host(m->y_pin);
+  bpf_free_host(m->rec_map); bpf_free_host(m->mir_map);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   return BPF_OK;
@@ -443,13 +443,13 @@ static int create_impl(GpuBpfState* s, Impl* m, int n, float rho, float sigma_z,
   Plan& p = m->plan;
   CK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
   CK(plan_alloc(p, n));
-  CK(cudaMalloc(&m->rec_dev, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
-  CK(cudaMalloc(&m->y_dev, kGraphChunk * sizeof(float)));
-  CK(cudaMallocHost(&m->rec_pin, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
-  CK(cudaMallocHost(&m->st_pin, sizeof(DevState)));
-  CK(cudaMallocHost(&m->y_pin, kGraphChunk * sizeof(float)));
-  CK(cudaHostAlloc(&m->rec_map, sizeof(BpfTickRecord), cudaHostAllocMapped));
-  CK(cudaHostAlloc(&m->mir_map, sizeof(TickMirror), cudaHostAllocMapped));
+  CK(bpf_malloc(&m->rec_dev, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
+  CK(bpf_malloc(&m->y_dev, kGraphChunk * sizeof(float)));
+  CK(bpf_malloc_host(&m->rec_pin, (1 + kGraphChunk) * sizeof(BpfTickRecord)));
+  CK(bpf_malloc_host(&m->st_pin, sizeof(DevState)));
+  CK(bpf_malloc_host(&m->y_pin, kGraphChunk * sizeof(float)));
+  CK(bpf_host_alloc(&m->rec_map, sizeof(BpfTickRecord), cudaHostAllocMapped));
+  CK(bpf_host_alloc(&m->mir_map, sizeof(TickMirror), cudaHostAllocMapped));
   CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->rec_map_dev), m->rec_map, 0));
   CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->mir_map_dev), m->mir_map, 0));
   std::memset(m->rec_map, 0, sizeof(BpfTickRecord));
@@ -822,7 +822,7 @@ int gpu_bpf_record_ancestors(GpuBpfState* s, int enable) {
   int rc = ensure_device(m);
   if (rc) return rc;
   if (enable && !m->anc_dev) {
-    CK(cudaMalloc(&m->anc_dev, (size_t)m->plan.N * sizeof(int32_t)));
+    CK(bpf_malloc(&m->anc_dev, (size_t)m->plan.N * sizeof(int32_t)));
     CK(cudaMemsetAsync(m->anc_dev, 0xff, (size_t)m->plan.N * sizeof(int32_t), m->stream));
   }
   m->record_anc = enable != 0;
@@ -851,16 +851,128 @@ int gpu_bpf_get_resample_inputs(GpuBpfState* s, float* w_out, int32_t* tile_exp_
   CK(cudaStreamSynchronize(m->stream));
   if (w_out) {
     float* w_dev = nullptr;
-    CK(cudaMalloc(&w_dev, (size_t)m->plan.N * sizeof(float)));
+    CK(bpf_malloc(&w_dev, (size_t)m->plan.N * sizeof(float)));
     cudaError_t e = launch_tile_weights(m->plan, w_dev, m->stream);
     g_launches += 1;
     if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
     if (e == cudaSuccess) e = cudaMemcpy(w_out, w_dev, (size_t)m->plan.N * sizeof(float), cudaMemcpyDeviceToHost);
-    cudaFree(w_dev);
+    bpf_free(w_dev);
     CK(e);
   }
   if (tile_exp_out) CK(cudaMemcpy(tile_exp_out, m->plan.nexp, (size_t)m->plan.G * sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (u23_out) *u23_out = m->st_pin->u23;
+  return BPF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoint / resume: the filter's whole stochastic state in one byte string.
+// The PCG32 streams are counter-based, so the state holds no RNG arrays: the
+// device state's stream constants and tick index, plus the resampling-uniform
+// stream position, determine every later draw.
+// ---------------------------------------------------------------------------
+namespace {
+struct CkptHeader {
+  char magic[8];                 // "GPUBPF\0\1"
+  uint32_t version;              // 1
+  uint32_t devstate_bytes;       // sizeof(DevState)
+  int32_t n, G;
+  float rho, sigma_z, mu, nu_state, nu_obs, ess_threshold, silverman_shrink;
+  int32_t seed;
+};
+constexpr char kCkptMagic[8] = {'G', 'P', 'U', 'B', 'P', 'F', 0, 1};
+
+size_t ckpt_bytes(const Impl* m) {
+  return sizeof(CkptHeader) + sizeof(DevState) + (size_t)m->plan.G * sizeof(int32_t) +
+         2 * (size_t)m->plan.N * sizeof(float);
+}
+}  // namespace
+
+size_t gpu_bpf_checkpoint_bytes(GpuBpfState* s) {
+  Impl* m = impl_of(s);
+  if (!m) { set_err(BPF_ERR_STATE); return 0; }
+  return ckpt_bytes(m);
+}
+
+int gpu_bpf_save(GpuBpfState* s, void* buf, size_t cap) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  if (!buf || cap < ckpt_bytes(m)) return set_err(BPF_ERR_ARG);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(m->stream));
+  unsigned char* out = static_cast<unsigned char*>(buf);
+  CkptHeader h{};
+  std::memcpy(h.magic, kCkptMagic, sizeof(h.magic));
+  h.version = 1;
+  h.devstate_bytes = (uint32_t)sizeof(DevState);
+  h.n = m->plan.N; h.G = m->plan.G;
+  h.rho = s->rho; h.sigma_z = s->sigma_z; h.mu = s->mu; h.nu_state = s->nu_state; h.nu_obs = s->nu_obs;
+  h.ess_threshold = s->ess_threshold; h.silverman_shrink = s->silverman_shrink;
+  h.seed = m->seed;
+  std::memcpy(out, &h, sizeof(h));
+  out += sizeof(h);
+  DevState st;
+  CK(cudaMemcpy(&st, m->plan.st, sizeof(DevState), cudaMemcpyDeviceToHost));
+  std::memcpy(out, &st, sizeof(st));
+  out += sizeof(st);
+  const size_t nb = (size_t)m->plan.N * sizeof(float);
+  CK(cudaMemcpy(out, m->plan.nexp, (size_t)m->plan.G * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  out += (size_t)m->plan.G * sizeof(int32_t);
+  CK(cudaMemcpy(out, st.cur ? m->plan.h1 : m->plan.h0, nb, cudaMemcpyDeviceToHost));
+  out += nb;
+  CK(cudaMemcpy(out, m->plan.w, nb, cudaMemcpyDeviceToHost));
+  return BPF_OK;
+}
+
+int gpu_bpf_load(GpuBpfState* s, const void* buf, size_t len) {
+  Impl* m = impl_of(s);
+  if (!m) return set_err(BPF_ERR_STATE);
+  if (!buf || len < ckpt_bytes(m)) return set_err(BPF_ERR_ARG);
+  const unsigned char* in = static_cast<const unsigned char*>(buf);
+  CkptHeader h;
+  std::memcpy(&h, in, sizeof(h));
+  if (std::memcmp(h.magic, kCkptMagic, sizeof(h.magic)) != 0 || h.version != 1 ||
+      h.devstate_bytes != (uint32_t)sizeof(DevState) || h.n != m->plan.N || h.G != m->plan.G)
+    return set_err(BPF_ERR_ARG);
+  if (!std::isfinite(h.rho) || !(std::fabs(h.rho) < 1.0f) || !(h.sigma_z > 0.0f) || !std::isfinite(h.mu) ||
+      !(h.nu_obs >= 0.0f) || !std::isfinite(h.nu_obs) || !(h.nu_state == 0.0f || h.nu_state >= 0.5f))
+    return set_err(BPF_ERR_ARG);
+  int rc = ensure_device(m);
+  if (rc) return rc;
+  in += sizeof(h);
+  DevState st;
+  std::memcpy(&st, in, sizeof(st));
+  in += sizeof(st);
+  const size_t nb = (size_t)m->plan.N * sizeof(float);
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(m->plan.st, &st, sizeof(DevState), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m->plan.nexp, in, (size_t)m->plan.G * sizeof(int32_t), cudaMemcpyHostToDevice));
+  in += (size_t)m->plan.G * sizeof(int32_t);
+  CK(cudaMemcpy(st.cur ? m->plan.h1 : m->plan.h0, in, nb, cudaMemcpyHostToDevice));
+  in += nb;
+  CK(cudaMemcpy(m->plan.w, in, nb, cudaMemcpyHostToDevice));
+  s->rho = h.rho; s->sigma_z = h.sigma_z; s->mu = h.mu; s->nu_state = h.nu_state; s->nu_obs = h.nu_obs;
+  s->ess_threshold = h.ess_threshold; s->silverman_shrink = h.silverman_shrink;
+  m->seed = h.seed;
+  m->obs = ObsModel{};
+  m->obs.nu = h.nu_obs;
+  if (h.nu_obs > 0.0f) {
+    m->obs.c_obs = (float)(std::lgamma((h.nu_obs + 1.0) / 2.0) - std::lgamma(h.nu_obs / 2.0) -
+                           0.5 * std::log(h.nu_obs * 3.14159265358979323846));
+    m->obs.inv_nu = 1.0f / h.nu_obs;
+    m->obs.nu_p1h = (h.nu_obs + 1.0f) * 0.5f;
+  }
+  // captured graphs hold the observation model and parameters of their capture: drop them
+  if (m->graph) { cudaGraphExecDestroy(m->graph); m->graph = nullptr; }
+  if (m->dgraph) { cudaGraphExecDestroy(m->dgraph); m->dgraph = nullptr; }
+  if (m->tgraph) { cudaGraphExecDestroy(m->tgraph); m->tgraph = nullptr; }
+  if (m->t_g) { cudaGraphDestroy(m->t_g); m->t_g = nullptr; }
+  m->ticks_enqueued = 0;
+  m->last_in_map = false;
+  m->grad_count = 0;
+  s->timestep = st.tick;
+  s->resample_count = st.resample_count;
+  s->did_resample = st.resampled_prev;
   return BPF_OK;
 }
 
@@ -915,15 +1027,15 @@ static int debug_probe(int seed, int n, int t, uint32_t* out, float* norm) {
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return set_err(BPF_ERR_NODEVICE); }
   uint32_t* d_out = nullptr;
   float* d_norm = nullptr;
-  CK(cudaMalloc(&d_out, n * sizeof(uint32_t)));
-  CK(cudaMalloc(&d_norm, n * sizeof(float)));
+  CK(bpf_malloc(&d_out, n * sizeof(uint32_t)));
+  CK(bpf_malloc(&d_norm, n * sizeof(float)));
   cudaError_t e = launch_debug_pcg(seed, n, t, d_out, d_norm, 0);
   g_launches += 1;
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e == cudaSuccess && out) e = cudaMemcpy(out, d_out, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && norm) e = cudaMemcpy(norm, d_norm, n * sizeof(float), cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
-  cudaFree(d_norm);
+  bpf_free(d_out);
+  bpf_free(d_norm);
   CK(e);
   return BPF_OK;
 }

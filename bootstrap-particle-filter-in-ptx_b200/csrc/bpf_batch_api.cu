@@ -32,13 +32,13 @@ void free_batch(GpuBpfBatch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->ggraph) cudaGraphExecDestroy(b->ggraph);
   if (b->sgraph) cudaGraphExecDestroy(b->sgraph);
-  cudaFree(b->d_st); cudaFree(b->d_sth); cudaFree(b->d_stw); cudaFree(b->d_stoff); cudaFree(b->d_tick);
-  cudaFree(b->d_scounters);
-  for (int c = 0; c < kClasses; ++c) cudaFree(b->g_tape[c]);
-  cudaFree(b->d_AB);
-  cudaFree(b->d_nzoff);
-  cudaFree(b->d_filters); cudaFree(b->d_order); cudaFree(b->d_counters);
-  cudaFree(b->d_hfinal); cudaFree(b->d_resamples); cudaFree(b->d_loglik); cudaFree(b->d_y);
+  bpf_free(b->d_st); bpf_free(b->d_sth); bpf_free(b->d_stw); bpf_free(b->d_stoff); bpf_free(b->d_tick);
+  bpf_free(b->d_scounters);
+  for (int c = 0; c < kClasses; ++c) bpf_free(b->g_tape[c]);
+  bpf_free(b->d_AB);
+  bpf_free(b->d_nzoff);
+  bpf_free(b->d_filters); bpf_free(b->d_order); bpf_free(b->d_counters);
+  bpf_free(b->d_hfinal); bpf_free(b->d_resamples); bpf_free(b->d_loglik); bpf_free(b->d_y);
   for (int c = 0; c < kClasses; ++c) {
     if (b->cls_stream[c]) cudaStreamDestroy(b->cls_stream[c]);
     if (b->join[c]) cudaEventDestroy(b->join[c]);
@@ -133,18 +133,18 @@ int prepare_grad(GpuBpfBatch* b, int T) {
     b->g_grid[c] = std::max(1, std::min(b->class_cnt[c], b->sms * occ));
     const size_t need = slot_layout(kClassMaxN[c], T).total * (size_t)b->g_grid[c];
     if (b->g_tape_bytes[c] < need) {
-      cudaFree(b->g_tape[c]);
+      bpf_free(b->g_tape[c]);
       b->g_tape[c] = nullptr;
       b->g_tape_bytes[c] = 0;
-      BCK(cudaMalloc(&b->g_tape[c], need));
+      BCK(bpf_malloc(&b->g_tape[c], need));
       b->g_tape_bytes[c] = need;
     }
   }
   if (b->ab_T < T + 1) {
-    cudaFree(b->d_AB);
+    bpf_free(b->d_AB);
     b->d_AB = nullptr;
     b->ab_T = 0;
-    BCK(cudaMalloc(&b->d_AB, (size_t)(T + 1) * sizeof(ulonglong2)));
+    BCK(bpf_malloc(&b->d_AB, (size_t)(T + 1) * sizeof(ulonglong2)));
     std::vector<ulonglong2> ab(T + 1);
     unsigned long long At = 1ull, Bt = 0ull;
     for (int t = 0; t <= T; ++t) {
@@ -194,12 +194,12 @@ int batch_prepare_steps(GpuBpfBatch* b) {
   std::vector<long long> off(b->B);
   long long tot = 0;
   for (int i = 0; i < b->B; ++i) { off[i] = tot; tot += (b->n_of[i] + 3) & ~3; }
-  BCK(cudaMalloc(&b->d_st, (size_t)b->B * sizeof(BatchFilterState)));
-  BCK(cudaMalloc(&b->d_sth, (size_t)tot * sizeof(float)));
-  BCK(cudaMalloc(&b->d_stw, (size_t)tot * sizeof(float)));
-  BCK(cudaMalloc(&b->d_stoff, (size_t)b->B * sizeof(long long)));
-  BCK(cudaMalloc(&b->d_tick, sizeof(int)));
-  BCK(cudaMalloc(&b->d_scounters, (kClasses + 1) * sizeof(int)));
+  BCK(bpf_malloc(&b->d_st, (size_t)b->B * sizeof(BatchFilterState)));
+  BCK(bpf_malloc(&b->d_sth, (size_t)tot * sizeof(float)));
+  BCK(bpf_malloc(&b->d_stw, (size_t)tot * sizeof(float)));
+  BCK(bpf_malloc(&b->d_stoff, (size_t)b->B * sizeof(long long)));
+  BCK(bpf_malloc(&b->d_tick, sizeof(int)));
+  BCK(bpf_malloc(&b->d_scounters, (kClasses + 1) * sizeof(int)));
   BCK(cudaMemcpy(b->d_stoff, off.data(), (size_t)b->B * sizeof(long long), cudaMemcpyHostToDevice));
   BCK(cudaMemset(b->d_tick, 0, sizeof(int)));
   BCK(cudaMemset(b->d_scounters, 0, (kClasses + 1) * sizeof(int)));
@@ -371,12 +371,12 @@ GpuBpfBatch* gpu_bpf_batch_create(const BpfBatchFilter* filters, int n_filters, 
       return fail(BPF_ERR_CUDA);
   }
   if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return fail(BPF_ERR_CUDA);
-  if (cudaMalloc(&b->d_filters, n_filters * sizeof(BatchFilterDev)) != cudaSuccess ||
-      cudaMalloc(&b->d_order, n_filters * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&b->d_counters, kClasses * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&b->d_hfinal, n_filters * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&b->d_resamples, n_filters * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&b->d_loglik, n_filters * sizeof(double)) != cudaSuccess)
+  if (bpf_malloc(&b->d_filters, n_filters * sizeof(BatchFilterDev)) != cudaSuccess ||
+      bpf_malloc(&b->d_order, n_filters * sizeof(int)) != cudaSuccess ||
+      bpf_malloc(&b->d_counters, kClasses * sizeof(int)) != cudaSuccess ||
+      bpf_malloc(&b->d_hfinal, n_filters * sizeof(float)) != cudaSuccess ||
+      bpf_malloc(&b->d_resamples, n_filters * sizeof(int)) != cudaSuccess ||
+      bpf_malloc(&b->d_loglik, n_filters * sizeof(double)) != cudaSuccess)
     return fail(BPF_ERR_ALLOC);
   if (cudaMemcpy(b->d_filters, tab.data(), n_filters * sizeof(BatchFilterDev), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->d_order, order.data(), n_filters * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -568,10 +568,10 @@ int gpu_bpf_batch_run(GpuBpfBatch* b, const float* y, int n_ticks, double* logli
   int rc = ensure_device_b(b);
   if (rc) return rc;
   if (b->y_cap < n_ticks) {
-    cudaFree(b->d_y);
+    bpf_free(b->d_y);
     b->d_y = nullptr;
     b->y_cap = 0;
-    BCK(cudaMalloc(&b->d_y, n_ticks * sizeof(float)));
+    BCK(bpf_malloc(&b->d_y, n_ticks * sizeof(float)));
     b->y_cap = n_ticks;
   }
   BCK(cudaMemcpyAsync(b->d_y, y, n_ticks * sizeof(float), cudaMemcpyHostToDevice, b->stream));
@@ -617,7 +617,7 @@ int gpu_bpf_batch_run_correlated(GpuBpfBatch* b, const float* y_dev, int n_ticks
     BCK(cudaStreamSynchronize(b->stream));           // the old offsets may be in use
     std::vector<long long> off(b->B);
     for (int i = 0; i < b->B; ++i) off[i] = gpu_bpf_batch_noise_offset(b, i, n_ticks);
-    if (!b->d_nzoff) BCK(cudaMalloc(&b->d_nzoff, (size_t)b->B * sizeof(long long)));
+    if (!b->d_nzoff) BCK(bpf_malloc(&b->d_nzoff, (size_t)b->B * sizeof(long long)));
     BCK(cudaMemcpy(b->d_nzoff, off.data(), (size_t)b->B * sizeof(long long), cudaMemcpyHostToDevice));
     b->nz_T = n_ticks;
   }
@@ -651,8 +651,8 @@ int gpu_bpf_batch_autotune(GpuBpfBatch* b, const float* y, int n_ticks, const ch
   const std::string key = gpu_key(b->device);
   float* d_y = nullptr;
   double* d_ll = nullptr;
-  BCK(cudaMalloc(&d_y, n_ticks * sizeof(float)));
-  if (cudaMalloc(&d_ll, b->B * sizeof(double)) != cudaSuccess) { cudaFree(d_y); return bpf_record_error(BPF_ERR_ALLOC); }
+  BCK(bpf_malloc(&d_y, n_ticks * sizeof(float)));
+  if (bpf_malloc(&d_ll, b->B * sizeof(double)) != cudaSuccess) { bpf_free(d_y); return bpf_record_error(BPF_ERR_ALLOC); }
   cudaMemcpy(d_y, y, n_ticks * sizeof(float), cudaMemcpyHostToDevice);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -691,8 +691,8 @@ int gpu_bpf_batch_autotune(GpuBpfBatch* b, const float* y, int n_ticks, const ch
   configure_classes(b);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(d_y);
-  cudaFree(d_ll);
+  bpf_free(d_y);
+  bpf_free(d_ll);
   if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
   return result;
 }

@@ -118,9 +118,9 @@ void free_grad(GpuBpfGrad* g) {
   if (g->fgraph) cudaGraphExecDestroy(g->fgraph);
   if (g->bgraph) cudaGraphExecDestroy(g->bgraph);
   plan_free(g->plan);
-  cudaFree(g->csr); cudaFree(g->ckpt); cudaFree(g->aux); cudaFree(g->rec); cudaFree(g->seg);
-  cudaFree(g->lam[0]); cudaFree(g->lam[1]); cudaFree(g->acc);
-  cudaFree(g->rs[0]); cudaFree(g->rs[1]); cudaFree(g->part); cudaFree(g->per_tick); cudaFree(g->rtotal);
+  bpf_free(g->csr); bpf_free(g->ckpt); bpf_free(g->aux); bpf_free(g->rec); bpf_free(g->seg);
+  bpf_free(g->lam[0]); bpf_free(g->lam[1]); bpf_free(g->acc);
+  bpf_free(g->rs[0]); bpf_free(g->rs[1]); bpf_free(g->part); bpf_free(g->per_tick); bpf_free(g->rtotal);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }
@@ -264,7 +264,7 @@ GpuBpfGrad* gpu_bpf_grad_create(int n_particles, int max_ticks, int checkpoint_e
   g->ckpt_stride = (size_t)g->plan.G * kTile;
   g->pass2_grid = pass2_grid_size(g->device);
   const size_t N4 = (size_t)g->N4;
-  auto al = [&](auto** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
+  auto al = [&](auto** p, size_t bytes) { if (e == cudaSuccess) e = bpf_malloc(p, bytes); };
   al(&g->csr, (size_t)max_ticks * N4 * sizeof(int32_t));
   al(&g->ckpt, (size_t)g->n_ckpt * g->ckpt_stride * sizeof(float));
   al(&g->aux, (size_t)max_ticks * sizeof(float2));
@@ -351,7 +351,7 @@ int gpu_bpf_grad_replay(GpuBpfGrad* g, double mu, double rho, double sigma_z, do
   if (rc) return rc;
   const size_t N4 = (size_t)g->N4;
   cudaError_t e = cudaSuccess;
-  auto al = [&](auto** p, size_t bytes) { if (e == cudaSuccess && !*p) e = cudaMalloc(p, bytes); };
+  auto al = [&](auto** p, size_t bytes) { if (e == cudaSuccess && !*p) e = bpf_malloc(p, bytes); };
   al(&g->rs[0], 4 * N4 * sizeof(double));
   al(&g->rs[1], 4 * N4 * sizeof(double));
   al(&g->part, (size_t)g->T_max * g->G1 * 5 * sizeof(double));

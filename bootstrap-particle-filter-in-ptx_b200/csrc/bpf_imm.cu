@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/gpu_bpf.h"
+#include "bpf_alloc.cuh"
 
 int bpf_record_error(int code);
 
@@ -59,7 +60,7 @@ struct ImmImpl {
 void free_impl(ImmImpl* m) {
   if (!m) return;
   if (m->batch) gpu_bpf_batch_destroy(m->batch);
-  cudaFreeHost(m->y_pin); cudaFreeHost(m->dll_pin); cudaFreeHost(m->hm_pin);
+  bpf_free_host(m->y_pin); bpf_free_host(m->dll_pin); bpf_free_host(m->hm_pin);
   delete m;
 }
 
@@ -110,9 +111,9 @@ GpuImmState* gpu_imm_create(const ImmModelParams* models, int n_models, int n_pa
     if (!m->batch) return fail(gpu_bpf_last_error());
     if (cudaGetDevice(&m->device) != cudaSuccess) return fail(BPF_ERR_CUDA);
     m->stream = (cudaStream_t)gpu_bpf_batch_stream(m->batch);
-    if (cudaHostAlloc(&m->y_pin, sizeof(float), cudaHostAllocMapped) != cudaSuccess ||
-        cudaHostAlloc(&m->dll_pin, K * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
-        cudaHostAlloc(&m->hm_pin, K * sizeof(float), cudaHostAllocMapped) != cudaSuccess) {
+    if (bpf_host_alloc(&m->y_pin, sizeof(float), cudaHostAllocMapped) != cudaSuccess ||
+        bpf_host_alloc(&m->dll_pin, K * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
+        bpf_host_alloc(&m->hm_pin, K * sizeof(float), cudaHostAllocMapped) != cudaSuccess) {
       cudaGetLastError();
       return fail(BPF_ERR_ALLOC);
     }

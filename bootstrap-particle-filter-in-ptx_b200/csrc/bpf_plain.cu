@@ -1293,7 +1293,7 @@ cudaError_t plan_alloc(Plan& p, int N) {
   p.max_items = p.G + (N + kOutChunk - 1) / kOutChunk + 1;
   const size_t npad = (size_t)p.G * kTile;
   cudaError_t e = cudaSuccess;
-  auto al = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(ptr, bytes); };
+  auto al = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = bpf_malloc(ptr, bytes); };
   al(&p.h0, npad * sizeof(float));
   al(&p.h1, npad * sizeof(float));
   al(&p.w, npad * sizeof(float));
@@ -1314,10 +1314,10 @@ cudaError_t plan_alloc(Plan& p, int N) {
 }
 
 void plan_free(Plan& p) {
-  cudaFree(p.h0); cudaFree(p.h1); cudaFree(p.w);
-  cudaFree(p.nexp); cudaFree(p.E); cudaFree(p.rec); cudaFree(p.rec2);
-  cudaFree(p.P); cudaFree(p.ofirst); cudaFree(p.items); cudaFree(p.st);
-  cudaFree(p.jpart); cudaFree(p.jticket);
+  bpf_free(p.h0); bpf_free(p.h1); bpf_free(p.w);
+  bpf_free(p.nexp); bpf_free(p.E); bpf_free(p.rec); bpf_free(p.rec2);
+  bpf_free(p.P); bpf_free(p.ofirst); bpf_free(p.items); bpf_free(p.st);
+  bpf_free(p.jpart); bpf_free(p.jticket);
   p = Plan{};
 }
 

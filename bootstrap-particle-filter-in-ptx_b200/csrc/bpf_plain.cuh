@@ -13,6 +13,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "bpf_alloc.cuh"
 #include "bpf_common.cuh"
 #include "../../include/gpu_bpf.h"
 

@@ -145,12 +145,12 @@ void free_smc2(GpuBpfSmc2* s) {
   if (!s) return;
   if (s->cur) gpu_bpf_batch_destroy(s->cur);
   if (s->prop) gpu_bpf_batch_destroy(s->prop);
-  cudaFree(s->d_y); cudaFree(s->d_idx); cudaFree(s->d_mask); cudaFree(s->d_seed);
-  cudaFree(s->s_tab); cudaFree(s->s_st); cudaFree(s->s_h); cudaFree(s->s_w);
-  cudaFreeHost(s->y_pin); cudaFreeHost(s->dll_pin); cudaFreeHost(s->i_pin); cudaFreeHost(s->st_pin);
-  cudaFreeHost(s->ll_pin);
-  cudaFree(s->d_nz); cudaFree(s->d_off_cur); cudaFree(s->d_off_oth); cudaFree(s->d_off_src);
-  cudaFreeHost(s->off_pin);
+  bpf_free(s->d_y); bpf_free(s->d_idx); bpf_free(s->d_mask); bpf_free(s->d_seed);
+  bpf_free(s->s_tab); bpf_free(s->s_st); bpf_free(s->s_h); bpf_free(s->s_w);
+  bpf_free_host(s->y_pin); bpf_free_host(s->dll_pin); bpf_free_host(s->i_pin); bpf_free_host(s->st_pin);
+  bpf_free_host(s->ll_pin);
+  bpf_free(s->d_nz); bpf_free(s->d_off_cur); bpf_free(s->d_off_oth); bpf_free(s->d_off_src);
+  bpf_free_host(s->off_pin);
   delete s;
 }
 
@@ -346,8 +346,8 @@ GpuBpfSmc2* gpu_bpf_smc2_create(int n_theta, int n_particles, int max_ticks, con
   s->stream = s->cur->stream;
   const size_t nh = (size_t)n_theta * ((n_particles + 3) & ~3);
   cudaError_t e = cudaSuccess;
-  auto al = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(ptr, bytes); };
-  auto ah = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = cudaMallocHost(ptr, bytes); };
+  auto al = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = bpf_malloc(ptr, bytes); };
+  auto ah = [&](auto** ptr, size_t bytes) { if (e == cudaSuccess) e = bpf_malloc_host(ptr, bytes); };
   al(&s->d_y, (size_t)max_ticks * sizeof(float));
   al(&s->d_idx, n_theta * sizeof(int));
   al(&s->d_mask, n_theta * sizeof(int));
@@ -357,7 +357,7 @@ GpuBpfSmc2* gpu_bpf_smc2_create(int n_theta, int n_particles, int max_ticks, con
   al(&s->s_h, nh * sizeof(float));
   al(&s->s_w, nh * sizeof(float));
   ah(&s->y_pin, sizeof(float));
-  if (e == cudaSuccess) e = cudaHostAlloc(&s->dll_pin, n_theta * sizeof(double), cudaHostAllocMapped);
+  if (e == cudaSuccess) e = bpf_host_alloc(&s->dll_pin, n_theta * sizeof(double), cudaHostAllocMapped);
   if (e == cudaSuccess) e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_dll), s->dll_pin, 0);
   ah(&s->i_pin, 2 * n_theta * sizeof(int));
   ah(&s->st_pin, n_theta * sizeof(BatchFilterState));
@@ -472,15 +472,15 @@ int gpu_bpf_smc2_set_cpmmh_rho(GpuBpfSmc2* s, float rho) {
   const int M = s->n_theta;
   if (on && !s->d_nz) {
     s->area = (long long)s->max_ticks * batch_noise_stride(s->n);
-    cudaError_t e = cudaMalloc(&s->d_nz, (size_t)(2LL * M * s->area) * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_off_cur, M * sizeof(long long));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_off_oth, M * sizeof(long long));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_off_src, M * sizeof(long long));
-    if (e == cudaSuccess) e = cudaMallocHost(&s->off_pin, 3 * M * sizeof(long long));
+    cudaError_t e = bpf_malloc(&s->d_nz, (size_t)(2LL * M * s->area) * sizeof(float));
+    if (e == cudaSuccess) e = bpf_malloc(&s->d_off_cur, M * sizeof(long long));
+    if (e == cudaSuccess) e = bpf_malloc(&s->d_off_oth, M * sizeof(long long));
+    if (e == cudaSuccess) e = bpf_malloc(&s->d_off_src, M * sizeof(long long));
+    if (e == cudaSuccess) e = bpf_malloc_host(&s->off_pin, 3 * M * sizeof(long long));
     if (e != cudaSuccess) {
       cudaGetLastError();
-      cudaFree(s->d_nz); cudaFree(s->d_off_cur); cudaFree(s->d_off_oth); cudaFree(s->d_off_src);
-      cudaFreeHost(s->off_pin);
+      bpf_free(s->d_nz); bpf_free(s->d_off_cur); bpf_free(s->d_off_oth); bpf_free(s->d_off_src);
+      bpf_free_host(s->off_pin);
       s->d_nz = nullptr; s->d_off_cur = s->d_off_oth = s->d_off_src = nullptr; s->off_pin = nullptr;
       return bpf_record_error(BPF_ERR_ALLOC);
     }

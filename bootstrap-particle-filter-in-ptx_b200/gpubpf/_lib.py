@@ -133,9 +133,15 @@ SIGNATURES = {
     "gpu_bpf_get_resample_inputs": (_i, [P_STATE, C.POINTER(_f), C.POINTER(C.c_int32), C.POINTER(C.c_uint32)]),
     "gpu_bpf_profile": (_i, [P_STATE, _i]),
     "gpu_bpf_set_fused_small": (_i, [P_STATE, _i]),
+    "gpu_bpf_checkpoint_bytes": (C.c_size_t, [P_STATE]),
+    "gpu_bpf_save": (_i, [P_STATE, _vp, C.c_size_t]),
+    "gpu_bpf_load": (_i, [P_STATE, _vp, C.c_size_t]),
     "gpu_bpf_profile_read": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), C.POINTER(_i),
                                   C.POINTER(_i)]),
     "gpu_bpf_launch_count": (C.c_longlong, []),
+    "gpu_bpf_debug_fail_alloc": (_i, [C.c_longlong]),
+    "gpu_bpf_debug_alloc_count": (C.c_longlong, []),
+    "gpu_bpf_debug_live_allocs": (C.c_longlong, []),
     "gpu_bpf_get_learning_sums": (_i, [P_STATE, C.POINTER(_d), C.POINTER(_i)]),
     "gpu_bpf_run_static": (_i, [_i, _f, _f, _f, _f, _i, _f, _vp, _i, _vp, _vp]),
     # batched filters

@@ -163,6 +163,18 @@ class GpuBpf:
         check(self._lib.gpu_bpf_get_resample_inputs(self._s, w, te, C.byref(u)), "gpu_bpf_get_resample_inputs")
         return w, te, u.value
 
+    def save(self) -> bytes:
+        """Checkpoint of the filter's whole state (gpu_bpf_save)."""
+        n = self._lib.gpu_bpf_checkpoint_bytes(self._s)
+        buf = (C.c_ubyte * n)()
+        check(self._lib.gpu_bpf_save(self._s, buf, n), "gpu_bpf_save")
+        return bytes(buf)
+
+    def load(self, blob: bytes) -> None:
+        """Restore a checkpoint made by save() of a filter with the same particle count."""
+        buf = (C.c_ubyte * len(blob)).from_buffer_copy(blob)
+        check(self._lib.gpu_bpf_load(self._s, buf, len(blob)), "gpu_bpf_load")
+
     def set_fused_small(self, enable: bool = True) -> None:
         """Fused one-launch ticks for filters of at most 16384 particles (default on)."""
         check(self._lib.gpu_bpf_set_fused_small(self._s, int(bool(enable))), "gpu_bpf_set_fused_small")

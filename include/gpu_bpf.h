@@ -212,6 +212,23 @@ int gpu_bpf_get_ancestors(GpuBpfState* state, int32_t* anc_out);
 int gpu_bpf_get_resample_inputs(GpuBpfState* state, float* w_out, int32_t* tile_exp_out,
                                 uint32_t* u23_out);
 
+/* Checkpoint / resume (addition). A checkpoint holds the filter's whole
+ * stochastic state: particles, carried log2-weights and tile exponents, the
+ * device tick state (tick index, PCG32 stream constants, resampling-uniform
+ * stream, log-likelihood sums, Silverman and online-learning state) and the
+ * parameters (rho, sigma_z, mu, nu_state, nu_obs, ess_threshold,
+ * silverman_shrink, seed). The PCG32 streams are counter-based, so no per-particle
+ * RNG state is stored. gpu_bpf_save writes gpu_bpf_checkpoint_bytes(state)
+ * bytes into buf (waits for the filter's stream); gpu_bpf_load restores them into
+ * a filter with the same n_particles (BPF_ERR_ARG otherwise), after which the
+ * filter continues exactly as the saved one would have. Host-side settings
+ * (online-learning schedule, ancestor recording, log-likelihood semantics,
+ * profiling) are not part of the checkpoint; the result of the tick before the
+ * save is not either (gpu_bpf_get_result needs a tick after the load). */
+size_t gpu_bpf_checkpoint_bytes(GpuBpfState* state);
+int    gpu_bpf_save(GpuBpfState* state, void* buf, size_t cap);
+int    gpu_bpf_load(GpuBpfState* state, const void* buf, size_t len);
+
 /* Fused small-filter ticks (addition): a filter of at most 16384 particles runs
  * each tick as one launch of one CTA (pass 1, the resampling decision and the
  * resampling without leaving the SM), and a captured run of ticks
@@ -531,6 +548,17 @@ int         gpu_bpf_smc2_get_last_update(GpuBpfSmc2* smc2, double* dll, int* res
  * seen; layout of gpu_bpf_batch_run_correlated's areas) into the host array out. Needs
  * rho > 0. */
 int         gpu_bpf_smc2_get_noise(GpuBpfSmc2* smc2, int j, int n_ticks, float* out);
+
+/* Allocation fault injection (addition; testing aid). Every device and pinned
+ * allocation of the library goes through one set of wrappers. After
+ * gpu_bpf_debug_fail_alloc(k) the next k allocations succeed and the one after
+ * them fails as an out-of-memory allocation would (once; k < 0 disarms), so the
+ * error path of any create function can be exercised on the host without a GPU
+ * fault. gpu_bpf_debug_alloc_count: allocations attempted since the library was
+ * loaded; gpu_bpf_debug_live_allocs: allocations not yet freed. */
+int       gpu_bpf_debug_fail_alloc(long long k);
+long long gpu_bpf_debug_alloc_count(void);
+long long gpu_bpf_debug_live_allocs(void);
 
 /* Number of kernel launches this library has issued (all filters). */
 long long gpu_bpf_launch_count(void);
