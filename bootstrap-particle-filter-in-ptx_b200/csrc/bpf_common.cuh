@@ -26,7 +26,7 @@ constexpr int kThreads   = 256;              // threads per CTA (pass 1 and pass
 constexpr int kPerThread = 16;               // particles per thread
 constexpr int kTile      = kThreads * kPerThread;   // 4096 particles per tile
 constexpr int kOutChunk  = 2 * kTile;        // outputs per pass-2 work item (2x the mean per tile)
-constexpr int kPlanThreads = 512;            // threads of the single-CTA plan kernel
+constexpr int kPlanThreads = 1024;           // threads of the single-CTA plan kernel
 constexpr int kPlanSmemTiles = 12800;        // tiles the plan kernel stages in shared memory (N <= 52.4M)
 constexpr int kSmallTiles = 4;              // tiles of the fused small-filter tick
 constexpr int kSmallMaxN  = kSmallTiles * kTile;    // 16384 particles

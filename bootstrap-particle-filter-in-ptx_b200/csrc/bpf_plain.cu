@@ -630,6 +630,18 @@ __device__ __noinline__ unsigned long long udiv_slow(unsigned long long a, unsig
   return udiv_fp64(a, d);
 }
 
+// Exact count of targets up to element `upto` of a thread's 16 staged log2-weights d:
+// #{m >= 0 : R0 + m D <= sum_{i <= upto} floor(2^d_i 2^50)}, at most cap. The rare path of
+// the FP32 estimate in pass 2's child count.
+__device__ __noinline__ int exact_count(const float* d, int upto, unsigned long long R0, unsigned long long D,
+                                        int cap) {
+  unsigned long long l = 0ull;
+  for (int i = 0; i <= upto; ++i) l += fix_weight(tile_weight(d[i]));
+  if (l < R0) return 0;
+  const unsigned long long c = udiv_fp64(l - R0, D) + 1ull;
+  return c >= (unsigned long long)cap ? cap : (int)c;
+}
+
 __device__ __forceinline__ void pass2_fetch(const Plan& p, const float* hsrc, int it, unsigned char* buf,
                                             uint64_t* bar) {
   const int k = p.items[it].x;
@@ -720,19 +732,27 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     // Element j owns the output slots [q_{j-1}, q_j): the targets t_q below its CDF value
     // C_j = P_k + (A_j >> r) (A_j its tile-local inclusive prefix) and not below the previous
     // element's. In the tile's own frame, C_j > t_q  <=>  A_j >= ((t_q - P_k + 1) << r), and
-    // consecutive targets are delta << r apart there, so the count needs neither the shift nor
-    // P_k per element: each thread tracks its next target's threshold relative to its first
-    // element's exclusive prefix (capped, see kThCap). The count has no branch per element (a
-    // warp vote guards the division of parents with more than four children); each element
-    // with children writes one start mark, at its first slot inside this window.
+    // consecutive targets are D = delta << r apart there. Relative to the thread's first
+    // element (exclusive prefix A_s, first target q0 at relative threshold R0), the count up to
+    // element j is c_j = #{m >= 0 : R0 + m D <= l_j}, l_j = A_j - A_s, so q_j = min(q0 + c_j, N).
+    // c_j is estimated in FP32 from the FP32 running sum of the weights, with a bound on the
+    // estimate's error (every rounding and the fixed-point truncation counted): when no integer
+    // boundary lies within the bound the estimate's floor is exact, otherwise (a warp vote)
+    // the element recounts in exact 64-bit integers. Each element with children writes one
+    // start mark, at its first slot inside this window.
     const int lane = tid & 31, warp = tid >> 5;
-    int q = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
-    unsigned long long th = kThCap, D = kThCap;
-    if (massive && q < N) {
-      const unsigned long long m = base + (unsigned long long)q * delta - Pk + 1ull;   // t_q >= P_k
-      if (m <= (~0ull >> r)) th = min((m << r) - excl, kThCap);                           // (m << r) > excl
+    const int q0 = targets_below(Pk + shr64(excl, r), base, delta, magic, N);
+    unsigned long long R0 = kThCap, D = kThCap;      // capped: never reached (see kThCap)
+    if (massive && q0 < N) {
+      const unsigned long long m = base + (unsigned long long)q0 * delta - Pk + 1ull;   // t_q0 >= P_k
+      if (m <= (~0ull >> r)) R0 = min((m << r) - excl, kThCap);                          // (m << r) > excl
       if (delta <= (kThCap >> r)) D = delta << r;
     }
+    const float R0w = (float)R0 * 0x1p-50f;           // in units of the tile's largest weight
+    const float invDw = 1.0f / ((float)D * 0x1p-50f);
+    // bound on the estimate's error: (lf + R0w) 2^-18 / Dw + 2^-44 / Dw + |x| 2^-21
+    const float eL = 0x1p-18f * invDw, e0 = fmaf(R0w, eL, 0x1p-44f * invDw);
+    const float* wsel = ws + tid * kPerThread;
     int32_t* csr = (a.csr && (item.w & 1)) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
     // Compile-time variants: WHOLE (the item holds every output of the tile, so each
     // counted child lands in the window), TAPE (first-child list for the gradient tape).
@@ -740,8 +760,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     auto count_children = [&](auto whole_tag, auto tape_tag) {
       constexpr bool WHOLE = decltype(whole_tag)::value;
       constexpr bool TAPE = decltype(tape_tag)::value;
-      const unsigned long long D2 = 2ull * D, D3 = 3ull * D, D4 = 4ull * D;
-      unsigned long long acc = 0ull;
+      float lf = 0.0f;
+      int qp = q0;                                   // first slot of the next element's children
 #pragma unroll 1
       for (int g = 0; g < 4; ++g) {
         const float4 f4 = wt[g];
@@ -749,19 +769,21 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int j = tid * kPerThread + 4 * g + e;
-          if (TAPE && j < nA) csr[j] = q;
-          acc += fix_weight(tile_weight(ff[e]));
-          const bool ge = acc >= th;
-          const unsigned long long diff = acc - th;
-          int c = ge ? 1 + (int)(diff >= D) + (int)(diff >= D2) + (int)(diff >= D3) : 0;
-          const bool slow = ge && diff >= D4;
-          if (__any_sync(0xffffffffu, slow)) {
-            if (slow) c = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
+          if (TAPE && j < nA) csr[j] = qp;
+          lf += tile_weight(ff[e]);
+          const float x = (lf - R0w) * invDw;
+          const float fl = floorf(x);
+          const float fr = x - fl;                       // exact
+          const float err = fmaf(lf, eL, fmaf(fabsf(x), 0x1p-21f, e0));
+          const bool recount = !(fr > err && fr < 1.0f - err && fl < 0x1p22f);
+          // floor(x) + 1 for x >= 0, 0 for x < 0 (from the float's bits: fl + 2^23 is exact)
+          int c = max(__float_as_int(fl + 0x1p23f) - 0x4AFFFFFF, 0);
+          if (__any_sync(0xffffffffu, recount)) {
+            if (recount) c = exact_count(wsel, 4 * g + e, R0, D, N);
           }
-          const int q1 = min(q + c, N);
-          if (c > 0 && (WHOLE || (q < ob && q1 > oa))) marks[(WHOLE ? q : max(q, oa)) - wa] = (unsigned short)(j + 1);
-          th = (q1 >= N) ? kThCap : th + (unsigned long long)c * D;
-          q = q1;
+          const int q1 = min(q0 + c, N);
+          if (q1 > qp && (WHOLE || (qp < ob && q1 > oa))) marks[(WHOLE ? qp : max(qp, oa)) - wa] = (unsigned short)(j + 1);
+          qp = q1;
         }
       }
     };
@@ -770,8 +792,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       else if (whole) count_children(std::true_type{}, std::false_type{});
       else count_children(std::false_type{}, std::false_type{});
     } else if (csr) {
-      for (int e = 0; e < kPerThread; ++e)       // no mass: every element's children start at q
-        if (tid * kPerThread + e < nA) csr[tid * kPerThread + e] = q;
+      for (int e = 0; e < kPerThread; ++e)       // no mass: every element's children start at q0
+        if (tid * kPerThread + e < nA) csr[tid * kPerThread + e] = q0;
     }
     __syncthreads();
 
