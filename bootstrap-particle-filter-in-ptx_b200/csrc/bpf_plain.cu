@@ -35,6 +35,7 @@
 // ptx_assembly/bpf_kernels_full.ptx:231-842.
 #include "bpf_plain.cuh"
 #include "bpf_block.cuh"
+#include <cooperative_groups.h>
 #include <cmath>
 #include <mutex>
 #include <type_traits>
@@ -330,23 +331,37 @@ __host__ __device__ constexpr size_t plan_smem_bytes(int G) {
   return G <= kPlanSmemTiles ? (size_t)G * 8 + (size_t)(2 * G + 1) * 4 : 0;
 }
 
+// Where the plan finds the tile records of the tick and puts the tile prefixes: the plan
+// kernel reads the global copies pass 1 wrote (through L2) and writes P to global memory.
+struct PlanGlobalIO {
+  const Plan* p;
+  static constexpr bool kStoreState = true;      // write the device state back to p.st
+  __device__ __forceinline__ float4 rec(int k) const { return __ldcg(p->rec + k); }
+  __device__ __forceinline__ int nexp(int k) const { return __ldcg(p->nexp + k); }
+  __device__ __forceinline__ unsigned long long E(int k) const { return __ldcg(p->E + k); }
+  __device__ __forceinline__ void set_P(int k, unsigned long long v) const { p->P[k] = v; }
+};
+
 // The plan of one tick by a CTA of NT threads on the device state s_st held in
 // shared memory (the body's first barrier comes before its first read of s_st);
-// it ends by writing s_st back to p.st. ITEMS: also write pass 2's work items.
-template <int NT, bool ITEMS>
+// it ends by writing s_st back to p.st when IO::kStoreState. ITEMS: also write pass 2's
+// work items.
+template <int NT, bool ITEMS, class IO>
 __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevState& s_st, PlanShared<NT>& sh,
-                                          unsigned char* plan_smem) {
+                                          unsigned char* plan_smem, const IO& io, BpfTickRecord* rec_out,
+                                          TickMirror* mirror_out) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = p.G, N = p.N;
   DevState* st = &s_st;
   auto store_state = [&]() {
     nt_sync<NT>();
+    if (!IO::kStoreState) return;
     if (tid < kStWords)
       reinterpret_cast<unsigned long long*>(p.st)[tid] = reinterpret_cast<const unsigned long long*>(&s_st)[tid];
-    if (tid == 0 && a.mirror) {
+    if (tid == 0 && mirror_out) {
       TickMirror mm;
       mm.resample_count = st->resample_count; mm.tick = st->tick; mm.error = st->error; mm.pad = 0;
-      *a.mirror = mm;
+      *mirror_out = mm;
     }
   };
 
@@ -359,7 +374,7 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int k = k0 + u * NT + tid;
-      r8[u] = (k < G) ? __ldcg(p.rec + k) : make_float4(0.f, 0.f, 0.f, __int_as_float(kNkEmpty));
+      r8[u] = (k < G) ? io.rec(k) : make_float4(0.f, 0.f, 0.f, __int_as_float(kNkEmpty));
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -386,31 +401,41 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
   if (lane == 0) { sh.red[0][warp] = S; sh.red[1][warp] = Q; sh.red[2][warp] = H; }
   nt_sync<NT>();
 
-  // 3. tick statistics: the three FP64 transcendental/division chains run on
-  //    different warps, then thread 0 takes the decision
-  // one thread per chain: lane 0 of warps 0..3 (lanes 0..3 of the single warp when NT = 32)
-  const int slot = (NT >= 128) ? warp : lane;
-  const bool slot_lead = (NT >= 128) ? (lane == 0) : true;
-  if (slot_lead && slot < 3) {
-    double v = 0.0;
-    for (int w = 0; w < NT / 32; ++w) v += sh.red[slot][w];
-    sh.tot[slot] = v;
+  // 3. tick statistics: the FP64 transcendental/division chains (on different warps
+  //    of a full CTA; in every lane of a single warp, which avoids serialising
+  //    divergent branches), then thread 0 takes the decision
+  constexpr double kLn2d = 0.693147180559945309417232121458;
+  double tS, tQ, tH;
+  if constexpr (NT == 32) {
+    tS = S; tQ = Q; tH = H;                        // the warp sums, complete in every lane
+  } else {
+    if (lane == 0 && warp < 3) {
+      double v = 0.0;
+      for (int w = 0; w < NT / 32; ++w) v += sh.red[warp][w];
+      sh.tot[warp] = v;
+    }
+    nt_sync<NT>();
+    tS = sh.tot[0]; tQ = sh.tot[1]; tH = sh.tot[2];
   }
-  nt_sync<NT>();
-  const double tS = sh.tot[0], tQ = sh.tot[1], tH = sh.tot[2];
   const bool degenerate = (nM == kNkEmpty) || !(tS > 0.0);
-  if (slot_lead && !degenerate) {
-    if (slot == 0) sh.res[0] = (double)nM * 0.693147180559945309417232121458 + log(tS);   // log-sum in the carry frame
-    if (slot == 1) sh.res[1] = tS * tS / tQ;                                                // ESS
-    if (slot == 2) sh.res[2] = tH / tS;                                                     // filtered mean
-    if (slot == 3) sh.res[3] = log(tS);
+  if (!degenerate) {
+    if constexpr (NT == 32) {
+      const double L = log(tS);
+      const double r0 = __fma_rn((double)nM, kLn2d, L), r1 = tS * tS / tQ, r2 = tH / tS;
+      if (lane == 0) { sh.res[0] = r0; sh.res[1] = r1; sh.res[2] = r2; sh.res[3] = L; }
+    } else if (lane == 0) {
+      if (warp == 0) sh.res[0] = __fma_rn((double)nM, kLn2d, log(tS));   // log-sum in the carry frame
+      if (warp == 1) sh.res[1] = tS * tS / tQ;                            // ESS
+      if (warp == 2) sh.res[2] = tH / tS;                                 // filtered mean
+      if (warp == 3) sh.res[3] = log(tS);
+    }
   }
   nt_sync<NT>();
   // online learning: normalised score sums of this tick, FP64 in the global frame
   if (a.learn && p.rec2 && st->tick > 0 && !degenerate) {
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int k = tid; k < G; k += NT) {
-      const int nk = __float_as_int(__ldcg(p.rec + k).w);
+      const int nk = __float_as_int(io.rec(k).w);
       if (nk == kNkEmpty) continue;
       const float4 r2 = __ldcg(p.rec2 + k);
       const double sc = pow2d(nk - nM);
@@ -460,11 +485,11 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
     if (a.apf != 1) st->ll_total += rec_dll;
     if (a.aux) *a.aux = degenerate ? make_float2(0.0f, __int_as_float(0))
                                    : make_float2((float)(1.0 / tS), __int_as_float(nM));
-    if (a.rec) {
+    if (rec_out) {
       BpfTickRecord r;
       r.dloglik = rec_dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
       r.h_mean = (float)hm; r.ess = (float)ess; r.resampled = resample; r.tick = tick;
-      *a.rec = r;
+      *rec_out = r;
     }
     {
       // pass 2 runs opposite to this pass 1; the next pass 1 opposite to the
@@ -516,7 +541,7 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const int k = k0 + u * NT + tid;
-        if (k < G) { nk[u] = __ldcg(p.nexp + k); e4[u] = __ldcg(p.E + k); }
+        if (k < G) { nk[u] = io.nexp(k); e4[u] = io.E(k); }
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
@@ -562,7 +587,7 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
   int o = targets_below(run, base, delta, magic, N);
   int n_it = 0;
   for (int k = k0; k < k1; ++k) {
-    p.P[k] = run;
+    io.set_P(k, run);
     o_s[k] = o;
     run += ehat(k);
     const int o_next = targets_below(run, base, delta, magic, N);
@@ -599,7 +624,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs 
   if (threadIdx.x < kStWords)
     reinterpret_cast<unsigned long long*>(&s_st)[threadIdx.x] =
         __ldcg(reinterpret_cast<const unsigned long long*>(p.st) + threadIdx.x);
-  plan_body<kPlanThreads, true>(p, a, s_st, sh, plan_smem);
+  plan_body<kPlanThreads, true>(p, a, s_st, sh, plan_smem, PlanGlobalIO{&p}, a.rec, a.mirror);
   griddep_release();
 }
 
@@ -981,124 +1006,159 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 }
 
 // ---------------------------------------------------------------------------
-// Fused tick for small filters (N <= kSmallMaxN, at most kSmallTiles tiles):
-// one CTA runs n consecutive ticks, each as pass 1, the plan and the
-// resampling, without leaving the SM, so a tick costs one launch (or a run of
-// ticks one launch) instead of three dependent launches.
-//   pass 1    group g of kThreads threads runs tile g with the pass-1 code and
-//             its own barrier, so every tile record is bit for bit pass 1's;
-//   plan      the plan code on warp 0 alone (warp barriers only; with at most
-//             four tiles it forms the same FP64 sums), device state in shared memory;
-//   resample  the whole filter at once: the same fixed-point rule (integer
-//             exact, so the ancestors do not depend on how the work is split),
-//             a per-output start mark in shared memory and the max-scan gather.
-// Results equal the three-kernel tick's bit for bit.
+// Fused tick for small filters (N <= kSmallMaxN, at most kSmallTiles tiles): a
+// thread-block cluster of one CTA per tile runs n consecutive ticks in one
+// launch. The particles, log2-weights and tile records stay in shared memory
+// from the first tick to the last; the CTAs read each other's records, start
+// marks and particles through distributed shared memory and meet at one
+// cluster barrier per tick (two on resampling ticks).
+//   pass 1    each CTA runs its tile with pass 1's per-particle arithmetic on
+//             four times as many threads and hands the FP32 running sums along
+//             in pass 1's element order, so every tile record is bit for bit
+//             pass 1's;
+//   plan      every CTA runs the plan code on its warp 0 over all the tile
+//             records (the same FP64 sums in the same order, so every CTA takes
+//             the same decision and holds the same device state); CTA 0 writes
+//             the tick's record;
+//   resample  the same fixed-point rule (integer exact, so the ancestors do not
+//             depend on how the work is split): each CTA counts its tile's
+//             children, marks the first output of each parent's run of children
+//             in the shared memory of the CTA that owns that output (and the
+//             first output of every further CTA the run reaches), then gathers
+//             its own outputs from the parents' CTAs.
+// Results equal the three-kernel tick's bit for bit: both particle buffers, the
+// log2-weights and tile exponents are loaded at the start and written back at
+// the end of the launch, with the device state.
 // ---------------------------------------------------------------------------
-constexpr int kSmallThreads = kSmallTiles * kThreads;
-constexpr size_t kSmallMarkBytes = ((size_t)kSmallMaxN + kGatherStep) * 2;
-static_assert(kSmallMaxN % kGatherStep == 0, "the small gather reads marks in 256-slot steps");
+constexpr int kSmallSplit = 4;                          // threads per pass-1 thread
+constexpr int kSmallThreads = kSmallSplit * kThreads;   // 1024 threads per CTA (one tile)
+constexpr int kMarkWarps = kTile / kGatherStep;         // warps of the gather (256 outputs each)
+static_assert(kTile % kGatherStep == 0, "the gather reads marks in 256-slot steps");
+static_assert(kSmallMaxN < 65536, "start marks hold parent + 1 in 16 bits");
 
-// Pass 1 of tile k for a filter of one or two tiles, spread over SPLIT times as many
-// threads as pass 1 uses (group barrier `bar`, rt = 0..SPLIT*kThreads-1 inside the group).
-// Pass-1 thread v's sixteen particles (four float4 groups r) go to SPLIT adjacent threads,
-// 4/SPLIT groups each, with the per-particle arithmetic of pass1_tile; the FP32 tile
-// partials are then accumulated in pass 1's order by handing the running sums from one of
-// those threads to the next, so every tile record is bit for bit pass 1's.
-struct SplitShared {
+struct FusedShared {
+  float h[2][kTile];                          // particle buffers (DevState::cur / src), this CTA's tile
+  float w[kTile];                             // log2-weights of the tile
+  unsigned short marks[kTile + kGatherStep];  // start marks of this CTA's outputs: parent + 1, 0 = none
+  float4 rec[2];                              // tile record {S, Q, H, n_k}, by tick parity
+  unsigned long long E[2];                    // exact fixed-point tile mass, by tick parity
+  int nexp[2];                                // tile exponent, by tick parity
+  FusedShared* peer[kSmallTiles];             // every CTA's FusedShared (distributed shared memory)
+  __align__(16) DevState st;
+  PlanShared<32> pl;
+  __align__(16) unsigned char plan_stage[(plan_smem_bytes(kSmallTiles) + 15) & ~(size_t)15];
+  unsigned long long P[kSmallTiles];          // the tick's tile prefixes (all tiles)
   float s_max[kSmallThreads / 32];
   float s_part[3][kThreads];
   unsigned long long s_E[kThreads];
+  unsigned long long scan[kSmallThreads / 32 + 1];
+  unsigned wmax[kSmallThreads / 32];
 };
 
-template <bool TSTATE, bool GAUSS, int SPLIT>
-__device__ __forceinline__ void pass1_split(const Plan& p, const TickArgs& a, const DevState* st, int k, int rt,
-                                            int bar, SplitShared& sh) {
-  constexpr int R = 4 / SPLIT;                 // float4 groups of this thread
-  constexpr int NTG = kThreads * SPLIT;        // threads of the tile's group
-  const int v = rt / SPLIT, sidx = rt % SPLIT;
-  const int lane = rt & 31, warp = rt >> 5;
-  auto gsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(NTG) : "memory"); };
-  const int tick = st->tick;
-  const bool carry = st->resampled_prev == 0;
-  const int nM_prev = st->nM_prev;
-  const uint64_t k1 = st->k1, k2 = st->k2;
-  float* hb = st->cur ? p.h1 : p.h0;
-  const float y = a.y_ptr ? __ldg(a.y_ptr) : a.obs.y;
+// The plan of the fused tick reads every CTA's tile record of the tick through distributed
+// shared memory and keeps the tile prefixes in its own CTA.
+struct PlanClusterIO {
+  FusedShared* const* peer;
+  int par;
+  unsigned long long* P;
+  static constexpr bool kStoreState = false;
+  __device__ __forceinline__ float4 rec(int k) const { return peer[k]->rec[par]; }
+  __device__ __forceinline__ int nexp(int k) const { return peer[k]->nexp[par]; }
+  __device__ __forceinline__ unsigned long long E(int k) const { return peer[k]->E[par]; }
+  __device__ __forceinline__ void set_P(int k, unsigned long long v) const { P[k] = v; }
+};
+
+template <int NCTA>
+__device__ __forceinline__ void cluster_sync_all() {
+  if constexpr (NCTA == 1) {
+    __syncthreads();
+  } else {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+  }
+}
+
+// Pass 1 of this CTA's tile (global slots tile0 .. tile0 + kTile - 1) on the shared-memory
+// copies: pass-1 thread v's sixteen particles (four float4 groups) go to the kSmallSplit
+// adjacent threads 4v .. 4v + 3, one group each, with the per-particle arithmetic of
+// pass1_tile; the FP32 tile partials are accumulated in pass 1's order by handing the running
+// sums from one of those threads to the next, and warp 0 forms the FP64 tile record in pass
+// 1's order. nk_prev: the tile's exponent of the previous tick (the carried weights' frame).
+template <bool TSTATE, bool GAUSS>
+__device__ __forceinline__ void pass1_fused(const TickArgs& a, const float* y_ptr, int N, int tile0, int par,
+                                            int nk_prev, FusedShared& sh) {
+  constexpr int SPLIT = kSmallSplit;
+  const int tid = threadIdx.x;
+  const int v = tid / SPLIT, sidx = tid % SPLIT;
+  const int lane = tid & 31, warp = tid >> 5;
+  const DevState& st = sh.st;
+  const int tick = st.tick;
+  const bool carry = st.resampled_prev == 0;
+  const uint64_t k1 = st.k1, k2 = st.k2;
+  float* hb = sh.h[st.cur];
+  const float y = y_ptr ? __ldg(y_ptr) : a.obs.y;
   ObsModel obs = a.obs;
   obs.y = y;
   const float y2 = y * y;
   float carry_off = 0.0f;
-  if (carry) {
-    const int nkp = p.nexp[k];
-    carry_off = (nkp == kNkEmpty) ? -INFINITY : (float)(nkp - nM_prev);
-  }
+  if (carry) carry_off = (nk_prev == kNkEmpty) ? -INFINITY : (float)(nk_prev - st.nM_prev);
   const float gauss_c = kGaussLog2C + carry_off;
   const float t_c = __fmul_rn(obs.c_obs, kLog2e) + carry_off;
   const float y2nu = __fmul_rn(y2, obs.inv_nu);
   const unsigned long long k33 = k2 << 33;
-  const int tile0 = k * kTile;
 
-  float x[4 * R], hv[4 * R];
+  const int l0 = 4 * (v + kThreads * sidx);      // the group's first slot in the tile
+  const float4 h4 = *reinterpret_cast<const float4*>(hb + l0);
+  const float4 w4 = carry ? *reinterpret_cast<const float4*>(sh.w + l0) : make_float4(0.f, 0.f, 0.f, 0.f);
+  float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+  const float wp[4] = {w4.x, w4.y, w4.z, w4.w};
+  float x[4];
 #pragma unroll
-  for (int rr = 0; rr < R; ++rr) {
-    const int i0 = tile0 + 4 * (v + kThreads * (sidx * R + rr));
-    const float4 h4 = *reinterpret_cast<const float4*>(hb + i0);
-    const float4 w4 = carry ? *reinterpret_cast<const float4*>(p.w + i0) : make_float4(0.f, 0.f, 0.f, 0.f);
-    float hh[4] = {h4.x, h4.y, h4.z, h4.w};
-    const float wp[4] = {w4.x, w4.y, w4.z, w4.w};
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      float h = hh[e];
-      if (tick > 0) {
-        const uint64_t sst = k1 + k2 * pcg_inc((uint32_t)(i0 + e));
-        float z = icdf_normal_warp(pcg_uniform(pcg_output(sst)));
-        if (TSTATE) z *= tstate_scale_warp(sst, k33, a.nu_int, a.nu_state);
-        h = propagate(h, a.mu, a.rho, a.sigma, z);
-      }
-      float xx = GAUSS ? obs_log2pdf_gauss_plus(y2, h, gauss_c) : obs_log2pdf_t_plus(obs, y2nu, h, t_c);
-      if (carry) xx += wp[e];
-      if (i0 + e >= p.N) xx = -INFINITY;          // padding slots carry no weight
-      hh[e] = h;
-      x[4 * rr + e] = xx;
-      hv[4 * rr + e] = h;
+  for (int e = 0; e < 4; ++e) {
+    const int i = tile0 + l0 + e;
+    float h = hh[e];
+    if (tick > 0) {
+      const uint64_t s = k1 + k2 * pcg_inc((uint32_t)i);
+      float z = icdf_normal_warp(pcg_uniform(pcg_output(s)));
+      if (TSTATE) z *= tstate_scale_warp(s, k33, a.nu_int, a.nu_state);
+      h = propagate(h, a.mu, a.rho, a.sigma, z);
     }
-    *reinterpret_cast<float4*>(hb + i0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
+    float xx = GAUSS ? obs_log2pdf_gauss_plus(y2, h, gauss_c) : obs_log2pdf_t_plus(obs, y2nu, h, t_c);
+    if (carry) xx += wp[e];
+    if (i >= N) xx = -INFINITY;                   // padding slots carry no weight
+    hh[e] = h;
+    x[e] = xx;
   }
-  float mx = x[0];
-#pragma unroll
-  for (int e = 1; e < 4 * R; ++e) mx = fmaxf(mx, x[e]);
+  *reinterpret_cast<float4*>(hb + l0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
+
+  float mx = fmaxf(fmaxf(x[0], x[1]), fmaxf(x[2], x[3]));
   mx = warp_max_f(mx);
   if (lane == 0) sh.s_max[warp] = mx;
-  gsync();
+  __syncthreads();
   mx = sh.s_max[0];
-  for (int w = 1; w < NTG / 32; ++w) mx = fmaxf(mx, sh.s_max[w]);
+#pragma unroll 8
+  for (int w = 1; w < kSmallThreads / 32; ++w) mx = fmaxf(mx, sh.s_max[w]);
   const int nk = (mx == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(mx, -1.0e9f));
   const float fnk = (nk == kNkEmpty) ? INFINITY : (float)nk;
 
-  float wv[4 * R];
+  float wv[4], dv[4];
   unsigned long long E = 0ull;
 #pragma unroll
-  for (int rr = 0; rr < R; ++rr) {
-    const int i0 = tile0 + 4 * (v + kThreads * (sidx * R + rr));
-    float dv[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      dv[e] = x[4 * rr + e] - fnk;
-      wv[4 * rr + e] = tile_weight(dv[e]);
-      E += fix_weight(wv[4 * rr + e]);
-    }
-    *reinterpret_cast<float4*>(p.w + i0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+  for (int e = 0; e < 4; ++e) {
+    dv[e] = x[e] - fnk;
+    wv[e] = tile_weight(dv[e]);
+    E += fix_weight(wv[e]);
   }
+  *reinterpret_cast<float4*>(sh.w + l0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
   // pass 1's per-thread FP32 sums, in its element order, handed along the SPLIT threads
   float aS = 0.f, aQ = 0.f, aH = 0.f;
 #pragma unroll
   for (int step = 0; step < SPLIT; ++step) {
     if (sidx == step) {
 #pragma unroll
-      for (int e = 0; e < 4 * R; ++e) {
+      for (int e = 0; e < 4; ++e) {
         aS += wv[e];
         aQ = fmaf(wv[e], wv[e], aQ);
-        aH = fmaf(wv[e], hv[e], aH);
+        aH = fmaf(wv[e], hh[e], aH);
       }
     }
     const float nS = __shfl_up_sync(0xffffffffu, aS, 1);
@@ -1110,7 +1170,7 @@ __device__ __forceinline__ void pass1_split(const Plan& p, const TickArgs& a, co
   for (int o = 1; o < SPLIT; o <<= 1) E += __shfl_xor_sync(0xffffffffu, E, o);
   if (sidx == SPLIT - 1) { sh.s_part[0][v] = aS; sh.s_part[1][v] = aQ; sh.s_part[2][v] = aH; }
   if (sidx == 0) sh.s_E[v] = E;
-  gsync();
+  __syncthreads();
   if (warp == 0) {                              // pass 1's FP64 tile combine, same order
     double tS = 0.0, tQ = 0.0, tH = 0.0;
     unsigned long long tE = 0ull;
@@ -1124,54 +1184,43 @@ __device__ __forceinline__ void pass1_split(const Plan& p, const TickArgs& a, co
     tS = warp_sum_d(tS); tQ = warp_sum_d(tQ); tH = warp_sum_d(tH);
     tE = warp_sum_u64(tE);
     if (lane == 0) {
-      p.nexp[k] = nk;
-      p.E[k] = tE;
-      p.rec[k] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
+      sh.nexp[par] = nk;
+      sh.E[par] = tE;
+      sh.rec[par] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
     }
   }
 }
 
-struct SmallShared {
-  Pass1Shared p1[kSmallTiles];
-  PlanShared<32> pl;
-  __align__(16) DevState st;
-  __align__(16) unsigned char plan_stage[(plan_smem_bytes(kSmallTiles) + 15) & ~(size_t)15];
-  unsigned long long scan[kSmallThreads / 32 + 1];
-  unsigned long long tstart[kSmallTiles];   // block-scan value at each tile's first element
-  unsigned wmax[kSmallThreads / 32];
-  SplitShared sp[2];
-};
+// Start mark of output o (parent + 1) in the shared memory of the CTA that owns o.
+template <int NCTA>
+__device__ __forceinline__ void put_mark(FusedShared& sh, int o, int val) {
+  if constexpr (NCTA == 1) sh.marks[o] = (unsigned short)val;
+  else sh.peer[o >> 12]->marks[o & (kTile - 1)] = (unsigned short)val;
+}
 
-__device__ __forceinline__ void small_resample(const Plan& p, const TickArgs& a, SmallShared& sh,
-                                               unsigned short* marks) {
+// Resampling of a fused tick, this CTA's part: the children of its tile's particles (start
+// marks into the owners' shared memory), a cluster barrier, then the gather of its own outputs.
+template <int NCTA>
+__device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, int par, FusedShared& sh) {
+  static_assert(kTile == 1 << 12, "output owner = o >> 12");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int N = p.N;
+  const int tile0 = k * kTile;
   const DevState& st = sh.st;
   const unsigned long long base = st.base, delta = st.delta, magic = st.delta_magic;
-  const int nM = st.nM, Fg = st.Fg;
-  const float* hsrc = st.src ? p.h1 : p.h0;
-  float* hdst = st.src ? p.h0 : p.h1;
-  const int Ns = (N + kGatherStep - 1) & ~(kGatherStep - 1);
-  for (int x = tid; x < Ns / 8; x += kSmallThreads) reinterpret_cast<uint4*>(marks)[x] = make_uint4(0u, 0u, 0u, 0u);
+  const int nk = sh.nexp[par];
+  const int r = (nk == kNkEmpty) ? 64 : st.nM - nk + kFixF - st.Fg;
+  const unsigned long long Pk = sh.P[k];
 
-  // each thread a power-of-two chunk of consecutive elements (chunks never straddle a tile)
-  int chunk = 1;
-  while (chunk * kSmallThreads < N) chunk <<= 1;
-  const int j0 = tid * chunk, j1 = min(N, j0 + chunk);
-  const int k = min(j0, N - 1) >> 12;
-  const int nk = p.nexp[k];
-  const int r = (nk == kNkEmpty) ? 64 : nM - nk + kFixF - Fg;
-  const unsigned long long Pk = p.P[k];
-  unsigned long long run = 0ull;
-  if (r < 64)
-    for (int j = j0; j < j1; ++j) run += fix_weight(tile_weight(p.w[j]));
+  // four consecutive slots per thread; the tile-local exclusive prefix of the exact weights
+  const int l0 = 4 * tid, j0 = tile0 + l0;
+  const float4 w4 = *reinterpret_cast<const float4*>(sh.w + l0);
+  const unsigned long long f[4] = {fix_weight(tile_weight(w4.x)), fix_weight(tile_weight(w4.y)),
+                                   fix_weight(tile_weight(w4.z)), fix_weight(tile_weight(w4.w))};
+  const unsigned long long run = (r < 64) ? (f[0] + f[1]) + (f[2] + f[3]) : 0ull;
   unsigned long long tot;
-  const unsigned long long excl = block_excl_scan_add<kSmallThreads>(run, &tot, sh.scan);
-  if (j0 < N && (j0 & (kTile - 1)) == 0) sh.tstart[k] = excl;
-  __syncthreads();
-  const unsigned long long loc = excl - sh.tstart[k];   // tile-local exclusive prefix
+  const unsigned long long loc = block_excl_scan_add<kSmallThreads>(run, &tot, sh.scan);
 
-  // child counts against tile-frame thresholds, as pass 2 (every output is in the window)
+  // child counts against tile-frame thresholds, as pass 2
   int q = targets_below(Pk + shr64(loc, r), base, delta, magic, N);
   unsigned long long th = kThCap, D = kThCap;
   if (r < 64 && q < N && j0 < N) {
@@ -1180,37 +1229,40 @@ __device__ __forceinline__ void small_resample(const Plan& p, const TickArgs& a,
     if (delta <= (kThCap >> r)) D = delta << r;
   }
   unsigned long long acc = 0ull;
-  for (int j = j0; j < j1; ++j) {
-    acc += fix_weight(tile_weight(p.w[j]));
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    acc += f[e];
     if (acc >= th) {
       const unsigned long long diff = acc - th;
       int c = 1 + (diff >= D) + (diff >= 2ull * D) + (diff >= 3ull * D);
       if (c == 4 && diff >= 4ull * D) c = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
       const int q1 = min(q + c, N);
-      marks[q] = (unsigned short)(j + 1);
+      const int val = j0 + e + 1;
+      put_mark<NCTA>(sh, q, val);
+      for (int b = ((q >> 12) + 1) << 12; b < q1; b += kTile) put_mark<NCTA>(sh, b, val);   // first output of each further CTA
       th = (q1 >= N) ? kThCap : th + (unsigned long long)c * D;
       q = q1;
     }
   }
-  __syncthreads();
+  cluster_sync_all<NCTA>();                      // every start mark is in place
 
-  // gather: the ancestor of output o is the last start mark at or before o
-  constexpr int W = kSmallThreads / 32;
-  const int wchunk = ((N + W - 1) / W + kGatherStep - 1) & ~(kGatherStep - 1);
-  const int cs = warp * wchunk, ce = min(cs + wchunk, N);
-  unsigned wmax = 0u;
-  for (int o0 = cs; o0 < ce; o0 += kGatherStep) {
-    const uint4 m = reinterpret_cast<const uint4*>(marks + o0)[lane];
-    const unsigned v = __vmaxu2(__vmaxu2(m.x, m.y), __vmaxu2(m.z, m.w));
-    wmax = max(wmax, max(v & 0xffffu, v >> 16));
+  // gather: the ancestor of output o is the last start mark at or before o; the first output of
+  // every CTA has one, so no CTA needs another's marks
+  const int n_out = min(N - tile0, kTile);
+  const int o0 = warp * kGatherStep;
+  const bool active = warp < kMarkWarps && o0 < n_out;
+  uint4 m = make_uint4(0u, 0u, 0u, 0u);
+  if (active) {
+    m = reinterpret_cast<const uint4*>(sh.marks + o0)[lane];
+    const unsigned vv = __vmaxu2(__vmaxu2(m.x, m.y), __vmaxu2(m.z, m.w));
+    unsigned wm = max(vv & 0xffffu, vv >> 16);
+    wm = __reduce_max_sync(0xffffffffu, wm);
+    if (lane == 0) sh.wmax[warp] = wm;
   }
-  wmax = __reduce_max_sync(0xffffffffu, wmax);
-  if (lane == 0) sh.wmax[warp] = wmax;
   __syncthreads();
-  unsigned carry = 0u;
-  for (int w = 0; w < warp; ++w) carry = max(carry, sh.wmax[w]);
-  for (int o0 = cs; o0 < ce; o0 += kGatherStep) {
-    const uint4 m = reinterpret_cast<const uint4*>(marks + o0)[lane];
+  if (active) {
+    unsigned carry = 0u;
+    for (int w = 0; w < warp; ++w) carry = max(carry, sh.wmax[w]);
     unsigned am[8];
     am[0] = m.x & 0xffffu;
     am[1] = max(am[0], m.x >> 16);
@@ -1220,53 +1272,82 @@ __device__ __forceinline__ void small_resample(const Plan& p, const TickArgs& a,
     am[5] = max(am[4], m.z >> 16);
     am[6] = max(am[5], m.w & 0xffffu);
     am[7] = max(am[6], m.w >> 16);
-    unsigned x = am[7];
+    unsigned xm = am[7];
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const unsigned t = __shfl_up_sync(0xffffffffu, x, off);
-      if (lane >= off) x = max(x, t);
+      const unsigned t = __shfl_up_sync(0xffffffffu, xm, off);
+      if (lane >= off) xm = max(xm, t);
     }
-    unsigned pre = __shfl_up_sync(0xffffffffu, x, 1);
+    unsigned pre = __shfl_up_sync(0xffffffffu, xm, 1);
     pre = max(carry, lane == 0 ? 0u : pre);
+    const int src = st.src;
+    float* hd = sh.h[st.cur];
     const int o = o0 + 8 * lane;
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      if (o + u < ce) {
-        const unsigned jj = max(max(pre, am[u]), 1u);    // output 0 has the first mark: jj >= 1
-        hdst[o + u] = hsrc[jj - 1u];
-        if (a.anc) a.anc[o + u] = (int)(jj - 1u);
+      if (o + u < n_out) {
+        const int parent = (int)max(max(pre, am[u]), 1u) - 1;
+        hd[o + u] = (NCTA == 1) ? sh.h[src][parent] : sh.peer[parent >> 12]->h[src][parent & (kTile - 1)];
+        if (a.anc) a.anc[tile0 + o + u] = parent;
       }
     }
-    carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
+    reinterpret_cast<uint4*>(sh.marks + o0)[lane] = make_uint4(0u, 0u, 0u, 0u);   // clear for the next resampling
   }
 }
 
-template <bool TSTATE, bool GAUSS>
-__global__ void __launch_bounds__(kSmallThreads, 1) small_kernel(Plan p, TickArgs a, int n_ticks) {
-  __shared__ SmallShared sh;
+template <bool TSTATE, bool GAUSS, int NCTA>
+__global__ void __cluster_dims__(NCTA, 1, 1) __launch_bounds__(kSmallThreads, 1)
+small_kernel(Plan p, TickArgs a, int n_ticks) {
   extern __shared__ __align__(16) unsigned char small_smem[];
-  unsigned short* marks = reinterpret_cast<unsigned short*>(small_smem);
+  FusedShared& sh = *reinterpret_cast<FusedShared*>(small_smem);
+  const int tid = threadIdx.x;
+  int k = 0;
+  if constexpr (NCTA > 1) k = (int)cooperative_groups::this_cluster().block_rank();
+  const int N = p.N, tile0 = k * kTile;
   griddep_wait();
-  const int tid = threadIdx.x, g = tid / kThreads;
   if (tid < kStWords)
     reinterpret_cast<unsigned long long*>(&sh.st)[tid] = __ldcg(reinterpret_cast<const unsigned long long*>(p.st) + tid);
+  if (tid < NCTA) {
+    if constexpr (NCTA > 1) sh.peer[tid] = cooperative_groups::this_cluster().map_shared_rank(&sh, tid);
+    else sh.peer[tid] = &sh;
+  }
+  if (tid == 0) sh.nexp[1] = __ldcg(p.nexp + k);      // the exponent the first tick's carry reads
+  reinterpret_cast<float4*>(sh.h[0])[tid] = __ldcg(reinterpret_cast<const float4*>(p.h0 + tile0) + tid);
+  reinterpret_cast<float4*>(sh.h[1])[tid] = __ldcg(reinterpret_cast<const float4*>(p.h1 + tile0) + tid);
+  reinterpret_cast<float4*>(sh.w)[tid] = __ldcg(reinterpret_cast<const float4*>(p.w + tile0) + tid);
+  constexpr int kMarkVecs = (int)(sizeof(sh.marks) / 16);
+  if (tid < kMarkVecs) reinterpret_cast<uint4*>(sh.marks)[tid] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
+
   for (int t = 0; t < n_ticks; ++t) {
-    TickArgs at = a;
-    at.y_ptr = a.y_ptr ? a.y_ptr + t : nullptr;
-    at.rec = a.rec ? a.rec + t : nullptr;
-    if (p.G == 1) {                          // one tile: four threads per pass-1 thread
-      pass1_split<TSTATE, GAUSS, 4>(p, at, &sh.st, 0, tid, 1, sh.sp[0]);
-    } else if (p.G == 2) {                   // two tiles: two threads per pass-1 thread
-      pass1_split<TSTATE, GAUSS, 2>(p, at, &sh.st, tid >> 9, tid & 511, 1 + (tid >> 9), sh.sp[tid >> 9]);
-    } else if (g < p.G) {
-      pass1_tile<TSTATE, false, 0, GAUSS>(p, at, &sh.st, g, tid & (kThreads - 1), 1 + g, sh.p1[g]);
+    const int par = t & 1;
+    pass1_fused<TSTATE, GAUSS>(a, a.y_ptr ? a.y_ptr + t : nullptr, N, tile0, par, sh.nexp[par ^ 1], sh);
+    cluster_sync_all<NCTA>();                   // every tile record of the tick is in place
+    if (tid < 32)
+      plan_body<32, false>(p, a, sh.st, sh.pl, sh.plan_stage, PlanClusterIO{sh.peer, par, sh.P},
+                           (a.rec && k == 0) ? a.rec + t : nullptr, nullptr);
+    __syncthreads();
+    if (sh.st.do_resample) resample_fused<NCTA>(a, N, k, par, sh);
+    __syncthreads();
+  }
+  cluster_sync_all<NCTA>();                     // no CTA leaves while another may read its shared memory
+  reinterpret_cast<float4*>(p.h0 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[0])[tid];
+  reinterpret_cast<float4*>(p.h1 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[1])[tid];
+  reinterpret_cast<float4*>(p.w + tile0)[tid] = reinterpret_cast<const float4*>(sh.w)[tid];
+  if (tid == 0) {
+    const int last = (n_ticks - 1) & 1;
+    p.nexp[k] = sh.nexp[last];
+    p.E[k] = sh.E[last];
+    p.rec[k] = sh.rec[last];
+  }
+  if (k == 0) {
+    if (tid < kStWords)
+      reinterpret_cast<unsigned long long*>(p.st)[tid] = reinterpret_cast<const unsigned long long*>(&sh.st)[tid];
+    if (tid == 0 && a.mirror) {
+      TickMirror mm;
+      mm.resample_count = sh.st.resample_count; mm.tick = sh.st.tick; mm.error = sh.st.error; mm.pad = 0;
+      *a.mirror = mm;
     }
-    __syncthreads();                       // the tile records are visible to the plan
-    if (tid < 32) plan_body<32, false>(p, at, sh.st, sh.pl, sh.plan_stage);   // warp 0, warp barriers
-    __syncthreads();
-    if (sh.st.do_resample) small_resample(p, at, sh, marks);
-    __syncthreads();
   }
   griddep_release();
 }
@@ -1353,6 +1434,15 @@ size_t pass2_smem_bytes() { return kPass2Smem; }
 
 constexpr int kMaxConfiguredDevices = 64;
 
+template <int NCTA>
+static void configure_small() {
+  constexpr int bytes = (int)sizeof(FusedShared);
+  cudaFuncSetAttribute(small_kernel<false, true, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(small_kernel<true, true, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(small_kernel<false, false, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(small_kernel<true, false, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 // Called with `device` current. The shared-memory attributes are set once per
 // device (they belong to the device's context), under a lock so filters
 // created from several threads do not race.
@@ -1365,10 +1455,10 @@ int pass2_grid_size(int device) {
       cudaFuncSetAttribute(pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPass2Smem);
       cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)plan_smem_bytes(kPlanSmemTiles));
-      cudaFuncSetAttribute(small_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
-      cudaFuncSetAttribute(small_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
-      cudaFuncSetAttribute(small_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
-      cudaFuncSetAttribute(small_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallMarkBytes);
+      configure_small<1>();
+      configure_small<2>();
+      configure_small<3>();
+      configure_small<4>();
       if (device >= 0 && device < kMaxConfiguredDevices) configured[device] = true;
     }
   }
@@ -1409,15 +1499,26 @@ bool small_eligible(const Plan& p, const TickArgs& a) {
   return p.N <= kSmallMaxN && !a.learn && a.apf == 0 && !(a.silverman > 0.0f) && !a.ckpt && !a.csr && !a.aux;
 }
 
-cudaError_t launch_small(const Plan& p, const TickArgs& a, int n_ticks, cudaStream_t s, bool pdl) {
-  if (p.N > kSmallMaxN || n_ticks < 1) return cudaErrorInvalidValue;
-  const dim3 grid(1), block(kSmallThreads);
+template <int NCTA>
+static cudaError_t launch_small_cluster(const Plan& p, const TickArgs& a, int n_ticks, cudaStream_t s, bool pdl) {
+  const dim3 grid(NCTA), block(kSmallThreads);
+  constexpr size_t bytes = sizeof(FusedShared);
   if (a.obs.nu > 0.0f) {
-    if (a.nu_int > 0) return launch_ex(small_kernel<true, false>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
-    return launch_ex(small_kernel<false, false>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
+    if (a.nu_int > 0) return launch_ex(small_kernel<true, false, NCTA>, grid, block, bytes, s, pdl, p, a, n_ticks);
+    return launch_ex(small_kernel<false, false, NCTA>, grid, block, bytes, s, pdl, p, a, n_ticks);
   }
-  if (a.nu_int > 0) return launch_ex(small_kernel<true, true>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
-  return launch_ex(small_kernel<false, true>, grid, block, kSmallMarkBytes, s, pdl, p, a, n_ticks);
+  if (a.nu_int > 0) return launch_ex(small_kernel<true, true, NCTA>, grid, block, bytes, s, pdl, p, a, n_ticks);
+  return launch_ex(small_kernel<false, true, NCTA>, grid, block, bytes, s, pdl, p, a, n_ticks);
+}
+
+cudaError_t launch_small(const Plan& p, const TickArgs& a, int n_ticks, cudaStream_t s, bool pdl) {
+  if (p.N > kSmallMaxN || p.G < 1 || p.G > kSmallTiles || n_ticks < 1) return cudaErrorInvalidValue;
+  switch (p.G) {
+    case 1: return launch_small_cluster<1>(p, a, n_ticks, s, pdl);
+    case 2: return launch_small_cluster<2>(p, a, n_ticks, s, pdl);
+    case 3: return launch_small_cluster<3>(p, a, n_ticks, s, pdl);
+    default: return launch_small_cluster<4>(p, a, n_ticks, s, pdl);
+  }
 }
 
 cudaError_t launch_jitter(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
