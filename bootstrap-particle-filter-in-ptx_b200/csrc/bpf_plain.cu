@@ -331,6 +331,81 @@ __host__ __device__ constexpr size_t plan_smem_bytes(int G) {
   return G <= kPlanSmemTiles ? (size_t)G * 8 + (size_t)(2 * G + 1) * 4 : 0;
 }
 
+// The tick's outcome from its statistics, by one thread: the log-likelihood increment and the
+// tick's record, the resampling decision and the device state of the next tick.
+// res = {log-sum of the weights in the carry frame, ESS, filtered mean, ln S}.
+// Returns the resampling decision.
+__device__ __forceinline__ int plan_decide(const TickArgs& a, DevState* st, int N, int nM, bool degenerate,
+                                           const double* res, double tS, BpfTickRecord* rec_out) {
+  const int tick = st->tick, cur = st->cur;
+  double dll, ess, hm;
+  int resample = 0;
+  if (degenerate) {
+    dll = -INFINITY; ess = 0.0; hm = __longlong_as_double(0x7FF8000000000000LL);
+    st->error = BPF_ERR_DEGENERATE;
+  } else {
+    dll = res[0] - st->logS_prev;
+    ess = res[1];
+    hm = res[2];
+    resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
+  }
+  // Auxiliary particle filter: the first stage leaves log mean v (its weights)
+  // in ll_ref for the second, whose increment is log mean v + log mean w; the
+  // record's loglik_ref is log mean w, the value the reference reports
+  // (gpu_bpf_ptx_full.cu:1155-1164). The tick advances after the second stage.
+  double rec_dll = dll, ll_ref;
+  if (a.apf == 1) {
+    ll_ref = dll;
+  } else if (a.apf == 2) {
+    rec_dll = st->ll_ref + dll;
+    ll_ref = dll;
+  } else {
+    ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
+  }
+  st->ll_ref = ll_ref;
+  st->hm = degenerate ? 0.0 : hm;
+  if (a.apf != 1) st->ll_total += rec_dll;
+  if (a.aux) *a.aux = degenerate ? make_float2(0.0f, __int_as_float(0))
+                                 : make_float2((float)(1.0 / tS), __int_as_float(nM));
+  if (rec_out) {
+    BpfTickRecord r;
+    r.dloglik = rec_dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
+    r.h_mean = (float)hm; r.ess = (float)ess; r.resampled = resample; r.tick = tick;
+    *rec_out = r;
+  }
+  {
+    // pass 2 runs opposite to this pass 1; the next pass 1 opposite to the
+    // last pass that wrote the particles (pass 2 on a resampling tick)
+    const int d1 = st->dirs & 1;
+    st->dirs = (resample ? d1 : (d1 ^ 1)) | ((d1 ^ 1) << 1);
+  }
+  if (a.apf != 1) {
+    st->k1 = st->k1 * kPcgMult;          // next tick's stream constants
+    st->k2 = st->k2 * kPcgMult + 1ull;
+    st->tick = tick + 1;
+  }
+  st->do_resample = resample;
+  st->nM = nM;
+  if (resample) {
+    const uint64_t old = st->u_state;
+    st->u_state = old * kPcgMult + kHostInc;
+    st->u23 = pcg_output(old) >> 9;
+    st->logS_prev = a.log_n;
+    st->resampled_prev = 1;
+    st->resample_count += 1;
+    st->src = cur;
+    st->cur = cur ^ 1;
+  } else if (degenerate) {
+    st->logS_prev = a.log_n;             // restart from uniform weights
+    st->resampled_prev = 1;
+  } else {
+    st->logS_prev = res[3];
+    st->resampled_prev = 0;
+    st->nM_prev = nM;
+  }
+  return resample;
+}
+
 // Where the plan finds the tile records of the tick and puts the tile prefixes: the plan
 // kernel reads the global copies pass 1 wrote (through L2) and writes P to global memory.
 struct PlanGlobalIO {
@@ -455,73 +530,7 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
     nt_sync<NT>();
   }
   if (tid == 0) {
-    const int tick = st->tick, cur = st->cur;
-    double dll, ess, hm;
-    int resample = 0;
-    if (degenerate) {
-      dll = -INFINITY; ess = 0.0; hm = __longlong_as_double(0x7FF8000000000000LL);
-      st->error = BPF_ERR_DEGENERATE;
-    } else {
-      dll = sh.res[0] - st->logS_prev;
-      ess = sh.res[1];
-      hm = sh.res[2];
-      resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
-    }
-    // Auxiliary particle filter: the first stage leaves log mean v (its weights)
-    // in ll_ref for the second, whose increment is log mean v + log mean w; the
-    // record's loglik_ref is log mean w, the value the reference reports
-    // (gpu_bpf_ptx_full.cu:1155-1164). The tick advances after the second stage.
-    double rec_dll = dll, ll_ref;
-    if (a.apf == 1) {
-      ll_ref = dll;
-    } else if (a.apf == 2) {
-      rec_dll = st->ll_ref + dll;
-      ll_ref = dll;
-    } else {
-      ll_ref = (st->resampled_prev ? 0.0 : st->ll_ref) + dll;
-    }
-    st->ll_ref = ll_ref;
-    st->hm = degenerate ? 0.0 : hm;
-    if (a.apf != 1) st->ll_total += rec_dll;
-    if (a.aux) *a.aux = degenerate ? make_float2(0.0f, __int_as_float(0))
-                                   : make_float2((float)(1.0 / tS), __int_as_float(nM));
-    if (rec_out) {
-      BpfTickRecord r;
-      r.dloglik = rec_dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
-      r.h_mean = (float)hm; r.ess = (float)ess; r.resampled = resample; r.tick = tick;
-      *rec_out = r;
-    }
-    {
-      // pass 2 runs opposite to this pass 1; the next pass 1 opposite to the
-      // last pass that wrote the particles (pass 2 on a resampling tick)
-      const int d1 = st->dirs & 1;
-      st->dirs = (resample ? d1 : (d1 ^ 1)) | ((d1 ^ 1) << 1);
-    }
-    if (a.apf != 1) {
-      st->k1 = st->k1 * kPcgMult;          // next tick's stream constants
-      st->k2 = st->k2 * kPcgMult + 1ull;
-      st->tick = tick + 1;
-    }
-    st->do_resample = resample;
-    st->nM = nM;
-    if (resample) {
-      const uint64_t old = st->u_state;
-      st->u_state = old * kPcgMult + kHostInc;
-      st->u23 = pcg_output(old) >> 9;
-      st->logS_prev = a.log_n;
-      st->resampled_prev = 1;
-      st->resample_count += 1;
-      st->src = cur;
-      st->cur = cur ^ 1;
-    } else if (degenerate) {
-      st->logS_prev = a.log_n;             // restart from uniform weights
-      st->resampled_prev = 1;
-    } else {
-      st->logS_prev = sh.res[3];
-      st->resampled_prev = 0;
-      st->nM_prev = nM;
-    }
-    sh.b_resample = resample;
+    sh.b_resample = plan_decide(a, st, N, nM, degenerate, sh.res, tS, rec_out);
     sh.b_Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
   }
   nt_sync<NT>();
@@ -1015,24 +1024,28 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 //   pass 1    each CTA runs its tile with pass 1's per-particle arithmetic on
 //             four times as many threads and hands the FP32 running sums along
 //             in pass 1's element order, so every tile record is bit for bit
-//             pass 1's;
-//   plan      every CTA runs the plan code on its warp 0 over all the tile
-//             records (the same FP64 sums in the same order, so every CTA takes
+//             pass 1's; while warp 0 forms the FP64 record, half the CTA scans
+//             the tile's exact fixed-point masses (needed if the tick resamples);
+//   plan      one thread per CTA runs the plan over all the tile records: the
+//             operations of the plan kernel in the same order (so every CTA takes
 //             the same decision and holds the same device state); CTA 0 writes
 //             the tick's record;
 //   resample  the same fixed-point rule (integer exact, so the ancestors do not
 //             depend on how the work is split): each CTA counts its tile's
 //             children, marks the first output of each parent's run of children
 //             in the shared memory of the CTA that owns that output (and the
-//             first output of every further CTA the run reaches), then gathers
-//             its own outputs from the parents' CTAs.
+//             first output of every further 256-output block the run reaches),
+//             then gathers its own outputs from the parents' CTAs.
 // Results equal the three-kernel tick's bit for bit: both particle buffers, the
 // log2-weights and tile exponents are loaded at the start and written back at
 // the end of the launch, with the device state.
 // ---------------------------------------------------------------------------
 constexpr int kSmallSplit = 4;                          // threads per pass-1 thread
 constexpr int kSmallThreads = kSmallSplit * kThreads;   // 1024 threads per CTA (one tile)
+constexpr int kChunks = kTile / 4;                      // four-slot chunks of a tile (one per thread)
 constexpr int kMarkWarps = kTile / kGatherStep;         // warps of the gather (256 outputs each)
+constexpr int kYStage = kSmallThreads;                  // observations staged per refill
+static_assert(kChunks == kSmallThreads, "one four-slot chunk per thread");
 static_assert(kTile % kGatherStep == 0, "the gather reads marks in 256-slot steps");
 static_assert(kSmallMaxN < 65536, "start marks hold parent + 1 in 16 bits");
 
@@ -1040,32 +1053,19 @@ struct FusedShared {
   float h[2][kTile];                          // particle buffers (DevState::cur / src), this CTA's tile
   float w[kTile];                             // log2-weights of the tile
   unsigned short marks[kTile + kGatherStep];  // start marks of this CTA's outputs: parent + 1, 0 = none
+  unsigned long long chunkE[kChunks];         // exact fixed-point mass of each four-slot chunk
+  unsigned long long chunkP[kChunks];         // its exclusive prefix within the tile
+  float ys[kYStage];                          // observations of the next ticks
   float4 rec[2];                              // tile record {S, Q, H, n_k}, by tick parity
   unsigned long long E[2];                    // exact fixed-point tile mass, by tick parity
   int nexp[2];                                // tile exponent, by tick parity
   FusedShared* peer[kSmallTiles];             // every CTA's FusedShared (distributed shared memory)
   __align__(16) DevState st;
-  PlanShared<32> pl;
-  __align__(16) unsigned char plan_stage[(plan_smem_bytes(kSmallTiles) + 15) & ~(size_t)15];
   unsigned long long P[kSmallTiles];          // the tick's tile prefixes (all tiles)
   float s_max[kSmallThreads / 32];
   float s_part[3][kThreads];
   unsigned long long s_E[kThreads];
-  unsigned long long scan[kSmallThreads / 32 + 1];
-  unsigned wmax[kSmallThreads / 32];
-};
-
-// The plan of the fused tick reads every CTA's tile record of the tick through distributed
-// shared memory and keeps the tile prefixes in its own CTA.
-struct PlanClusterIO {
-  FusedShared* const* peer;
-  int par;
-  unsigned long long* P;
-  static constexpr bool kStoreState = false;
-  __device__ __forceinline__ float4 rec(int k) const { return peer[k]->rec[par]; }
-  __device__ __forceinline__ int nexp(int k) const { return peer[k]->nexp[par]; }
-  __device__ __forceinline__ unsigned long long E(int k) const { return peer[k]->E[par]; }
-  __device__ __forceinline__ void set_P(int k, unsigned long long v) const { P[k] = v; }
+  unsigned long long scan2[16];
 };
 
 template <int NCTA>
@@ -1082,10 +1082,12 @@ __device__ __forceinline__ void cluster_sync_all() {
 // adjacent threads 4v .. 4v + 3, one group each, with the per-particle arithmetic of
 // pass1_tile; the FP32 tile partials are accumulated in pass 1's order by handing the running
 // sums from one of those threads to the next, and warp 0 forms the FP64 tile record in pass
-// 1's order. nk_prev: the tile's exponent of the previous tick (the carried weights' frame).
+// 1's order. Thread 4v + s's group is the four-slot chunk c = v + 256 s (slots 4c .. 4c + 3);
+// warps 16..31 scan the chunks' exact masses into chunkP meanwhile.
+// nk_prev: the tile's exponent of the previous tick (the carried weights' frame).
 template <bool TSTATE, bool GAUSS>
-__device__ __forceinline__ void pass1_fused(const TickArgs& a, const float* y_ptr, int N, int tile0, int par,
-                                            int nk_prev, FusedShared& sh) {
+__device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, int tile0, int par, int nk_prev,
+                                            FusedShared& sh) {
   constexpr int SPLIT = kSmallSplit;
   const int tid = threadIdx.x;
   const int v = tid / SPLIT, sidx = tid % SPLIT;
@@ -1095,7 +1097,6 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, const float* y_pt
   const bool carry = st.resampled_prev == 0;
   const uint64_t k1 = st.k1, k2 = st.k2;
   float* hb = sh.h[st.cur];
-  const float y = y_ptr ? __ldg(y_ptr) : a.obs.y;
   ObsModel obs = a.obs;
   obs.y = y;
   const float y2 = y * y;
@@ -1106,7 +1107,8 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, const float* y_pt
   const float y2nu = __fmul_rn(y2, obs.inv_nu);
   const unsigned long long k33 = k2 << 33;
 
-  const int l0 = 4 * (v + kThreads * sidx);      // the group's first slot in the tile
+  const int c = v + kThreads * sidx;             // this thread's chunk
+  const int l0 = 4 * c;
   const float4 h4 = *reinterpret_cast<const float4*>(hb + l0);
   const float4 w4 = carry ? *reinterpret_cast<const float4*>(sh.w + l0) : make_float4(0.f, 0.f, 0.f, 0.f);
   float hh[4] = {h4.x, h4.y, h4.z, h4.w};
@@ -1149,6 +1151,7 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, const float* y_pt
     E += fix_weight(wv[e]);
   }
   *reinterpret_cast<float4*>(sh.w + l0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+  sh.chunkE[c] = E;
   // pass 1's per-thread FP32 sums, in its element order, handed along the SPLIT threads
   float aS = 0.f, aQ = 0.f, aH = 0.f;
 #pragma unroll
@@ -1188,7 +1191,106 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, const float* y_pt
       sh.E[par] = tE;
       sh.rec[par] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
     }
+  } else if (warp >= 16) {                      // exclusive prefix of the chunk masses, 2 chunks a thread
+    const int t2 = tid - 512;
+    const unsigned long long e0 = sh.chunkE[2 * t2], e1 = sh.chunkE[2 * t2 + 1];
+    const unsigned long long s2 = e0 + e1;
+    const unsigned long long inc = warp_incl_scan_add(s2, lane);
+    if (lane == 31) sh.scan2[warp - 16] = inc;
+    asm volatile("bar.sync 1, 512;" ::: "memory");
+    unsigned long long off = 0ull;
+    for (int w = 16; w < warp; ++w) off += sh.scan2[w - 16];
+    const unsigned long long ex = off + inc - s2;
+    sh.chunkP[2 * t2] = ex;
+    sh.chunkP[2 * t2 + 1] = ex + e0;
   }
+}
+
+// The plan of a fused tick by one thread, for NCTA <= kSmallTiles tiles: the operations of
+// plan_body on one warp in the same order. There lane k holds tile k's FP64 sums (the other
+// lanes exact zeros, so the warp's butterfly sums reduce to the pairwise sums below and every
+// lane holds the same totals), and the integer resampling plan is exact. Returns the decision.
+template <int NCTA>
+__device__ __forceinline__ int plan_fused(const TickArgs& a, int N, FusedShared& sh, int par, BpfTickRecord* rec_out) {
+  static_assert(NCTA >= 1 && NCTA <= 4, "the pairwise sums below cover four lanes");
+  DevState* st = &sh.st;
+  float4 r[4];
+  unsigned long long E[4];
+  int nk[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k < NCTA) {
+      r[k] = sh.peer[k]->rec[par];
+      E[k] = sh.peer[k]->E[par];
+      nk[k] = __float_as_int(r[k].w);
+    } else {
+      r[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      E[k] = 0ull;
+      nk[k] = kNkEmpty;
+    }
+  }
+  int nM = kNkEmpty;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) nM = max(nM, nk[k]);
+  // each lane's running frame is its own tile's, then the global frame 2^nM
+  double S[4], Q[4], H[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (nk[k] != kNkEmpty) {
+      const double sc = pow2d(nk[k] - nM);
+      S[k] = __dmul_rn(__dadd_rn(0.0, (double)r[k].x), sc);
+      Q[k] = __dmul_rn(__dadd_rn(0.0, (double)r[k].y), __dmul_rn(sc, sc));
+      H[k] = __dmul_rn(__dadd_rn(0.0, (double)r[k].z), sc);
+    } else {
+      S[k] = 0.0; Q[k] = 0.0; H[k] = 0.0;
+    }
+  }
+  // the butterfly of warp_sum_d: the first three levels add the zero lanes 16.., 8.., 4..
+  auto wsum = [](const double* v) {
+    const double a0 = __dadd_rn(v[0], 0.0), a1 = __dadd_rn(v[1], 0.0);
+    const double a2 = __dadd_rn(v[2], 0.0), a3 = __dadd_rn(v[3], 0.0);
+    return __dadd_rn(__dadd_rn(a0, a2), __dadd_rn(a1, a3));
+  };
+  const double tS = wsum(S), tQ = wsum(Q), tH = wsum(H);
+  const bool degenerate = (nM == kNkEmpty) || !(tS > 0.0);
+  constexpr double kLn2d = 0.693147180559945309417232121458;
+  double res[4] = {0.0, 0.0, 0.0, 0.0};
+  if (!degenerate) {
+    const double L = log(tS);
+    res[0] = __fma_rn((double)nM, kLn2d, L);
+    res[1] = tS * tS / tQ;
+    res[2] = tH / tS;
+    res[3] = L;
+  }
+  const int resample = plan_decide(a, st, N, nM, degenerate, res, tS, rec_out);
+  if (!resample) return 0;
+
+  // fixed-point CDF over the tiles, target spacing and base, item count (as plan_body)
+  const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
+  unsigned long long Pk[5];
+  Pk[0] = 0ull;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    Pk[k + 1] = Pk[k] + ((k < NCTA && nk[k] != kNkEmpty) ? shr64(E[k], nM - nk[k] + kFixF - Fg) : 0ull);
+  const unsigned long long total = Pk[NCTA];
+  unsigned long long delta = udiv_fp64(total, (unsigned long long)N);
+  if (delta == 0ull) { delta = 1ull; st->error = BPF_ERR_DEGENERATE; }
+  const unsigned long long u = st->u23;
+  const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
+  const unsigned long long base = (hi << 41) | (lo >> 23);       // floor(u * delta / 2^23)
+  const unsigned long long magic = udiv_magic_of(delta);
+  st->base = base; st->delta = delta; st->delta_magic = magic; st->total = total; st->Fg = Fg;
+  int n_items = 0;
+  int o = targets_below(Pk[0], base, delta, magic, N);
+#pragma unroll
+  for (int k = 0; k < NCTA; ++k) {
+    sh.P[k] = Pk[k];
+    const int o_next = targets_below(Pk[k + 1], base, delta, magic, N);
+    n_items += (o_next - o + kOutChunk - 1) / kOutChunk;
+    o = o_next;
+  }
+  st->n_items = n_items;
+  return 1;
 }
 
 // Start mark of output o (parent + 1) in the shared memory of the CTA that owns o.
@@ -1211,14 +1313,12 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
   const int r = (nk == kNkEmpty) ? 64 : st.nM - nk + kFixF - st.Fg;
   const unsigned long long Pk = sh.P[k];
 
-  // four consecutive slots per thread; the tile-local exclusive prefix of the exact weights
+  // chunk tid: slots 4 tid .. 4 tid + 3, its tile-local exclusive prefix from pass 1's scan
   const int l0 = 4 * tid, j0 = tile0 + l0;
   const float4 w4 = *reinterpret_cast<const float4*>(sh.w + l0);
   const unsigned long long f[4] = {fix_weight(tile_weight(w4.x)), fix_weight(tile_weight(w4.y)),
                                    fix_weight(tile_weight(w4.z)), fix_weight(tile_weight(w4.w))};
-  const unsigned long long run = (r < 64) ? (f[0] + f[1]) + (f[2] + f[3]) : 0ull;
-  unsigned long long tot;
-  const unsigned long long loc = block_excl_scan_add<kSmallThreads>(run, &tot, sh.scan);
+  const unsigned long long loc = sh.chunkP[tid];
 
   // child counts against tile-frame thresholds, as pass 2
   int q = targets_below(Pk + shr64(loc, r), base, delta, magic, N);
@@ -1234,35 +1334,25 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
     acc += f[e];
     if (acc >= th) {
       const unsigned long long diff = acc - th;
-      int c = 1 + (diff >= D) + (diff >= 2ull * D) + (diff >= 3ull * D);
-      if (c == 4 && diff >= 4ull * D) c = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
-      const int q1 = min(q + c, N);
+      int cn = 1 + (diff >= D) + (diff >= 2ull * D) + (diff >= 3ull * D);
+      if (cn == 4 && diff >= 4ull * D) cn = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
+      const int q1 = min(q + cn, N);
       const int val = j0 + e + 1;
       put_mark<NCTA>(sh, q, val);
-      for (int b = ((q >> 12) + 1) << 12; b < q1; b += kTile) put_mark<NCTA>(sh, b, val);   // first output of each further CTA
-      th = (q1 >= N) ? kThCap : th + (unsigned long long)c * D;
+      // the first output of every further 256-output block the run reaches
+      for (int b = (q | (kGatherStep - 1)) + 1; b < q1; b += kGatherStep) put_mark<NCTA>(sh, b, val);
+      th = (q1 >= N) ? kThCap : th + (unsigned long long)cn * D;
       q = q1;
     }
   }
   cluster_sync_all<NCTA>();                      // every start mark is in place
 
   // gather: the ancestor of output o is the last start mark at or before o; the first output of
-  // every CTA has one, so no CTA needs another's marks
+  // every 256-output block has one, so each warp's block stands alone
   const int n_out = min(N - tile0, kTile);
   const int o0 = warp * kGatherStep;
-  const bool active = warp < kMarkWarps && o0 < n_out;
-  uint4 m = make_uint4(0u, 0u, 0u, 0u);
-  if (active) {
-    m = reinterpret_cast<const uint4*>(sh.marks + o0)[lane];
-    const unsigned vv = __vmaxu2(__vmaxu2(m.x, m.y), __vmaxu2(m.z, m.w));
-    unsigned wm = max(vv & 0xffffu, vv >> 16);
-    wm = __reduce_max_sync(0xffffffffu, wm);
-    if (lane == 0) sh.wmax[warp] = wm;
-  }
-  __syncthreads();
-  if (active) {
-    unsigned carry = 0u;
-    for (int w = 0; w < warp; ++w) carry = max(carry, sh.wmax[w]);
+  if (warp < kMarkWarps && o0 < n_out) {
+    const uint4 m = reinterpret_cast<const uint4*>(sh.marks + o0)[lane];
     unsigned am[8];
     am[0] = m.x & 0xffffu;
     am[1] = max(am[0], m.x >> 16);
@@ -1279,7 +1369,7 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
       if (lane >= off) xm = max(xm, t);
     }
     unsigned pre = __shfl_up_sync(0xffffffffu, xm, 1);
-    pre = max(carry, lane == 0 ? 0u : pre);
+    if (lane == 0) pre = 0u;
     const int src = st.src;
     float* hd = sh.h[st.cur];
     const int o = o0 + 8 * lane;
@@ -1317,18 +1407,20 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
   reinterpret_cast<float4*>(sh.w)[tid] = __ldcg(reinterpret_cast<const float4*>(p.w + tile0) + tid);
   constexpr int kMarkVecs = (int)(sizeof(sh.marks) / 16);
   if (tid < kMarkVecs) reinterpret_cast<uint4*>(sh.marks)[tid] = make_uint4(0u, 0u, 0u, 0u);
-  __syncthreads();
 
   for (int t = 0; t < n_ticks; ++t) {
     const int par = t & 1;
-    pass1_fused<TSTATE, GAUSS>(a, a.y_ptr ? a.y_ptr + t : nullptr, N, tile0, par, sh.nexp[par ^ 1], sh);
+    if (a.y_ptr && (t & (kYStage - 1)) == 0) {       // the next kYStage observations
+      __syncthreads();
+      if (t + tid < n_ticks) sh.ys[tid] = __ldg(a.y_ptr + t + tid);
+    }
+    __syncthreads();
+    const float y = a.y_ptr ? sh.ys[t & (kYStage - 1)] : a.obs.y;
+    pass1_fused<TSTATE, GAUSS>(a, y, N, tile0, par, sh.nexp[par ^ 1], sh);
     cluster_sync_all<NCTA>();                   // every tile record of the tick is in place
-    if (tid < 32)
-      plan_body<32, false>(p, a, sh.st, sh.pl, sh.plan_stage, PlanClusterIO{sh.peer, par, sh.P},
-                           (a.rec && k == 0) ? a.rec + t : nullptr, nullptr);
+    if (tid == 0) plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
     __syncthreads();
     if (sh.st.do_resample) resample_fused<NCTA>(a, N, k, par, sh);
-    __syncthreads();
   }
   cluster_sync_all<NCTA>();                     // no CTA leaves while another may read its shared memory
   reinterpret_cast<float4*>(p.h0 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[0])[tid];
