@@ -1040,14 +1040,19 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 // log2-weights and tile exponents are loaded at the start and written back at
 // the end of the launch, with the device state.
 // ---------------------------------------------------------------------------
-constexpr int kSmallSplit = 4;                          // threads per pass-1 thread
-constexpr int kSmallThreads = kSmallSplit * kThreads;   // 1024 threads per CTA (one tile)
+constexpr int kSmallThreads = 4 * kThreads;             // 1024 threads per CTA (one tile)
+constexpr int kSmallSplit = 2;                          // threads per pass-1 thread in the fused pass 1
 constexpr int kChunks = kTile / 4;                      // four-slot chunks of a tile (one per thread)
 constexpr int kMarkWarps = kTile / kGatherStep;         // warps of the gather (256 outputs each)
 constexpr int kYStage = kSmallThreads;                  // observations staged per refill
 static_assert(kChunks == kSmallThreads, "one four-slot chunk per thread");
 static_assert(kTile % kGatherStep == 0, "the gather reads marks in 256-slot steps");
 static_assert(kSmallMaxN < 65536, "start marks hold parent + 1 in 16 bits");
+
+struct FusedPlan {
+  unsigned long long base, delta, magic, total;
+  int nM, Fg, items, zero_spacing;
+};
 
 struct FusedShared {
   float h[2][kTile];                          // particle buffers (DevState::cur / src), this CTA's tile
@@ -1062,6 +1067,7 @@ struct FusedShared {
   FusedShared* peer[kSmallTiles];             // every CTA's FusedShared (distributed shared memory)
   __align__(16) DevState st;
   unsigned long long P[kSmallTiles];          // the tick's tile prefixes (all tiles)
+  FusedPlan pl;                               // the tick's resampling plan
   float s_max[kSmallThreads / 32];
   float s_part[3][kThreads];
   unsigned long long s_E[kThreads];
@@ -1078,101 +1084,118 @@ __device__ __forceinline__ void cluster_sync_all() {
 }
 
 // Pass 1 of this CTA's tile (global slots tile0 .. tile0 + kTile - 1) on the shared-memory
-// copies: pass-1 thread v's sixteen particles (four float4 groups) go to the kSmallSplit
-// adjacent threads 4v .. 4v + 3, one group each, with the per-particle arithmetic of
-// pass1_tile; the FP32 tile partials are accumulated in pass 1's order by handing the running
-// sums from one of those threads to the next, and warp 0 forms the FP64 tile record in pass
-// 1's order. Thread 4v + s's group is the four-slot chunk c = v + 256 s (slots 4c .. 4c + 3);
-// warps 16..31 scan the chunks' exact masses into chunkP meanwhile.
+// copies, by the first kThreads * SPLIT threads: pass-1 thread v's sixteen particles (four
+// float4 groups r) go to SPLIT threads, 4 / SPLIT consecutive groups each, with the
+// per-particle arithmetic of pass1_tile; the FP32 tile partials are accumulated in pass 1's
+// order by handing the running sums from one of those threads to the next, and warp 0 forms
+// the FP64 tile record in pass 1's order. Within a warp the SPLIT threads of v sit 32 / SPLIT
+// lanes apart, so the float4 accesses of a warp cover whole 128-byte rows. Group r of v is the
+// four-slot chunk c = v + 256 r (slots 4c .. 4c + 3); warps 16..31 scan the chunks' exact
+// masses into chunkP while warp 0 forms the record.
 // nk_prev: the tile's exponent of the previous tick (the carried weights' frame).
-template <bool TSTATE, bool GAUSS>
+template <bool TSTATE, bool GAUSS, int SPLIT>
 __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, int tile0, int par, int nk_prev,
                                             FusedShared& sh) {
-  constexpr int SPLIT = kSmallSplit;
+  static_assert(SPLIT == 1 || SPLIT == 2 || SPLIT == 4, "four float4 groups per pass-1 thread");
+  constexpr int R = 4 / SPLIT;                   // float4 groups of a thread
+  constexpr int NT1 = kThreads * SPLIT;          // threads of pass 1
+  constexpr int LW = 32 / SPLIT;                 // lanes of a warp with the same s
   const int tid = threadIdx.x;
-  const int v = tid / SPLIT, sidx = tid % SPLIT;
   const int lane = tid & 31, warp = tid >> 5;
-  const DevState& st = sh.st;
-  const int tick = st.tick;
-  const bool carry = st.resampled_prev == 0;
-  const uint64_t k1 = st.k1, k2 = st.k2;
-  float* hb = sh.h[st.cur];
-  ObsModel obs = a.obs;
-  obs.y = y;
-  const float y2 = y * y;
-  float carry_off = 0.0f;
-  if (carry) carry_off = (nk_prev == kNkEmpty) ? -INFINITY : (float)(nk_prev - st.nM_prev);
-  const float gauss_c = kGaussLog2C + carry_off;
-  const float t_c = __fmul_rn(obs.c_obs, kLog2e) + carry_off;
-  const float y2nu = __fmul_rn(y2, obs.inv_nu);
-  const unsigned long long k33 = k2 << 33;
-
-  const int c = v + kThreads * sidx;             // this thread's chunk
-  const int l0 = 4 * c;
-  const float4 h4 = *reinterpret_cast<const float4*>(hb + l0);
-  const float4 w4 = carry ? *reinterpret_cast<const float4*>(sh.w + l0) : make_float4(0.f, 0.f, 0.f, 0.f);
-  float hh[4] = {h4.x, h4.y, h4.z, h4.w};
-  const float wp[4] = {w4.x, w4.y, w4.z, w4.w};
-  float x[4];
+  const int s = lane / LW, v = LW * warp + (lane % LW);
+  float wv[4 * R], dv[4 * R], hv[4 * R];
+  int nk = kNkEmpty;
+  if (tid < NT1) {
+    const DevState& st = sh.st;
+    const int tick = st.tick;
+    const bool carry = st.resampled_prev == 0;
+    const uint64_t k1 = st.k1, k2 = st.k2;
+    float* hb = sh.h[st.cur];
+    ObsModel obs = a.obs;
+    obs.y = y;
+    const float y2 = y * y;
+    float carry_off = 0.0f;
+    if (carry) carry_off = (nk_prev == kNkEmpty) ? -INFINITY : (float)(nk_prev - st.nM_prev);
+    const float gauss_c = kGaussLog2C + carry_off;
+    const float t_c = __fmul_rn(obs.c_obs, kLog2e) + carry_off;
+    const float y2nu = __fmul_rn(y2, obs.inv_nu);
+    const unsigned long long k33 = k2 << 33;
+    float x[4 * R];
 #pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const int i = tile0 + l0 + e;
-    float h = hh[e];
-    if (tick > 0) {
-      const uint64_t s = k1 + k2 * pcg_inc((uint32_t)i);
-      float z = icdf_normal_warp(pcg_uniform(pcg_output(s)));
-      if (TSTATE) z *= tstate_scale_warp(s, k33, a.nu_int, a.nu_state);
-      h = propagate(h, a.mu, a.rho, a.sigma, z);
-    }
-    float xx = GAUSS ? obs_log2pdf_gauss_plus(y2, h, gauss_c) : obs_log2pdf_t_plus(obs, y2nu, h, t_c);
-    if (carry) xx += wp[e];
-    if (i >= N) xx = -INFINITY;                   // padding slots carry no weight
-    hh[e] = h;
-    x[e] = xx;
-  }
-  *reinterpret_cast<float4*>(hb + l0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
-
-  float mx = fmaxf(fmaxf(x[0], x[1]), fmaxf(x[2], x[3]));
-  mx = warp_max_f(mx);
-  if (lane == 0) sh.s_max[warp] = mx;
-  __syncthreads();
-  mx = sh.s_max[0];
-#pragma unroll 8
-  for (int w = 1; w < kSmallThreads / 32; ++w) mx = fmaxf(mx, sh.s_max[w]);
-  const int nk = (mx == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(mx, -1.0e9f));
-  const float fnk = (nk == kNkEmpty) ? INFINITY : (float)nk;
-
-  float wv[4], dv[4];
-  unsigned long long E = 0ull;
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    dv[e] = x[e] - fnk;
-    wv[e] = tile_weight(dv[e]);
-    E += fix_weight(wv[e]);
-  }
-  *reinterpret_cast<float4*>(sh.w + l0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
-  sh.chunkE[c] = E;
-  // pass 1's per-thread FP32 sums, in its element order, handed along the SPLIT threads
-  float aS = 0.f, aQ = 0.f, aH = 0.f;
-#pragma unroll
-  for (int step = 0; step < SPLIT; ++step) {
-    if (sidx == step) {
+    for (int rr = 0; rr < R; ++rr) {
+      const int l0 = 4 * (v + kThreads * (s * R + rr));
+      const float4 h4 = *reinterpret_cast<const float4*>(hb + l0);
+      const float4 w4 = carry ? *reinterpret_cast<const float4*>(sh.w + l0) : make_float4(0.f, 0.f, 0.f, 0.f);
+      float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+      const float wp[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        aS += wv[e];
-        aQ = fmaf(wv[e], wv[e], aQ);
-        aH = fmaf(wv[e], hh[e], aH);
+        const int i = tile0 + l0 + e;
+        float h = hh[e];
+        if (tick > 0) {
+          const uint64_t st64 = k1 + k2 * pcg_inc((uint32_t)i);
+          float z = icdf_normal_warp(pcg_uniform(pcg_output(st64)));
+          if (TSTATE) z *= tstate_scale_warp(st64, k33, a.nu_int, a.nu_state);
+          h = propagate(h, a.mu, a.rho, a.sigma, z);
+        }
+        float xx = GAUSS ? obs_log2pdf_gauss_plus(y2, h, gauss_c) : obs_log2pdf_t_plus(obs, y2nu, h, t_c);
+        if (carry) xx += wp[e];
+        if (i >= N) xx = -INFINITY;               // padding slots carry no weight
+        hh[e] = h;
+        x[4 * rr + e] = xx;
+        hv[4 * rr + e] = h;
+      }
+      *reinterpret_cast<float4*>(hb + l0) = make_float4(hh[0], hh[1], hh[2], hh[3]);
+    }
+    float mx = x[0];
+#pragma unroll
+    for (int e = 1; e < 4 * R; ++e) mx = fmaxf(mx, x[e]);
+    mx = warp_max_f(mx);
+    if (lane == 0) sh.s_max[warp] = mx;
+    if constexpr (NT1 == kSmallThreads) __syncthreads();
+    else asm volatile("bar.sync 1, %0;" ::"n"(NT1) : "memory");
+    mx = warp_max_f(lane < NT1 / 32 ? sh.s_max[lane] : -INFINITY);
+    nk = (mx == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(mx, -1.0e9f));
+    const float fnk = (nk == kNkEmpty) ? INFINITY : (float)nk;
+    unsigned long long E = 0ull;
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      unsigned long long Ec = 0ull;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        dv[4 * rr + e] = x[4 * rr + e] - fnk;
+        wv[4 * rr + e] = tile_weight(dv[4 * rr + e]);
+        Ec += fix_weight(wv[4 * rr + e]);
+      }
+      const int c = v + kThreads * (s * R + rr);
+      *reinterpret_cast<float4*>(sh.w + 4 * c) = make_float4(dv[4 * rr], dv[4 * rr + 1], dv[4 * rr + 2], dv[4 * rr + 3]);
+      sh.chunkE[c] = Ec;
+      E += Ec;
+    }
+    // pass 1's per-thread FP32 sums, in its element order, handed along the SPLIT threads
+    float aS = 0.f, aQ = 0.f, aH = 0.f;
+#pragma unroll
+    for (int step = 0; step < SPLIT; ++step) {
+      if (s == step) {
+#pragma unroll
+        for (int e = 0; e < 4 * R; ++e) {
+          aS += wv[e];
+          aQ = fmaf(wv[e], wv[e], aQ);
+          aH = fmaf(wv[e], hv[e], aH);
+        }
+      }
+      if (step + 1 < SPLIT) {
+        const float nS = __shfl_up_sync(0xffffffffu, aS, LW);
+        const float nQ = __shfl_up_sync(0xffffffffu, aQ, LW);
+        const float nH = __shfl_up_sync(0xffffffffu, aH, LW);
+        if (s == step + 1) { aS = nS; aQ = nQ; aH = nH; }
       }
     }
-    const float nS = __shfl_up_sync(0xffffffffu, aS, 1);
-    const float nQ = __shfl_up_sync(0xffffffffu, aQ, 1);
-    const float nH = __shfl_up_sync(0xffffffffu, aH, 1);
-    if (step + 1 < SPLIT && sidx == step + 1) { aS = nS; aQ = nQ; aH = nH; }
-  }
 #pragma unroll
-  for (int o = 1; o < SPLIT; o <<= 1) E += __shfl_xor_sync(0xffffffffu, E, o);
-  if (sidx == SPLIT - 1) { sh.s_part[0][v] = aS; sh.s_part[1][v] = aQ; sh.s_part[2][v] = aH; }
-  if (sidx == 0) sh.s_E[v] = E;
+    for (int o = LW; o < 32; o <<= 1) E += __shfl_xor_sync(0xffffffffu, E, o);
+    if (s == SPLIT - 1) { sh.s_part[0][v] = aS; sh.s_part[1][v] = aQ; sh.s_part[2][v] = aH; }
+    if (s == 0) sh.s_E[v] = E;
+  }
   __syncthreads();
   if (warp == 0) {                              // pass 1's FP64 tile combine, same order
     double tS = 0.0, tQ = 0.0, tH = 0.0;
@@ -1197,7 +1220,7 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
     const unsigned long long s2 = e0 + e1;
     const unsigned long long inc = warp_incl_scan_add(s2, lane);
     if (lane == 31) sh.scan2[warp - 16] = inc;
-    asm volatile("bar.sync 1, 512;" ::: "memory");
+    asm volatile("bar.sync 2, 512;" ::: "memory");
     unsigned long long off = 0ull;
     for (int w = 16; w < warp; ++w) off += sh.scan2[w - 16];
     const unsigned long long ex = off + inc - s2;
@@ -1206,26 +1229,23 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
   }
 }
 
-// The plan of a fused tick by one thread, for NCTA <= kSmallTiles tiles: the operations of
-// plan_body on one warp in the same order. There lane k holds tile k's FP64 sums (the other
-// lanes exact zeros, so the warp's butterfly sums reduce to the pairwise sums below and every
-// lane holds the same totals), and the integer resampling plan is exact. Returns the decision.
+// The plan of a fused tick by one thread, for NCTA <= kSmallTiles tiles: the statistics and
+// the decision, the operations of plan_body on one warp in the same order. There lane k holds
+// tile k's FP64 sums (the other lanes exact zeros, so the warp's butterfly sums reduce to the
+// pairwise sums below and every lane holds the same totals).
 template <int NCTA>
-__device__ __forceinline__ int plan_fused(const TickArgs& a, int N, FusedShared& sh, int par, BpfTickRecord* rec_out) {
+__device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared& sh, int par, BpfTickRecord* rec_out) {
   static_assert(NCTA >= 1 && NCTA <= 4, "the pairwise sums below cover four lanes");
   DevState* st = &sh.st;
   float4 r[4];
-  unsigned long long E[4];
   int nk[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     if (k < NCTA) {
       r[k] = sh.peer[k]->rec[par];
-      E[k] = sh.peer[k]->E[par];
       nk[k] = __float_as_int(r[k].w);
     } else {
       r[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-      E[k] = 0ull;
       nk[k] = kNkEmpty;
     }
   }
@@ -1262,10 +1282,29 @@ __device__ __forceinline__ int plan_fused(const TickArgs& a, int N, FusedShared&
     res[2] = tH / tS;
     res[3] = L;
   }
-  const int resample = plan_decide(a, st, N, nM, degenerate, res, tS, rec_out);
-  if (!resample) return 0;
+  plan_decide(a, st, N, nM, degenerate, res, tS, rec_out);
+}
 
-  // fixed-point CDF over the tiles, target spacing and base, item count (as plan_body)
+// The tick's resampling plan by one thread, whether or not the tick resamples (it runs beside
+// the decision): the fixed-point CDF over the tiles, the target spacing, base and reciprocal and
+// the item count, as plan_body. u_state: the resampling-uniform state at the start of the tick.
+template <int NCTA>
+__device__ __forceinline__ void plan_fused_targets(int N, FusedShared& sh, int par, unsigned long long u_state) {
+  unsigned long long E[4];
+  int nk[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k < NCTA) {
+      nk[k] = sh.peer[k]->nexp[par];
+      E[k] = sh.peer[k]->E[par];
+    } else {
+      nk[k] = kNkEmpty;
+      E[k] = 0ull;
+    }
+  }
+  int nM = kNkEmpty;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) nM = max(nM, nk[k]);
   const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
   unsigned long long Pk[5];
   Pk[0] = 0ull;
@@ -1274,23 +1313,64 @@ __device__ __forceinline__ int plan_fused(const TickArgs& a, int N, FusedShared&
     Pk[k + 1] = Pk[k] + ((k < NCTA && nk[k] != kNkEmpty) ? shr64(E[k], nM - nk[k] + kFixF - Fg) : 0ull);
   const unsigned long long total = Pk[NCTA];
   unsigned long long delta = udiv_fp64(total, (unsigned long long)N);
-  if (delta == 0ull) { delta = 1ull; st->error = BPF_ERR_DEGENERATE; }
-  const unsigned long long u = st->u23;
+  const bool zero_spacing = delta == 0ull;
+  if (zero_spacing) delta = 1ull;
+  const unsigned long long u = pcg_output(u_state) >> 9;       // the tick's resampling uniform
   const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
-  const unsigned long long base = (hi << 41) | (lo >> 23);       // floor(u * delta / 2^23)
+  const unsigned long long base = (hi << 41) | (lo >> 23);     // floor(u * delta / 2^23)
   const unsigned long long magic = udiv_magic_of(delta);
-  st->base = base; st->delta = delta; st->delta_magic = magic; st->total = total; st->Fg = Fg;
   int n_items = 0;
   int o = targets_below(Pk[0], base, delta, magic, N);
 #pragma unroll
   for (int k = 0; k < NCTA; ++k) {
-    sh.P[k] = Pk[k];
     const int o_next = targets_below(Pk[k + 1], base, delta, magic, N);
     n_items += (o_next - o + kOutChunk - 1) / kOutChunk;
     o = o_next;
+    sh.P[k] = Pk[k];
   }
-  st->n_items = n_items;
-  return 1;
+  FusedPlan& pl = sh.pl;
+  pl.base = base; pl.delta = delta; pl.magic = magic; pl.total = total;
+  pl.nM = nM; pl.Fg = Fg; pl.items = n_items; pl.zero_spacing = zero_spacing ? 1 : 0;
+}
+
+// The resampling plan into the device state (thread 0, on a resampling tick).
+__device__ __forceinline__ void store_fused_plan(DevState* st, const FusedShared& sh) {
+  const FusedPlan& pl = sh.pl;
+  if (pl.zero_spacing) st->error = BPF_ERR_DEGENERATE;
+  st->base = pl.base; st->delta = pl.delta; st->delta_magic = pl.magic; st->total = pl.total;
+  st->Fg = pl.Fg; st->n_items = pl.items;
+}
+
+// A thread's four-slot chunk (slots 4 tid .. 4 tid + 3 of the tile) against the tick's
+// targets: its exact weights, tile-local prefix, first target and tile-frame thresholds.
+struct ChunkTargets {
+  unsigned long long f[4];
+  unsigned long long th, D;
+  int q;
+};
+
+template <int NCTA>
+__device__ __forceinline__ ChunkTargets chunk_targets(int N, int k, int par, const FusedShared& sh) {
+  const int tid = threadIdx.x;
+  const FusedPlan& pl = sh.pl;
+  const int nk = sh.nexp[par];
+  const int r = (nk == kNkEmpty) ? 64 : pl.nM - nk + kFixF - pl.Fg;
+  const unsigned long long Pk = sh.P[k], base = pl.base, delta = pl.delta;
+  const int l0 = 4 * tid, j0 = k * kTile + l0;
+  const float4 w4 = *reinterpret_cast<const float4*>(sh.w + l0);
+  ChunkTargets ct;
+  ct.f[0] = fix_weight(tile_weight(w4.x)); ct.f[1] = fix_weight(tile_weight(w4.y));
+  ct.f[2] = fix_weight(tile_weight(w4.z)); ct.f[3] = fix_weight(tile_weight(w4.w));
+  const unsigned long long loc = sh.chunkP[tid];
+  // child counts against tile-frame thresholds, as pass 2
+  ct.q = targets_below(Pk + shr64(loc, r), base, delta, pl.magic, N);
+  ct.th = kThCap; ct.D = kThCap;
+  if (r < 64 && ct.q < N && j0 < N) {
+    const unsigned long long m = base + (unsigned long long)ct.q * delta - Pk + 1ull;
+    if (m <= (~0ull >> r)) ct.th = min((m << r) - loc, kThCap);
+    if (delta <= (kThCap >> r)) ct.D = delta << r;
+  }
+  return ct;
 }
 
 // Start mark of output o (parent + 1) in the shared memory of the CTA that owns o.
@@ -1303,35 +1383,20 @@ __device__ __forceinline__ void put_mark(FusedShared& sh, int o, int val) {
 // Resampling of a fused tick, this CTA's part: the children of its tile's particles (start
 // marks into the owners' shared memory), a cluster barrier, then the gather of its own outputs.
 template <int NCTA>
-__device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, int par, FusedShared& sh) {
+__device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, const ChunkTargets& ct,
+                                               FusedShared& sh) {
   static_assert(kTile == 1 << 12, "output owner = o >> 12");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tile0 = k * kTile;
   const DevState& st = sh.st;
-  const unsigned long long base = st.base, delta = st.delta, magic = st.delta_magic;
-  const int nk = sh.nexp[par];
-  const int r = (nk == kNkEmpty) ? 64 : st.nM - nk + kFixF - st.Fg;
-  const unsigned long long Pk = sh.P[k];
-
-  // chunk tid: slots 4 tid .. 4 tid + 3, its tile-local exclusive prefix from pass 1's scan
-  const int l0 = 4 * tid, j0 = tile0 + l0;
-  const float4 w4 = *reinterpret_cast<const float4*>(sh.w + l0);
-  const unsigned long long f[4] = {fix_weight(tile_weight(w4.x)), fix_weight(tile_weight(w4.y)),
-                                   fix_weight(tile_weight(w4.z)), fix_weight(tile_weight(w4.w))};
-  const unsigned long long loc = sh.chunkP[tid];
-
-  // child counts against tile-frame thresholds, as pass 2
-  int q = targets_below(Pk + shr64(loc, r), base, delta, magic, N);
-  unsigned long long th = kThCap, D = kThCap;
-  if (r < 64 && q < N && j0 < N) {
-    const unsigned long long m = base + (unsigned long long)q * delta - Pk + 1ull;
-    if (m <= (~0ull >> r)) th = min((m << r) - loc, kThCap);
-    if (delta <= (kThCap >> r)) D = delta << r;
-  }
+  const int j0 = tile0 + 4 * tid;
+  const unsigned long long D = ct.D;
+  unsigned long long th = ct.th;
+  int q = ct.q;
   unsigned long long acc = 0ull;
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
-    acc += f[e];
+    acc += ct.f[e];
     if (acc >= th) {
       const unsigned long long diff = acc - th;
       int cn = 1 + (diff >= D) + (diff >= 2ull * D) + (diff >= 3ull * D);
@@ -1348,11 +1413,15 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
   cluster_sync_all<NCTA>();                      // every start mark is in place
 
   // gather: the ancestor of output o is the last start mark at or before o; the first output of
-  // every 256-output block has one, so each warp's block stands alone
+  // every 256-output block has one, so each warp's block stands alone. Each lane resolves eight
+  // consecutive outputs (a running max and a warp max-scan) and writes parent + 1 back over the
+  // marks; the warp then reads them lane-interleaved, so the particle reads and writes and the
+  // ancestor stores of a warp touch consecutive slots.
   const int n_out = min(N - tile0, kTile);
   const int o0 = warp * kGatherStep;
   if (warp < kMarkWarps && o0 < n_out) {
-    const uint4 m = reinterpret_cast<const uint4*>(sh.marks + o0)[lane];
+    uint4* mrow = reinterpret_cast<uint4*>(sh.marks + o0);
+    const uint4 m = mrow[lane];
     unsigned am[8];
     am[0] = m.x & 0xffffu;
     am[1] = max(am[0], m.x >> 16);
@@ -1370,18 +1439,24 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
     }
     unsigned pre = __shfl_up_sync(0xffffffffu, xm, 1);
     if (lane == 0) pre = 0u;
+    unsigned jj[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) jj[u] = max(max(pre, am[u]), 1u);   // parent + 1
+    mrow[lane] = make_uint4(jj[0] | (jj[1] << 16), jj[2] | (jj[3] << 16), jj[4] | (jj[5] << 16), jj[6] | (jj[7] << 16));
+    __syncwarp();
     const int src = st.src;
     float* hd = sh.h[st.cur];
-    const int o = o0 + 8 * lane;
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      if (o + u < n_out) {
-        const int parent = (int)max(max(pre, am[u]), 1u) - 1;
-        hd[o + u] = (NCTA == 1) ? sh.h[src][parent] : sh.peer[parent >> 12]->h[src][parent & (kTile - 1)];
-        if (a.anc) a.anc[tile0 + o + u] = parent;
+      const int o = o0 + 32 * u + lane;
+      if (o < n_out) {
+        const int parent = (int)sh.marks[o] - 1;
+        hd[o] = (NCTA == 1) ? sh.h[src][parent] : sh.peer[parent >> 12]->h[src][parent & (kTile - 1)];
+        if (a.anc) a.anc[tile0 + o] = parent;
       }
     }
-    reinterpret_cast<uint4*>(sh.marks + o0)[lane] = make_uint4(0u, 0u, 0u, 0u);   // clear for the next resampling
+    __syncwarp();
+    mrow[lane] = make_uint4(0u, 0u, 0u, 0u);     // clear for the next resampling
   }
 }
 
@@ -1416,11 +1491,33 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
     }
     __syncthreads();
     const float y = a.y_ptr ? sh.ys[t & (kYStage - 1)] : a.obs.y;
-    pass1_fused<TSTATE, GAUSS>(a, y, N, tile0, par, sh.nexp[par ^ 1], sh);
+    const unsigned long long u_state = sh.st.u_state;
+    pass1_fused<TSTATE, GAUSS, kSmallSplit>(a, y, N, tile0, par, sh.nexp[par ^ 1], sh);
     cluster_sync_all<NCTA>();                   // every tile record of the tick is in place
-    if (tid == 0) plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
+    // thread 0 takes the decision. When every tick resamples (threshold 0), thread 32 meanwhile
+    // forms the resampling plan and warps 1..31 place their chunks against its targets; else
+    // that waits for the decision and runs on resampling ticks only.
+    const bool ahead = a.ess_threshold <= 0.0f;
+    ChunkTargets ct{};
+    if (tid == 0) {
+      plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
+    } else if (ahead && tid >= 32) {
+      if (tid == 32) plan_fused_targets<NCTA>(N, sh, par, u_state);
+      asm volatile("bar.sync 3, %0;" ::"n"(kSmallThreads - 32) : "memory");
+      ct = chunk_targets<NCTA>(N, k, par, sh);
+    }
     __syncthreads();
-    if (sh.st.do_resample) resample_fused<NCTA>(a, N, k, par, sh);
+    if (sh.st.do_resample) {
+      if (!ahead) {
+        if (tid == 32) plan_fused_targets<NCTA>(N, sh, par, u_state);
+        __syncthreads();
+        ct = chunk_targets<NCTA>(N, k, par, sh);
+      } else if (tid < 32) {
+        ct = chunk_targets<NCTA>(N, k, par, sh);
+      }
+      if (tid == 0) store_fused_plan(&sh.st, sh);
+      resample_fused<NCTA>(a, N, k, ct, sh);
+    }
   }
   cluster_sync_all<NCTA>();                     // no CTA leaves while another may read its shared memory
   reinterpret_cast<float4*>(p.h0 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[0])[tid];
