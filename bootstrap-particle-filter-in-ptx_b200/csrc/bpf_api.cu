@@ -6,6 +6,7 @@
 // never waits for the host and runs of ticks are captured in CUDA graphs.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -59,6 +60,7 @@ struct Impl {
   TickMirror* mir_map = nullptr;
   TickMirror* mir_map_dev = nullptr;
   bool last_in_map = false;             // the last enqueued tick wrote rec_map (not rec_dev[0])
+  int seq = 0;                          // request number of the last tick that writes the mirror
   float* y_dev = nullptr;               // [kGraphChunk]
   float* y_pin = nullptr;               // [kGraphChunk]
   int32_t* anc_dev = nullptr;           // [N] when recording
@@ -252,10 +254,30 @@ int enqueue_tick(GpuBpfState* s, Impl* m, const TickArgs& a) {
   return BPF_OK;
 }
 
+// Waits until the last single tick's outcome is in host-mapped memory: the plan writes the
+// record, then (after a system-scope fence) the mirror carrying the tick's request number, so
+// seeing that number means the record is complete although the tick's resampling may still run
+// on the stream (later work on the stream is ordered after it). The wait spins on the mirror for
+// up to 2 ms, then falls back to a stream synchronise, which also reports launch failures.
+int wait_single_tick(Impl* m) {
+  const volatile int* seq = &m->mir_map->seq;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int i = 0;; ++i) {
+    if (*seq == m->seq) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      return BPF_OK;
+    }
+    if ((i & 255) == 255 && std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(2)) break;
+  }
+  CK(cudaStreamSynchronize(m->stream));
+  return BPF_OK;
+}
+
 int read_back(GpuBpfState* s, Impl* m, int slot, BpfTickRecord* out) {
   if (slot == 0 && m->last_in_map) {
-    CK(cudaStreamSynchronize(m->stream));
-    *out = *m->rec_map;                    // written by this tick's kernels, complete after the synchronise
+    const int rc = wait_single_tick(m);
+    if (rc) return rc;
+    *out = *m->rec_map;                    // written by this tick's plan before its mirror
     const TickMirror mm = *m->mir_map;
     s->did_resample = out->resampled;
     s->resample_count = mm.resample_count;
@@ -528,6 +550,7 @@ static int step_async_rc(GpuBpfState* s, float y_t, bool one_shot) {
   if (one_shot && !m->profiling && !m->learn_mode) {  // learning updates need the host every K ticks
     if (tick_graph_stale(s, m)) { rc = build_tick_graph(s, m); if (rc) return rc; }
     m->t_args.obs.y = y_t;
+    m->t_args.seq = ++m->seq;
     CK(cudaGraphExecKernelNodeSetParams(m->tgraph, m->t_pass1, &m->t_params));
     CK(cudaGraphLaunch(m->tgraph, m->stream));
     g_launches += tick_launches(m, m->t_args);
@@ -537,6 +560,7 @@ static int step_async_rc(GpuBpfState* s, float y_t, bool one_shot) {
   }
   TickArgs a = make_args(s, m, y_t, nullptr, m->rec_map_dev);
   a.mirror = m->mir_map_dev;
+  a.seq = ++m->seq;
   rc = enqueue_tick(s, m, a);
   if (rc == BPF_OK) m->last_in_map = true;
   return rc;
@@ -837,7 +861,9 @@ int gpu_bpf_get_ancestors(GpuBpfState* s, int32_t* anc_out) {
   BpfTickRecord r;
   int rc = read_back(s, m, 0, &r);
   if (rc) return -rc;
-  if (cudaMemcpy(anc_out, m->anc_dev, (size_t)m->plan.N * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+  // the ancestors are written by the tick's resampling, which may still run after its record
+  if (cudaStreamSynchronize(m->stream) != cudaSuccess ||
+      cudaMemcpy(anc_out, m->anc_dev, (size_t)m->plan.N * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
     return -set_err(BPF_ERR_CUDA);
   return r.resampled ? 1 : 0;
 }

@@ -300,6 +300,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   __shared__ Pass1Shared sh;
   griddep_wait();
   const DevState* st = p.st;
+  if (a.mirror && blockIdx.x == 0 && threadIdx.x == 0) p.st->seq = a.seq;   // for the plan's mirror
   // Each pass walks the tiles in the order opposite to the previous pass over
   // the particle arrays, so it starts on the tiles that pass wrote last, still
   // in L2 (the arrays are rewritten in place every tick).
@@ -434,8 +435,9 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
     if (tid < kStWords)
       reinterpret_cast<unsigned long long*>(p.st)[tid] = reinterpret_cast<const unsigned long long*>(&s_st)[tid];
     if (tid == 0 && mirror_out) {
+      __threadfence_system();                 // the record first, then the mirror naming its request
       TickMirror mm;
-      mm.resample_count = st->resample_count; mm.tick = st->tick; mm.error = st->error; mm.pad = 0;
+      mm.resample_count = st->resample_count; mm.tick = st->tick; mm.error = st->error; mm.seq = st->seq;
       *mirror_out = mm;
     }
   };
@@ -1519,6 +1521,7 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
       resample_fused<NCTA>(a, N, k, ct, sh);
     }
   }
+  if (tid == 0 && a.mirror) sh.st.seq = a.seq;
   cluster_sync_all<NCTA>();                     // no CTA leaves while another may read its shared memory
   reinterpret_cast<float4*>(p.h0 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[0])[tid];
   reinterpret_cast<float4*>(p.h1 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[1])[tid];
@@ -1533,8 +1536,9 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
     if (tid < kStWords)
       reinterpret_cast<unsigned long long*>(p.st)[tid] = reinterpret_cast<const unsigned long long*>(&sh.st)[tid];
     if (tid == 0 && a.mirror) {
+      __threadfence_system();                 // the record first, then the mirror naming its request
       TickMirror mm;
-      mm.resample_count = sh.st.resample_count; mm.tick = sh.st.tick; mm.error = sh.st.error; mm.pad = 0;
+      mm.resample_count = sh.st.resample_count; mm.tick = sh.st.tick; mm.error = sh.st.error; mm.seq = a.seq;
       *a.mirror = mm;
     }
   }

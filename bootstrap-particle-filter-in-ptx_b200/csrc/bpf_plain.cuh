@@ -50,7 +50,7 @@ struct DevState {
   double   hm;              // filtered mean of the current tick (FP64): the centre of Silverman jitter
   uint64_t jk1, jk2;        // PCG32 stream constants of the current tick's jitter draw
   float    bw;              // Silverman jitter bandwidth of the current tick
-  int      pad_;
+  int      seq;             // host request number of the current tick (copied into the mirror)
 };
 static_assert(sizeof(DevState) == 200, "DevState layout");
 
@@ -71,7 +71,8 @@ struct TickMirror {
   int resample_count;
   int tick;                  // ticks completed
   int error;                 // DevState::error
-  int pad;
+  int seq;                   // host request number of the tick that wrote it (written last, after a
+                             // system fence: the host may take the record once it sees its number)
 };
 
 struct TickArgs {
@@ -93,6 +94,7 @@ struct TickArgs {
   int32_t* csr;              // on resampling ticks: first child slot of every parent (N ints) or null
   float2* aux;               // {1/S, nM}: normalised weight W_i = 2^(x_i - nM) / S of this tick, or null
   TickMirror* mirror;        // host-mapped mirror of this tick's outcome, or null
+  int seq;                   // host request number of this tick (pass 1 stores it in the device state)
   float silverman;           // Silverman jitter shrink after resampling (0 = off; needs p.jpart)
 };
 

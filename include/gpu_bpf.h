@@ -97,7 +97,12 @@ GpuBpfState* gpu_bpf_create(int n_particles, float rho, float sigma_z, float mu,
 void gpu_bpf_destroy(GpuBpfState* state);
 
 /* gpu_bpf/gpu_bpf.cuh:59 (gpu_bpf_ptx_full.cu:764-771): one tick, synchronous.
- * On error returns {NaN, NaN} and sets gpu_bpf_last_error(). */
+ * Returns as soon as the tick's result is final (it waits for the tick's record in
+ * host-mapped memory); the tick's resampling may still be running on state->stream,
+ * ordered before any later work there, and every accessor that reads the particles,
+ * ancestors or device state waits for it. On error returns {NaN, NaN} and sets
+ * gpu_bpf_last_error(); a device-side error detected by that resampling is reported
+ * by the next call that reads a result. */
 BpfResult gpu_bpf_step(GpuBpfState* state, float y_t);
 
 /* gpu_bpf/gpu_bpf.cuh:60 (gpu_bpf_ptx_full.cu:550-748): enqueue one tick on
@@ -106,7 +111,7 @@ BpfResult gpu_bpf_step(GpuBpfState* state, float y_t);
 void gpu_bpf_step_async(GpuBpfState* state, float y_t);
 
 /* gpu_bpf/gpu_bpf.cuh:61 (gpu_bpf_ptx_full.cu:754-762): result of the last
- * enqueued tick; waits for it. */
+ * enqueued tick; waits for its result (as gpu_bpf_step). */
 BpfResult gpu_bpf_get_result(GpuBpfState* state);
 
 /* gpu_bpf/gpu_bpf.cuh:63-67 (gpu_bpf_ptx_full.cu:834-852): run a filter over a

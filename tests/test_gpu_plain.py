@@ -319,7 +319,8 @@ def test_independent_filters_do_not_interact(bpf):
 # fused small-filter tick (N <= 16384): bit-identical to the three-kernel tick
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("N,thr,nu_obs,nu_state", [(1, 0.0, 0.0, 0.0), (31, 0.5, 0.0, 0.0), (4096, 0.0, 0.0, 0.0),
-                                                   (4097, 0.5, 5.0, 0.0), (12388, 0.5, 0.0, 5.0),
+                                                   (4097, 0.5, 5.0, 0.0), (8192, 0.0, 0.0, 0.0),
+                                                   (9000, 0.5, 0.0, 0.0), (12388, 0.5, 0.0, 5.0),
                                                    (16384, 0.3, 5.0, 5.0)])
 def test_fused_small_matches_three_kernel_path(bpf, N, thr, nu_obs, nu_state):
     """Records, ancestors and particles of the fused one-launch tick equal the three-kernel
@@ -361,18 +362,23 @@ def test_fused_small_matches_three_kernel_path(bpf, N, thr, nu_obs, nu_state):
         assert a[1] == b[1] and a[2] == b[2] and a[3:] == b[3:], mode
 
 
-def test_fused_small_long_device_run(bpf):
-    """A whole device-resident run of 1000 ticks as one fused launch equals the three-kernel run."""
+@pytest.mark.parametrize("N,thr", [(4096, 0.0), (12000, 0.5), (16384, 0.0)])
+def test_fused_small_long_device_run(bpf, N, thr):
+    """A whole device-resident run of 2500 ticks as one fused launch (one CTA, or a cluster of
+    three or four; the observations are restaged in shared memory every 1024 ticks) equals the
+    three-kernel run."""
     import torch
-    _, y = series(1000, 42)
+    T = 2500
+    _, y = series(T, 42)
     yd = torch.tensor(y, device="cuda")
     out = []
     for fused in (True, False):
-        f = bpf.GpuBpf(4096, RHO, SIG, MU, seed=42, ess_threshold=0.0)
+        f = bpf.GpuBpf(N, RHO, SIG, MU, seed=42, ess_threshold=thr)
         f.set_fused_small(fused)
-        rec = torch.zeros(1000 * 40, dtype=torch.uint8, device="cuda")
-        f.step_many_device(yd.data_ptr(), 1000, rec.data_ptr())
+        rec = torch.zeros(T * 40, dtype=torch.uint8, device="cuda")
+        f.step_many_device(yd.data_ptr(), T, rec.data_ptr())
         torch.cuda.synchronize()
-        out.append((rec.cpu().numpy().tobytes(), bytes(f.get_particles())))
+        w, te, u23 = f.get_resample_inputs()
+        out.append((rec.cpu().numpy().tobytes(), bytes(f.get_particles()), bytes(w), bytes(te), u23))
         f.close()
     assert out[0] == out[1]
