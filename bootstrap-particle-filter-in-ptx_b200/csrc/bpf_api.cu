@@ -134,19 +134,27 @@ bool use_small(const Impl* m, const TickArgs& a) {
   return m->fused_small && !m->profiling && small_eligible(m->plan, a);
 }
 
-// Kernels one tick launches: the fused kernel alone, or pass 1, plan, pass 2 and the two
-// Silverman jitter kernels when on.
+// Filters of at most kTailTiles tiles run the plan in pass 1's last CTA instead of a plan
+// launch (the same results; per-kernel profiling keeps the separate plan kernel).
+bool use_tail(const Impl* m, const TickArgs& a) {
+  return !m->profiling && tail_plan_eligible(m->plan, a);
+}
+
+// Kernels one tick launches: the fused kernel alone, or pass 1, the plan (unless pass 1 runs
+// it), pass 2 and the two Silverman jitter kernels when on.
 int tick_launches(const Impl* m, const TickArgs& a) {
   if (use_small(m, a)) return 1;
-  return a.silverman > 0.0f ? 5 : 3;
+  return (use_tail(m, a) ? 2 : 3) + (a.silverman > 0.0f ? 2 : 0);
 }
 
 cudaError_t launch_tick3(Impl* m, const TickArgs& a) {
   if (use_small(m, a)) return launch_small(m->plan, a, 1, m->stream, m->pdl);
-  cudaError_t e = launch_pass1(m->plan, a, m->stream, m->pdl);
-  if (e == cudaSuccess) e = launch_plan(m->plan, a, m->stream, m->pdl);
-  if (e == cudaSuccess) e = launch_pass2(m->plan, a, m->pass2_grid, m->stream, m->pdl);
-  if (e == cudaSuccess && a.silverman > 0.0f) e = launch_jitter(m->plan, a, m->stream, m->pdl);
+  TickArgs at = a;
+  at.tail_plan = use_tail(m, a) ? 1 : 0;
+  cudaError_t e = launch_pass1(m->plan, at, m->stream, m->pdl);
+  if (e == cudaSuccess && !at.tail_plan) e = launch_plan(m->plan, at, m->stream, m->pdl);
+  if (e == cudaSuccess) e = launch_pass2(m->plan, at, m->pass2_grid, m->stream, m->pdl);
+  if (e == cudaSuccess && a.silverman > 0.0f) e = launch_jitter(m->plan, at, m->stream, m->pdl);
   return e;
 }
 
@@ -415,6 +423,7 @@ int build_tick_graph(GpuBpfState* s, Impl* m) {
   m->t_plan = m->plan;                     // the root kernel's arguments, as its launcher passed them
   m->t_n = 1;
   m->t_args = a;
+  m->t_args.tail_plan = use_tail(m, a) ? 1 : 0;  // as launch_tick3 passed it to the root (pass 1)
   m->t_argv[0] = &m->t_plan;
   m->t_argv[1] = &m->t_args;
   m->t_argv[2] = &m->t_n;                  // read only by the fused kernel (three parameters)

@@ -295,7 +295,11 @@ __device__ __forceinline__ void pass1_tile(const Plan& p, const TickArgs& a, con
   }
 }
 
-template <bool TSTATE, bool LEARN, int APF, bool GAUSS>
+__device__ __forceinline__ void tail_plan(const Plan& p, const TickArgs& a);
+
+// TAIL: the last CTA to finish (a ticket taken after each CTA's tile record is out) runs the
+// plan for the whole filter, in place of the plan kernel (filters of at most kTailTiles tiles).
+template <bool TSTATE, bool LEARN, int APF, bool GAUSS, bool TAIL>
 __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) {
   __shared__ Pass1Shared sh;
   griddep_wait();
@@ -306,6 +310,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass1_kernel(Plan p, TickArgs a) 
   // in L2 (the arrays are rewritten in place every tick).
   const int k = (st->dirs & 1) ? (p.G - 1 - (int)blockIdx.x) : (int)blockIdx.x;
   pass1_tile<TSTATE, LEARN, APF, GAUSS>(p, a, st, k, (int)threadIdx.x, 0, sh);
+  if constexpr (TAIL) tail_plan(p, a);
   griddep_release();
 }
 
@@ -624,6 +629,28 @@ __device__ __forceinline__ void plan_body(const Plan& p, const TickArgs& a, DevS
   }
   if (tid == 0) st->n_items = n_items_total;
   store_state();
+}
+
+// The plan in pass 1's last CTA: every CTA's tile record is out before its ticket (a fence
+// between), so the CTA that takes the last ticket sees them all after a second fence.
+__device__ __forceinline__ void tail_plan(const Plan& p, const TickArgs& a) {
+  __shared__ PlanShared<kThreads> sh;
+  __shared__ __align__(16) DevState s_st;
+  __shared__ __align__(16) unsigned char stage[plan_smem_bytes(kTailTiles)];
+  __shared__ unsigned s_last;
+  __syncthreads();                               // the tile record of this CTA is written
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = (atomicAdd(p.pticket, 1u) == (unsigned)(p.G - 1)) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < kStWords)
+    reinterpret_cast<unsigned long long*>(&s_st)[threadIdx.x] =
+        __ldcg(reinterpret_cast<const unsigned long long*>(p.st) + threadIdx.x);
+  if (threadIdx.x == 0) *p.pticket = 0u;          // for the next tick
+  plan_body<kThreads, true>(p, a, s_st, sh, stage, PlanGlobalIO{&p}, a.rec, a.mirror);
 }
 
 __global__ void __launch_bounds__(kPlanThreads, 1) plan_kernel(Plan p, TickArgs a) {
@@ -1602,9 +1629,11 @@ cudaError_t plan_alloc(Plan& p, int N) {
   al(&p.items, p.max_items * sizeof(int4));
   al(&p.jpart, p.G * sizeof(double));
   al(&p.jticket, sizeof(unsigned));
+  al(&p.pticket, sizeof(unsigned));
   al(&p.st, sizeof(DevState));
   if (e == cudaSuccess) e = cudaMemset(p.nexp, 0, p.G * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(p.jticket, 0, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(p.pticket, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaDeviceSynchronize();   // visible to every stream before first use
   return e;
 }
@@ -1613,7 +1642,7 @@ void plan_free(Plan& p) {
   bpf_free(p.h0); bpf_free(p.h1); bpf_free(p.w);
   bpf_free(p.nexp); bpf_free(p.E); bpf_free(p.rec); bpf_free(p.rec2);
   bpf_free(p.P); bpf_free(p.ofirst); bpf_free(p.items); bpf_free(p.st);
-  bpf_free(p.jpart); bpf_free(p.jticket);
+  bpf_free(p.jpart); bpf_free(p.jticket); bpf_free(p.pticket);
   p = Plan{};
 }
 
@@ -1665,17 +1694,26 @@ int pass2_grid_size(int device) {
 template <bool GAUSS>
 static cudaError_t launch_pass1_model(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {
   const dim3 grid(p.G), block(kThreads);
-  if (a.apf == 1) return launch_ex(pass1_kernel<false, false, 1, GAUSS>, grid, block, 0, s, pdl, p, a);
+  if (a.apf == 1) return launch_ex(pass1_kernel<false, false, 1, GAUSS, false>, grid, block, 0, s, pdl, p, a);
   if (a.apf == 2) {
-    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 2, GAUSS>, grid, block, 0, s, pdl, p, a);
-    return launch_ex(pass1_kernel<false, false, 2, GAUSS>, grid, block, 0, s, pdl, p, a);
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 2, GAUSS, false>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, false, 2, GAUSS, false>, grid, block, 0, s, pdl, p, a);
   }
   if (a.learn && p.rec2) {
-    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, true, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
-    return launch_ex(pass1_kernel<false, true, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, true, 0, GAUSS, false>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, true, 0, GAUSS, false>, grid, block, 0, s, pdl, p, a);
   }
-  if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
-  return launch_ex(pass1_kernel<false, false, 0, GAUSS>, grid, block, 0, s, pdl, p, a);
+  if (a.tail_plan) {
+    if (!tail_plan_eligible(p, a)) return cudaErrorInvalidValue;
+    if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 0, GAUSS, true>, grid, block, 0, s, pdl, p, a);
+    return launch_ex(pass1_kernel<false, false, 0, GAUSS, true>, grid, block, 0, s, pdl, p, a);
+  }
+  if (a.nu_int > 0) return launch_ex(pass1_kernel<true, false, 0, GAUSS, false>, grid, block, 0, s, pdl, p, a);
+  return launch_ex(pass1_kernel<false, false, 0, GAUSS, false>, grid, block, 0, s, pdl, p, a);
+}
+
+bool tail_plan_eligible(const Plan& p, const TickArgs& a) {
+  return p.G <= kTailTiles && p.pticket && a.apf == 0 && !a.learn && !a.ckpt && !a.csr && !a.aux;
 }
 
 cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {

@@ -62,6 +62,7 @@ struct Plan {
   unsigned long long* P; int* ofirst; int4* items;
   double* jpart;             // per tile, Silverman jitter only: sum of (h - hm)^2 over the tile's particles
   unsigned* jticket;         // CTAs of the jitter-variance kernel done this tick (the last one resets it)
+  unsigned* pticket;         // pass-1 CTAs done this tick when the last one runs the plan (it resets it)
   DevState* st;
 };
 
@@ -95,6 +96,7 @@ struct TickArgs {
   float2* aux;               // {1/S, nM}: normalised weight W_i = 2^(x_i - nM) / S of this tick, or null
   TickMirror* mirror;        // host-mapped mirror of this tick's outcome, or null
   int seq;                   // host request number of this tick (pass 1 stores it in the device state)
+  int tail_plan;             // the last pass-1 CTA runs the plan (G <= kTailTiles; no plan launch)
   float silverman;           // Silverman jitter shrink after resampling (0 = off; needs p.jpart)
 };
 
@@ -107,6 +109,11 @@ void plan_free(Plan& p);
 cudaError_t launch_init(const Plan& p, float mu, float std_stat, int seed, cudaStream_t s);
 // pdl = programmatic dependent launch on the previous kernel in the stream.
 cudaError_t launch_pass1(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
+// Filters of at most kTailTiles tiles may run the plan in pass 1's last CTA (a.tail_plan):
+// the same plan code on 256 threads, one tile per thread, so the results equal the plan
+// kernel's bit for bit; bootstrap ticks without learning or a gradient tape only.
+constexpr int kTailTiles = 256;
+bool tail_plan_eligible(const Plan& p, const TickArgs& a);
 cudaError_t launch_plan(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl);
 cudaError_t launch_pass2(const Plan& p, const TickArgs& a, int grid, cudaStream_t s, bool pdl);
 // Silverman jitter of a resampling tick (both kernels exit at once on other ticks): the bandwidth

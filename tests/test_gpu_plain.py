@@ -382,3 +382,32 @@ def test_fused_small_long_device_run(bpf, N, thr):
         out.append((rec.cpu().numpy().tobytes(), bytes(f.get_particles()), bytes(w), bytes(te), u23))
         f.close()
     assert out[0] == out[1]
+
+
+@pytest.mark.parametrize("N,thr", [(20000, 0.0), (65536, 0.5), (300000, 0.5), (1 << 20, 0.0)])
+def test_tail_plan_matches_plan_kernel(bpf, N, thr):
+    """Filters of at most 256 tiles run the plan in pass 1's last CTA; with per-kernel profiling
+    on, the same ticks run the separate plan kernel. Records, ancestors and particles agree bit
+    for bit, tick by tick and over a captured run."""
+    _, y = series(120, 11)
+
+    def run(profile):
+        f = bpf.GpuBpf(N, RHO, SIG, MU, 0.0, 0.0, 23, ess_threshold=thr)
+        f.record_ancestors(True)
+        if profile:
+            f.profile(True)
+        recs, ancs = [], []
+        for v in y[:40]:
+            f.step(float(v))
+            recs.append(f.get_record())
+            ancs.append(bytes(f.get_ancestors()[1]))
+        recs += f.step_many(y[40:].tolist(), records=True)
+        parts = bytes(f.get_particles())
+        f.close()
+        key = [(r.dloglik, r.loglik_ref, r.loglik_total, r.h_mean, r.ess, r.resampled, r.tick) for r in recs]
+        return key, ancs, parts
+
+    a, b = run(False), run(True)
+    assert sum(r[5] for r in a[0]) > 0
+    assert a[0] == b[0]
+    assert a[1] == b[1] and a[2] == b[2]
