@@ -103,6 +103,7 @@ struct Impl {
   // filters of at most kSmallMaxN particles run each tick (or each captured run of ticks) as one
   // fused launch (gpu_bpf_set_fused_small)
   bool fused_small = true;
+  int small_tiles = 4;                  // largest fused cluster on the filter's device (tiles)
 
   // profiling
   bool profiling = false;
@@ -131,7 +132,7 @@ int ensure_device(Impl* m) {
 // needs nothing that only the three-kernel path provides (learning, Silverman jitter, per-kernel
 // profiling); the two give bit-identical results.
 bool use_small(const Impl* m, const TickArgs& a) {
-  return m->fused_small && !m->profiling && small_eligible(m->plan, a);
+  return m->fused_small && !m->profiling && m->plan.G <= m->small_tiles && small_eligible(m->plan, a);
 }
 
 // Filters of at most kTailTiles tiles run the plan in pass 1's last CTA instead of a plan
@@ -487,6 +488,7 @@ static int create_impl(GpuBpfState* s, Impl* m, int n, float rho, float sigma_z,
   std::memset(m->mir_map, 0, sizeof(TickMirror));
   CK(cudaMemsetAsync(m->rec_dev, 0, (1 + kGraphChunk) * sizeof(BpfTickRecord), m->stream));
   m->pass2_grid = pass2_grid_size(m->device);
+  m->small_tiles = small_max_tiles(m->device);
   if (const char* v = std::getenv("BPF_DISABLE_PDL")) m->pdl = (v[0] == '0');
 
   // observation model (gpu_bpf_ptx_full.cu:406-412)

@@ -28,8 +28,8 @@ constexpr int kTile      = kThreads * kPerThread;   // 4096 particles per tile
 constexpr int kOutChunk  = 2 * kTile;        // outputs per pass-2 work item (2x the mean per tile)
 constexpr int kPlanThreads = 1024;           // threads of the single-CTA plan kernel
 constexpr int kPlanSmemTiles = 12800;        // tiles the plan kernel stages in shared memory (N <= 52.4M)
-constexpr int kSmallTiles = 4;              // tiles of the fused small-filter tick
-constexpr int kSmallMaxN  = kSmallTiles * kTile;    // 16384 particles
+constexpr int kSmallTiles = 16;             // tiles of the fused small-filter tick (one CTA each)
+constexpr int kSmallMaxN  = kSmallTiles * kTile;    // 65536 particles
 constexpr int kFixF      = 50;               // tile-frame fraction bits: 62 - log2(kTile)
 constexpr int kNkEmpty   = -(1 << 30);       // tile exponent of a tile with no mass
 

@@ -1076,7 +1076,7 @@ constexpr int kMarkWarps = kTile / kGatherStep;         // warps of the gather (
 constexpr int kYStage = kSmallThreads;                  // observations staged per refill
 static_assert(kChunks == kSmallThreads, "one four-slot chunk per thread");
 static_assert(kTile % kGatherStep == 0, "the gather reads marks in 256-slot steps");
-static_assert(kSmallMaxN < 65536, "start marks hold parent + 1 in 16 bits");
+static_assert(kSmallMaxN < (1 << 30), "start marks hold parent + 1");
 
 struct FusedPlan {
   unsigned long long base, delta, magic, total;
@@ -1086,7 +1086,9 @@ struct FusedPlan {
 struct FusedShared {
   float h[2][kTile];                          // particle buffers (DevState::cur / src), this CTA's tile
   float w[kTile];                             // log2-weights of the tile
-  unsigned short marks[kTile + kGatherStep];  // start marks of this CTA's outputs: parent + 1, 0 = none
+  // start marks of this CTA's outputs, parent + 1 (0 = none): 16-bit for clusters of up to 8
+  // CTAs (parent + 1 <= 32768), 32-bit for 16 (see MarkOf)
+  __align__(16) unsigned marks_raw[kTile + kGatherStep];
   unsigned long long chunkE[kChunks];         // exact fixed-point mass of each four-slot chunk
   unsigned long long chunkP[kChunks];         // its exclusive prefix within the tile
   float ys[kYStage];                          // observations of the next ticks
@@ -1260,47 +1262,55 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
 
 // The plan of a fused tick by one thread, for NCTA <= kSmallTiles tiles: the statistics and
 // the decision, the operations of plan_body on one warp in the same order. There lane k holds
-// tile k's FP64 sums (the other lanes exact zeros, so the warp's butterfly sums reduce to the
-// pairwise sums below and every lane holds the same totals).
+// tile k's FP64 sums and the lanes past the tiles exact zeros, so lane 0's butterfly sum is
+// the pairwise tree below: v_i + v_{i+8}, then i + 4, i + 2, i + 1, each lane's value first
+// normalised by adding lane i + 16's zero (every lane holds the same totals).
 template <int NCTA>
 __device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared& sh, int par, BpfTickRecord* rec_out) {
-  static_assert(NCTA >= 1 && NCTA <= 4, "the pairwise sums below cover four lanes");
+  static_assert(NCTA >= 1 && NCTA <= 16, "the tree below covers sixteen lanes");
   DevState* st = &sh.st;
-  float4 r[4];
-  int nk[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k < NCTA) {
-      r[k] = sh.peer[k]->rec[par];
-      nk[k] = __float_as_int(r[k].w);
-    } else {
-      r[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-      nk[k] = kNkEmpty;
-    }
-  }
   int nM = kNkEmpty;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) nM = max(nM, nk[k]);
-  // each lane's running frame is its own tile's, then the global frame 2^nM
-  double S[4], Q[4], H[4];
+  for (int k = 0; k < NCTA; ++k) nM = max(nM, sh.peer[k]->nexp[par]);
+  // lane k's sums: its running frame is its own tile's, then the global frame 2^nM; each is
+  // normalised by the butterfly's first addition of a zero lane (v + 0 turns -0 into +0)
+  auto lane_sums = [&](int k, double& S, double& Q, double& H) {
+    S = Q = H = 0.0;
+    const float4 r = sh.peer[k]->rec[par];
+    const int nk = __float_as_int(r.w);
+    if (nk != kNkEmpty) {
+      const double sc = pow2d(nk - nM);
+      S = __dmul_rn(__dadd_rn(0.0, (double)r.x), sc);
+      Q = __dmul_rn(__dadd_rn(0.0, (double)r.y), __dmul_rn(sc, sc));
+      H = __dmul_rn(__dadd_rn(0.0, (double)r.z), sc);
+    }
+    S = __dadd_rn(S, 0.0); Q = __dadd_rn(Q, 0.0); H = __dadd_rn(H, 0.0);
+  };
+  // The tree pruned where a subtree holds only zero lanes: x + (+0) is x once x has been
+  // normalised, so only the live lanes' additions remain and the result is the full
+  // butterfly's bit for bit. Level 8 is formed as the lanes are read.
+  double bS[8], bQ[8], bH[8];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (nk[k] != kNkEmpty) {
-      const double sc = pow2d(nk[k] - nM);
-      S[k] = __dmul_rn(__dadd_rn(0.0, (double)r[k].x), sc);
-      Q[k] = __dmul_rn(__dadd_rn(0.0, (double)r[k].y), __dmul_rn(sc, sc));
-      H[k] = __dmul_rn(__dadd_rn(0.0, (double)r[k].z), sc);
-    } else {
-      S[k] = 0.0; Q[k] = 0.0; H[k] = 0.0;
+  for (int i = 0; i < 8; ++i) {
+    bS[i] = bQ[i] = bH[i] = 0.0;
+    if (i < NCTA) {
+      lane_sums(i, bS[i], bQ[i], bH[i]);
+      if (i + 8 < NCTA) {
+        double s1, q1, h1;
+        lane_sums(i + 8, s1, q1, h1);
+        bS[i] = __dadd_rn(bS[i], s1); bQ[i] = __dadd_rn(bQ[i], q1); bH[i] = __dadd_rn(bH[i], h1);
+      }
     }
   }
-  // the butterfly of warp_sum_d: the first three levels add the zero lanes 16.., 8.., 4..
-  auto wsum = [](const double* v) {
-    const double a0 = __dadd_rn(v[0], 0.0), a1 = __dadd_rn(v[1], 0.0);
-    const double a2 = __dadd_rn(v[2], 0.0), a3 = __dadd_rn(v[3], 0.0);
-    return __dadd_rn(__dadd_rn(a0, a2), __dadd_rn(a1, a3));
+  auto tree = [](double* v) {                    // levels 4, 2, 1 into v[0]
+#pragma unroll
+    for (int w = 4; w >= 1; w >>= 1)
+#pragma unroll
+      for (int i = 0; i < w; ++i)
+        if (i + w < NCTA) v[i] = __dadd_rn(v[i], v[i + w]);
+    return v[0];
   };
-  const double tS = wsum(S), tQ = wsum(Q), tH = wsum(H);
+  const double tS = tree(bS), tQ = tree(bQ), tH = tree(bH);
   const bool degenerate = (nM == kNkEmpty) || !(tS > 0.0);
   constexpr double kLn2d = 0.693147180559945309417232121458;
   double res[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1319,27 +1329,17 @@ __device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared
 // the item count, as plan_body. u_state: the resampling-uniform state at the start of the tick.
 template <int NCTA>
 __device__ __forceinline__ void plan_fused_targets(int N, FusedShared& sh, int par, unsigned long long u_state) {
-  unsigned long long E[4];
-  int nk[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k < NCTA) {
-      nk[k] = sh.peer[k]->nexp[par];
-      E[k] = sh.peer[k]->E[par];
-    } else {
-      nk[k] = kNkEmpty;
-      E[k] = 0ull;
-    }
-  }
   int nM = kNkEmpty;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) nM = max(nM, nk[k]);
+  for (int k = 0; k < NCTA; ++k) nM = max(nM, sh.peer[k]->nexp[par]);
   const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
-  unsigned long long Pk[5];
+  unsigned long long Pk[NCTA + 1];
   Pk[0] = 0ull;
 #pragma unroll
-  for (int k = 0; k < 4; ++k)
-    Pk[k + 1] = Pk[k] + ((k < NCTA && nk[k] != kNkEmpty) ? shr64(E[k], nM - nk[k] + kFixF - Fg) : 0ull);
+  for (int k = 0; k < NCTA; ++k) {
+    const int nk = sh.peer[k]->nexp[par];
+    Pk[k + 1] = Pk[k] + ((nk != kNkEmpty) ? shr64(sh.peer[k]->E[par], nM - nk + kFixF - Fg) : 0ull);
+  }
   const unsigned long long total = Pk[NCTA];
   unsigned long long delta = udiv_fp64(total, (unsigned long long)N);
   const bool zero_spacing = delta == 0ull;
@@ -1402,11 +1402,19 @@ __device__ __forceinline__ ChunkTargets chunk_targets(int N, int k, int par, con
   return ct;
 }
 
+// The start-mark element of a cluster of NCTA CTAs.
+template <int NCTA>
+using MarkOf = std::conditional_t<(NCTA > 8), unsigned, unsigned short>;
+template <int NCTA>
+__device__ __forceinline__ MarkOf<NCTA>* marks_of(FusedShared& sh) {
+  return reinterpret_cast<MarkOf<NCTA>*>(sh.marks_raw);
+}
+
 // Start mark of output o (parent + 1) in the shared memory of the CTA that owns o.
 template <int NCTA>
 __device__ __forceinline__ void put_mark(FusedShared& sh, int o, int val) {
-  if constexpr (NCTA == 1) sh.marks[o] = (unsigned short)val;
-  else sh.peer[o >> 12]->marks[o & (kTile - 1)] = (unsigned short)val;
+  if constexpr (NCTA == 1) marks_of<NCTA>(sh)[o] = (MarkOf<NCTA>)val;
+  else marks_of<NCTA>(*sh.peer[o >> 12])[o & (kTile - 1)] = (MarkOf<NCTA>)val;
 }
 
 // Resampling of a fused tick, this CTA's part: the children of its tile's particles (start
@@ -1449,17 +1457,24 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
   const int n_out = min(N - tile0, kTile);
   const int o0 = warp * kGatherStep;
   if (warp < kMarkWarps && o0 < n_out) {
-    uint4* mrow = reinterpret_cast<uint4*>(sh.marks + o0);
-    const uint4 m = mrow[lane];
+    using M = MarkOf<NCTA>;
+    M* marks = marks_of<NCTA>(sh);
+    constexpr int VPL = (int)(8 * sizeof(M)) / 16;   // uint4 per lane: eight marks
+    uint4* mrow = reinterpret_cast<uint4*>(marks + o0);
+    unsigned mv[8];
+    if constexpr (VPL == 1) {
+      const uint4 m0 = mrow[lane];
+      mv[0] = m0.x & 0xffffu; mv[1] = m0.x >> 16; mv[2] = m0.y & 0xffffu; mv[3] = m0.y >> 16;
+      mv[4] = m0.z & 0xffffu; mv[5] = m0.z >> 16; mv[6] = m0.w & 0xffffu; mv[7] = m0.w >> 16;
+    } else {
+      const uint4 m0 = mrow[2 * lane], m1 = mrow[2 * lane + 1];
+      mv[0] = m0.x; mv[1] = m0.y; mv[2] = m0.z; mv[3] = m0.w;
+      mv[4] = m1.x; mv[5] = m1.y; mv[6] = m1.z; mv[7] = m1.w;
+    }
     unsigned am[8];
-    am[0] = m.x & 0xffffu;
-    am[1] = max(am[0], m.x >> 16);
-    am[2] = max(am[1], m.y & 0xffffu);
-    am[3] = max(am[2], m.y >> 16);
-    am[4] = max(am[3], m.z & 0xffffu);
-    am[5] = max(am[4], m.z >> 16);
-    am[6] = max(am[5], m.w & 0xffffu);
-    am[7] = max(am[6], m.w >> 16);
+    am[0] = mv[0];
+#pragma unroll
+    for (int u = 1; u < 8; ++u) am[u] = max(am[u - 1], mv[u]);
     unsigned xm = am[7];
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -1471,7 +1486,12 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
     unsigned jj[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) jj[u] = max(max(pre, am[u]), 1u);   // parent + 1
-    mrow[lane] = make_uint4(jj[0] | (jj[1] << 16), jj[2] | (jj[3] << 16), jj[4] | (jj[5] << 16), jj[6] | (jj[7] << 16));
+    if constexpr (VPL == 1) {
+      mrow[lane] = make_uint4(jj[0] | (jj[1] << 16), jj[2] | (jj[3] << 16), jj[4] | (jj[5] << 16), jj[6] | (jj[7] << 16));
+    } else {
+      mrow[2 * lane] = make_uint4(jj[0], jj[1], jj[2], jj[3]);
+      mrow[2 * lane + 1] = make_uint4(jj[4], jj[5], jj[6], jj[7]);
+    }
     __syncwarp();
     const int src = st.src;
     float* hd = sh.h[st.cur];
@@ -1479,13 +1499,14 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
     for (int u = 0; u < 8; ++u) {
       const int o = o0 + 32 * u + lane;
       if (o < n_out) {
-        const int parent = (int)sh.marks[o] - 1;
+        const int parent = (int)marks[o] - 1;
         hd[o] = (NCTA == 1) ? sh.h[src][parent] : sh.peer[parent >> 12]->h[src][parent & (kTile - 1)];
         if (a.anc) a.anc[tile0 + o] = parent;
       }
     }
     __syncwarp();
-    mrow[lane] = make_uint4(0u, 0u, 0u, 0u);     // clear for the next resampling
+#pragma unroll
+    for (int x = 0; x < VPL; ++x) mrow[VPL * lane + x] = make_uint4(0u, 0u, 0u, 0u);   // clear for the next resampling
   }
 }
 
@@ -1505,12 +1526,22 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
     if constexpr (NCTA > 1) sh.peer[tid] = cooperative_groups::this_cluster().map_shared_rank(&sh, tid);
     else sh.peer[tid] = &sh;
   }
-  if (tid == 0) sh.nexp[1] = __ldcg(p.nexp + k);      // the exponent the first tick's carry reads
-  reinterpret_cast<float4*>(sh.h[0])[tid] = __ldcg(reinterpret_cast<const float4*>(p.h0 + tile0) + tid);
-  reinterpret_cast<float4*>(sh.h[1])[tid] = __ldcg(reinterpret_cast<const float4*>(p.h1 + tile0) + tid);
-  reinterpret_cast<float4*>(sh.w)[tid] = __ldcg(reinterpret_cast<const float4*>(p.w + tile0) + tid);
-  constexpr int kMarkVecs = (int)(sizeof(sh.marks) / 16);
-  if (tid < kMarkVecs) reinterpret_cast<uint4*>(sh.marks)[tid] = make_uint4(0u, 0u, 0u, 0u);
+  // A cluster may hold more CTAs than the filter has tiles (5..8 tiles run as 8, 9..16 as 16): a
+  // CTA past the last tile holds only padding slots (weight 0, finite particles) and no outputs.
+  const bool real = k < p.G;
+  if (real) {
+    if (tid == 0) sh.nexp[1] = __ldcg(p.nexp + k);    // the exponent the first tick's carry reads
+    reinterpret_cast<float4*>(sh.h[0])[tid] = __ldcg(reinterpret_cast<const float4*>(p.h0 + tile0) + tid);
+    reinterpret_cast<float4*>(sh.h[1])[tid] = __ldcg(reinterpret_cast<const float4*>(p.h1 + tile0) + tid);
+    reinterpret_cast<float4*>(sh.w)[tid] = __ldcg(reinterpret_cast<const float4*>(p.w + tile0) + tid);
+  } else {
+    if (tid == 0) sh.nexp[1] = kNkEmpty;
+    reinterpret_cast<float4*>(sh.h[0])[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+    reinterpret_cast<float4*>(sh.h[1])[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+    reinterpret_cast<float4*>(sh.w)[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  constexpr int kMarkVecs = (int)(sizeof(MarkOf<NCTA>) * (kTile + kGatherStep) / 16);
+  for (int x = tid; x < kMarkVecs; x += kSmallThreads) reinterpret_cast<uint4*>(sh.marks_raw)[x] = make_uint4(0u, 0u, 0u, 0u);
 
   for (int t = 0; t < n_ticks; ++t) {
     const int par = t & 1;
@@ -1550,10 +1581,12 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
   }
   if (tid == 0 && a.mirror) sh.st.seq = a.seq;
   cluster_sync_all<NCTA>();                     // no CTA leaves while another may read its shared memory
-  reinterpret_cast<float4*>(p.h0 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[0])[tid];
-  reinterpret_cast<float4*>(p.h1 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[1])[tid];
-  reinterpret_cast<float4*>(p.w + tile0)[tid] = reinterpret_cast<const float4*>(sh.w)[tid];
-  if (tid == 0) {
+  if (real) {
+    reinterpret_cast<float4*>(p.h0 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[0])[tid];
+    reinterpret_cast<float4*>(p.h1 + tile0)[tid] = reinterpret_cast<const float4*>(sh.h[1])[tid];
+    reinterpret_cast<float4*>(p.w + tile0)[tid] = reinterpret_cast<const float4*>(sh.w)[tid];
+  }
+  if (real && tid == 0) {
     const int last = (n_ticks - 1) & 1;
     p.nexp[k] = sh.nexp[last];
     p.E[k] = sh.E[last];
@@ -1659,20 +1692,44 @@ constexpr int kMaxConfiguredDevices = 64;
 template <int NCTA>
 static void configure_small() {
   constexpr int bytes = (int)sizeof(FusedShared);
-  cudaFuncSetAttribute(small_kernel<false, true, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(small_kernel<true, true, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(small_kernel<false, false, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(small_kernel<true, false, NCTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  void (*k[4])(Plan, TickArgs, int) = {small_kernel<false, true, NCTA>, small_kernel<true, true, NCTA>,
+                                       small_kernel<false, false, NCTA>, small_kernel<true, false, NCTA>};
+  for (auto f : k) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (NCTA > 8) cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  }
 }
+
+// Largest fused cluster (in tiles) the device schedules: 16 when a cluster of sixteen 1024-thread
+// CTAs with the fused kernel's shared memory fits on one GPC, else 8 (the portable size).
+static int small_tiles_on_device() {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(16);
+  cfg.blockDim = dim3(kSmallThreads);
+  cfg.dynamicSmemBytes = sizeof(FusedShared);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 16; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, small_kernel<false, true, 16>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  return n >= 1 ? 16 : 8;
+}
+static int g_small_tiles[kMaxConfiguredDevices] = {};
 
 // Called with `device` current. The shared-memory attributes are set once per
 // device (they belong to the device's context), under a lock so filters
 // created from several threads do not race.
+static std::mutex g_config_lock;
+
 int pass2_grid_size(int device) {
-  static std::mutex lock;
   static bool configured[kMaxConfiguredDevices] = {};
   {
-    std::lock_guard<std::mutex> guard(lock);
+    std::lock_guard<std::mutex> guard(g_config_lock);
     if (device < 0 || device >= kMaxConfiguredDevices || !configured[device]) {
       cudaFuncSetAttribute(pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPass2Smem);
       cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1681,6 +1738,9 @@ int pass2_grid_size(int device) {
       configure_small<2>();
       configure_small<3>();
       configure_small<4>();
+      configure_small<8>();
+      configure_small<16>();
+      if (device >= 0 && device < kMaxConfiguredDevices) g_small_tiles[device] = small_tiles_on_device();
       if (device >= 0 && device < kMaxConfiguredDevices) configured[device] = true;
     }
   }
@@ -1744,12 +1804,22 @@ static cudaError_t launch_small_cluster(const Plan& p, const TickArgs& a, int n_
 
 cudaError_t launch_small(const Plan& p, const TickArgs& a, int n_ticks, cudaStream_t s, bool pdl) {
   if (p.N > kSmallMaxN || p.G < 1 || p.G > kSmallTiles || n_ticks < 1) return cudaErrorInvalidValue;
-  switch (p.G) {
-    case 1: return launch_small_cluster<1>(p, a, n_ticks, s, pdl);
-    case 2: return launch_small_cluster<2>(p, a, n_ticks, s, pdl);
-    case 3: return launch_small_cluster<3>(p, a, n_ticks, s, pdl);
-    default: return launch_small_cluster<4>(p, a, n_ticks, s, pdl);
+  if (p.G <= 4) {
+    switch (p.G) {
+      case 1: return launch_small_cluster<1>(p, a, n_ticks, s, pdl);
+      case 2: return launch_small_cluster<2>(p, a, n_ticks, s, pdl);
+      case 3: return launch_small_cluster<3>(p, a, n_ticks, s, pdl);
+      default: return launch_small_cluster<4>(p, a, n_ticks, s, pdl);
+    }
   }
+  if (p.G <= 8) return launch_small_cluster<8>(p, a, n_ticks, s, pdl);
+  return launch_small_cluster<16>(p, a, n_ticks, s, pdl);
+}
+
+int small_max_tiles(int device) {
+  if (device < 0 || device >= kMaxConfiguredDevices) return 4;
+  std::lock_guard<std::mutex> guard(g_config_lock);
+  return g_small_tiles[device] ? g_small_tiles[device] : 4;
 }
 
 cudaError_t launch_jitter(const Plan& p, const TickArgs& a, cudaStream_t s, bool pdl) {

@@ -127,6 +127,8 @@ cudaError_t launch_jitter(const Plan& p, const TickArgs& a, cudaStream_t s, bool
 bool small_eligible(const Plan& p, const TickArgs& a);
 cudaError_t launch_small(const Plan& p, const TickArgs& a, int n_ticks, cudaStream_t s, bool pdl);
 int pass2_grid_size(int device);
+// Tiles the fused tick takes on this device (16, else 8; 4 before pass2_grid_size configured it).
+int small_max_tiles(int device);
 size_t pass2_smem_bytes();
 cudaError_t launch_debug_pcg(int seed, int n, int t, uint32_t* d_out, float* d_norm, cudaStream_t s);
 // w_out[i] = 2^d_i of the stored tile-relative log2-weights (N floats, device).

@@ -234,13 +234,15 @@ size_t gpu_bpf_checkpoint_bytes(GpuBpfState* state);
 int    gpu_bpf_save(GpuBpfState* state, void* buf, size_t cap);
 int    gpu_bpf_load(GpuBpfState* state, const void* buf, size_t len);
 
-/* Fused small-filter ticks (addition): a filter of at most 16384 particles runs
- * each tick as one launch of one CTA (pass 1, the resampling decision and the
- * resampling without leaving the SM), and a captured run of ticks
- * (gpu_bpf_step_many, gpu_bpf_step_many_device) as one launch for the whole
- * run, with results bit-identical to the three-kernel tick. On by default;
- * enable = 0 selects the three-kernel tick. Learning filters, Silverman jitter
- * and profiled ticks always take the three-kernel path. */
+/* Fused small-filter ticks (addition): a filter of at most 65536 particles runs
+ * each tick as one launch of a thread-block cluster, one CTA per 4096 particles
+ * (pass 1, the resampling decision and the resampling in shared memory, the CTAs
+ * reading each other's through distributed shared memory), and a captured run of
+ * ticks (gpu_bpf_step_many, gpu_bpf_step_many_device) as one launch for the whole
+ * run, with results bit-identical to the three-kernel tick. Filters of more than
+ * 32768 particles take it where the device schedules a cluster of 16 CTAs. On by
+ * default; enable = 0 selects the three-kernel tick. Learning filters, Silverman
+ * jitter and profiled ticks always take the three-kernel path. */
 int gpu_bpf_set_fused_small(GpuBpfState* state, int enable);
 
 /* Kernel profiling: when enabled, every tick's three kernels (pass 1, plan,

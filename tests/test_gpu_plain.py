@@ -316,12 +316,14 @@ def test_independent_filters_do_not_interact(bpf):
 
 
 # ---------------------------------------------------------------------------
-# fused small-filter tick (N <= 16384): bit-identical to the three-kernel tick
+# fused small-filter tick (N <= 65536): bit-identical to the three-kernel tick
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("N,thr,nu_obs,nu_state", [(1, 0.0, 0.0, 0.0), (31, 0.5, 0.0, 0.0), (4096, 0.0, 0.0, 0.0),
                                                    (4097, 0.5, 5.0, 0.0), (8192, 0.0, 0.0, 0.0),
                                                    (9000, 0.5, 0.0, 0.0), (12388, 0.5, 0.0, 5.0),
-                                                   (16384, 0.3, 5.0, 5.0)])
+                                                   (16384, 0.3, 5.0, 5.0), (20000, 0.0, 0.0, 0.0),
+                                                   (32768, 0.5, 5.0, 0.0), (40000, 0.0, 0.0, 5.0),
+                                                   (65536, 0.5, 0.0, 0.0)])
 def test_fused_small_matches_three_kernel_path(bpf, N, thr, nu_obs, nu_state):
     """Records, ancestors and particles of the fused one-launch tick equal the three-kernel
     tick's bit for bit: through step_many (a captured run of 64 ticks as one launch), the
@@ -362,11 +364,11 @@ def test_fused_small_matches_three_kernel_path(bpf, N, thr, nu_obs, nu_state):
         assert a[1] == b[1] and a[2] == b[2] and a[3:] == b[3:], mode
 
 
-@pytest.mark.parametrize("N,thr", [(4096, 0.0), (12000, 0.5), (16384, 0.0)])
+@pytest.mark.parametrize("N,thr", [(4096, 0.0), (12000, 0.5), (16384, 0.0), (30000, 0.5), (65536, 0.0)])
 def test_fused_small_long_device_run(bpf, N, thr):
     """A whole device-resident run of 2500 ticks as one fused launch (one CTA, or a cluster of
-    three or four; the observations are restaged in shared memory every 1024 ticks) equals the
-    three-kernel run."""
+    3, 4, 8 or 16, padding CTAs included; the observations are restaged in shared memory every
+    1024 ticks) equals the three-kernel run."""
     import torch
     T = 2500
     _, y = series(T, 42)
@@ -384,7 +386,7 @@ def test_fused_small_long_device_run(bpf, N, thr):
     assert out[0] == out[1]
 
 
-@pytest.mark.parametrize("N,thr", [(20000, 0.0), (65536, 0.5), (300000, 0.5), (1 << 20, 0.0)])
+@pytest.mark.parametrize("N,thr", [(65537, 0.0), (100000, 0.5), (300000, 0.5), (1 << 20, 0.0)])
 def test_tail_plan_matches_plan_kernel(bpf, N, thr):
     """Filters of at most 256 tiles run the plan in pass 1's last CTA; with per-kernel profiling
     on, the same ticks run the separate plan kernel. Records, ancestors and particles agree bit
