@@ -208,7 +208,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
           if (ck) ck[i] = h;
           if (t > 0) {
             const uint64_t s = c.k1 + c.k2 * pcg_inc((uint32_t)i);
-            float z = icdf_normal(pcg_uniform(pcg_output(s)));
+            float z = icdf_normal_active(pcg_uniform(pcg_output(s)));
             if (f.nu_int > 0) z *= tstate_scale(c, (uint32_t)i, f.nu_int, f.nu_state);
             if constexpr (NOISE) {
               if (zi) z = fmaf(cr, zi[(size_t)t * nzs + i], cs * z);
@@ -240,8 +240,7 @@ __device__ void batch_run_filter(const BatchArgs& a, const BatchFilterDev& f, in
 #pragma unroll
     for (int k = 0; k < kBatchMaxTiles; ++k) {
       float m = -INFINITY;
-      if (k < G)
-        for (int w = 0; w < W; ++w) m = fmaxf(m, sh.tmax[k][w]);
+      if (k < G) m = warp_max_f(lane < W ? sh.tmax[k][lane] : -INFINITY);   // every warp, the same max
       nk[k] = (m == -INFINITY) ? kNkEmpty : (int)ceilf(fmaxf(m, -1.0e9f));
     }
 

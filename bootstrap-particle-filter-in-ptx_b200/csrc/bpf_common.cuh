@@ -175,6 +175,21 @@ __device__ __forceinline__ float icdf_normal_warp(float u) {
   return p * xs;
 }
 
+// The same for code whose warp may be partly active (a loop over particles whose trip count
+// differs between lanes): the vote covers the active lanes only.
+__device__ __forceinline__ float icdf_normal_active(float u) {
+  const float t = u * (1.0f - u);
+  const float l2 = lg2_approx(t);
+  const float xs = fmaf(2.82842712474619010f, u, -1.41421356237309505f);
+  float p = icdf_central_poly(l2);
+  const bool tail = !(l2 > kIcdfTailL2);
+  if (__any_sync(__activemask(), tail)) {
+    const float pt = icdf_tail_poly(l2);
+    if (tail) p = pt;
+  }
+  return p * xs;
+}
+
 // ---------------------------------------------------------------------------
 // Observation log-density log p(y | h) (PTX :414-451; gpu_bpf.cu:226)
 //   Gaussian:  -1/2 ln(2 pi) - 1/2 y^2 e^{-h} - 1/2 h
