@@ -781,12 +781,15 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     const float4* wt = reinterpret_cast<const float4*>(ws + tid * kPerThread);
     const bool massive = r < 64;
     unsigned long long run = 0ull;
+    float lfT = 0.0f;            // FP32 sum of the thread's weights, in the child count's order
     if (massive) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const float4 f = wt[v];
-        run += fix_weight(tile_weight(f.x)) + fix_weight(tile_weight(f.y));
-        run += fix_weight(tile_weight(f.z)) + fix_weight(tile_weight(f.w));
+        const float a0 = tile_weight(f.x), a1 = tile_weight(f.y), a2 = tile_weight(f.z), a3 = tile_weight(f.w);
+        run += fix_weight(a0) + fix_weight(a1);
+        run += fix_weight(a2) + fix_weight(a3);
+        lfT += a0; lfT += a1; lfT += a2; lfT += a3;
       }
     }
     unsigned long long tot;
@@ -813,10 +816,25 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
     }
     const float R0w = (float)R0 * 0x1p-50f;           // in units of the tile's largest weight
     const float invDw = 1.0f / ((float)D * 0x1p-50f);
-    // bound on the estimate's error: (lf + R0w) 2^-18 / Dw + 2^-44 / Dw + |x| 2^-21
+    const float R0x = R0w * invDw;                    // the estimate is x = lf invDw - R0x (one FMA)
+    // Bound on the estimate's error at an element with running sum lf and estimate x:
+    // (lf + R0w) 2^-18 / Dw + 2^-44 / Dw + |x| 2^-21. Every term is non-negative and the
+    // roundings are monotone, so it is largest at the thread's largest lf (lfT, the same
+    // additions in the same order) and largest |x| (x runs from at least -R0x up to xT): the
+    // thread takes that one bound for all its elements. A wider bound only sends more elements
+    // to the exact recount. Estimates of 2^22 and more (xT) recount every element.
     const float eL = 0x1p-18f * invDw, e0 = fmaf(R0w, eL, 0x1p-44f * invDw);
+    const float xT = fmaf(lfT, invDw, -R0x);
+    float err = fmaf(lfT, eL, fmaf(fmaxf(fabsf(xT), R0x), 0x1p-21f, e0));
+    if (!(xT < 0x1p22f)) err = 1.0f;
+    const float err_hi = 1.0f - err;
     const float* wsel = ws + tid * kPerThread;
     int32_t* csr = (a.csr && (item.w & 1)) ? a.csr + j0 : nullptr;   // children of j: [csr[j], csr[j+1])
+    // Output slots below are relative to the window origin wa. The end of element j's children,
+    // min(q0 + c_j, N) with c_j = max(floor(x) + 1, 0), is formed from the bits of fl + 2^23
+    // (exact for the fl that pass the bound) as min(max(bits - Kq, qlo), nr).
+    const int qlo = q0 - wa, nr = N - wa, oar = oa - wa, obr = ob - wa;
+    const int Kq = 0x4AFFFFFF - qlo;
     // Compile-time variants: WHOLE (the item holds every output of the tile, so each
     // counted child lands in the window), TAPE (first-child list for the gradient tape).
     const bool whole = (item.w & 2) != 0;
@@ -824,28 +842,34 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       constexpr bool WHOLE = decltype(whole_tag)::value;
       constexpr bool TAPE = decltype(tape_tag)::value;
       float lf = 0.0f;
-      int qp = q0;                                   // first slot of the next element's children
+      int qp = qlo;                                  // first slot of the next element's children
 #pragma unroll 1
       for (int g = 0; g < 4; ++g) {
         const float4 f4 = wt[g];
         const float ff[4] = {f4.x, f4.y, f4.z, f4.w};
+        int qq[4];
+        bool rc[4], any = false;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          lf += tile_weight(ff[e]);
+          const float x = fmaf(lf, invDw, -R0x);
+          const float fl = floorf(x);
+          const float fr = x - fl;                       // exact
+          rc[e] = !(fr > err && fr < err_hi);
+          any |= rc[e];
+          qq[e] = min(max(__float_as_int(fl + 0x1p23f) - Kq, qlo), nr);
+        }
+        if (__any_sync(0xffffffffu, any)) {            // one vote per four elements
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (rc[e]) qq[e] = min(qlo + exact_count(wsel, 4 * g + e, R0, D, N), nr);
+        }
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int j = tid * kPerThread + 4 * g + e;
-          if (TAPE && j < nA) csr[j] = qp;
-          lf += tile_weight(ff[e]);
-          const float x = (lf - R0w) * invDw;
-          const float fl = floorf(x);
-          const float fr = x - fl;                       // exact
-          const float err = fmaf(lf, eL, fmaf(fabsf(x), 0x1p-21f, e0));
-          const bool recount = !(fr > err && fr < 1.0f - err && fl < 0x1p22f);
-          // floor(x) + 1 for x >= 0, 0 for x < 0 (from the float's bits: fl + 2^23 is exact)
-          int c = max(__float_as_int(fl + 0x1p23f) - 0x4AFFFFFF, 0);
-          if (__any_sync(0xffffffffu, recount)) {
-            if (recount) c = exact_count(wsel, 4 * g + e, R0, D, N);
-          }
-          const int q1 = min(q0 + c, N);
-          if (q1 > qp && (WHOLE || (qp < ob && q1 > oa))) marks[(WHOLE ? qp : max(qp, oa)) - wa] = (unsigned short)(j + 1);
+          if (TAPE && j < nA) csr[j] = qp + wa;
+          const int q1 = qq[e];
+          if (q1 > qp && (WHOLE || (qp < obr && q1 > oar))) marks[WHOLE ? qp : max(qp, oar)] = (unsigned short)(j + 1);
           qp = q1;
         }
       }
