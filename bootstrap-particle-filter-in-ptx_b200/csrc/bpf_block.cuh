@@ -156,9 +156,13 @@ __device__ __forceinline__ unsigned long long shr64(unsigned long long x, int r)
   return r >= 64 ? 0ull : (x >> r);
 }
 __host__ __device__ inline int ceil_log2_u(unsigned n) {
+#ifdef __CUDA_ARCH__
+  return n <= 1u ? 0 : 32 - __clz((int)(n - 1u));
+#else
   int c = 0;
   while ((1ull << c) < (unsigned long long)n) ++c;
   return c;
+#endif
 }
 
 // #{ i in [0,N) : base + i*delta < c } (targets strictly below c)

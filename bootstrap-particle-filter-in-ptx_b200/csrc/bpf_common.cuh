@@ -326,6 +326,14 @@ __device__ __forceinline__ uint64_t udiv_fp64(uint64_t a, uint64_t b) {
   while (a - q * b >= b) ++q;
   return q;
 }
+// The same quotient from an FP64 reciprocal rb of b (1/b rounded once): for a / b < 2^50 the
+// estimate is within one of the quotient, and the same corrections make it exact.
+__device__ __forceinline__ uint64_t udiv_fp64_rcp(uint64_t a, uint64_t b, double rb) {
+  uint64_t q = __double2ull_rz((double)a * rb);
+  while (q > 0ull && q * b > a) --q;
+  while (a - q * b >= b) ++q;
+  return q;
+}
 // Reciprocal for udiv_magic: m <= floor((2^64-1)/d) with a relative deficit
 // below 2^-48, so the quotient estimate is short by at most 3 for a/d < 2^31.
 __device__ __forceinline__ uint64_t udiv_magic_of(uint64_t d) {

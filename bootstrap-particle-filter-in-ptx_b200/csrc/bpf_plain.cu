@@ -688,11 +688,6 @@ static_assert((size_t)kOutChunk % kGatherStep == 0, "the gather reads marks in s
 // below 2^57 for every count c the loop forms.
 constexpr unsigned long long kThCap = 1ull << 55;
 
-// floor(a / d) for 1 <= d, a < 2^62: the rare path of a parent with more than four children.
-__device__ __noinline__ unsigned long long udiv_slow(unsigned long long a, unsigned long long d) {
-  return udiv_fp64(a, d);
-}
-
 // Exact count of targets up to element `upto` of a thread's 16 staged log2-weights d:
 // #{m >= 0 : R0 + m D <= sum_{i <= upto} floor(2^d_i 2^50)}, at most cap. The rare path of
 // the FP32 estimate in pass 2's child count.
@@ -1105,6 +1100,7 @@ static_assert(kSmallMaxN < (1 << 30), "start marks hold parent + 1");
 struct FusedPlan {
   unsigned long long base, delta, magic, total;
   int nM, Fg, items, zero_spacing;
+  int live;                                   // threshold 0: the tick resamples (not degenerate)
 };
 
 struct FusedShared {
@@ -1284,18 +1280,15 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
   }
 }
 
-// The plan of a fused tick by one thread, for NCTA <= kSmallTiles tiles: the statistics and
-// the decision, the operations of plan_body on one warp in the same order. There lane k holds
-// tile k's FP64 sums and the lanes past the tiles exact zeros, so lane 0's butterfly sum is
-// the pairwise tree below: v_i + v_{i+8}, then i + 4, i + 2, i + 1, each lane's value first
-// normalised by adding lane i + 16's zero (every lane holds the same totals).
+// The FP64 sums of a fused tick over all tiles' records, for NCTA <= kSmallTiles tiles, by one
+// thread: the operations of plan_body on one warp in the same order. There lane k holds tile k's
+// FP64 sums and the lanes past the tiles exact zeros, so lane 0's butterfly sum is the pairwise
+// tree below: v_i + v_{i+8}, then i + 4, i + 2, i + 1, each lane's value first normalised by
+// adding lane i + 16's zero (every lane holds the same totals). nM: the tick's global exponent.
 template <int NCTA>
-__device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared& sh, int par, BpfTickRecord* rec_out) {
+__device__ __forceinline__ void fused_sums(const FusedShared& sh, int par, int nM, double& tS, double& tQ,
+                                           double& tH) {
   static_assert(NCTA >= 1 && NCTA <= 16, "the tree below covers sixteen lanes");
-  DevState* st = &sh.st;
-  int nM = kNkEmpty;
-#pragma unroll
-  for (int k = 0; k < NCTA; ++k) nM = max(nM, sh.peer[k]->nexp[par]);
   // lane k's sums: its running frame is its own tile's, then the global frame 2^nM; each is
   // normalised by the butterfly's first addition of a zero lane (v + 0 turns -0 into +0)
   auto lane_sums = [&](int k, double& S, double& Q, double& H) {
@@ -1334,7 +1327,44 @@ __device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared
         if (i + w < NCTA) v[i] = __dadd_rn(v[i], v[i + w]);
     return v[0];
   };
-  const double tS = tree(bS), tQ = tree(bQ), tH = tree(bH);
+  tS = tree(bS); tQ = tree(bQ); tH = tree(bH);
+}
+
+template <int NCTA>
+__device__ __forceinline__ int fused_nM(const FusedShared& sh, int par) {
+  int nM = kNkEmpty;
+#pragma unroll
+  for (int k = 0; k < NCTA; ++k) nM = max(nM, sh.peer[k]->nexp[par]);
+  return nM;
+}
+
+// The plan of a fused tick by warp 0: the statistics (for more than two tiles lane k reads tile k's
+// record and the warp's butterfly forms the sums, which is the tree of fused_sums), then lane 0
+// takes the decision, writes the record and the next tick's state.
+template <int NCTA>
+__device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared& sh, int par, BpfTickRecord* rec_out) {
+  const int lane = threadIdx.x & 31;
+  int nM;
+  double tS, tQ, tH;
+  if constexpr (NCTA <= 2) {
+    nM = fused_nM<NCTA>(sh, par);
+    fused_sums<NCTA>(sh, par, nM, tS, tQ, tH);
+  } else {
+    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+    int nk = kNkEmpty;
+    if (lane < NCTA) { r = sh.peer[lane]->rec[par]; nk = __float_as_int(r.w); }
+    nM = warp_max_i(nk);
+    double S = 0.0, Q = 0.0, H = 0.0;
+    if (nk != kNkEmpty) {
+      const double sc = pow2d(nk - nM);
+      S = __dmul_rn(__dadd_rn(0.0, (double)r.x), sc);
+      Q = __dmul_rn(__dadd_rn(0.0, (double)r.y), __dmul_rn(sc, sc));
+      H = __dmul_rn(__dadd_rn(0.0, (double)r.z), sc);
+    }
+    tS = warp_sum_d(S); tQ = warp_sum_d(Q); tH = warp_sum_d(H);
+  }
+  if (lane != 0) return;
+  DevState* st = &sh.st;
   const bool degenerate = (nM == kNkEmpty) || !(tS > 0.0);
   constexpr double kLn2d = 0.693147180559945309417232121458;
   double res[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1348,45 +1378,7 @@ __device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared
   plan_decide(a, st, N, nM, degenerate, res, tS, rec_out);
 }
 
-// The tick's resampling plan by one thread, whether or not the tick resamples (it runs beside
-// the decision): the fixed-point CDF over the tiles, the target spacing, base and reciprocal and
-// the item count, as plan_body. u_state: the resampling-uniform state at the start of the tick.
-template <int NCTA>
-__device__ __forceinline__ void plan_fused_targets(int N, FusedShared& sh, int par, unsigned long long u_state) {
-  int nM = kNkEmpty;
-#pragma unroll
-  for (int k = 0; k < NCTA; ++k) nM = max(nM, sh.peer[k]->nexp[par]);
-  const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
-  unsigned long long Pk[NCTA + 1];
-  Pk[0] = 0ull;
-#pragma unroll
-  for (int k = 0; k < NCTA; ++k) {
-    const int nk = sh.peer[k]->nexp[par];
-    Pk[k + 1] = Pk[k] + ((nk != kNkEmpty) ? shr64(sh.peer[k]->E[par], nM - nk + kFixF - Fg) : 0ull);
-  }
-  const unsigned long long total = Pk[NCTA];
-  unsigned long long delta = udiv_fp64(total, (unsigned long long)N);
-  const bool zero_spacing = delta == 0ull;
-  if (zero_spacing) delta = 1ull;
-  const unsigned long long u = pcg_output(u_state) >> 9;       // the tick's resampling uniform
-  const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
-  const unsigned long long base = (hi << 41) | (lo >> 23);     // floor(u * delta / 2^23)
-  const unsigned long long magic = udiv_magic_of(delta);
-  int n_items = 0;
-  int o = targets_below(Pk[0], base, delta, magic, N);
-#pragma unroll
-  for (int k = 0; k < NCTA; ++k) {
-    const int o_next = targets_below(Pk[k + 1], base, delta, magic, N);
-    n_items += (o_next - o + kOutChunk - 1) / kOutChunk;
-    o = o_next;
-    sh.P[k] = Pk[k];
-  }
-  FusedPlan& pl = sh.pl;
-  pl.base = base; pl.delta = delta; pl.magic = magic; pl.total = total;
-  pl.nM = nM; pl.Fg = Fg; pl.items = n_items; pl.zero_spacing = zero_spacing ? 1 : 0;
-}
-
-// The resampling plan into the device state (thread 0, on a resampling tick).
+// The resampling plan into the device state (on a resampling tick).
 __device__ __forceinline__ void store_fused_plan(DevState* st, const FusedShared& sh) {
   const FusedPlan& pl = sh.pl;
   if (pl.zero_spacing) st->error = BPF_ERR_DEGENERATE;
@@ -1394,27 +1386,94 @@ __device__ __forceinline__ void store_fused_plan(DevState* st, const FusedShared
   st->Fg = pl.Fg; st->n_items = pl.items;
 }
 
-// A thread's four-slot chunk (slots 4 tid .. 4 tid + 3 of the tile) against the tick's
-// targets: its exact weights, tile-local prefix, first target and tile-frame thresholds.
+// The tick's resampling plan by warp 1, lane k for tile k (NCTA <= 32): the fixed-point CDF over
+// the tiles (an exact u64 scan), the target spacing, base and reciprocal and the item count, as
+// plan_body; lane 0 writes the plan and, when the tick resamples, its fields of the device state.
+// u_state: the resampling-uniform state at the start of the tick. ahead (threshold 0, the plan runs
+// beside the decision): whether the tick resamples is found here too, as the plan's decision would,
+// not degenerate: its FP64 weight sum is a sum of the tiles' non-negative terms, positive exactly
+// when no term is NaN and one is positive. Returns whether the plan is stored.
+template <int NCTA>
+__device__ __forceinline__ bool plan_fused_targets(int N, double rcpN, FusedShared& sh, int par,
+                                                   unsigned long long u_state, bool ahead) {
+  static_assert(NCTA <= 32, "one lane per tile");
+  const int lane = threadIdx.x & 31;
+  int nk = kNkEmpty;
+  unsigned long long E = 0ull;
+  float S = 0.0f;
+  if (lane < NCTA) {
+    const FusedShared* pk = sh.peer[lane];
+    nk = pk->nexp[par];
+    E = pk->E[par];
+    S = pk->rec[par].x;
+  }
+  const int nM = warp_max_i(nk);
+  const int Fg = min(kFixF, 62 - ceil_log2_u((unsigned)N));
+  const unsigned long long mass = (nk != kNkEmpty) ? shr64(E, nM - nk + kFixF - Fg) : 0ull;
+  const unsigned long long incl = warp_incl_scan_add(mass, lane);
+  const unsigned long long excl = incl - mass;
+  const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long delta = udiv_fp64_rcp(total, (unsigned long long)N, rcpN);
+  const bool zero_spacing = delta == 0ull;
+  if (zero_spacing) delta = 1ull;
+  const unsigned long long u = pcg_output(u_state) >> 9;       // the tick's resampling uniform
+  const unsigned long long hi = __umul64hi(u, delta), lo = u * delta;
+  const unsigned long long base = (hi << 41) | (lo >> 23);     // floor(u * delta / 2^23)
+  const unsigned long long magic = udiv_magic_of(delta);
+  int ni = 0;
+  if (lane < NCTA) {
+    const int o = targets_below(excl, base, delta, magic, N), o_next = targets_below(incl, base, delta, magic, N);
+    ni = (o_next - o + kOutChunk - 1) / kOutChunk;
+    sh.P[lane] = excl;
+  }
+  const int n_items = __reduce_add_sync(0xffffffffu, ni);
+  bool live = true;
+  if (ahead) {
+    double term = 0.0;
+    if (nk != kNkEmpty) term = __dmul_rn((double)S, pow2d(nk - nM));
+    live = (nM != kNkEmpty) && !__any_sync(0xffffffffu, term != term) && __any_sync(0xffffffffu, term > 0.0);
+  }
+  if (lane == 0) {
+    FusedPlan& pl = sh.pl;
+    pl.base = base; pl.delta = delta; pl.magic = magic; pl.total = total;
+    pl.nM = nM; pl.Fg = Fg; pl.items = n_items; pl.zero_spacing = zero_spacing ? 1 : 0;
+    pl.live = live ? 1 : 0;
+    if (live) store_fused_plan(&sh.st, sh);
+  }
+  return live;
+}
+
+// A chunk of CH consecutive slots of the tile (slots CH c .. CH c + CH - 1) against the tick's
+// targets: its weights, their FP32 sum in order, its first target and tile-frame thresholds
+// (th = kThCap: no target is reachable from the chunk).
+template <int CH>
 struct ChunkTargets {
-  unsigned long long f[4];
+  float wf[CH];
+  float lfT;
   unsigned long long th, D;
-  int q;
+  int q, c;
 };
 
-template <int NCTA>
-__device__ __forceinline__ ChunkTargets chunk_targets(int N, int k, int par, const FusedShared& sh) {
-  const int tid = threadIdx.x;
+template <int NCTA, int CH>
+__device__ __forceinline__ ChunkTargets<CH> chunk_targets(int N, int k, int par, int c, const FusedShared& sh) {
+  static_assert(CH % 4 == 0, "whole four-slot chunks");
   const FusedPlan& pl = sh.pl;
   const int nk = sh.nexp[par];
   const int r = (nk == kNkEmpty) ? 64 : pl.nM - nk + kFixF - pl.Fg;
   const unsigned long long Pk = sh.P[k], base = pl.base, delta = pl.delta;
-  const int l0 = 4 * tid, j0 = k * kTile + l0;
-  const float4 w4 = *reinterpret_cast<const float4*>(sh.w + l0);
-  ChunkTargets ct;
-  ct.f[0] = fix_weight(tile_weight(w4.x)); ct.f[1] = fix_weight(tile_weight(w4.y));
-  ct.f[2] = fix_weight(tile_weight(w4.z)); ct.f[3] = fix_weight(tile_weight(w4.w));
-  const unsigned long long loc = sh.chunkP[tid];
+  const int l0 = CH * c, j0 = k * kTile + l0;
+  ChunkTargets<CH> ct;
+  ct.c = c;
+  ct.lfT = 0.0f;
+#pragma unroll
+  for (int v = 0; v < CH / 4; ++v) {
+    const float4 w4 = *reinterpret_cast<const float4*>(sh.w + l0 + 4 * v);
+    ct.wf[4 * v] = tile_weight(w4.x); ct.wf[4 * v + 1] = tile_weight(w4.y);
+    ct.wf[4 * v + 2] = tile_weight(w4.z); ct.wf[4 * v + 3] = tile_weight(w4.w);
+  }
+#pragma unroll
+  for (int e = 0; e < CH; ++e) ct.lfT += ct.wf[e];
+  const unsigned long long loc = sh.chunkP[l0 / 4];   // exclusive prefix of its first four-slot chunk
   // child counts against tile-frame thresholds, as pass 2
   ct.q = targets_below(Pk + shr64(loc, r), base, delta, pl.magic, N);
   ct.th = kThCap; ct.D = kThCap;
@@ -1441,46 +1500,79 @@ __device__ __forceinline__ void put_mark(FusedShared& sh, int o, int val) {
   else marks_of<NCTA>(*sh.peer[o >> 12])[o & (kTile - 1)] = (MarkOf<NCTA>)val;
 }
 
-// Resampling of a fused tick, this CTA's part: the children of its tile's particles (start
-// marks into the owners' shared memory), a cluster barrier, then the gather of its own outputs.
+// Resampling of a fused tick, this CTA's part: the children of its tile's particles (start marks
+// into the owners' shared memory, count_marks), a barrier over the cluster, then the gather of its
+// own outputs (gather_fused).
+template <int NCTA, int CH>
+__device__ __forceinline__ void count_marks(int N, int k, const ChunkTargets<CH>& ct, FusedShared& sh) {
+  // The children of the chunk's elements as in pass 2: the running count c_j = #{m >= 0 :
+  // th + m D <= l_j} (l_j the exact fixed-point sum of the chunk's weights up to j) estimated in
+  // FP32 from the running sum of the weights, with pass 2's bound on the estimate's error taken at
+  // the chunk's largest sum; near a target boundary (one vote per four elements) the element
+  // recounts in exact 64-bit integers. The output slots of element j are [q_{j-1}, q_j),
+  // q_j = min(q + c_j, N); element j marks the first one and the first of every further 256-output
+  // block. A chunk from which no target is reachable (th = kThCap) has no children.
+  const int j0 = k * kTile + CH * ct.c;
+  const float* d = sh.w + CH * ct.c;               // its log2-weights, for the exact recount
+  const unsigned long long R0 = ct.th, D = ct.D;
+  const bool none = R0 >= kThCap;
+  const float R0w = (float)R0 * 0x1p-50f;
+  const float invDw = 1.0f / ((float)D * 0x1p-50f);
+  const float R0x = R0w * invDw;
+  const float eL = 0x1p-18f * invDw, e0 = fmaf(R0w, eL, 0x1p-44f * invDw);
+  const float xT = fmaf(ct.lfT, invDw, -R0x);
+  float err = fmaf(ct.lfT, eL, fmaf(fmaxf(fabsf(xT), R0x), 0x1p-21f, e0));
+  if (!(xT < 0x1p22f)) err = 1.0f;
+  const float err_hi = 1.0f - err;
+  const int q0 = ct.q, Kq = 0x4AFFFFFF - q0;
+  float lf = 0.0f;
+  int qp = q0;
+#pragma unroll
+  for (int g = 0; g < CH / 4; ++g) {
+    int qq[4];
+    bool rc[4], any = false;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      lf += ct.wf[4 * g + e];
+      const float x = fmaf(lf, invDw, -R0x);
+      const float fl = floorf(x);
+      const float fr = x - fl;                       // exact
+      rc[e] = !none && !(fr > err && fr < err_hi);
+      any |= rc[e];
+      qq[e] = none ? q0 : min(max(__float_as_int(fl + 0x1p23f) - Kq, q0), N);
+    }
+    if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (rc[e]) qq[e] = min(q0 + exact_count(d, 4 * g + e, R0, D, N), N);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int q1 = qq[e];
+      if (q1 > qp) {
+        const int val = j0 + 4 * g + e + 1;
+        put_mark<NCTA>(sh, qp, val);
+        for (int b = (qp | (kGatherStep - 1)) + 1; b < q1; b += kGatherStep) put_mark<NCTA>(sh, b, val);
+      }
+      qp = q1;
+    }
+  }
+}
+
+// The gather, by warps 1..kMarkWarps (warp 0 may still be taking the tick's decision): the
+// ancestor of output o is the last start mark at or before o; the first output of every 256-output
+// block has one, so each warp's block stands alone. Each lane resolves eight consecutive outputs (a
+// running max and a warp max-scan) and writes parent + 1 back over the marks; the warp then reads
+// them lane-interleaved, so the particle reads and writes and the ancestor stores of a warp touch
+// consecutive slots. src / dst: the particle buffers the resampling reads and writes.
 template <int NCTA>
-__device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, const ChunkTargets& ct,
-                                               FusedShared& sh) {
+__device__ __forceinline__ void gather_fused(const TickArgs& a, int N, int k, int src, int dst, FusedShared& sh) {
   static_assert(kTile == 1 << 12, "output owner = o >> 12");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tile0 = k * kTile;
-  const DevState& st = sh.st;
-  const int j0 = tile0 + 4 * tid;
-  const unsigned long long D = ct.D;
-  unsigned long long th = ct.th;
-  int q = ct.q;
-  unsigned long long acc = 0ull;
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    acc += ct.f[e];
-    if (acc >= th) {
-      const unsigned long long diff = acc - th;
-      int cn = 1 + (diff >= D) + (diff >= 2ull * D) + (diff >= 3ull * D);
-      if (cn == 4 && diff >= 4ull * D) cn = (int)min(udiv_slow(diff, D), (unsigned long long)N) + 1;
-      const int q1 = min(q + cn, N);
-      const int val = j0 + e + 1;
-      put_mark<NCTA>(sh, q, val);
-      // the first output of every further 256-output block the run reaches
-      for (int b = (q | (kGatherStep - 1)) + 1; b < q1; b += kGatherStep) put_mark<NCTA>(sh, b, val);
-      th = (q1 >= N) ? kThCap : th + (unsigned long long)cn * D;
-      q = q1;
-    }
-  }
-  cluster_sync_all<NCTA>();                      // every start mark is in place
-
-  // gather: the ancestor of output o is the last start mark at or before o; the first output of
-  // every 256-output block has one, so each warp's block stands alone. Each lane resolves eight
-  // consecutive outputs (a running max and a warp max-scan) and writes parent + 1 back over the
-  // marks; the warp then reads them lane-interleaved, so the particle reads and writes and the
-  // ancestor stores of a warp touch consecutive slots.
   const int n_out = min(N - tile0, kTile);
-  const int o0 = warp * kGatherStep;
-  if (warp < kMarkWarps && o0 < n_out) {
+  const int o0 = (warp - 1) * kGatherStep;
+  if (warp >= 1 && warp <= kMarkWarps && o0 < n_out) {
     using M = MarkOf<NCTA>;
     M* marks = marks_of<NCTA>(sh);
     constexpr int VPL = (int)(8 * sizeof(M)) / 16;   // uint4 per lane: eight marks
@@ -1517,8 +1609,7 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
       mrow[2 * lane + 1] = make_uint4(jj[4], jj[5], jj[6], jj[7]);
     }
     __syncwarp();
-    const int src = st.src;
-    float* hd = sh.h[st.cur];
+    float* hd = sh.h[dst];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int o = o0 + 32 * u + lane;
@@ -1532,6 +1623,24 @@ __device__ __forceinline__ void resample_fused(const TickArgs& a, int N, int k, 
 #pragma unroll
     for (int x = 0; x < VPL; ++x) mrow[VPL * lane + x] = make_uint4(0u, 0u, 0u, 0u);   // clear for the next resampling
   }
+}
+
+// The barrier between the start marks and the gather when warp 0 is taking the tick's decision
+// meanwhile: warp 0 arrives before it starts (it places no marks and gathers nothing) and waits
+// after it, the other warps arrive and wait together. Barrier 4 for one CTA, the cluster's otherwise.
+template <int NCTA>
+__device__ __forceinline__ void marks_barrier_arrive() {
+  if constexpr (NCTA == 1) asm volatile("bar.arrive 4, %0;" ::"n"(kSmallThreads) : "memory");
+  else asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+template <int NCTA>
+__device__ __forceinline__ void marks_barrier_wait() {
+  if constexpr (NCTA > 1) asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+template <int NCTA>
+__device__ __forceinline__ void marks_barrier_sync() {
+  if constexpr (NCTA == 1) asm volatile("bar.sync 4, %0;" ::"n"(kSmallThreads) : "memory");
+  else cluster_sync_all<NCTA>();
 }
 
 template <bool TSTATE, bool GAUSS, int NCTA>
@@ -1567,6 +1676,9 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
   constexpr int kMarkVecs = (int)(sizeof(MarkOf<NCTA>) * (kTile + kGatherStep) / 16);
   for (int x = tid; x < kMarkVecs; x += kSmallThreads) reinterpret_cast<uint4*>(sh.marks_raw)[x] = make_uint4(0u, 0u, 0u, 0u);
 
+  const double rcpN = 1.0 / (double)N;           // exact division by N: the quotient is corrected
+  const bool ahead = a.ess_threshold <= 0.0f;     // every tick that can resample does
+  const int warp = tid >> 5;
   for (int t = 0; t < n_ticks; ++t) {
     const int par = t & 1;
     if (a.y_ptr && (t & (kYStage - 1)) == 0) {       // the next kYStage observations
@@ -1576,31 +1688,41 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
     __syncthreads();
     const float y = a.y_ptr ? sh.ys[t & (kYStage - 1)] : a.obs.y;
     const unsigned long long u_state = sh.st.u_state;
+    const int cur0 = sh.st.cur;                    // a resampling reads buffer cur0, writes cur0 ^ 1
     pass1_fused<TSTATE, GAUSS, kSmallSplit>(a, y, N, tile0, par, sh.nexp[par ^ 1], sh);
     cluster_sync_all<NCTA>();                   // every tile record of the tick is in place
-    // thread 0 takes the decision. When every tick resamples (threshold 0), thread 32 meanwhile
-    // forms the resampling plan and warps 1..31 place their chunks against its targets; else
-    // that waits for the decision and runs on resampling ticks only.
-    const bool ahead = a.ess_threshold <= 0.0f;
-    ChunkTargets ct{};
-    if (tid == 0) {
-      plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
-    } else if (ahead && tid >= 32) {
-      if (tid == 32) plan_fused_targets<NCTA>(N, sh, par, u_state);
-      asm volatile("bar.sync 3, %0;" ::"n"(kSmallThreads - 32) : "memory");
-      ct = chunk_targets<NCTA>(N, k, par, sh);
-    }
-    __syncthreads();
-    if (sh.st.do_resample) {
-      if (!ahead) {
-        if (tid == 32) plan_fused_targets<NCTA>(N, sh, par, u_state);
-        __syncthreads();
-        ct = chunk_targets<NCTA>(N, k, par, sh);
-      } else if (tid < 32) {
-        ct = chunk_targets<NCTA>(N, k, par, sh);
+    if (ahead) {
+      // The resampling needs nothing from the decision but whether the tick is degenerate, so
+      // warp 0 takes the decision and writes the record beside it: warp 1 forms the plan (and
+      // the plan's fields of the device state, which the decision does not touch), warps 16..31
+      // count the children of eight-slot chunks, warps 1..16 gather.
+      if (warp == 0) {
+        marks_barrier_arrive<NCTA>();
+        plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
+        __syncwarp();
+        marks_barrier_wait<NCTA>();
+      } else {
+        if (warp == 1) plan_fused_targets<NCTA>(N, rcpN, sh, par, u_state, true);
+        asm volatile("bar.sync 3, %0;" ::"n"(kSmallThreads - 32) : "memory");   // warps 1..31
+        const bool live = sh.pl.live != 0;
+        if (live && tid >= kSmallThreads / 2) {
+          const ChunkTargets<8> ct = chunk_targets<NCTA, 8>(N, k, par, tid - kSmallThreads / 2, sh);
+          count_marks<NCTA, 8>(N, k, ct, sh);
+        }
+        marks_barrier_sync<NCTA>();               // every start mark is in place
+        if (live) gather_fused<NCTA>(a, N, k, cur0, cur0 ^ 1, sh);
       }
-      if (tid == 0) store_fused_plan(&sh.st, sh);
-      resample_fused<NCTA>(a, N, k, ct, sh);
+    } else {
+      if (warp == 0) plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
+      __syncthreads();
+      if (sh.st.do_resample) {
+        if (warp == 1) plan_fused_targets<NCTA>(N, rcpN, sh, par, u_state, false);
+        __syncthreads();
+        const ChunkTargets<4> ct = chunk_targets<NCTA, 4>(N, k, par, tid, sh);
+        count_marks<NCTA, 4>(N, k, ct, sh);
+        cluster_sync_all<NCTA>();                 // every start mark is in place
+        gather_fused<NCTA>(a, N, k, cur0, cur0 ^ 1, sh);
+      }
     }
   }
   if (tid == 0 && a.mirror) sh.st.seq = a.seq;
