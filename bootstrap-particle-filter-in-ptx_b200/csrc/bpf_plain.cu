@@ -1070,20 +1070,23 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 // marks and particles through distributed shared memory and meet at one
 // cluster barrier per tick (two on resampling ticks).
 //   pass 1    each CTA runs its tile with pass 1's per-particle arithmetic on
-//             four times as many threads and hands the FP32 running sums along
-//             in pass 1's element order, so every tile record is bit for bit
-//             pass 1's; while warp 0 forms the FP64 record, half the CTA scans
-//             the tile's exact fixed-point masses (needed if the tick resamples);
-//   plan      one thread per CTA runs the plan over all the tile records: the
-//             operations of the plan kernel in the same order (so every CTA takes
-//             the same decision and holds the same device state); CTA 0 writes
-//             the tick's record;
+//             twice as many threads and hands the FP32 running sums along in
+//             pass 1's element order, so every tile record is bit for bit pass 1's;
+//             while warp 0 forms the FP64 record, half the CTA scans the tile's
+//             exact fixed-point masses (needed if the tick resamples);
+//   plan      warp 0 of every CTA runs the plan over all the tile records (lane k
+//             reads tile k's): the operations of the plan kernel in the same order
+//             (so every CTA takes the same decision and holds the same device state);
+//             CTA 0 writes the tick's record; warp 1 forms the resampling plan;
 //   resample  the same fixed-point rule (integer exact, so the ancestors do not
 //             depend on how the work is split): each CTA counts its tile's
-//             children, marks the first output of each parent's run of children
+//             children (pass 2's FP32 estimate with an exact recount near target
+//             boundaries), marks the first output of each parent's run of children
 //             in the shared memory of the CTA that owns that output (and the
 //             first output of every further 256-output block the run reaches),
-//             then gathers its own outputs from the parents' CTAs.
+//             then gathers its own outputs from the parents' CTAs. When every tick
+//             resamples, the resampling runs beside the decision (it needs only
+//             whether the tick is degenerate, which warp 1 finds from the same sums).
 // Results equal the three-kernel tick's bit for bit: both particle buffers, the
 // log2-weights and tile exponents are loaded at the start and written back at
 // the end of the launch, with the device state.
