@@ -113,7 +113,9 @@ __device__ __forceinline__ T warp_incl_scan_add(T v, int lane) {
 }
 // Exclusive prefix sum over the NT threads of a CTA; *total gets the sum.
 // sh holds NT/32 + 1 entries. All threads must call it (it has barriers).
-template <int NT, typename T>
+// TRAIL = false leaves out the last barrier: the caller then passes another
+// barrier before sh is written again.
+template <int NT, typename T, bool TRAIL = true>
 __device__ T block_excl_scan_add(T v, T* total, T* sh) {
   constexpr int W = NT / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -130,7 +132,7 @@ __device__ T block_excl_scan_add(T v, T* total, T* sh) {
   nt_sync<NT>();
   const T r = sh[warp] + inc - v;
   *total = sh[W];
-  nt_sync<NT>();
+  if constexpr (TRAIL) nt_sync<NT>();
   return r;
 }
 template <int NT>

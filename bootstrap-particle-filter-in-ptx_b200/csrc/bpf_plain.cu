@@ -788,7 +788,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass2_kernel(Plan p, TickArgs a) 
       }
     }
     unsigned long long tot;
-    const unsigned long long excl = block_excl_scan_add<kThreads>(run, &tot, s_scan);
+    // (no trailing barrier: s_scan is next written by the next item's scan, three barriers on)
+    const unsigned long long excl = block_excl_scan_add<kThreads, unsigned long long, false>(run, &tot, s_scan);
 
     // Element j owns the output slots [q_{j-1}, q_j): the targets t_q below its CDF value
     // C_j = P_k + (A_j >> r) (A_j its tile-local inclusive prefix) and not below the previous
@@ -1072,8 +1073,9 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 //   pass 1    each CTA runs its tile with pass 1's per-particle arithmetic on
 //             twice as many threads and hands the FP32 running sums along in
 //             pass 1's element order, so every tile record is bit for bit pass 1's;
-//             while warp 0 forms the FP64 record, half the CTA scans the tile's
-//             exact fixed-point masses (needed if the tick resamples);
+//             warps 0..3 form the FP64 record (one sum each); the exact fixed-point
+//             masses of the tile's four-slot chunks are scanned only if the tick
+//             resamples, beside the forming of the resampling plan;
 //   plan      warp 0 of every CTA runs the plan over all the tile records (lane k
 //             reads tile k's): the operations of the plan kernel in the same order
 //             (so every CTA takes the same decision and holds the same device state);
@@ -1141,11 +1143,10 @@ __device__ __forceinline__ void cluster_sync_all() {
 // copies, by the first kThreads * SPLIT threads: pass-1 thread v's sixteen particles (four
 // float4 groups r) go to SPLIT threads, 4 / SPLIT consecutive groups each, with the
 // per-particle arithmetic of pass1_tile; the FP32 tile partials are accumulated in pass 1's
-// order by handing the running sums from one of those threads to the next, and warp 0 forms
-// the FP64 tile record in pass 1's order. Within a warp the SPLIT threads of v sit 32 / SPLIT
+// order by handing the running sums from one of those threads to the next, and warps 0..3 form
+// the FP64 tile record in pass 1's order (one sum each). Within a warp the SPLIT threads of v sit 32 / SPLIT
 // lanes apart, so the float4 accesses of a warp cover whole 128-byte rows. Group r of v is the
-// four-slot chunk c = v + 256 r (slots 4c .. 4c + 3); warps 16..31 scan the chunks' exact
-// masses into chunkP while warp 0 forms the record.
+// four-slot chunk c = v + 256 r (slots 4c .. 4c + 3), whose exact mass goes to chunkE.
 // nk_prev: the tile's exponent of the previous tick (the carried weights' frame).
 template <bool TSTATE, bool GAUSS, int SPLIT>
 __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, int tile0, int par, int nk_prev,
@@ -1251,36 +1252,41 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
     if (s == 0) sh.s_E[v] = E;
   }
   __syncthreads();
-  if (warp == 0) {                              // pass 1's FP64 tile combine, same order
-    double tS = 0.0, tQ = 0.0, tH = 0.0;
+  if (warp < 3) {                               // pass 1's FP64 tile sums S, Q, H, one a warp, same order
+    double tw = 0.0;
+    const float* part = sh.s_part[warp];
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) tw += (double)part[lane + 32 * w];
+    tw = warp_sum_d(tw);
+    if (lane == 0) reinterpret_cast<float*>(&sh.rec[par])[warp] = (float)tw;
+  } else if (warp == 3) {                       // and the exact tile mass
     unsigned long long tE = 0ull;
 #pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) {
-      tS += (double)sh.s_part[0][lane + 32 * w];
-      tQ += (double)sh.s_part[1][lane + 32 * w];
-      tH += (double)sh.s_part[2][lane + 32 * w];
-      tE += sh.s_E[lane + 32 * w];
-    }
-    tS = warp_sum_d(tS); tQ = warp_sum_d(tQ); tH = warp_sum_d(tH);
+    for (int w = 0; w < kThreads / 32; ++w) tE += sh.s_E[lane + 32 * w];
     tE = warp_sum_u64(tE);
     if (lane == 0) {
       sh.nexp[par] = nk;
       sh.E[par] = tE;
-      sh.rec[par] = make_float4((float)tS, (float)tQ, (float)tH, __int_as_float(nk));
+      reinterpret_cast<float*>(&sh.rec[par])[3] = __int_as_float(nk);
     }
-  } else if (warp >= 16) {                      // exclusive prefix of the chunk masses, 2 chunks a thread
-    const int t2 = tid - 512;
-    const unsigned long long e0 = sh.chunkE[2 * t2], e1 = sh.chunkE[2 * t2 + 1];
-    const unsigned long long s2 = e0 + e1;
-    const unsigned long long inc = warp_incl_scan_add(s2, lane);
-    if (lane == 31) sh.scan2[warp - 16] = inc;
-    asm volatile("bar.sync 2, 512;" ::: "memory");
-    unsigned long long off = 0ull;
-    for (int w = 16; w < warp; ++w) off += sh.scan2[w - 16];
-    const unsigned long long ex = off + inc - s2;
-    sh.chunkP[2 * t2] = ex;
-    sh.chunkP[2 * t2 + 1] = ex + e0;
   }
+}
+
+// Exclusive prefix of the tile's four-slot chunk masses within the tile (chunkP), by warps
+// 16..31, two chunks a thread; it is needed only when the tick resamples, and runs beside the
+// forming of the resampling plan.
+__device__ __forceinline__ void chunk_scan(FusedShared& sh) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t2 = tid - kSmallThreads / 2;
+  const unsigned long long e0 = sh.chunkE[2 * t2], e1 = sh.chunkE[2 * t2 + 1];
+  const unsigned long long s2 = e0 + e1;
+  const unsigned long long inc = warp_incl_scan_add(s2, lane);
+  if (lane == 31) sh.scan2[warp - 16] = inc;
+  asm volatile("bar.sync 2, %0;" ::"n"(kSmallThreads / 2) : "memory");
+  const unsigned long long off = warp_sum_u64((lane < warp - 16) ? sh.scan2[lane] : 0ull);
+  const unsigned long long ex = off + inc - s2;
+  sh.chunkP[2 * t2] = ex;
+  sh.chunkP[2 * t2 + 1] = ex + e0;
 }
 
 // The FP64 sums of a fused tick over all tiles' records, for NCTA <= kSmallTiles tiles, by one
@@ -1706,6 +1712,7 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
         marks_barrier_wait<NCTA>();
       } else {
         if (warp == 1) plan_fused_targets<NCTA>(N, rcpN, sh, par, u_state, true);
+        else if (warp >= 16) chunk_scan(sh);
         asm volatile("bar.sync 3, %0;" ::"n"(kSmallThreads - 32) : "memory");   // warps 1..31
         const bool live = sh.pl.live != 0;
         if (live && tid >= kSmallThreads / 2) {
@@ -1720,6 +1727,7 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
       __syncthreads();
       if (sh.st.do_resample) {
         if (warp == 1) plan_fused_targets<NCTA>(N, rcpN, sh, par, u_state, false);
+        else if (warp >= 16) chunk_scan(sh);
         __syncthreads();
         const ChunkTargets<4> ct = chunk_targets<NCTA, 4>(N, k, par, tid, sh);
         count_marks<NCTA, 4>(N, k, ct, sh);
