@@ -85,6 +85,9 @@ def parse_args():
                     help="ticks of the headline run followed by the FP64 oracle in lock step (0 = off)")
     ap.add_argument("--plumbing-check", action="store_true",
                     help="CPU-only check of the multi-rank path (gloo): rank launch, shard, gather, max-reduce")
+    ap.add_argument("--smc2-only", type=int, default=0, metavar="UPDATES",
+                    help="run only the SMC^2 workload of the extensions (50 warm-up updates, then UPDATES timed "
+                         "ones; for a kernel launch list of one update) and print its line")
     return ap.parse_args()
 
 
@@ -511,6 +514,31 @@ def bench_extensions(dev, args, lib, rank):
                     "theta_sd": [float(v) for v in sd], "stats": st,
                     "acceptance": st["accepted"] / max(1, st["proposed"])}
     return out
+
+
+def smc2_only(args):
+    """The extensions' SMC^2 workload alone (256 theta x 512 particles, one PMMH move per outer
+    resample, fresh inner filters): 50 warm-up updates, then args.smc2_only timed ones (wall clock
+    around synchronised calls, as in the extensions)."""
+    import torch
+    import gpubpf
+    from gpubpf import dgp
+    torch.cuda.set_device(0)
+    n = args.smc2_only
+    _, y2 = dgp.matched_series(50 + n, RHO, SIG, MU, 11)
+    s2 = gpubpf.Smc2(256, 512, 50 + n, seed=5)
+    s2.set_moves(1, 0.5, 1.0)
+    for v in y2[:50]:
+        s2.update(float(v))
+    t0 = time.perf_counter()
+    for v in y2[50:]:
+        s2.update(float(v))
+    ms = (time.perf_counter() - t0) * 1e3
+    st = s2.stats()
+    s2.close()
+    print(json.dumps({"workload": "SMC^2, 256 theta x 512 particles, one PMMH move per outer resample",
+                      "updates": n, "us_per_update": ms / n * 1e3, "stats": st}))
+    return 0
 
 
 COND_WORKLOAD = ("the reference's conditional-resampling workload (tests/test_cond_resample.cu): N = 300000, "
@@ -968,6 +996,8 @@ def main():
         return plumbing_check(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.smc2_only:
+        return smc2_only(args)
 
     import numpy as np
     import torch
