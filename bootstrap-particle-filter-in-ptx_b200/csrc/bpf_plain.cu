@@ -1111,6 +1111,7 @@ struct FusedPlan {
 struct FusedShared {
   float h[2][kTile];                          // particle buffers (DevState::cur / src), this CTA's tile
   float w[kTile];                             // log2-weights of the tile
+  __align__(16) float z[kTile];               // state noise of the tick's propagation, slot by slot
   // start marks of this CTA's outputs, parent + 1 (0 = none): 16-bit for clusters of up to 8
   // CTAs (parent + 1 <= 32768), 32-bit for 16 (see MarkOf)
   __align__(16) unsigned marks_raw[kTile + kGatherStep];
@@ -1128,6 +1129,7 @@ struct FusedShared {
   float s_part[3][kThreads];
   unsigned long long s_E[kThreads];
   unsigned long long scan2[16];
+  unsigned long long knext[2];                // the next tick's PCG32 stream constants k1, k2
 };
 
 template <int NCTA>
@@ -1142,7 +1144,8 @@ __device__ __forceinline__ void cluster_sync_all() {
 // Pass 1 of this CTA's tile (global slots tile0 .. tile0 + kTile - 1) on the shared-memory
 // copies, by the first kThreads * SPLIT threads: pass-1 thread v's sixteen particles (four
 // float4 groups r) go to SPLIT threads, 4 / SPLIT consecutive groups each, with the
-// per-particle arithmetic of pass1_tile; the FP32 tile partials are accumulated in pass 1's
+// per-particle arithmetic of pass1_tile (the state noise read from sh.z, formed beforehand by
+// fused_noise with the same draws); the FP32 tile partials are accumulated in pass 1's
 // order by handing the running sums from one of those threads to the next, and warps 0..3 form
 // the FP64 tile record in pass 1's order (one sum each). Within a warp the SPLIT threads of v sit 32 / SPLIT
 // lanes apart, so the float4 accesses of a warp cover whole 128-byte rows. Group r of v is the
@@ -1164,7 +1167,6 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
     const DevState& st = sh.st;
     const int tick = st.tick;
     const bool carry = st.resampled_prev == 0;
-    const uint64_t k1 = st.k1, k2 = st.k2;
     float* hb = sh.h[st.cur];
     ObsModel obs = a.obs;
     obs.y = y;
@@ -1174,7 +1176,6 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
     const float gauss_c = kGaussLog2C + carry_off;
     const float t_c = __fmul_rn(obs.c_obs, kLog2e) + carry_off;
     const float y2nu = __fmul_rn(y2, obs.inv_nu);
-    const unsigned long long k33 = k2 << 33;
     float x[4 * R];
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
@@ -1187,12 +1188,7 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
       for (int e = 0; e < 4; ++e) {
         const int i = tile0 + l0 + e;
         float h = hh[e];
-        if (tick > 0) {
-          const uint64_t st64 = k1 + k2 * pcg_inc((uint32_t)i);
-          float z = icdf_normal_warp(pcg_uniform(pcg_output(st64)));
-          if (TSTATE) z *= tstate_scale_warp(st64, k33, a.nu_int, a.nu_state);
-          h = propagate(h, a.mu, a.rho, a.sigma, z);
-        }
+        if (tick > 0) h = propagate(h, a.mu, a.rho, a.sigma, sh.z[l0 + e]);
         float xx = GAUSS ? obs_log2pdf_gauss_plus(y2, h, gauss_c) : obs_log2pdf_t_plus(obs, y2nu, h, t_c);
         if (carry) xx += wp[e];
         if (i >= N) xx = -INFINITY;               // padding slots carry no weight
@@ -1269,6 +1265,28 @@ __device__ __forceinline__ void pass1_fused(const TickArgs& a, float y, int N, i
       sh.E[par] = tE;
       reinterpret_cast<float*>(&sh.rec[par])[3] = __int_as_float(nk);
     }
+  }
+}
+
+// The state noise of a tick for this CTA's tile into sh.z, by the threads from thread `first` on,
+// in steps of `stride` four-slot groups (both multiples of 32, so every warp runs whole groups and the
+// normal's warp vote sees all its lanes): slot i's draw of the tick with stream constants (k1, k2),
+// pass 1's arithmetic (the draws are counter-based, so they are formed before the tick's particles
+// are known, by warps that would otherwise wait).
+template <bool TSTATE>
+__device__ __forceinline__ void fused_noise(const TickArgs& a, int tile0, uint64_t k1, uint64_t k2, int first,
+                                            int stride, FusedShared& sh) {
+  const uint64_t k33 = k2 << 33;
+  for (int g = (int)threadIdx.x - first; g < kTile / 4; g += stride) {
+    float zz[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint64_t st64 = k1 + k2 * pcg_inc((uint32_t)(tile0 + 4 * g + e));
+      float z = icdf_normal_warp(pcg_uniform(pcg_output(st64)));
+      if (TSTATE) z *= tstate_scale_warp(st64, k33, a.nu_int, a.nu_state);
+      zz[e] = z;
+    }
+    *reinterpret_cast<float4*>(sh.z + 4 * g) = make_float4(zz[0], zz[1], zz[2], zz[3]);
   }
 }
 
@@ -1688,6 +1706,8 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
   const double rcpN = 1.0 / (double)N;           // exact division by N: the quotient is corrected
   const bool ahead = a.ess_threshold <= 0.0f;     // every tick that can resample does
   const int warp = tid >> 5;
+  __syncthreads();                                // the device state is in shared memory
+  if (sh.st.tick > 0) fused_noise<TSTATE>(a, tile0, sh.st.k1, sh.st.k2, 0, kSmallThreads, sh);   // the first tick's
   for (int t = 0; t < n_ticks; ++t) {
     const int par = t & 1;
     if (a.y_ptr && (t & (kYStage - 1)) == 0) {       // the next kYStage observations
@@ -1698,6 +1718,8 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
     const float y = a.y_ptr ? sh.ys[t & (kYStage - 1)] : a.obs.y;
     const unsigned long long u_state = sh.st.u_state;
     const int cur0 = sh.st.cur;                    // a resampling reads buffer cur0, writes cur0 ^ 1
+    const bool more = t + 1 < n_ticks;             // the launch runs another tick: form its noise
+    if (tid == 0) { sh.knext[0] = sh.st.k1 * kPcgMult; sh.knext[1] = sh.st.k2 * kPcgMult + 1ull; }
     pass1_fused<TSTATE, GAUSS, kSmallSplit>(a, y, N, tile0, par, sh.nexp[par ^ 1], sh);
     cluster_sync_all<NCTA>();                   // every tile record of the tick is in place
     if (ahead) {
@@ -1713,6 +1735,7 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
       } else {
         if (warp == 1) plan_fused_targets<NCTA>(N, rcpN, sh, par, u_state, true);
         else if (warp >= 16) chunk_scan(sh);
+        else if (more) fused_noise<TSTATE>(a, tile0, sh.knext[0], sh.knext[1], 64, 14 * 32, sh);   // warps 2..15
         asm volatile("bar.sync 3, %0;" ::"n"(kSmallThreads - 32) : "memory");   // warps 1..31
         const bool live = sh.pl.live != 0;
         if (live && tid >= kSmallThreads / 2) {
@@ -1724,6 +1747,7 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
       }
     } else {
       if (warp == 0) plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
+      else if (more) fused_noise<TSTATE>(a, tile0, sh.knext[0], sh.knext[1], 32, kSmallThreads - 32, sh);
       __syncthreads();
       if (sh.st.do_resample) {
         if (warp == 1) plan_fused_targets<NCTA>(N, rcpN, sh, par, u_state, false);
