@@ -1067,9 +1067,9 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 // Fused tick for small filters (N <= kSmallMaxN, at most kSmallTiles tiles): a
 // thread-block cluster of one CTA per tile runs n consecutive ticks in one
 // launch. The particles, log2-weights and tile records stay in shared memory
-// from the first tick to the last; the CTAs read each other's records, start
-// marks and particles through distributed shared memory and meet at one
-// cluster barrier per tick (two on resampling ticks).
+// from the first tick to the last; the CTAs read each other's records and write
+// each other's resampled particles through distributed shared memory and meet at
+// one cluster barrier per tick (two on resampling ticks).
 //   pass 1    each CTA runs its tile with pass 1's per-particle arithmetic on
 //             twice as many threads and hands the FP32 running sums along in
 //             pass 1's element order, so every tile record is bit for bit pass 1's;
@@ -1083,10 +1083,9 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 //   resample  the same fixed-point rule (integer exact, so the ancestors do not
 //             depend on how the work is split): each CTA counts its tile's
 //             children (pass 2's FP32 estimate with an exact recount near target
-//             boundaries), marks the first output of each parent's run of children
-//             in the shared memory of the CTA that owns that output (and the
-//             first output of every further 256-output block the run reaches),
-//             then gathers its own outputs from the parents' CTAs. When every tick
+//             boundaries) and each parent writes its particle into its children's
+//             output slots, in the shared memory of the CTA that owns each slot;
+//             a barrier over the cluster ends the resampling. When every tick
 //             resamples, the resampling runs beside the decision (it needs only
 //             whether the tick is degenerate, which warp 1 finds from the same sums).
 // Results equal the three-kernel tick's bit for bit: both particle buffers, the
@@ -1096,11 +1095,8 @@ __global__ void __launch_bounds__(kThreads) jitter_apply_kernel(Plan p, float mu
 constexpr int kSmallThreads = 4 * kThreads;             // 1024 threads per CTA (one tile)
 constexpr int kSmallSplit = 2;                          // threads per pass-1 thread in the fused pass 1
 constexpr int kChunks = kTile / 4;                      // four-slot chunks of a tile (one per thread)
-constexpr int kMarkWarps = kTile / kGatherStep;         // warps of the gather (256 outputs each)
 constexpr int kYStage = kSmallThreads;                  // observations staged per refill
 static_assert(kChunks == kSmallThreads, "one four-slot chunk per thread");
-static_assert(kTile % kGatherStep == 0, "the gather reads marks in 256-slot steps");
-static_assert(kSmallMaxN < (1 << 30), "start marks hold parent + 1");
 
 struct FusedPlan {
   unsigned long long base, delta, magic, total;
@@ -1112,9 +1108,6 @@ struct FusedShared {
   float h[2][kTile];                          // particle buffers (DevState::cur / src), this CTA's tile
   float w[kTile];                             // log2-weights of the tile
   __align__(16) float z[kTile];               // state noise of the tick's propagation, slot by slot
-  // start marks of this CTA's outputs, parent + 1 (0 = none): 16-bit for clusters of up to 8
-  // CTAs (parent + 1 <= 32768), 32-bit for 16 (see MarkOf)
-  __align__(16) unsigned marks_raw[kTile + kGatherStep];
   unsigned long long chunkE[kChunks];         // exact fixed-point mass of each four-slot chunk
   unsigned long long chunkP[kChunks];         // its exclusive prefix within the tile
   float ys[kYStage];                          // observations of the next ticks
@@ -1512,35 +1505,22 @@ __device__ __forceinline__ ChunkTargets<CH> chunk_targets(int N, int k, int par,
   return ct;
 }
 
-// The start-mark element of a cluster of NCTA CTAs.
-template <int NCTA>
-using MarkOf = std::conditional_t<(NCTA > 8), unsigned, unsigned short>;
-template <int NCTA>
-__device__ __forceinline__ MarkOf<NCTA>* marks_of(FusedShared& sh) {
-  return reinterpret_cast<MarkOf<NCTA>*>(sh.marks_raw);
-}
-
-// Start mark of output o (parent + 1) in the shared memory of the CTA that owns o.
-template <int NCTA>
-__device__ __forceinline__ void put_mark(FusedShared& sh, int o, int val) {
-  if constexpr (NCTA == 1) marks_of<NCTA>(sh)[o] = (MarkOf<NCTA>)val;
-  else marks_of<NCTA>(*sh.peer[o >> 12])[o & (kTile - 1)] = (MarkOf<NCTA>)val;
-}
-
-// Resampling of a fused tick, this CTA's part: the children of its tile's particles (start marks
-// into the owners' shared memory, count_marks), a barrier over the cluster, then the gather of its
-// own outputs (gather_fused).
+// Resampling of a fused tick, this CTA's part: every parent of its tile writes its particle into
+// the output slots of its children, in the particle buffer of the CTA that owns each slot
+// (distributed shared memory), then one barrier over the cluster ends the tick's resampling.
+// The children of the chunk's elements as in pass 2: the running count c_j = #{m >= 0 :
+// th + m D <= l_j} (l_j the exact fixed-point sum of the chunk's weights up to j) estimated in
+// FP32 from the running sum of the weights, with pass 2's bound on the estimate's error taken at
+// the chunk's largest sum; near a target boundary (one vote per four elements) the element
+// recounts in exact 64-bit integers. The output slots of element j are [q_{j-1}, q_j),
+// q_j = min(q + c_j, N). A chunk from which no target is reachable (th = kThCap) has no children.
+// src / dst: the particle buffers the resampling reads and writes.
 template <int NCTA, int CH>
-__device__ __forceinline__ void count_marks(int N, int k, const ChunkTargets<CH>& ct, FusedShared& sh) {
-  // The children of the chunk's elements as in pass 2: the running count c_j = #{m >= 0 :
-  // th + m D <= l_j} (l_j the exact fixed-point sum of the chunk's weights up to j) estimated in
-  // FP32 from the running sum of the weights, with pass 2's bound on the estimate's error taken at
-  // the chunk's largest sum; near a target boundary (one vote per four elements) the element
-  // recounts in exact 64-bit integers. The output slots of element j are [q_{j-1}, q_j),
-  // q_j = min(q + c_j, N); element j marks the first one and the first of every further 256-output
-  // block. A chunk from which no target is reachable (th = kThCap) has no children.
+__device__ __forceinline__ void count_write(const TickArgs& a, int N, int k, const ChunkTargets<CH>& ct, int src,
+                                            int dst, FusedShared& sh) {
   const int j0 = k * kTile + CH * ct.c;
   const float* d = sh.w + CH * ct.c;               // its log2-weights, for the exact recount
+  const float* hs = sh.h[src] + CH * ct.c;         // its particles
   const unsigned long long R0 = ct.th, D = ct.D;
   const bool none = R0 >= kThCap;
   const float R0w = (float)R0 * 0x1p-50f;
@@ -1577,84 +1557,22 @@ __device__ __forceinline__ void count_marks(int N, int k, const ChunkTargets<CH>
     for (int e = 0; e < 4; ++e) {
       const int q1 = qq[e];
       if (q1 > qp) {
-        const int val = j0 + 4 * g + e + 1;
-        put_mark<NCTA>(sh, qp, val);
-        for (int b = (qp | (kGatherStep - 1)) + 1; b < q1; b += kGatherStep) put_mark<NCTA>(sh, b, val);
+        const float hv = hs[4 * g + e];
+        const int parent = j0 + 4 * g + e;
+        for (int o = qp; o < q1; ++o) {
+          if constexpr (NCTA == 1) sh.h[dst][o] = hv;
+          else sh.peer[o >> 12]->h[dst][o & (kTile - 1)] = hv;
+          if (a.anc) a.anc[o] = parent;
+        }
       }
       qp = q1;
     }
   }
 }
 
-// The gather, by warps 1..kMarkWarps (warp 0 may still be taking the tick's decision): the
-// ancestor of output o is the last start mark at or before o; the first output of every 256-output
-// block has one, so each warp's block stands alone. Each lane resolves eight consecutive outputs (a
-// running max and a warp max-scan) and writes parent + 1 back over the marks; the warp then reads
-// them lane-interleaved, so the particle reads and writes and the ancestor stores of a warp touch
-// consecutive slots. src / dst: the particle buffers the resampling reads and writes.
-template <int NCTA>
-__device__ __forceinline__ void gather_fused(const TickArgs& a, int N, int k, int src, int dst, FusedShared& sh) {
-  static_assert(kTile == 1 << 12, "output owner = o >> 12");
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tile0 = k * kTile;
-  const int n_out = min(N - tile0, kTile);
-  const int o0 = (warp - 1) * kGatherStep;
-  if (warp >= 1 && warp <= kMarkWarps && o0 < n_out) {
-    using M = MarkOf<NCTA>;
-    M* marks = marks_of<NCTA>(sh);
-    constexpr int VPL = (int)(8 * sizeof(M)) / 16;   // uint4 per lane: eight marks
-    uint4* mrow = reinterpret_cast<uint4*>(marks + o0);
-    unsigned mv[8];
-    if constexpr (VPL == 1) {
-      const uint4 m0 = mrow[lane];
-      mv[0] = m0.x & 0xffffu; mv[1] = m0.x >> 16; mv[2] = m0.y & 0xffffu; mv[3] = m0.y >> 16;
-      mv[4] = m0.z & 0xffffu; mv[5] = m0.z >> 16; mv[6] = m0.w & 0xffffu; mv[7] = m0.w >> 16;
-    } else {
-      const uint4 m0 = mrow[2 * lane], m1 = mrow[2 * lane + 1];
-      mv[0] = m0.x; mv[1] = m0.y; mv[2] = m0.z; mv[3] = m0.w;
-      mv[4] = m1.x; mv[5] = m1.y; mv[6] = m1.z; mv[7] = m1.w;
-    }
-    unsigned am[8];
-    am[0] = mv[0];
-#pragma unroll
-    for (int u = 1; u < 8; ++u) am[u] = max(am[u - 1], mv[u]);
-    unsigned xm = am[7];
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const unsigned t = __shfl_up_sync(0xffffffffu, xm, off);
-      if (lane >= off) xm = max(xm, t);
-    }
-    unsigned pre = __shfl_up_sync(0xffffffffu, xm, 1);
-    if (lane == 0) pre = 0u;
-    unsigned jj[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) jj[u] = max(max(pre, am[u]), 1u);   // parent + 1
-    if constexpr (VPL == 1) {
-      mrow[lane] = make_uint4(jj[0] | (jj[1] << 16), jj[2] | (jj[3] << 16), jj[4] | (jj[5] << 16), jj[6] | (jj[7] << 16));
-    } else {
-      mrow[2 * lane] = make_uint4(jj[0], jj[1], jj[2], jj[3]);
-      mrow[2 * lane + 1] = make_uint4(jj[4], jj[5], jj[6], jj[7]);
-    }
-    __syncwarp();
-    float* hd = sh.h[dst];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int o = o0 + 32 * u + lane;
-      if (o < n_out) {
-        const int parent = (int)marks[o] - 1;
-        hd[o] = (NCTA == 1) ? sh.h[src][parent] : sh.peer[parent >> 12]->h[src][parent & (kTile - 1)];
-        if (a.anc) a.anc[tile0 + o] = parent;
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int x = 0; x < VPL; ++x) mrow[VPL * lane + x] = make_uint4(0u, 0u, 0u, 0u);   // clear for the next resampling
-  }
-}
-
-// The barrier between the start marks and the gather when warp 0 is taking the tick's decision
-// meanwhile: warp 0 arrives before it starts (it places no marks and gathers nothing) and waits
-// after it, the other warps arrive and wait together. Barrier 4 for one CTA, the cluster's otherwise.
+// The barrier that ends a resampling (every child written) when warp 0 is taking the tick's
+// decision meanwhile: warp 0 arrives before it starts (it writes no children) and waits after
+// it, the other warps arrive and wait together. Barrier 4 for one CTA, the cluster's otherwise.
 template <int NCTA>
 __device__ __forceinline__ void marks_barrier_arrive() {
   if constexpr (NCTA == 1) asm volatile("bar.arrive 4, %0;" ::"n"(kSmallThreads) : "memory");
@@ -1700,8 +1618,6 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
     reinterpret_cast<float4*>(sh.h[1])[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
     reinterpret_cast<float4*>(sh.w)[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  constexpr int kMarkVecs = (int)(sizeof(MarkOf<NCTA>) * (kTile + kGatherStep) / 16);
-  for (int x = tid; x < kMarkVecs; x += kSmallThreads) reinterpret_cast<uint4*>(sh.marks_raw)[x] = make_uint4(0u, 0u, 0u, 0u);
 
   const double rcpN = 1.0 / (double)N;           // exact division by N: the quotient is corrected
   const bool ahead = a.ess_threshold <= 0.0f;     // every tick that can resample does
@@ -1726,7 +1642,7 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
       // The resampling needs nothing from the decision but whether the tick is degenerate, so
       // warp 0 takes the decision and writes the record beside it: warp 1 forms the plan (and
       // the plan's fields of the device state, which the decision does not touch), warps 16..31
-      // count the children of eight-slot chunks, warps 1..16 gather.
+      // count the children of eight-slot chunks and write them.
       if (warp == 0) {
         marks_barrier_arrive<NCTA>();
         plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
@@ -1736,14 +1652,14 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
         if (warp == 1) plan_fused_targets<NCTA>(N, rcpN, sh, par, u_state, true);
         else if (warp >= 16) chunk_scan(sh);
         else if (more) fused_noise<TSTATE>(a, tile0, sh.knext[0], sh.knext[1], 64, 14 * 32, sh);   // warps 2..15
-        asm volatile("bar.sync 3, %0;" ::"n"(kSmallThreads - 32) : "memory");   // warps 1..31
-        const bool live = sh.pl.live != 0;
-        if (live && tid >= kSmallThreads / 2) {
-          const ChunkTargets<8> ct = chunk_targets<NCTA, 8>(N, k, par, tid - kSmallThreads / 2, sh);
-          count_marks<NCTA, 8>(N, k, ct, sh);
+        if (warp == 1 || warp >= 16) {             // the plan's producer and its users meet; warps 2..15 do not wait
+          asm volatile("bar.sync 3, %0;" ::"n"(32 + kSmallThreads / 2) : "memory");
+          if (sh.pl.live && warp >= 16) {
+            const ChunkTargets<8> ct = chunk_targets<NCTA, 8>(N, k, par, tid - kSmallThreads / 2, sh);
+            count_write<NCTA, 8>(a, N, k, ct, cur0, cur0 ^ 1, sh);
+          }
         }
-        marks_barrier_sync<NCTA>();               // every start mark is in place
-        if (live) gather_fused<NCTA>(a, N, k, cur0, cur0 ^ 1, sh);
+        marks_barrier_sync<NCTA>();               // every child is written
       }
     } else {
       if (warp == 0) plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
@@ -1754,9 +1670,8 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
         else if (warp >= 16) chunk_scan(sh);
         __syncthreads();
         const ChunkTargets<4> ct = chunk_targets<NCTA, 4>(N, k, par, tid, sh);
-        count_marks<NCTA, 4>(N, k, ct, sh);
-        cluster_sync_all<NCTA>();                 // every start mark is in place
-        gather_fused<NCTA>(a, N, k, cur0, cur0 ^ 1, sh);
+        count_write<NCTA, 4>(a, N, k, ct, cur0, cur0 ^ 1, sh);
+        cluster_sync_all<NCTA>();                 // every child is written
       }
     }
   }
