@@ -1047,3 +1047,123 @@ int orc_num_threads(void) {
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------------------------
+ * Host restatement of the FP32 child-count estimate of the resampling kernels (pass 2 and the
+ * fused small-filter tick in bootstrap-particle-filter-in-ptx_b200/csrc/bpf_plain.cu), used to
+ * check the error bound that decides when the estimate may be used instead of the exact count.
+ *
+ * For a run of n <= 16 weights w_j in [0, 1] (FP32, tile frame), a relative threshold R0 and a
+ * spacing D (u64 fixed point, 2^-50 units), the exact running count is
+ *   c_j = #{m >= 0 : R0 + m D <= l_j},  l_j = sum_{i <= j} floor(w_i 2^50),
+ * and the kernels estimate it as floor(x) + 1 (0 for x < 0) with x = fmaf(lf_j, 1/Dw, -R0/Dw) from
+ * the FP32 running sum lf_j, trusting the estimate only when x is farther than the run's bound from
+ * an integer. The operations below are the kernels' own, in their order (this file is compiled
+ * without floating-point contraction). bound_scale multiplies the bound: 1 is the kernels' bound;
+ * a smaller value plants a mistake that the check must find.
+ * Returns the number of elements declared safe whose estimate differs from the exact count;
+ * *n_safe and *n_recount count the two kinds of elements.
+ * ------------------------------------------------------------------------------------------ */
+long long orc_count_estimate_run(const float* w, int n, uint64_t R0, uint64_t D, float bound_scale,
+                                 long long* n_safe, long long* n_recount) {
+    long long bad = 0;
+    float lfT = 0.0f;
+    for (int j = 0; j < n; ++j) lfT += w[j];
+    const float R0w = (float)R0 * 0x1p-50f;
+    const float invDw = 1.0f / ((float)D * 0x1p-50f);
+    const float R0x = R0w * invDw;
+    const float eL = 0x1p-18f * invDw, e0 = fmaf(R0w, eL, 0x1p-44f * invDw);
+    const float xT = fmaf(lfT, invDw, -R0x);
+    float err = fmaf(lfT, eL, fmaf(fmaxf(fabsf(xT), R0x), 0x1p-21f, e0));
+    err *= bound_scale;
+    if (!(xT < 0x1p22f)) err = 1.0f;
+    const float err_hi = 1.0f - err;
+    float lf = 0.0f;
+    uint64_t l = 0;
+    for (int j = 0; j < n; ++j) {
+        lf += w[j];
+        l += (uint64_t)(w[j] * 0x1p50f);
+        const float x = fmaf(lf, invDw, -R0x);
+        const float fl = floorf(x);
+        const float fr = x - fl;
+        const int safe = (fr > err && fr < err_hi);
+        const float v = fl + 0x1p23f;
+        int32_t bits;
+        memcpy(&bits, &v, sizeof bits);
+        int c_est = bits - 0x4AFFFFFF;
+        if (c_est < 0) c_est = 0;
+        const uint64_t c = (l < R0) ? 0u : (l - R0) / D + 1u;
+        if (safe) {
+            ++*n_safe;
+            if ((uint64_t)c_est != c) ++bad;
+        } else {
+            ++*n_recount;
+        }
+    }
+    return bad;
+}
+
+static uint64_t orc_splitmix(uint64_t* s) {
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* n_runs random runs of n weights each (mode 0: weights spread over [0, 1] with tiny values,
+ * zeros and exact ones mixed in, thresholds and spacings over many magnitudes; mode 1: the
+ * thresholds placed on target boundaries: the m-th target sits exactly on, or one unit either side of, an element's
+ * running sum). out3 = {violations, safe elements, recounted elements}. */
+void orc_count_estimate_fuzz(uint64_t seed, long long n_runs, int n, int mode, float bound_scale, long long* out3) {
+    uint64_t s = seed;
+    long long bad = 0, n_safe = 0, n_rec = 0;
+    float w[16];
+    if (n < 1) n = 1;
+    if (n > 16) n = 16;
+    for (long long r = 0; r < n_runs; ++r) {
+        /* weights */
+        const int kind = (mode == 2) ? 0 : (int)(orc_splitmix(&s) % 5);
+        for (int j = 0; j < n; ++j) {
+            const uint64_t u = orc_splitmix(&s);
+            float v;
+            switch (kind) {
+                case 0: v = (float)((u >> 40) * 0x1p-24); break;                               /* uniform */
+                case 1: v = ldexpf((float)((u >> 41) | 1u) * 0x1p-23f, -(int)((u >> 8) % 60)); break;   /* 2^-60 .. 1 */
+                case 2: v = (u & 1) ? 1.0f : 0.0f; break;                                        /* ones and zeros */
+                case 3: v = ldexpf(1.0f, -(int)((u >> 8) % 52)); break;                          /* powers of two */
+                default: v = 1.0f - (float)((u >> 45) * 0x1p-19); break;                          /* near one */
+            }
+            if (v > 1.0f) v = 1.0f;
+            if (v < 0x1p-126f) v = 0.0f;                                                        /* flushed */
+            w[j] = v;
+        }
+        uint64_t l[16], acc = 0;
+        for (int j = 0; j < n; ++j) { acc += (uint64_t)(w[j] * 0x1p50f); l[j] = acc; }
+        /* spacing: 1 .. 2^55, log-uniform; mode 2: about one target per weight (the mean weight
+           times 2^50, within a factor of two either way), as in a filter's resampling */
+        const int dexp = (int)(orc_splitmix(&s) % 56);
+        uint64_t D = (orc_splitmix(&s) >> (64 - dexp - 1)) | (1ull << dexp);
+        if (mode == 2) {
+            const double mean = (double)acc / n;
+            D = (uint64_t)(mean * (0.5 + 1.5 * (double)(orc_splitmix(&s) >> 11) * 0x1p-53));
+        }
+        if (D == 0) D = 1;
+        if (D > (1ull << 55)) D = 1ull << 55;
+        uint64_t R0;
+        if (mode == 0 || mode == 2) {
+            R0 = 1 + orc_splitmix(&s) % (D > (1ull << 54) ? D : 2 * D);                         /* 1 .. 2D */
+            if (mode == 0 && (orc_splitmix(&s) & 31) == 0) R0 = 1ull << 55;                     /* no target */
+        } else {
+            /* a boundary: R0 + m D = l_j + delta for a random element j, m and delta in {-1, 0, 1} */
+            const int j = (int)(orc_splitmix(&s) % n);
+            const uint64_t lj = l[j];
+            const uint64_t m = lj ? (lj - 1) / D : 0;                                              /* lj - m D in [1, D] */
+            const int delta = (int)(orc_splitmix(&s) % 3) - 1;
+            int64_t r0 = (int64_t)(lj - m * D) + delta;
+            if (r0 < 1) r0 = 1;
+            R0 = (uint64_t)r0;
+        }
+        bad += orc_count_estimate_run(w, n, R0, D, bound_scale, &n_safe, &n_rec);
+    }
+    out3[0] = bad; out3[1] = n_safe; out3[2] = n_rec;
+}

@@ -95,6 +95,10 @@ def lib(native: bool = False) -> C.CDLL:
     L.orc_ref_resample.restype = C.c_int
     L.orc_ref_resample.argtypes = [C.c_int, C.c_void_p, f32, C.c_void_p]
     L.orc_num_threads.restype = C.c_int; L.orc_num_threads.argtypes = []
+    L.orc_count_estimate_run.restype = C.c_longlong
+    L.orc_count_estimate_run.argtypes = [P(f32), C.c_int, u64, u64, f32, P(C.c_longlong), P(C.c_longlong)]
+    L.orc_count_estimate_fuzz.restype = None
+    L.orc_count_estimate_fuzz.argtypes = [u64, C.c_longlong, C.c_int, C.c_int, f32, P(C.c_longlong)]
     L.orc_tstate_scale.restype = f64
     L.orc_tstate_scale.argtypes = [C.c_int, u32, C.c_int, C.c_int, f64]
     L.orc_grad_f64.restype = C.c_int
@@ -229,6 +233,26 @@ def apf_f64(n_particles, rho, sigma_z, mu, y, seed=42, nu_obs=0.0, nu_state=0.0,
     if rc != 0:
         raise RuntimeError(f"orc_apf_f64 failed ({rc})")
     return out
+
+
+def count_estimate_fuzz(seed: int, n_runs: int, n: int, mode: int, bound_scale: float = 1.0) -> dict:
+    """Host check of the resampling kernels' FP32 child-count estimate (orc_count_estimate_fuzz):
+    n_runs random runs of n weights; mode 0 spread weights and spacings, 1 thresholds on target
+    boundaries, 2 a filter's typical case. Returns the estimates declared safe that differ from
+    the exact count ('violations'), and the safe and recounted element counts."""
+    out = (C.c_longlong * 3)()
+    lib().orc_count_estimate_fuzz(seed, n_runs, n, mode, bound_scale, out)
+    return {"violations": out[0], "safe": out[1], "recount": out[2]}
+
+
+def count_estimate_run(w, R0: int, D: int, bound_scale: float = 1.0) -> dict:
+    """One run of weights w (FP32, in [0, 1], at most 16) against relative threshold R0 and spacing D."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    assert 1 <= w.size <= 16
+    ns, nr = C.c_longlong(0), C.c_longlong(0)
+    bad = lib().orc_count_estimate_run(w.ctypes.data_as(C.POINTER(C.c_float)), int(w.size), int(R0), int(D),
+                                       bound_scale, C.byref(ns), C.byref(nr))
+    return {"violations": bad, "safe": ns.value, "recount": nr.value}
 
 
 def resample_fixed(w, tile_exp, u23):
