@@ -1533,7 +1533,7 @@ __device__ __forceinline__ void count_write(const TickArgs& a, int N, int k, con
   const float err_hi = 1.0f - err;
   const int q0 = ct.q, Kq = 0x4AFFFFFF - q0;
   float lf = 0.0f;
-  int qp = q0;
+  int qe[CH];                                      // q_j: the end of element j's children
 #pragma unroll
   for (int g = 0; g < CH / 4; ++g) {
     int qq[4];
@@ -1554,18 +1554,26 @@ __device__ __forceinline__ void count_write(const TickArgs& a, int N, int k, con
         if (rc[e]) qq[e] = min(q0 + exact_count(d, 4 * g + e, R0, D, N), N);
     }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int q1 = qq[e];
-      if (q1 > qp) {
-        const float hv = hs[4 * g + e];
-        const int parent = j0 + 4 * g + e;
-        for (int o = qp; o < q1; ++o) {
-          if constexpr (NCTA == 1) sh.h[dst][o] = hv;
-          else sh.peer[o >> 12]->h[dst][o & (kTile - 1)] = hv;
-          if (a.anc) a.anc[o] = parent;
-        }
-      }
-      qp = q1;
+    for (int e = 0; e < 4; ++e) qe[4 * g + e] = qq[e];
+  }
+  // The chunk's children fill the slots [q0, q_last): slot o belongs to element #{j : q_j <= o}.
+  // Each lane writes its run in one loop, starting at an offset rotated by lane / 4: the runs of
+  // a warp's lanes start about eight slots apart, so without the rotation eight lanes would store
+  // to the same bank at every step.
+  const int n_run = qe[CH - 1] - q0;
+  if (n_run > 0) {
+    int p = (int)(threadIdx.x & 31) >> 2;
+    while (p >= n_run) p -= n_run;
+    for (int m = 0; m < n_run; ++m) {
+      const int o = q0 + p;
+      int e = 0;
+#pragma unroll
+      for (int j = 0; j < CH - 1; ++j) e += (qe[j] <= o) ? 1 : 0;
+      const float hv = hs[e];
+      if constexpr (NCTA == 1) sh.h[dst][o] = hv;
+      else sh.peer[o >> 12]->h[dst][o & (kTile - 1)] = hv;
+      if (a.anc) a.anc[o] = j0 + e;
+      if (++p == n_run) p = 0;
     }
   }
 }
