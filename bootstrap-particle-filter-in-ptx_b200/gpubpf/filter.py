@@ -176,7 +176,7 @@ class GpuBpf:
         check(self._lib.gpu_bpf_load(self._s, buf, len(blob)), "gpu_bpf_load")
 
     def set_fused_small(self, enable: bool = True) -> None:
-        """Fused one-launch ticks for filters of at most 16384 particles (default on)."""
+        """Fused one-launch ticks for filters of at most 65536 particles (default on)."""
         check(self._lib.gpu_bpf_set_fused_small(self._s, int(bool(enable))), "gpu_bpf_set_fused_small")
 
     def profile(self, enable: bool = True) -> None:
