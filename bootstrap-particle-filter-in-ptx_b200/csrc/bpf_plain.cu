@@ -1098,6 +1098,12 @@ constexpr int kChunks = kTile / 4;                      // four-slot chunks of a
 constexpr int kYStage = kSmallThreads;                  // observations staged per refill
 static_assert(kChunks == kSmallThreads, "one four-slot chunk per thread");
 
+// What the finish of a tick's plan needs from its decision (plan_fused_decide -> plan_fused_finish).
+struct FusedTail {
+  double tS, tH, ess, logS_prev_old;
+  int nM, degenerate, resample, resampled_prev_old, tick_old;
+};
+
 struct FusedPlan {
   unsigned long long base, delta, magic, total;
   int nM, Fg, items, zero_spacing;
@@ -1118,6 +1124,7 @@ struct FusedShared {
   __align__(16) DevState st;
   unsigned long long P[kSmallTiles];          // the tick's tile prefixes (all tiles)
   FusedPlan pl;                               // the tick's resampling plan
+  FusedTail tail;                             // the tick's decision, for the finish of its plan
   float s_max[kSmallThreads / 32];
   float s_part[3][kThreads];
   unsigned long long s_E[kThreads];
@@ -1398,6 +1405,100 @@ __device__ __forceinline__ void plan_fused(const TickArgs& a, int N, FusedShared
   plan_decide(a, st, N, nM, degenerate, res, tS, rec_out);
 }
 
+// The same plan in two parts, for ticks whose next tick should not wait for the record: the
+// decision (plan_fused_decide, warp 0) computes the statistics as plan_fused and writes the
+// device-state fields that the next tick's pass 1 and the resampling read: plan_decide's
+// operations on them, in its order; the finish (plan_fused_finish, lane 0 of warp 0, later in
+// the tick) computes the log-likelihood increment and the filtered mean and writes the record, the
+// running sums and, when the tick keeps its particles, the log of its weight sum, from the values
+// the decision left in sh.tail. The two parts together write what plan_decide writes, with the
+// same arithmetic.
+template <int NCTA>
+__device__ __forceinline__ void plan_fused_decide(const TickArgs& a, int N, FusedShared& sh, int par) {
+  const int lane = threadIdx.x & 31;
+  int nM;
+  double tS, tQ, tH;
+  if constexpr (NCTA <= 2) {
+    nM = fused_nM<NCTA>(sh, par);
+    fused_sums<NCTA>(sh, par, nM, tS, tQ, tH);
+  } else {
+    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+    int nk = kNkEmpty;
+    if (lane < NCTA) { r = sh.peer[lane]->rec[par]; nk = __float_as_int(r.w); }
+    nM = warp_max_i(nk);
+    double S = 0.0, Q = 0.0, H = 0.0;
+    if (nk != kNkEmpty) {
+      const double sc = pow2d(nk - nM);
+      S = __dmul_rn(__dadd_rn(0.0, (double)r.x), sc);
+      Q = __dmul_rn(__dadd_rn(0.0, (double)r.y), __dmul_rn(sc, sc));
+      H = __dmul_rn(__dadd_rn(0.0, (double)r.z), sc);
+    }
+    tS = warp_sum_d(S); tQ = warp_sum_d(Q); tH = warp_sum_d(H);
+  }
+  if (lane != 0) return;
+  DevState* st = &sh.st;
+  FusedTail& tl = sh.tail;
+  const bool degenerate = (nM == kNkEmpty) || !(tS > 0.0);
+  double ess = 0.0;
+  int resample = 0;
+  if (!degenerate) {
+    ess = tS * tS / tQ;
+    resample = (a.ess_threshold <= 0.0f) || (ess / (double)N < (double)a.ess_threshold);
+  }
+  tl.tS = tS; tl.tH = tH; tl.ess = ess; tl.nM = nM;
+  tl.degenerate = degenerate ? 1 : 0; tl.resample = resample;
+  tl.logS_prev_old = st->logS_prev; tl.resampled_prev_old = st->resampled_prev; tl.tick_old = st->tick;
+  const int cur = st->cur;
+  if (degenerate) st->error = BPF_ERR_DEGENERATE;
+  {
+    const int d1 = st->dirs & 1;
+    st->dirs = (resample ? d1 : (d1 ^ 1)) | ((d1 ^ 1) << 1);
+  }
+  st->k1 = st->k1 * kPcgMult;
+  st->k2 = st->k2 * kPcgMult + 1ull;
+  st->tick = tl.tick_old + 1;
+  st->do_resample = resample;
+  st->nM = nM;
+  if (resample) {
+    const uint64_t old = st->u_state;
+    st->u_state = old * kPcgMult + kHostInc;
+    st->u23 = pcg_output(old) >> 9;
+    st->logS_prev = a.log_n;
+    st->resampled_prev = 1;
+    st->resample_count += 1;
+    st->src = cur;
+    st->cur = cur ^ 1;
+  } else if (degenerate) {
+    st->logS_prev = a.log_n;
+    st->resampled_prev = 1;
+  } else {
+    st->resampled_prev = 0;
+    st->nM_prev = nM;
+  }
+}
+
+__device__ __forceinline__ void plan_fused_finish(const FusedShared& sh_in, DevState* st, BpfTickRecord* rec_out) {
+  const FusedTail& tl = sh_in.tail;
+  constexpr double kLn2d = 0.693147180559945309417232121458;
+  double dll = -INFINITY, hm = __longlong_as_double(0x7FF8000000000000LL), L = 0.0;
+  if (!tl.degenerate) {
+    L = log(tl.tS);
+    dll = __fma_rn((double)tl.nM, kLn2d, L) - tl.logS_prev_old;
+    hm = tl.tH / tl.tS;
+  }
+  const double ll_ref = (tl.resampled_prev_old ? 0.0 : st->ll_ref) + dll;
+  st->ll_ref = ll_ref;
+  st->hm = tl.degenerate ? 0.0 : hm;
+  st->ll_total += dll;
+  if (rec_out) {
+    BpfTickRecord r;
+    r.dloglik = dll; r.loglik_ref = ll_ref; r.loglik_total = st->ll_total;
+    r.h_mean = (float)hm; r.ess = (float)tl.ess; r.resampled = tl.resample; r.tick = tl.tick_old;
+    *rec_out = r;
+  }
+  if (!tl.resample && !tl.degenerate) st->logS_prev = L;
+}
+
 // The resampling plan into the device state (on a resampling tick).
 __device__ __forceinline__ void store_fused_plan(DevState* st, const FusedShared& sh) {
   const FusedPlan& pl = sh.pl;
@@ -1637,8 +1738,16 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
     if (a.y_ptr && (t & (kYStage - 1)) == 0) {       // the next kYStage observations
       __syncthreads();
       if (t + tid < n_ticks) sh.ys[tid] = __ldg(a.y_ptr + t + tid);
+      __syncthreads();
+    } else if (ahead || t == 0) {
+      // With a threshold the decision barrier (and on resampling ticks the barrier after the
+      // children's writes) already orders everything this tick's pass 1 reads: the particles, the
+      // noise and the device-state fields the decision wrote; the finish of the previous tick's
+      // plan (warp 31, outside pass 1) writes only the record and fields pass 1 does not read, and
+      // the next decision reads them after the records barrier, which warp 31 reaches after the
+      // finish. When every tick resamples, warp 0 did not wait for the children.
+      __syncthreads();
     }
-    __syncthreads();
     const float y = a.y_ptr ? sh.ys[t & (kYStage - 1)] : a.obs.y;
     const unsigned long long u_state = sh.st.u_state;
     const int cur0 = sh.st.cur;                    // a resampling reads buffer cur0, writes cur0 ^ 1
@@ -1670,7 +1779,7 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
         marks_barrier_sync<NCTA>();               // every child is written
       }
     } else {
-      if (warp == 0) plan_fused<NCTA>(a, N, sh, par, (a.rec && k == 0) ? a.rec + t : nullptr);
+      if (warp == 0) plan_fused_decide<NCTA>(a, N, sh, par);
       else if (more) fused_noise<TSTATE>(a, tile0, sh.knext[0], sh.knext[1], 32, kSmallThreads - 32, sh);
       __syncthreads();
       if (sh.st.do_resample) {
@@ -1681,6 +1790,9 @@ small_kernel(Plan p, TickArgs a, int n_ticks) {
         count_write<NCTA, 4>(a, N, k, ct, cur0, cur0 ^ 1, sh);
         cluster_sync_all<NCTA>();                 // every child is written
       }
+      // the tick's record and running sums, on a warp outside pass 1, while the others start the
+      // next tick
+      if (tid == kSmallThreads - 32) plan_fused_finish(sh, &sh.st, (a.rec && k == 0) ? a.rec + t : nullptr);
     }
   }
   if (tid == 0 && a.mirror) sh.st.seq = a.seq;
